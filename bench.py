@@ -1,0 +1,432 @@
+"""Benchmark: full NLO BK evolution to Y = 10 on B200.
+
+Workload (the configuration the headline metric is quoted on): 400 log-spaced
+parent sizes r in [1e-7, 1e2] GeV^-1, MV initial condition (Qs0^2 = 0.2 GeV^2,
+gamma = 1, Lambda = 0.241 GeV), smooth-freeze Balitsky/smallest-dipole running
+coupling, RK4 in rapidity with step 0.1 up to Y = 10, 2^20 scrambled Sobol points
+per parent per stage for K2+Kf, the fixed 8 x 24 rule per r interval for K1;
+FP32 integrands with FP64 sums, spline refit and RK update.
+
+A bench "step" is one RK4 step (four right-hand sides).  With the default
+--steps 100 the timed region is exactly the evolution from Y = 0 to Y = 10;
+``value`` is seconds to Y = 10 (scaled by 100/K when K != 100).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference algorithm on the host cores (the oracle's
+C restatement, all threads) on a bounded sample of every step and reports the
+same metric extrapolated to the full workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from dataclasses import replace
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "NLO BK s to Y=10 & DIS points/s at <=1e-4 rel err; served p50/p99 latency"
+UNIT = "s to Y=10 (NLO BK evolution)"
+MAXY = 10.0
+STEP = 0.1
+RPOINTS = 399
+MINR, MAXR = 1e-7, 1e2
+SAMPLES = 1 << 20
+QS0SQR = 0.2
+# Hand count of FP32 operations in k2_point<float, true> (csrc/k2kf.cu) per
+# (sample, parent) evaluation: FMA = 2, every other arithmetic op or MUFU
+# transcendental = 1, compares/selects excluded.
+FLOPS_PER_EVAL = 181
+# Launches of our kernels per RK4 step: 4 right-hand sides x (spline refit, active
+# list, K1, K2+Kf, K2+Kf finalize, assemble) + 4 stage combinations.
+LAUNCHES_PER_STEP = 4 * 6 + 4
+SM_COUNT = 148
+FP32_LANES_PER_SM = 128
+
+
+def workload_config():
+    from nlo_bk_optimized_b200 import BKConfig
+
+    return BKConfig(RPOINTS=RPOINTS, MINR=MINR, MAXR=MAXR, MCINTPOINTS=SAMPLES, DE_SOLVER_STEP=STEP,
+                    STEPPER="rk4", PRECISION="mixed")
+
+
+def workload_description(extra: dict | None = None) -> dict:
+    out = {
+        "workload": "full NLO BK evolution: 400 r in [1e-7,1e2] GeV^-1, MV Qs0^2=0.2, RK4 h=0.1 to Y=10, "
+                    "2^20 scrambled Sobol points per r per stage, fixed 8x24 K1 rule",
+        "r_points": RPOINTS + 1,
+        "samples_per_r_per_stage": SAMPLES,
+        "rk_step": STEP,
+        "maxy": MAXY,
+        "stepper": "rk4",
+        "precision": "FP32 integrands, FP64 sums/spline/RK",
+        "l2": "256 MiB buffer written between timed steps (working set is L2-resident by nature)",
+    }
+    if extra:
+        out.update(extra)
+    return out
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        return False
+
+    def summary(self) -> dict | None:
+        if self.proc is None or self.file is None:
+            return None
+        self.file.flush()
+        rows = []
+        with open(self.file.name) as fh:
+            for line in fh:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    rows.append((float(parts[1]), float(parts[2]), float(parts[3]) if parts[3] not in ("", "[N/A]") else 0.0,
+                                 parts[5], parts[6], parts[7], parts[8]))
+                except ValueError:
+                    continue
+        os.unlink(self.file.name)
+        if not rows:
+            return None
+        reasons = set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for row in rows:
+            for name, flag in zip(names, row[3:]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        loaded = [row[0] for row in rows]
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(row[1] for row in rows),
+                "power_w_max": max(row[2] for row in rows), "samples": len(rows), "reasons": sorted(reasons)}
+
+
+# ---------------------------------------------------------------------------
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_ours(args) -> None:
+    import torch
+    import torch.distributed as dist
+
+    from nlo_bk_optimized_b200 import MV, _native, solve_bk
+    from nlo_bk_optimized_b200.bk.evolution import _r_grid, nlo_box, params_of, workspace
+
+    world, rank, local = dist_setup()
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=device)
+
+    config = workload_config()
+    lib = _native.load()
+    params = params_of(config, _native.PRECISION_MIXED)
+    r_host = _r_grid(config, device="cpu", dtype=torch.float64)
+    N0_host = MV(qs0sqr=QS0SQR).dipole_amplitude(r_host)
+    r = r_host.to(device)
+    points = r.numel()
+    lower, width = nlo_box(float(r_host[0]), float(r_host[-1]))
+    box = _native.box(lower, width)
+    dirs = _native.sobol_dirs(4, 0)
+    ws = workspace(device, points)
+    status = torch.zeros(1, dtype=torch.int32, device=device)
+    stream = torch.cuda.current_stream(device)
+    steps, warmup = args.steps, args.warmup
+    table = torch.empty((max(steps, warmup) + 1, points), dtype=torch.float64, device=device)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)
+
+    def rk4_step(row: int) -> None:
+        _native.check(lib.nlo_bk_evolve(params, r.data_ptr(), points, 1, STEP, _native.STEPPERS["rk4"], dirs,
+                                        SAMPLES, box, table[row].data_ptr(), status.data_ptr(), ws.data_ptr(),
+                                        ws.numel(), stream.cuda_stream))
+
+    # warm-up: W steps from the initial condition (discarded)
+    table[0].copy_(N0_host.to(device))
+    for i in range(warmup):
+        rk4_step(i)
+    torch.cuda.synchronize()
+
+    # timed region: K steps from the initial condition
+    table[0].copy_(N0_host.to(device))
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    wall0 = time.perf_counter()
+    with ClockSampler(local) as sampler:
+        for i in range(steps):
+            flush.zero_()
+            starts[i].record(stream)
+            rk4_step(i)
+            ends[i].record(stream)
+        torch.cuda.synchronize()
+    wall = time.perf_counter() - wall0
+    if world > 1:
+        dist.barrier()
+    device_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    if int(status.item()) != 0:
+        raise FloatingPointError("non-finite amplitude in the benchmark evolution")
+    clocks = sampler.summary()
+    final_N = table[steps].clone()
+
+    # dominant kernel (K2+Kf) timed alone with events on its stream, at the final state
+    idx = torch.empty(points, dtype=torch.int32, device=device)
+    count = torch.empty(1, dtype=torch.int32, device=device)
+    spline = torch.empty(int(lib.nlo_bk_spline_doubles(points)), dtype=torch.float64, device=device)
+    _native.check(lib.nlo_bk_splines(r.data_ptr(), final_N.data_ptr(), points, 1, spline.data_ptr(), stream.cuda_stream))
+    _native.check(lib.nlo_bk_active(final_N.data_ptr(), points, idx.data_ptr(), count.data_ptr(), stream.cuda_stream))
+    k2_out = torch.empty((points, 3), dtype=torch.float64, device=device)
+    k2_ws = torch.empty(int(lib.nlo_bk_k2kf_workspace_bytes(points)), dtype=torch.uint8, device=device)
+    reps = 3
+    k_start = [torch.cuda.Event(enable_timing=True) for _ in range(reps + 1)]
+    k_end = [torch.cuda.Event(enable_timing=True) for _ in range(reps + 1)]
+    for i in range(reps + 1):
+        flush.zero_()
+        k_start[i].record(stream)
+        _native.check(lib.nlo_bk_k2kf(params, r.data_ptr(), points, spline.data_ptr(), idx.data_ptr(),
+                                      count.data_ptr(), dirs, 0, SAMPLES, box, k2_out.data_ptr(), k2_ws.data_ptr(),
+                                      k2_ws.numel(), stream.cuda_stream))
+        k_end[i].record(stream)
+    torch.cuda.synchronize()
+    k2_ms = sum(k_start[i].elapsed_time(k_end[i]) for i in range(1, reps + 1)) / reps
+    n_active = int(count.item())
+
+    # end to end through the public API with host buffers: host IC -> device -> evolve -> host table
+    e2e_config = config
+    e2e_maxy = steps * STEP
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    result = solve_bk(MV(qs0sqr=QS0SQR), e2e_maxy, e2e_config, device=device, dtype=torch.float32, seed=0)
+    host_table = result.N.cpu()
+    e2e_s = time.perf_counter() - t0
+    h2d = 2 * points * 8
+    d2h = host_table.numel() * host_table.element_size() + 4
+
+    step_ms = device_ms / steps
+    seconds = step_ms * (MAXY / STEP) / 1000.0
+    e2e_seconds = e2e_s * (MAXY / e2e_maxy)
+    if world > 1:
+        t = torch.tensor([seconds, e2e_seconds], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        seconds, e2e_seconds = float(t[0]), float(t[1])
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    # roofline of the dominant kernel: algorithmic FP32 flops per launch / launch time
+    evals = n_active * SAMPLES
+    achieved = evals * FLOPS_PER_EVAL / (k2_ms * 1e-3) / 1e12
+    sm_mhz = 1965.0
+    peak = SM_COUNT * FP32_LANES_PER_SM * 2 * sm_mhz * 1e6 / 1e12
+    roofline = {
+        "bound": "fp32",
+        "achieved": round(achieved, 3),
+        "peak": round(peak, 2),
+        "unit": "TFLOP/s",
+        "frac": round(achieved / peak, 4),
+        "traffic": None,
+        "kernel": "k2kf_kernel<float,true> (csrc/k2kf.cu)",
+        "peak_source": "nominal FP32 (148 SM x 128 lanes x 2 x 1965 MHz); MEASURED_PEAKS.json has only HBM and bf16",
+        "flops_per_eval": FLOPS_PER_EVAL,
+        "evals_per_launch": evals,
+        "launch_ms": round(k2_ms, 4),
+        "evals_per_s": round(evals / (k2_ms * 1e-3), 1),
+    }
+    traffic_file = ROOT / "profiles" / "k2kf_traffic.json"
+    if traffic_file.exists():
+        try:
+            roofline["traffic"] = json.loads(traffic_file.read_text()).get("bytes_per_launch_full_workload")
+        except Exception:
+            pass
+
+    line = {
+        "metric": METRIC,
+        "value": round(seconds, 4),
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": steps,
+        "warmup": warmup,
+        "ms_per_step": round(step_ms, 4),
+        "higher_is_better": False,
+        "scaling": "weak" if world > 1 else "strong",
+        "vs_baseline": None,
+        "dtype": "f32+f64",
+        "data": "synthetic (MV initial condition)",
+        "config": workload_description({"parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                                        "active_parents_final": n_active}),
+        "e2e": {"value": round(e2e_seconds, 4), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "api": "nlo_bk_optimized_b200.solve_bk + table.N.cpu()"},
+        "gpu_launches": LAUNCHES_PER_STEP * steps,
+        "roofline": roofline,
+        "clocks": clocks,
+        "wall_s_timed_region": round(wall, 3),
+    }
+    if not args.no_cpu_baseline and world == 1:
+        line["cpu_baseline"] = cpu_baseline(final_N.cpu().numpy(), r_host.numpy())
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+def _oracle_rates(N, r, k2_samples: int, k1_parents: int) -> dict:
+    """Time the oracle (C restatement, all host threads) on a bounded sample."""
+
+    import numpy as np
+
+    import oracle
+
+    config = workload_config()
+    phys = oracle.physics(config)
+    active = np.nonzero((np.arange(r.size) > 0) & (N <= 0.99999))[0]
+    nspl = oracle.loglog_spline(r, N, 0)
+    sspl = oracle.loglog_spline(r, N, 1)
+    state, shift = oracle.sobol_state(4, 0)
+    points = oracle.sobol(state, shift, 0, k2_samples, as_f32=True)
+    lower, width = oracle.nlo_box(r)
+    t0 = time.perf_counter()
+    oracle.k2kf_sums(r[active], points, lower, width, True, sspl, phys)
+    t_k2 = time.perf_counter() - t0
+    pick = active[:: max(1, active.size // k1_parents)][:k1_parents]
+    t0 = time.perf_counter()
+    oracle.k1_fixed(r[pick], nspl, phys)
+    t_k1 = time.perf_counter() - t0
+    k2_rate = active.size * k2_samples / t_k2
+    k1_per_parent = t_k1 / pick.size
+    stage = active.size * SAMPLES / k2_rate + active.size * k1_per_parent
+    return {"k2kf_evals_per_s": k2_rate, "k1_s_per_parent": k1_per_parent, "stage_s": stage,
+            "active": int(active.size), "k1_parents": int(pick.size), "elapsed": t_k2 + t_k1}
+
+
+def cpu_baseline(N, r) -> dict:
+    import oracle
+
+    rates = _oracle_rates(N, r, k2_samples=1 << 15, k1_parents=64)
+    stages = 4 * MAXY / STEP
+    return {
+        "value": round(rates["stage_s"] * stages, 1),
+        "unit": UNIT,
+        "cores": oracle.num_threads(),
+        "kind": "port",
+        "sample": (f"oracle (C, OpenMP) K2+Kf on {rates['active']} parents x 2^15 Sobol points and K1 on "
+                   f"{rates['k1_parents']} parents at the final state; extrapolated to 400 stages x 2^20 points "
+                   f"({rates['elapsed']:.1f} s measured)"),
+        "k2kf_evals_per_s": round(rates["k2kf_evals_per_s"], 1),
+    }
+
+
+def run_reference(args) -> None:
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return
+    import numpy as np
+
+    import oracle
+
+    config = workload_config()
+    r = oracle.r_grid(MINR, MAXR, RPOINTS)
+    N = oracle.mv_amplitude(r, QS0SQR)
+    k2_samples = 1 << 11
+
+    def step_sampled(N):
+        """One RK4 step's cost on a bounded sample: for each of the 4 stages, K2+Kf on all
+        active parents x 2^11 points and K1 on 32 parents, timed and extrapolated to the
+        full stage (2^20 points, every active parent)."""
+
+        return sum(_oracle_rates(N, r, k2_samples, 32)["stage_s"] for _ in range(4))
+
+    for _ in range(args.warmup):
+        step_sampled(N)
+    total = 0.0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        total += step_sampled(N)
+    elapsed = time.perf_counter() - t0
+    step_s = total / args.steps
+    seconds = step_s * MAXY / STEP
+    line = {
+        "metric": METRIC,
+        "impl": "reference",
+        "value": round(seconds, 2),
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(step_s * 1000, 2),
+        "higher_is_better": False,
+        "scaling": "strong",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (MV initial condition)",
+        "config": workload_description({"parallelism": "host cores"}),
+        "cpu_baseline": {"value": round(seconds, 2), "unit": UNIT, "cores": oracle.num_threads(), "kind": "port",
+                         "sample": "per stage: K2+Kf on all active parents x 2^11 Sobol points and K1 on 32 parents "
+                                   f"(oracle, C/OpenMP), extrapolated to the full stage; {elapsed:.1f} s measured"},
+        "e2e": {"value": round(seconds, 2), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main() -> None:
+    parser = argparse.ArgumentParser()
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=100)
+    parser.add_argument("--warmup", type=int, default=3)
+    parser.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    parser.add_argument("--no-cpu-baseline", action="store_true")
+    args = parser.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,145 @@
+/*
+ * nlo_b200.h -- C ABI of the B200 (sm_100a) NLO BK right-hand side and evolution.
+ *
+ * Plain pointers and sizes only.  Every array argument marked "device" is a CUDA
+ * device pointer owned by the caller; every call is asynchronous on the given
+ * stream (a cudaStream_t passed as void*, NULL = legacy default stream) and
+ * returns NLO_OK or an error code; nlo_last_error() describes the last failure
+ * of the calling thread.  No entry point allocates device memory: kernels that
+ * need scratch take a caller-provided workspace whose size the matching
+ * *_workspace_bytes() function returns.
+ *
+ * Each entry point replaces one operator of the reference package
+ * (HaowuDuan/nlo_bk_optimized, torch_nlo_clean/src/nlo_torch); the citation is
+ * given beside it.  The reference binds its operators through pybind with torch
+ * tensors on the current CUDA stream; these take the same data as raw buffers.
+ */
+#ifndef NLO_B200_H
+#define NLO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NLO_OK 0
+#define NLO_ERR_INVALID 1   /* argument rejected on the host; nothing launched */
+#define NLO_ERR_CUDA 2      /* a CUDA runtime call failed */
+#define NLO_ERR_WORKSPACE 3 /* workspace missing or too small */
+
+#define NLO_PRECISION_MIXED 0 /* FP32 integrands, FP64 sums, spline refit and RK update */
+#define NLO_PRECISION_FP64 1  /* everything in FP64 */
+
+#define NLO_STEPPER_EULER 0 /* bk/evolution.py:110-122 */
+#define NLO_STEPPER_RK3 1   /* Kutta RK3, bk/evolution.py:190-236 (_fixed_rk23_step) */
+#define NLO_STEPPER_RK4 2   /* classical RK4 (no reference counterpart) */
+
+/* Physics and numerical switches of BKConfig (bk/config.py:66-124) that the
+ * right-hand side depends on.  Only the reference's production K1/K2 choices
+ * are implemented on the device: RC_LO = BALITSKY_LO (or FIXED_LO),
+ * RC_NLO = SMALLEST_NLO (or FIXED_NLO), RESUM_RC = RESUM_RC_SMALLEST,
+ * Order = NLO_RESUM_DLOG_SLOG, NF <= 3 smooth-freeze coupling (coupling.py:81-97). */
+typedef struct nlo_bk_params {
+    double nc;            /* NC */
+    double nf;            /* NF */
+    double lambda_qcd;    /* LambdaQCD */
+    double c2;            /* C2 */
+    double minr;          /* MINR (double-log resummation switch r > 1.01 MINR, k1.py:117) */
+    double ksub;          /* KSUB */
+    double fixed_alpha_s; /* FIXED_AS, used when fixed_coupling != 0 */
+    double alpha_cap;     /* > 0: alpha_s = min(alpha_s, alpha_cap) (frozen-coupling variant) */
+    int32_t symmetrize;   /* SYMMETRIZE_Z_Z2_INTEGRATION */
+    int32_t fixed_coupling;
+    int32_t force_positive; /* FORCE_POSITIVE_N */
+    int32_t precision;      /* NLO_PRECISION_* */
+} nlo_bk_params;
+
+/* Scrambled Sobol direction numbers of torch.quasirandom.SobolEngine
+ * (sobolstate[d][30] and shift[d]; values < 2^30). */
+typedef struct nlo_sobol_dirs {
+    int32_t dims; /* <= 8 */
+    uint32_t state[8][30];
+    uint32_t shift[8];
+} nlo_sobol_dirs;
+
+/* The K2+Kf integration box in (log z, log z', theta_z, theta_z'):
+ * lower + width * u for u in the unit cube (bk/derivatives.py:424-431). */
+typedef struct nlo_bk_box {
+    double lower[4];
+    double width[4];
+} nlo_bk_box;
+
+const char* nlo_last_error(void);
+int nlo_abi_version(void);
+
+/* Scrambled Sobol points u[n][dims] of indices offset .. offset+n-1, bit-exact to
+ * SobolEngine(dims, scramble=True, seed).draw(...) in float32 (precision 0) or
+ * float64 (precision 1).  Replaces the host-side draw and host-to-device copy of
+ * dis/fixed_sobol.py:87-92 and the Philox draws of custom_kernels/integration.cu:60-93.
+ * out: device float[n*dims] or double[n*dims]. */
+int nlo_sobol_draw(const nlo_sobol_dirs* dirs, int64_t offset, int64_t n, int32_t precision, void* out,
+                   void* stream);
+
+/* Spline buffer size in doubles for a grid of `points` knots:
+ * x[points] (log r) followed by the log N and log S coefficient blocks,
+ * each [points-1][4] (a, b, c, d). */
+size_t nlo_bk_spline_doubles(int32_t points);
+
+/* Natural-cubic log N and log S splines of an amplitude row (FP64).
+ * Replaces evolution_loglog_splines_mixed (custom_kernels/interpolation.cu:374-450)
+ * and LogLogSpline (numerics/interpolation.py:95-121, bk/evolution.py:536-560).
+ * r, N: device double[points]; spline: device double[nlo_bk_spline_doubles(points)]. */
+int nlo_bk_splines(const double* r, const double* N, int32_t points, int32_t force_positive, double* spline,
+                   void* stream);
+
+/* Active parents (index > 0 and N <= 0.99999; bk/evolution.py:501) as a list:
+ * active: device int32[points] (slot -> grid index), count: device int32[1]. */
+int nlo_bk_active(const double* N, int32_t points, int32_t* active, int32_t* count, void* stream);
+
+/* K1 for every active parent by the fixed rule of 8 Gauss-Legendre nodes in
+ * log z per grid interval times 24 nodes in v with theta = pi v^2
+ * (custom_kernels/bk/k1/kernel.cu:2040-2092, integrand bk/derivatives.py:434-468).
+ * Replaces mixed_fixed_grid_integrals (custom_kernels/bk/k1/kernel.cu:2321-2418).
+ * out: device double[points]; entries of inactive parents are set to 0. */
+int nlo_bk_k1(const nlo_bk_params* params, const double* r, int32_t points, const double* spline,
+              const int32_t* active, const int32_t* count, double* out, void* stream);
+
+/* Workspace bytes for nlo_bk_k2kf with `points` grid points. */
+size_t nlo_bk_k2kf_workspace_bytes(int32_t points);
+
+/* K2+Kf sums over `samples` scrambled Sobol points (indices offset ..) for every
+ * active parent: out[i][0] = sum w K2, out[i][1] = sum w Kf, out[i][2] = sum w^2 (K2+Kf)^2,
+ * with w the box volume (bk/derivatives.py:322-335, 490-612).  Replaces
+ * bk_nlo_mixed_vegas_summaries (custom_kernels/bk/k2_kf/kernel.cu:877-1063).
+ * out: device double[points*3]; inactive parents get zeros. */
+int nlo_bk_k2kf(const nlo_bk_params* params, const double* r, int32_t points, const double* spline,
+                const int32_t* active, const int32_t* count, const nlo_sobol_dirs* dirs, int64_t offset,
+                int64_t samples, const nlo_bk_box* box, double* out, void* workspace, size_t workspace_bytes,
+                void* stream);
+
+/* Workspace bytes for nlo_bk_rhs / nlo_bk_evolve. */
+size_t nlo_bk_rhs_workspace_bytes(int32_t points);
+
+/* dN/dY = K1 + (K2+Kf) at active parents, 0 elsewhere, non-finite -> 0
+ * (_evolve_derivative, bk/evolution.py:329-351 with _derivative_components :354-488).
+ * N, dndy: device double[points]; k1, k2kf: optional device double[points] (may be NULL). */
+int nlo_bk_rhs(const nlo_bk_params* params, const double* r, const double* N, int32_t points,
+               const nlo_sobol_dirs* dirs, int64_t samples, const nlo_bk_box* box, double* dndy, double* k1,
+               double* k2kf, void* workspace, size_t workspace_bytes, void* stream);
+
+/* Rapidity evolution of one amplitude row through `steps` steps of size `step`
+ * (_bk_steps, bk/evolution.py:85-159): each step applies the stepper, clamps N to
+ * [0,1] when force_positive, and stores the row.  table: device double[(steps+1)*points]
+ * with row 0 = the initial condition (input).  status: device uint32[1], bit 0 set if
+ * a non-finite amplitude appeared (the host raises FloatingPointError). */
+int nlo_bk_evolve(const nlo_bk_params* params, const double* r, int32_t points, int32_t steps, double step,
+                  int32_t stepper, const nlo_sobol_dirs* dirs, int64_t samples, const nlo_bk_box* box,
+                  double* table, uint32_t* status, void* workspace, size_t workspace_bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NLO_B200_H */

@@ -1,0 +1,162 @@
+"""ctypes binding of ``libnlo_b200.so`` (include/nlo_b200.h).
+
+The library is the only compute path: there is no CPU or eager-PyTorch fallback.
+Loading fails loudly when the shared object is missing, and every call raises
+``RuntimeError`` with the library's message when it returns an error code
+(the reference raises ``RuntimeError`` from TORCH_CHECK in the same situations).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import threading
+from pathlib import Path
+
+import torch
+
+from nlo_bk_optimized_b200 import build as _build
+
+LIBRARY_PATH = _build.LIBRARY
+
+PRECISION_MIXED = 0
+PRECISION_FP64 = 1
+STEPPERS = {"euler": 0, "rk3": 1, "rk4": 2}
+
+
+class BKParams(ctypes.Structure):
+    _fields_ = [
+        ("nc", ctypes.c_double),
+        ("nf", ctypes.c_double),
+        ("lambda_qcd", ctypes.c_double),
+        ("c2", ctypes.c_double),
+        ("minr", ctypes.c_double),
+        ("ksub", ctypes.c_double),
+        ("fixed_alpha_s", ctypes.c_double),
+        ("alpha_cap", ctypes.c_double),
+        ("symmetrize", ctypes.c_int32),
+        ("fixed_coupling", ctypes.c_int32),
+        ("force_positive", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+    ]
+
+
+class SobolDirs(ctypes.Structure):
+    _fields_ = [
+        ("dims", ctypes.c_int32),
+        ("state", (ctypes.c_uint32 * 30) * 8),
+        ("shift", ctypes.c_uint32 * 8),
+    ]
+
+
+class Box(ctypes.Structure):
+    _fields_ = [("lower", ctypes.c_double * 4), ("width", ctypes.c_double * 4)]
+
+
+EXPORTED = (
+    "nlo_last_error",
+    "nlo_abi_version",
+    "nlo_sobol_draw",
+    "nlo_bk_spline_doubles",
+    "nlo_bk_splines",
+    "nlo_bk_active",
+    "nlo_bk_k1",
+    "nlo_bk_k2kf_workspace_bytes",
+    "nlo_bk_k2kf",
+    "nlo_bk_rhs_workspace_bytes",
+    "nlo_bk_rhs",
+    "nlo_bk_evolve",
+)
+
+_lock = threading.Lock()
+_handle: ctypes.CDLL | None = None
+
+
+def _declare(lib: ctypes.CDLL) -> None:
+    P = ctypes.POINTER
+    vp = ctypes.c_void_p
+    i32, i64, sz, d = ctypes.c_int32, ctypes.c_int64, ctypes.c_size_t, ctypes.c_double
+    lib.nlo_last_error.restype = ctypes.c_char_p
+    lib.nlo_last_error.argtypes = []
+    lib.nlo_abi_version.restype = ctypes.c_int
+    lib.nlo_sobol_draw.restype = ctypes.c_int
+    lib.nlo_sobol_draw.argtypes = [P(SobolDirs), i64, i64, i32, vp, vp]
+    lib.nlo_bk_spline_doubles.restype = sz
+    lib.nlo_bk_spline_doubles.argtypes = [i32]
+    lib.nlo_bk_splines.restype = ctypes.c_int
+    lib.nlo_bk_splines.argtypes = [vp, vp, i32, i32, vp, vp]
+    lib.nlo_bk_active.restype = ctypes.c_int
+    lib.nlo_bk_active.argtypes = [vp, i32, vp, vp, vp]
+    lib.nlo_bk_k1.restype = ctypes.c_int
+    lib.nlo_bk_k1.argtypes = [P(BKParams), vp, i32, vp, vp, vp, vp, vp]
+    lib.nlo_bk_k2kf_workspace_bytes.restype = sz
+    lib.nlo_bk_k2kf_workspace_bytes.argtypes = [i32]
+    lib.nlo_bk_k2kf.restype = ctypes.c_int
+    lib.nlo_bk_k2kf.argtypes = [P(BKParams), vp, i32, vp, vp, vp, P(SobolDirs), i64, i64, P(Box), vp, vp, sz, vp]
+    lib.nlo_bk_rhs_workspace_bytes.restype = sz
+    lib.nlo_bk_rhs_workspace_bytes.argtypes = [i32]
+    lib.nlo_bk_rhs.restype = ctypes.c_int
+    lib.nlo_bk_rhs.argtypes = [P(BKParams), vp, vp, i32, P(SobolDirs), i64, P(Box), vp, vp, vp, vp, sz, vp]
+    lib.nlo_bk_evolve.restype = ctypes.c_int
+    lib.nlo_bk_evolve.argtypes = [P(BKParams), vp, i32, i32, d, i32, P(SobolDirs), i64, P(Box), vp, vp, vp, sz, vp]
+
+
+def load(path: Path | None = None) -> ctypes.CDLL:
+    """Load (once) and return the C-ABI library; raises if it is absent."""
+
+    global _handle
+    with _lock:
+        if _handle is None:
+            target = Path(path) if path is not None else LIBRARY_PATH
+            if not target.exists():
+                raise RuntimeError(
+                    f"{target} is missing: build it with `python -m nlo_bk_optimized_b200.build` "
+                    "(the B200 kernels have no CPU fallback)"
+                )
+            lib = ctypes.CDLL(str(target))
+            _declare(lib)
+            _handle = lib
+        return _handle
+
+
+def check(code: int) -> None:
+    if code != 0:
+        message = load().nlo_last_error().decode("utf-8", "replace")
+        raise RuntimeError(f"nlo_b200 error {code}: {message}")
+
+
+def require_cuda(tensor: torch.Tensor, name: str) -> None:
+    if not tensor.is_cuda:
+        raise ValueError(f"{name} must be a CUDA tensor: the B200 path has no CPU fallback")
+    if not tensor.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+
+
+def ptr(tensor: torch.Tensor | None) -> int | None:
+    return None if tensor is None else tensor.data_ptr()
+
+
+def stream_handle(device: torch.device) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def sobol_dirs(dims: int, seed: int) -> SobolDirs:
+    """Direction numbers of SobolEngine(dims, scramble=True, seed)."""
+
+    engine = torch.quasirandom.SobolEngine(dims, scramble=True, seed=seed)
+    state = engine.sobolstate.tolist()
+    shift = engine.shift.tolist()
+    dirs = SobolDirs()
+    dirs.dims = dims
+    for d in range(dims):
+        for j in range(30):
+            dirs.state[d][j] = int(state[d][j])
+        dirs.shift[d] = int(shift[d])
+    return dirs
+
+
+def box(lower, width) -> Box:
+    b = Box()
+    for d in range(4):
+        b.lower[d] = float(lower[d])
+        b.width[d] = float(width[d])
+    return b

@@ -1,0 +1,265 @@
+"""BK rapidity evolution on the B200 (mirrors torch_nlo_clean/src/nlo_torch/bk/evolution.py).
+
+``solve_bk`` / ``compute_dndy`` keep the reference signatures.  The whole
+evolution runs on one CUDA stream through ``nlo_bk_evolve`` of libnlo_b200.so:
+per stage a FP64 spline refit, K1 (fixed 8 x 24 rule), K2+Kf (scrambled Sobol
+QMC) and the FP64 RK combination -- no host synchronisation between stages.
+The host reads back once, at the end, to check the non-finite flag
+(bk/evolution.py:152-153 raises FloatingPointError).
+"""
+
+from __future__ import annotations
+
+import math
+from collections.abc import Iterator
+from dataclasses import dataclass
+
+import torch
+
+from nlo_bk_optimized_b200 import _native
+from nlo_bk_optimized_b200.bk.config import BKConfig, RunningCouplingLO, device_supported
+from nlo_bk_optimized_b200.bk.initial_conditions import MV, ICDataFile
+from nlo_bk_optimized_b200.dipole.table import DipoleTable
+
+
+@dataclass(frozen=True, slots=True)
+class DNDYResult:
+    r: torch.Tensor
+    K1: torch.Tensor
+    K2_Kf: torch.Tensor
+    N: torch.Tensor
+
+
+def _r_grid(config: BKConfig, *, device: torch.device | str, dtype: torch.dtype) -> torch.Tensor:
+    """r_i = MINR (MAXR/MINR)^(i/RPOINTS), i = 0..RPOINTS (bk/evolution.py:584-592)."""
+
+    rind = torch.arange(config.RPOINTS + 1, dtype=dtype, device=device)
+    step = (config.MAXR / config.MINR) ** (1 / config.RPOINTS)
+    return config.MINR * torch.pow(rind.new_tensor(step), rind)
+
+
+def nlo_box(r_first: float, r_last: float) -> tuple[list[float], list[float]]:
+    """[log(r0/2), log(2 r_max)]^2 x [0, 2 pi]^2 (bk/derivatives.py:424-431) as (lower, width)."""
+
+    lo = math.log(0.5 * r_first)
+    hi = math.log(2 * r_last)
+    return [lo, lo, 0.0, 0.0], [hi - lo, hi - lo, 2 * math.pi, 2 * math.pi]
+
+
+def precision_of(config: BKConfig, dtype: torch.dtype) -> int:
+    choice = config.PRECISION or ("mixed" if dtype == torch.float32 else "fp64")
+    return _native.PRECISION_FP64 if choice == "fp64" else _native.PRECISION_MIXED
+
+
+def params_of(config: BKConfig, precision: int) -> _native.BKParams:
+    reason = device_supported(config)
+    if reason is not None:
+        raise NotImplementedError(reason)
+    p = _native.BKParams()
+    p.nc = float(config.NC)
+    p.nf = float(config.NF)
+    p.lambda_qcd = float(config.LambdaQCD)
+    p.c2 = float(config.C2)
+    p.minr = float(config.MINR)
+    p.ksub = float(config.KSUB)
+    p.fixed_alpha_s = float(config.FIXED_AS)
+    p.alpha_cap = float(config.ALPHA_S_CAP)
+    p.symmetrize = int(bool(config.SYMMETRIZE_Z_Z2_INTEGRATION))
+    p.fixed_coupling = int(config.RC_LO is RunningCouplingLO.FIXED_LO)
+    p.force_positive = int(bool(config.FORCE_POSITIVE_N))
+    p.precision = int(precision)
+    return p
+
+
+_workspaces: dict[tuple[int, int], torch.Tensor] = {}
+
+
+def workspace(device: torch.device, points: int) -> torch.Tensor:
+    """Device scratch for the right-hand side (cached per device and grid size)."""
+
+    lib = _native.load()
+    index = device.index if device.index is not None else torch.cuda.current_device()
+    key = (index, points)
+    need = int(lib.nlo_bk_rhs_workspace_bytes(points))
+    buffer = _workspaces.get(key)
+    if buffer is None or buffer.numel() < need:
+        buffer = torch.empty(need, dtype=torch.uint8, device=torch.device("cuda", index))
+        _workspaces[key] = buffer
+    return buffer
+
+
+def _cuda_device(device: torch.device | str) -> torch.device:
+    device = torch.device(device)
+    if device.type != "cuda":
+        raise ValueError(
+            f"device {device} is not supported: the B200 implementation runs on CUDA only (no CPU fallback)"
+        )
+    if not torch.cuda.is_available():
+        raise RuntimeError("CUDA is not available: the B200 implementation has no CPU fallback")
+    return device
+
+
+def _steps_to(y_start: float, maxy: float, step: float) -> list[float]:
+    """Rapidities after each step, as bk/evolution.py:108-159 accumulates them."""
+
+    ys = []
+    y = y_start
+    while True:
+        y = y + step
+        ys.append(y)
+        if y >= maxy - 1e-12 * max(1.0, abs(maxy), abs(step)):
+            break
+    return ys
+
+
+def rhs(
+    N: torch.Tensor,
+    r: torch.Tensor,
+    config: BKConfig = BKConfig(),
+    *,
+    seed: int | None = None,
+    precision: int | None = None,
+) -> tuple[torch.Tensor, torch.Tensor, torch.Tensor]:
+    """dN/dY, K1 and K2+Kf (each [R] float64) for one amplitude row (bk/evolution.py:329-488)."""
+
+    device = _cuda_device(r.device)
+    r64 = r.to(device=device, dtype=torch.float64).contiguous()
+    N64 = N.to(device=device, dtype=torch.float64).contiguous()
+    points = r64.numel()
+    prec = precision if precision is not None else precision_of(config, r.dtype)
+    params = params_of(config, prec)
+    lower, width = nlo_box(float(r64[0]), float(r64[-1]))
+    dirs = _native.sobol_dirs(4, 0 if seed is None else seed)
+    box = _native.box(lower, width)
+    dndy = torch.empty_like(N64)
+    k1 = torch.empty_like(N64)
+    k2kf = torch.empty_like(N64)
+    ws = workspace(device, points)
+    lib = _native.load()
+    with torch.cuda.device(device):
+        _native.check(
+            lib.nlo_bk_rhs(
+                params, r64.data_ptr(), N64.data_ptr(), points, dirs, int(config.MCINTPOINTS), box,
+                dndy.data_ptr(), k1.data_ptr(), k2kf.data_ptr(), ws.data_ptr(), ws.numel(),
+                _native.stream_handle(device),
+            )
+        )
+    return dndy, k1, k2kf
+
+
+def _evolve_rows(
+    N0: torch.Tensor,
+    r64: torch.Tensor,
+    steps: int,
+    config: BKConfig,
+    seed: int | None,
+    precision: int,
+) -> torch.Tensor:
+    device = r64.device
+    points = r64.numel()
+    table = torch.empty((steps + 1, points), dtype=torch.float64, device=device)
+    table[0] = N0
+    status = torch.zeros(1, dtype=torch.int32, device=device)
+    params = params_of(config, precision)
+    lower, width = nlo_box(float(r64[0]), float(r64[-1]))
+    dirs = _native.sobol_dirs(4, 0 if seed is None else seed)
+    box = _native.box(lower, width)
+    ws = workspace(device, points)
+    lib = _native.load()
+    with torch.cuda.device(device):
+        _native.check(
+            lib.nlo_bk_evolve(
+                params, r64.data_ptr(), points, steps, float(config.DE_SOLVER_STEP),
+                _native.STEPPERS[config.stepper], dirs, int(config.MCINTPOINTS), box, table.data_ptr(),
+                status.data_ptr(), ws.data_ptr(), ws.numel(), _native.stream_handle(device),
+            )
+        )
+    if int(status.item()) != 0:
+        raise FloatingPointError("non-finite BK amplitude during the rapidity evolution")
+    return table
+
+
+def solve_bk(
+    initial_condition: MV | ICDataFile,
+    maxy: float,
+    config: BKConfig = BKConfig(),
+    *,
+    device: torch.device | str = "cuda",
+    dtype: torch.dtype = torch.float32,
+    seed: int | None = None,
+) -> DipoleTable:
+    """Evolve the initial condition through full steps of DE_SOLVER_STEP up to maxy
+    and return the table (bk/evolution.py:33-58)."""
+
+    if isinstance(initial_condition, ICDataFile):
+        device = initial_condition.r.device if initial_condition.r.is_cuda else device
+        dtype = initial_condition.r.dtype
+    device = _cuda_device(device)
+    # the grid and the initial row are formed on the host in float64 and copied in
+    r_host = _r_grid(config, device="cpu", dtype=torch.float64)
+    if isinstance(initial_condition, ICDataFile):
+        N_host = initial_condition.dipole_amplitude(r_host.to(initial_condition.r.device)).to("cpu", torch.float64)
+    else:
+        N_host = initial_condition.dipole_amplitude(r_host).to(torch.float64)
+    r64 = r_host.to(device, non_blocking=True)
+    N0 = N_host.to(device, non_blocking=True)
+    ys = _steps_to(0.0, maxy, config.DE_SOLVER_STEP)
+    table = _evolve_rows(N0, r64, len(ys), config, seed, precision_of(config, dtype))
+    y = torch.tensor([0.0, *ys], dtype=dtype, device=device)
+    return DipoleTable(r=r64.to(dtype), y=y, N=table.to(dtype), x0=initial_condition.x0)
+
+
+def evolve_table(
+    table: DipoleTable,
+    maxy: float,
+    config: BKConfig = BKConfig(),
+    *,
+    seed: int | None = None,
+) -> DipoleTable:
+    """Continue an existing table (e.g. one read by load_bk_table) from its last row:
+    the resume path of bk/evolution.py:85-96."""
+
+    device = _cuda_device(table.r.device)
+    r64 = table.r.to(torch.float64)
+    start = float(table.y[-1].item())
+    ys = _steps_to(start, maxy, config.DE_SOLVER_STEP)
+    rows = _evolve_rows(table.N[-1].to(torch.float64), r64, len(ys), config, seed,
+                        precision_of(config, table.r.dtype))
+    y = torch.cat((table.y, torch.tensor(ys, dtype=table.y.dtype, device=device)))
+    N = torch.cat((table.N, rows[1:].to(table.N.dtype)), dim=0)
+    return DipoleTable(r=table.r, y=y, N=N, x0=table.x0)
+
+
+def bk_steps(table: DipoleTable, maxy: float, config: BKConfig = BKConfig(), *,
+             seed: int | None = None) -> Iterator[DipoleTable]:
+    """Yield the growing table after every step (the generator of bk/evolution.py:85-159)."""
+
+    current = table
+    for y in _steps_to(float(table.y[-1].item()), maxy, config.DE_SOLVER_STEP):
+        current = evolve_table(current, y, config, seed=seed)
+        yield current
+
+
+def compute_dndy(
+    initial_condition: MV | ICDataFile,
+    config: BKConfig = BKConfig(),
+    *,
+    device: torch.device | str = "cuda",
+    dtype: torch.dtype = torch.float32,
+    seed: int | None = None,
+) -> DNDYResult:
+    """K1 and K2+Kf at the initial rapidity for the active parents (bk/evolution.py:61-82)."""
+
+    if isinstance(initial_condition, ICDataFile):
+        device = initial_condition.r.device if initial_condition.r.is_cuda else device
+        dtype = initial_condition.r.dtype
+    device = _cuda_device(device)
+    r64 = _r_grid(config, device=device, dtype=torch.float64)
+    N = initial_condition.dipole_amplitude(r64).to(torch.float64)
+    _, K1, K2_Kf = rhs(N, r64, config, seed=seed, precision=precision_of(config, dtype))
+    keep = (torch.arange(r64.numel(), device=device) > 0) & (N <= 0.99999)
+    return DNDYResult(r=r64[keep].to(dtype), K1=K1[keep].to(dtype), K2_Kf=K2_Kf[keep].to(dtype),
+                      N=N[keep].to(dtype))
+
+
+__all__ = ["DNDYResult", "bk_steps", "compute_dndy", "evolve_table", "nlo_box", "rhs", "solve_bk"]

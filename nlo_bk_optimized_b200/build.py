@@ -1,0 +1,78 @@
+"""Build ``libnlo_b200.so`` (sm_100a) in-tree with nvcc.
+
+The library is plain C-ABI (include/nlo_b200.h); it links only the CUDA runtime.
+``python -m nlo_bk_optimized_b200.build`` rebuilds it; ``build()`` is what
+``__graft_entry__.build()`` calls.  nvcc cross-compiles without a GPU.
+"""
+
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PACKAGE = Path(__file__).resolve().parent
+ROOT = PACKAGE.parent
+CSRC = PACKAGE / "csrc"
+LIBDIR = PACKAGE / "lib"
+LIBRARY = LIBDIR / "libnlo_b200.so"
+HEADERS = [ROOT / "include" / "nlo_b200.h"]
+
+ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def sources() -> list[Path]:
+    return sorted(CSRC.glob("*.cu"))
+
+
+def _nvcc() -> str:
+    candidate = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not Path(candidate).exists():
+        raise RuntimeError("nvcc not found; the CUDA toolkit is required to build libnlo_b200.so")
+    return candidate
+
+
+def _stale() -> bool:
+    if not LIBRARY.exists():
+        return True
+    built = LIBRARY.stat().st_mtime
+    inputs = sources() + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + HEADERS + [Path(__file__)]
+    return any(path.stat().st_mtime > built for path in inputs)
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    if not force and not _stale():
+        return LIBRARY
+    LIBDIR.mkdir(parents=True, exist_ok=True)
+    tmp = LIBRARY.with_suffix(".so.tmp")
+    command = [
+        _nvcc(),
+        *ARCH_FLAGS,
+        "-O3",
+        "-lineinfo",
+        "-std=c++17",
+        "-Xcompiler",
+        "-fPIC",
+        "-shared",
+        "--expt-relaxed-constexpr",
+        "-o",
+        str(tmp),
+        *[str(s) for s in sources()],
+        "-lcudart",
+    ]
+    if verbose or os.environ.get("NLO_PTXAS_VERBOSE"):
+        command.insert(1, "-Xptxas=-v")
+    result = subprocess.run(command, capture_output=True, text=True)
+    if result.returncode != 0:
+        sys.stderr.write(result.stdout + result.stderr)
+        raise RuntimeError("nvcc failed to build libnlo_b200.so")
+    if verbose:
+        sys.stderr.write(result.stdout + result.stderr)
+    tmp.replace(LIBRARY)
+    return LIBRARY
+
+
+if __name__ == "__main__":
+    print(build(force=True, verbose="-v" in sys.argv))

@@ -1,0 +1,348 @@
+// extern "C" entry points of libnlo_b200.so (declared in include/nlo_b200.h):
+// argument checks, workspace carving and the host-side stage sequence.  Nothing
+// here allocates device memory and nothing synchronises the stream.
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "common.cuh"
+#include "internal.h"
+
+namespace nlo {
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& message)
+{
+    g_last_error = message;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* where)
+{
+    return fail(NLO_ERR_CUDA, std::string(where) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
+}
+
+// Gauss-Legendre nodes on [-1, 1] in ascending order by Newton iteration on P_n
+// (the same construction as numerics/integration.py:781-801).
+void gauss_legendre(int n, double* x, double* w)
+{
+    for (int i = 0; i < n; ++i) {
+        double t = std::cos(kPi * (i + 0.75) / (n + 0.5));
+        double dp = 0.0;
+        for (int it = 0; it < 100; ++it) {
+            double p0 = 1.0, p1 = t;
+            for (int k = 2; k <= n; ++k) {
+                const double p2 = ((2.0 * k - 1.0) * t * p1 - (k - 1.0) * p0) / k;
+                p0 = p1;
+                p1 = p2;
+            }
+            dp = n * (t * p1 - p0) / (t * t - 1.0);
+            const double dt = p1 / dp;
+            t -= dt;
+            if (std::fabs(dt) < 1e-16) break;
+        }
+        double p0 = 1.0, p1 = t;
+        for (int k = 2; k <= n; ++k) {
+            const double p2 = ((2.0 * k - 1.0) * t * p1 - (k - 1.0) * p0) / k;
+            p0 = p1;
+            p1 = p2;
+        }
+        dp = n * (t * p1 - p0) / (t * t - 1.0);
+        x[n - 1 - i] = t;
+        w[n - 1 - i] = 2.0 / ((1.0 - t * t) * dp * dp);
+    }
+}
+
+bool check_params(const nlo_bk_params* p, std::string& why)
+{
+    if (!p) { why = "params is NULL"; return false; }
+    if (!(p->nc > 0)) { why = "NC must be positive"; return false; }
+    if (!(p->nf == 0.0 || p->nf == 3.0)) { why = "the device kernels implement NF = 0 or 3 (smooth coupling)"; return false; }
+    if (!(p->lambda_qcd > 0) || !(p->c2 > 0) || !(p->ksub > 0)) { why = "LambdaQCD, C2 and KSUB must be positive"; return false; }
+    if (p->precision != NLO_PRECISION_MIXED && p->precision != NLO_PRECISION_FP64) { why = "unknown precision"; return false; }
+    return true;
+}
+
+bool check_dirs(const nlo_sobol_dirs* d, int need, std::string& why)
+{
+    if (!d) { why = "dirs is NULL"; return false; }
+    if (d->dims < need || d->dims > 8) { why = "Sobol dimension count out of range"; return false; }
+    for (int j = 0; j < d->dims; ++j) {
+        if (d->shift[j] >= (1u << 30)) { why = "Sobol shift exceeds 30 bits"; return false; }
+        for (int k = 0; k < 30; ++k)
+            if (d->state[j][k] >= (1u << 30)) { why = "Sobol direction number exceeds 30 bits"; return false; }
+    }
+    return true;
+}
+
+SobolDirsArg to_arg(const nlo_sobol_dirs* d)
+{
+    SobolDirsArg a;
+    std::memset(&a, 0, sizeof(a));
+    a.dims = d->dims;
+    std::memcpy(a.state, d->state, sizeof(a.state));
+    std::memcpy(a.shift, d->shift, sizeof(a.shift));
+    return a;
+}
+
+size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
+
+// Workspace layout of one right-hand-side evaluation.
+size_t rhs_bytes(int points, size_t* offsets /*[6] or NULL*/)
+{
+    size_t o = 0;
+    size_t off[6];
+    off[0] = o; o = align_up(o + sizeof(double) * spline_doubles(points));
+    off[1] = o; o = align_up(o + sizeof(int32_t) * (size_t)points);
+    off[2] = o; o = align_up(o + sizeof(int32_t) * 4);
+    off[3] = o; o = align_up(o + sizeof(double) * (size_t)points);
+    off[4] = o; o = align_up(o + sizeof(double) * 3 * (size_t)points);
+    off[5] = o; o = align_up(o + sizeof(double) * 3 * (size_t)points * (size_t)k2kf_max_blocks());
+    if (offsets) std::memcpy(offsets, off, sizeof(off));
+    return o;
+}
+
+RhsBuffers carve(void* ws, int points)
+{
+    size_t off[6];
+    rhs_bytes(points, off);
+    char* base = static_cast<char*>(ws);
+    RhsBuffers b;
+    b.spline = reinterpret_cast<double*>(base + off[0]);
+    b.active = reinterpret_cast<int32_t*>(base + off[1]);
+    b.count = reinterpret_cast<int32_t*>(base + off[2]);
+    b.k1 = reinterpret_cast<double*>(base + off[3]);
+    b.k2kf = reinterpret_cast<double*>(base + off[4]);
+    b.partial = reinterpret_cast<double*>(base + off[5]);
+    b.k2kf_blocks = k2kf_max_blocks();
+    return b;
+}
+
+int run_rhs(const nlo_bk_params& p, const double* r, const double* N, int points, const SobolDirsArg& dirs,
+            uint64_t samples, const nlo_bk_box& box, double* dndy, double* k1_out, double* k2kf_out,
+            const RhsBuffers& b, cudaStream_t stream)
+{
+    cudaError_t e;
+    if ((e = launch_splines(r, N, points, p.force_positive, b.spline, stream)) != cudaSuccess)
+        return cuda_fail(e, "splines");
+    if ((e = launch_active(N, points, b.active, b.count, stream)) != cudaSuccess) return cuda_fail(e, "active");
+    if ((e = launch_k1(p, r, points, b.spline, b.active, b.count, b.k1, stream)) != cudaSuccess)
+        return cuda_fail(e, "k1");
+    if ((e = launch_k2kf(p, r, points, b.spline, b.active, b.count, dirs, 0, samples, box, b.k2kf, b.partial,
+                         b.k2kf_blocks, stream)) != cudaSuccess)
+        return cuda_fail(e, "k2kf");
+    if ((e = launch_assemble(b.k1, b.k2kf, points, samples ? 1.0 / (double)samples : 0.0, dndy, k2kf_out, stream)) !=
+        cudaSuccess)
+        return cuda_fail(e, "assemble");
+    if (k1_out) {
+        if ((e = cudaMemcpyAsync(k1_out, b.k1, sizeof(double) * points, cudaMemcpyDeviceToDevice, stream)) !=
+            cudaSuccess)
+            return cuda_fail(e, "k1 copy");
+    }
+    return NLO_OK;
+}
+
+}  // namespace
+
+const K1Rule& k1_rule()
+{
+    static K1Rule rule = [] {
+        K1Rule q;
+        gauss_legendre(8, q.x8, q.w8);
+        gauss_legendre(24, q.x24, q.w24);
+        return q;
+    }();
+    return rule;
+}
+
+size_t spline_doubles(int points) { return (size_t)points + 8 * (size_t)(points - 1); }
+
+int k2kf_max_blocks()
+{
+    static int blocks = [] {
+        int device = 0, sms = 148;
+        if (cudaGetDevice(&device) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        return 4 * (sms > 0 ? sms : 148);
+    }();
+    return blocks;
+}
+
+}  // namespace nlo
+
+using namespace nlo;
+
+extern "C" {
+
+const char* nlo_last_error(void) { return g_last_error.c_str(); }
+
+int nlo_abi_version(void) { return 1; }
+
+int nlo_sobol_draw(const nlo_sobol_dirs* dirs, int64_t offset, int64_t n, int32_t precision, void* out, void* stream)
+{
+    std::string why;
+    if (!check_dirs(dirs, 1, why)) return fail(NLO_ERR_INVALID, why);
+    if (offset < 0 || n < 0 || offset + n > (int64_t(1) << 30)) return fail(NLO_ERR_INVALID, "Sobol index range exceeds 2^30");
+    if (precision != NLO_PRECISION_MIXED && precision != NLO_PRECISION_FP64) return fail(NLO_ERR_INVALID, "unknown precision");
+    if (n == 0) return NLO_OK;
+    if (!out) return fail(NLO_ERR_INVALID, "out is NULL");
+    cudaError_t e = launch_sobol(to_arg(dirs), (uint64_t)offset, (uint64_t)n, precision, out, (cudaStream_t)stream);
+    return e == cudaSuccess ? NLO_OK : cuda_fail(e, "sobol");
+}
+
+size_t nlo_bk_spline_doubles(int32_t points) { return points >= 2 ? spline_doubles(points) : 0; }
+
+int nlo_bk_splines(const double* r, const double* N, int32_t points, int32_t force_positive, double* spline, void* stream)
+{
+    if (points < 3 || points > 4096) return fail(NLO_ERR_INVALID, "a cubic spline requires 3..4096 points");
+    if (!r || !N || !spline) return fail(NLO_ERR_INVALID, "NULL buffer");
+    cudaError_t e = launch_splines(r, N, points, force_positive, spline, (cudaStream_t)stream);
+    return e == cudaSuccess ? NLO_OK : cuda_fail(e, "splines");
+}
+
+int nlo_bk_active(const double* N, int32_t points, int32_t* active, int32_t* count, void* stream)
+{
+    if (points < 1) return fail(NLO_ERR_INVALID, "points must be positive");
+    if (!N || !active || !count) return fail(NLO_ERR_INVALID, "NULL buffer");
+    cudaError_t e = launch_active(N, points, active, count, (cudaStream_t)stream);
+    return e == cudaSuccess ? NLO_OK : cuda_fail(e, "active");
+}
+
+int nlo_bk_k1(const nlo_bk_params* params, const double* r, int32_t points, const double* spline,
+              const int32_t* active, const int32_t* count, double* out, void* stream)
+{
+    std::string why;
+    if (!check_params(params, why)) return fail(NLO_ERR_INVALID, why);
+    if (points < 3 || points > 4096) return fail(NLO_ERR_INVALID, "points must be 3..4096");
+    if (!r || !spline || !active || !count || !out) return fail(NLO_ERR_INVALID, "NULL buffer");
+    cudaError_t e = launch_k1(*params, r, points, spline, active, count, out, (cudaStream_t)stream);
+    return e == cudaSuccess ? NLO_OK : cuda_fail(e, "k1");
+}
+
+size_t nlo_bk_k2kf_workspace_bytes(int32_t points)
+{
+    if (points < 1) return 0;
+    return sizeof(double) * 3 * (size_t)points * (size_t)k2kf_max_blocks();
+}
+
+int nlo_bk_k2kf(const nlo_bk_params* params, const double* r, int32_t points, const double* spline,
+                const int32_t* active, const int32_t* count, const nlo_sobol_dirs* dirs, int64_t offset,
+                int64_t samples, const nlo_bk_box* box, double* out, void* workspace, size_t workspace_bytes,
+                void* stream)
+{
+    std::string why;
+    if (!check_params(params, why)) return fail(NLO_ERR_INVALID, why);
+    if (!check_dirs(dirs, 4, why)) return fail(NLO_ERR_INVALID, why);
+    if (points < 3 || points > 4096) return fail(NLO_ERR_INVALID, "points must be 3..4096");
+    if (!r || !spline || !active || !count || !out || !box) return fail(NLO_ERR_INVALID, "NULL buffer");
+    if (offset < 0 || samples < 0 || offset + samples > (int64_t(1) << 30))
+        return fail(NLO_ERR_INVALID, "Sobol index range exceeds 2^30");
+    if (!workspace || workspace_bytes < nlo_bk_k2kf_workspace_bytes(points))
+        return fail(NLO_ERR_WORKSPACE, "workspace too small for nlo_bk_k2kf");
+    cudaError_t e = launch_k2kf(*params, r, points, spline, active, count, to_arg(dirs), (uint64_t)offset,
+                                (uint64_t)samples, *box, out, static_cast<double*>(workspace), k2kf_max_blocks(),
+                                (cudaStream_t)stream);
+    return e == cudaSuccess ? NLO_OK : cuda_fail(e, "k2kf");
+}
+
+size_t nlo_bk_rhs_workspace_bytes(int32_t points)
+{
+    if (points < 3) return 0;
+    // one right-hand side plus five stage rows for the steppers
+    return rhs_bytes(points, nullptr) + align_up(sizeof(double) * 5 * (size_t)points);
+}
+
+int nlo_bk_rhs(const nlo_bk_params* params, const double* r, const double* N, int32_t points,
+               const nlo_sobol_dirs* dirs, int64_t samples, const nlo_bk_box* box, double* dndy, double* k1,
+               double* k2kf, void* workspace, size_t workspace_bytes, void* stream)
+{
+    std::string why;
+    if (!check_params(params, why)) return fail(NLO_ERR_INVALID, why);
+    if (!check_dirs(dirs, 4, why)) return fail(NLO_ERR_INVALID, why);
+    if (points < 3 || points > 4096) return fail(NLO_ERR_INVALID, "points must be 3..4096");
+    if (!r || !N || !dndy || !box) return fail(NLO_ERR_INVALID, "NULL buffer");
+    if (samples < 0 || samples > (int64_t(1) << 30)) return fail(NLO_ERR_INVALID, "samples out of range");
+    if (!workspace || workspace_bytes < nlo_bk_rhs_workspace_bytes(points))
+        return fail(NLO_ERR_WORKSPACE, "workspace too small for nlo_bk_rhs");
+    const RhsBuffers b = carve(workspace, points);
+    return run_rhs(*params, r, N, points, to_arg(dirs), (uint64_t)samples, *box, dndy, k1, k2kf, b,
+                   (cudaStream_t)stream);
+}
+
+int nlo_bk_evolve(const nlo_bk_params* params, const double* r, int32_t points, int32_t steps, double step,
+                  int32_t stepper, const nlo_sobol_dirs* dirs, int64_t samples, const nlo_bk_box* box,
+                  double* table, uint32_t* status, void* workspace, size_t workspace_bytes, void* stream)
+{
+    std::string why;
+    if (!check_params(params, why)) return fail(NLO_ERR_INVALID, why);
+    if (!check_dirs(dirs, 4, why)) return fail(NLO_ERR_INVALID, why);
+    if (points < 3 || points > 4096) return fail(NLO_ERR_INVALID, "points must be 3..4096");
+    if (steps < 0) return fail(NLO_ERR_INVALID, "steps must be non-negative");
+    if (!(step > 0) || !std::isfinite(step)) return fail(NLO_ERR_INVALID, "step must be positive");
+    if (stepper != NLO_STEPPER_EULER && stepper != NLO_STEPPER_RK3 && stepper != NLO_STEPPER_RK4)
+        return fail(NLO_ERR_INVALID, "unknown stepper");
+    if (!r || !table || !status || !box) return fail(NLO_ERR_INVALID, "NULL buffer");
+    if (samples < 0 || samples > (int64_t(1) << 30)) return fail(NLO_ERR_INVALID, "samples out of range");
+    if (!workspace || workspace_bytes < nlo_bk_rhs_workspace_bytes(points))
+        return fail(NLO_ERR_WORKSPACE, "workspace too small for nlo_bk_evolve");
+    cudaStream_t s = (cudaStream_t)stream;
+    const RhsBuffers b = carve(workspace, points);
+    double* stage = reinterpret_cast<double*>(static_cast<char*>(workspace) + rhs_bytes(points, nullptr));
+    double* kk[4] = {stage, stage + points, stage + 2 * points, stage + 3 * points};
+    double* tmp = stage + 4 * points;
+    const SobolDirsArg dirs_arg = to_arg(dirs);
+    cudaError_t e = cudaMemsetAsync(status, 0, sizeof(uint32_t), s);
+    if (e != cudaSuccess) return cuda_fail(e, "status reset");
+    const int clamp = params->force_positive ? 1 : 0;
+    for (int it = 0; it < steps; ++it) {
+        const double* N = table + (size_t)it * points;
+        double* next = table + (size_t)(it + 1) * points;
+        int rc;
+        auto f = [&](const double* in, double* out) {
+            return run_rhs(*params, r, in, points, dirs_arg, (uint64_t)samples, *box, out, nullptr, nullptr, b, s);
+        };
+        if (stepper == NLO_STEPPER_EULER) {
+            if ((rc = f(N, kk[0])) != NLO_OK) return rc;
+            const double c[1] = {step};
+            if ((e = launch_axpy_stage(N, kk, c, 1, points, next, clamp, status, s)) != cudaSuccess)
+                return cuda_fail(e, "stage");
+        } else if (stepper == NLO_STEPPER_RK3) {
+            // Kutta RK3 (bk/evolution.py:204-236)
+            if ((rc = f(N, kk[0])) != NLO_OK) return rc;
+            const double c1[1] = {0.5 * step};
+            if ((e = launch_axpy_stage(N, kk, c1, 1, points, tmp, 0, nullptr, s)) != cudaSuccess) return cuda_fail(e, "stage");
+            if ((rc = f(tmp, kk[1])) != NLO_OK) return rc;
+            const double c2[2] = {-step, 2.0 * step};
+            if ((e = launch_axpy_stage(N, kk, c2, 2, points, tmp, 0, nullptr, s)) != cudaSuccess) return cuda_fail(e, "stage");
+            if ((rc = f(tmp, kk[2])) != NLO_OK) return rc;
+            const double c3[3] = {step / 6.0, 4.0 * step / 6.0, step / 6.0};
+            if ((e = launch_axpy_stage(N, kk, c3, 3, points, next, clamp, status, s)) != cudaSuccess)
+                return cuda_fail(e, "stage");
+        } else {
+            // classical RK4
+            if ((rc = f(N, kk[0])) != NLO_OK) return rc;
+            const double c1[1] = {0.5 * step};
+            if ((e = launch_axpy_stage(N, kk, c1, 1, points, tmp, 0, nullptr, s)) != cudaSuccess) return cuda_fail(e, "stage");
+            if ((rc = f(tmp, kk[1])) != NLO_OK) return rc;
+            const double* k2p[1] = {kk[1]};
+            if ((e = launch_axpy_stage(N, k2p, c1, 1, points, tmp, 0, nullptr, s)) != cudaSuccess) return cuda_fail(e, "stage");
+            if ((rc = f(tmp, kk[2])) != NLO_OK) return rc;
+            const double* k3p[1] = {kk[2]};
+            const double c3[1] = {step};
+            if ((e = launch_axpy_stage(N, k3p, c3, 1, points, tmp, 0, nullptr, s)) != cudaSuccess) return cuda_fail(e, "stage");
+            if ((rc = f(tmp, kk[3])) != NLO_OK) return rc;
+            const double c4[4] = {step / 6.0, 2.0 * step / 6.0, 2.0 * step / 6.0, step / 6.0};
+            if ((e = launch_axpy_stage(N, kk, c4, 4, points, next, clamp, status, s)) != cudaSuccess)
+                return cuda_fail(e, "stage");
+        }
+    }
+    return NLO_OK;
+}
+
+}  // extern "C"

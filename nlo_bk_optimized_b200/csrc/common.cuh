@@ -1,0 +1,256 @@
+// Shared device mathematics for the NLO BK kernels (sm_100a).
+//
+// Every kernel is templated on the arithmetic type T:
+//   T = float  : the mixed build -- integrands in FP32 on the FMA/MUFU pipes,
+//                compensated FP32 partial sums folded into FP64;
+//   T = double : the all-FP64 build used to check parity at 1e-10.
+// The formulas are the reference's (torch_nlo_clean/src/nlo_torch: bk_kernels/k1.py,
+// k2.py, kf.py, bk/derivatives.py, coupling.py) rewritten in algebraically identical
+// forms that have no catastrophic cancellation, so that FP32 keeps ~1e-6 relative
+// accuracy for every parent size r:
+//   X^2          = (r - z)^2 + 4 r z sin^2(theta/2)
+//   XY2^2-X2Y^2  = r [ r (z'^2 - z^2) - 2 z z' (z' cos th - z cos th') ]
+//   log(a/b)/(a-b) = 2 h(t)/(a+b),  h(t) = atanh(t)/t,  t = (a-b)/(a+b)
+//   alpha_Y - alpha_X from log1p/expm1 of the exact X^2 - Y^2
+//   N_A - N_B    = S_A expm1(p_B - p_A) from log-spline values p
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math_constants.h>
+#include <stdint.h>
+
+#include "../../include/nlo_b200.h"
+
+namespace nlo {
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kMinLog = -40.0;  // numerics/interpolation.py:8
+
+// ---------------------------------------------------------------------------
+// Precision traits: fast MUFU-based functions for float, libm for double.
+template <typename T>
+struct M;
+
+template <>
+struct M<float> {
+    static __device__ __forceinline__ float log_fast(float x) { return __logf(x); }
+    static __device__ __forceinline__ float exp_fast(float x) { return __expf(x); }
+    static __device__ __forceinline__ float log_acc(float x) { return logf(x); }
+    static __device__ __forceinline__ float exp_acc(float x) { return expf(x); }
+    static __device__ __forceinline__ float expm1(float x) { return expm1f(x); }
+    static __device__ __forceinline__ float log1p(float x) { return log1pf(x); }
+    static __device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
+    static __device__ __forceinline__ float div(float a, float b) { return __fdividef(a, b); }
+    static __device__ __forceinline__ float sqrt(float x) { return sqrtf(x); }
+    static __device__ __forceinline__ float sin(float x) { return sinf(x); }
+    static __device__ __forceinline__ float cos(float x) { return cosf(x); }
+    static __device__ __forceinline__ float j1(float x) { return j1f(x); }
+    static __device__ __forceinline__ float i1(float x) { return cyl_bessel_i1f(x); }
+    static __device__ __forceinline__ float fmin(float a, float b) { return fminf(a, b); }
+    static __device__ __forceinline__ float fmax(float a, float b) { return fmaxf(a, b); }
+    static __device__ __forceinline__ float fabs(float a) { return fabsf(a); }
+    static __device__ __forceinline__ bool finite(float a) { return isfinite(a); }
+    // explicitly rounded map operations (the oracle replays them in float32)
+    static __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+    static __device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+    static constexpr float tiny_square() { return 1e-38f; }
+};
+
+template <>
+struct M<double> {
+    static __device__ __forceinline__ double log_fast(double x) { return ::log(x); }
+    static __device__ __forceinline__ double exp_fast(double x) { return ::exp(x); }
+    static __device__ __forceinline__ double log_acc(double x) { return ::log(x); }
+    static __device__ __forceinline__ double exp_acc(double x) { return ::exp(x); }
+    static __device__ __forceinline__ double expm1(double x) { return ::expm1(x); }
+    static __device__ __forceinline__ double log1p(double x) { return ::log1p(x); }
+    static __device__ __forceinline__ double rcp(double x) { return 1.0 / x; }
+    static __device__ __forceinline__ double div(double a, double b) { return a / b; }
+    static __device__ __forceinline__ double sqrt(double x) { return ::sqrt(x); }
+    static __device__ __forceinline__ double sin(double x) { return ::sin(x); }
+    static __device__ __forceinline__ double cos(double x) { return ::cos(x); }
+    static __device__ __forceinline__ double j1(double x) { return ::j1(x); }
+    static __device__ __forceinline__ double i1(double x) { return ::cyl_bessel_i1(x); }
+    static __device__ __forceinline__ double fmin(double a, double b) { return ::fmin(a, b); }
+    static __device__ __forceinline__ double fmax(double a, double b) { return ::fmax(a, b); }
+    static __device__ __forceinline__ double fabs(double a) { return ::fabs(a); }
+    static __device__ __forceinline__ bool finite(double a) { return isfinite(a); }
+    static __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+    static __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+    static constexpr double tiny_square() { return 1e-40; }
+};
+
+// ---------------------------------------------------------------------------
+// Physics constants, converted once per launch to the arithmetic type.
+template <typename T>
+struct Phys {
+    T nc, nf, nf_over_nc;
+    T b0c;        // b0 * 0.2 with b0 = (11 Nc - 2 Nf)/(12 pi)          coupling.py:92-96
+    T left;       // 2/0.2 * log(2.5)                                     coupling.py:92
+    T log_sc;     // log(4 C2 / Lambda^2)                                 coupling.py:94
+    T fixed_as;   // fixed coupling value (if fixed)
+    T alpha_cap;  // > 0: cap
+    T minr;
+    T ksub, log_ksub;
+    bool fixed;
+    bool symmetrize;
+};
+
+template <typename T>
+__host__ Phys<T> make_phys(const nlo_bk_params& p)
+{
+    Phys<T> q;
+    q.nc = (T)p.nc;
+    q.nf = (T)p.nf;
+    q.nf_over_nc = (T)(p.nf / p.nc);
+    q.b0c = (T)((11.0 * p.nc - 2.0 * p.nf) / (12.0 * kPi) * 0.2);
+    q.left = (T)(2.0 / 0.2 * std::log(2.5));
+    q.log_sc = (T)std::log(4.0 * p.c2 / (p.lambda_qcd * p.lambda_qcd));
+    q.fixed_as = (T)p.fixed_alpha_s;
+    q.alpha_cap = (T)p.alpha_cap;
+    q.minr = (T)p.minr;
+    q.ksub = (T)p.ksub;
+    q.log_ksub = (T)std::log(p.ksub);
+    q.fixed = p.fixed_coupling != 0;
+    q.symmetrize = p.symmetrize != 0;
+    return q;
+}
+
+// logaddexp(left, right) with right = (log_sc - 2 log d)/0.2   (coupling.py:81-97)
+template <typename T>
+__device__ __forceinline__ T alpha_of_log(T log_d, const Phys<T>& ph)
+{
+    if (ph.fixed) return ph.fixed_as;
+    const T right = (ph.log_sc - (T)2 * log_d) * (T)5;
+    const T m = M<T>::fmax(ph.left, right);
+    const T lae = m + M<T>::log_fast((T)1 + M<T>::exp_fast(-M<T>::fabs(ph.left - right)));
+    T a = M<T>::rcp(ph.b0c * lae);
+    if (ph.alpha_cap > (T)0 && a > ph.alpha_cap) a = ph.alpha_cap;
+    return a;
+}
+
+// logaddexp(c, t + delta) - logaddexp(c, t) without cancellation.
+template <typename T>
+__device__ __forceinline__ T lae_difference(T c, T t, T delta)
+{
+    const T sigma = M<T>::rcp((T)1 + M<T>::exp_fast(c - t));
+    const T v = sigma * M<T>::expm1(delta);
+    if (v > (T)-0.5) return M<T>::log1p(v);
+    const T sigma_c = M<T>::rcp((T)1 + M<T>::exp_fast(t - c));
+    return M<T>::log_acc(sigma_c + sigma * M<T>::exp_fast(delta));
+}
+
+// ---------------------------------------------------------------------------
+// Log-log spline in shared memory: knots x[n] (log r), coefficients (a,b,c,d) per interval.
+// The r grid is logarithmically uniform, so the interval is found in O(1) from
+// (lx - x0)/h with a one-step fix-up against the stored knots; the result is the
+// interval that searchsorted(x, lx, right=True) - 1 (clamped) would return
+// (numerics/interpolation.py:70-76).
+template <typename T>
+struct SplineView {
+    const T* x;     // [n]
+    const T* coef;  // [n-1][4]
+    int n;
+    T x0, inv_h;
+};
+
+__device__ __forceinline__ int floor_to_int(float v) { return __float2int_rd(v); }
+__device__ __forceinline__ int floor_to_int(double v) { return __double2int_rd(v); }
+
+template <typename T>
+__device__ __forceinline__ int spline_interval(const SplineView<T>& s, T lx)
+{
+    int i = floor_to_int((lx - s.x0) * s.inv_h);
+    i = i < 0 ? 0 : (i > s.n - 2 ? s.n - 2 : i);
+    if (i > 0 && lx < s.x[i]) --i;
+    if (i < s.n - 2 && lx >= s.x[i + 1]) ++i;
+    return i;
+}
+
+template <typename T>
+__device__ __forceinline__ T spline_poly(const SplineView<T>& s, T lx)
+{
+    const T lo = s.x[0], hi = s.x[s.n - 1];
+    lx = lx < lo ? lo : (lx > hi ? hi : lx);
+    const int i = spline_interval(s, lx);
+    const T* c = s.coef + 4 * i;
+    const T dx = lx - s.x[i];
+    return c[0] + dx * (c[1] + dx * (c[2] + dx * c[3]));
+}
+
+// Amplitude at a distance with its log-S spline value (K2+Kf).
+template <typename T>
+struct NS {
+    T p, N, S;
+    int edge;  // -1 below r_min, 0 inside, +1 above r_max
+};
+
+// Edge rules of bk/derivatives.py:761-772 for the S row: S = 1 below r_min, 0 above r_max.
+template <typename T>
+__device__ __forceinline__ NS<T> eval_s_log(const SplineView<T>& s, T log_r)
+{
+    NS<T> v;
+    if (log_r < s.x[0]) { v.p = (T)0; v.N = (T)0; v.S = (T)1; v.edge = -1; return v; }
+    if (log_r > s.x[s.n - 1]) { v.p = (T)0; v.N = (T)1; v.S = (T)0; v.edge = 1; return v; }
+    v.edge = 0;
+    v.p = spline_poly(s, log_r);
+    v.S = M<T>::exp_fast(v.p);
+    v.N = -M<T>::expm1(v.p);
+    return v;
+}
+
+// N_A - N_B
+template <typename T>
+__device__ __forceinline__ T ndiff_s(const NS<T>& A, const NS<T>& B)
+{
+    if (A.edge == 0 && B.edge == 0) return A.S * M<T>::expm1(B.p - A.p);
+    if (A.N < (T)0.5 && B.N < (T)0.5) return A.N - B.N;
+    return B.S - A.S;
+}
+
+// Spline value at lx minus the knot value a_i; Taylor form about knot i for lx in
+// interval i or i-1 (no cancellation when lx is close to the knot).
+template <typename T>
+__device__ __forceinline__ T spline_delta_from_knot(const SplineView<T>& s, int i, T knot_value, T lx)
+{
+    const T lo = s.x[0], hi = s.x[s.n - 1];
+    lx = lx < lo ? lo : (lx > hi ? hi : lx);
+    const int j = spline_interval(s, lx);
+    const T dx = lx - s.x[i];
+    if (j == i) {
+        const T* c = s.coef + 4 * i;
+        return dx * (c[1] + dx * (c[2] + dx * c[3]));
+    }
+    if (j == i - 1) {
+        const T* c = s.coef + 4 * (i - 1);
+        const T h = s.x[i] - s.x[i - 1];
+        const T b1 = c[1] + h * ((T)2 * c[2] + (T)3 * h * c[3]);
+        const T c1 = c[2] + (T)3 * h * c[3];
+        return dx * (b1 + dx * (c1 + dx * c[3]));
+    }
+    const T* c = s.coef + 4 * j;
+    const T ddx = lx - s.x[j];
+    const T pv = c[0] + ddx * (c[1] + ddx * (c[2] + ddx * c[3]));
+    return pv - knot_value;
+}
+
+// Compensated (Kahan) accumulation.
+template <typename T>
+struct Kahan {
+    T sum, comp;
+    __device__ __forceinline__ void reset() { sum = (T)0; comp = (T)0; }
+    __device__ __forceinline__ void add(T v)
+    {
+        const T y = v - comp;
+        const T t = sum + y;
+        comp = (t - sum) - y;
+        sum = t;
+    }
+};
+
+// Status word bits written by kernels (never a trap).
+enum StatusBits : uint32_t {
+    kStatusNonFinite = 1u << 0,
+};
+
+}  // namespace nlo

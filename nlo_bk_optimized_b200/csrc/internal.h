@@ -1,0 +1,57 @@
+// Internal launch interfaces shared by the .cu files of the library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "../../include/nlo_b200.h"
+
+namespace nlo {
+
+// Sobol direction numbers passed by value as a kernel parameter.
+struct SobolDirsArg {
+    int dims;
+    uint32_t state[8][30];
+    uint32_t shift[8];
+};
+
+// Gauss-Legendre rules of the fixed K1 integration (8 radial x 24 angular).
+struct K1Rule {
+    double x8[8], w8[8];
+    double x24[24], w24[24];
+};
+
+const K1Rule& k1_rule();
+
+// Buffers of one right-hand-side evaluation carved from the caller's workspace.
+struct RhsBuffers {
+    double* spline;   // nlo_bk_spline_doubles(points)
+    int32_t* active;  // [points]
+    int32_t* count;   // [1]
+    double* k1;       // [points]
+    double* k2kf;     // [points][3]
+    double* partial;  // [k2kf_blocks][points][3]
+    int k2kf_blocks;
+};
+
+size_t spline_doubles(int points);
+int k2kf_max_blocks();
+
+cudaError_t launch_splines(const double* r, const double* N, int n, int force_positive, double* out,
+                           cudaStream_t stream);
+cudaError_t launch_active(const double* N, int n, int32_t* active, int32_t* count, cudaStream_t stream);
+cudaError_t launch_sobol(const SobolDirsArg& dirs, uint64_t offset, uint64_t n, int precision, void* out,
+                         cudaStream_t stream);
+cudaError_t launch_k1(const nlo_bk_params& p, const double* r, int points, const double* spline,
+                      const int32_t* active, const int32_t* count, double* out, cudaStream_t stream);
+cudaError_t launch_k2kf(const nlo_bk_params& p, const double* r, int points, const double* spline,
+                        const int32_t* active, const int32_t* count, const SobolDirsArg& dirs, uint64_t offset,
+                        uint64_t samples, const nlo_bk_box& box, double* out, double* partial, int max_blocks,
+                        cudaStream_t stream);
+cudaError_t launch_assemble(const double* k1, const double* k2kf, int points, double inv_samples, double* dndy,
+                            double* k2kf_total, cudaStream_t stream);
+cudaError_t launch_axpy_stage(const double* N, const double* const* k, const double* coef, int nk, int points,
+                              double* out, int clamp, uint32_t* status, cudaStream_t stream);
+
+}  // namespace nlo

@@ -1,0 +1,269 @@
+// K1: the LO-like part of the NLO BK right-hand side, by the fixed rule of
+// custom_kernels/bk/k1/kernel.cu:2040-2092 (per r-grid interval 8 Gauss-Legendre
+// nodes in log z times 24 nodes in v with theta = pi v^2, weight 2 z^2 * radial *
+// pi v * angular), with the integrand Kernel_lo x dipole of bk_kernels/k1.py:20-155
+// and bk/derivatives.py:434-468 for the production order NLO_RESUM_DLOG_SLOG,
+// RC_LO = BALITSKY_LO, RESUM_RC = RESUM_RC_SMALLEST.
+//
+// One CTA per active parent.  Threads own (interval, radial node) pairs and sweep
+// the 24 angular nodes; per-thread sums are FP64, the block reduction is a fixed
+// tree (deterministic).  In the mixed build the integrand runs in FP32 except on
+// the two intervals adjacent to the parent knot (z -> x, where X -> 0 and the
+// dipole N_Y - N_r cancels), which run in FP64.
+
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "internal.h"
+
+namespace nlo {
+
+namespace {
+
+constexpr int kK1Threads = 256;
+
+template <typename T>
+struct K1Parent {
+    T r, lr, r2;
+    T alpha_r;
+    T Nr, Sr, pr;  // amplitude at the knot and its log value
+    int knot;
+};
+
+// Amplitude at distance exp(lx) relative to the parent knot: N and D = N - N_r.
+template <typename T>
+__device__ __forceinline__ void k1_amplitude(const SplineView<T>& s, const K1Parent<T>& P, T lx, T& N, T& D)
+{
+    if (lx < s.x[0]) { N = (T)0; D = -P.Nr; return; }
+    if (lx > s.x[s.n - 1]) { N = (T)1; D = P.Sr; return; }
+    const T dp = spline_delta_from_knot(s, P.knot, P.pr, lx);
+    const T pv = P.pr + dp;
+    T nv = M<T>::exp_fast(pv);
+    if (!M<T>::finite(nv)) nv = (T)0;
+    if (nv >= (T)1) { N = (T)1; D = P.Sr; return; }
+    N = nv;
+    D = P.Nr * M<T>::expm1(dp);
+}
+
+// Per radial node (r-dependent but theta-independent) data.
+template <typename T>
+struct K1Z {
+    T z, lz, Ysq;
+    T NY, DY;
+    T alpha_Y;
+    T right_Y;  // (log_sc - 2 log z) / 0.2
+    T ly_minus_lr;
+};
+
+template <typename T>
+__device__ __forceinline__ K1Z<T> k1_prepare_z(const SplineView<T>& s, const K1Parent<T>& P, const Phys<T>& ph,
+                                              T lz)
+{
+    K1Z<T> Z;
+    Z.lz = lz;
+    Z.z = M<T>::exp_acc(lz);
+    Z.Ysq = Z.z * Z.z;
+    k1_amplitude(s, P, lz, Z.NY, Z.DY);
+    Z.alpha_Y = alpha_of_log(lz, ph);
+    Z.right_Y = (ph.log_sc - (T)2 * lz) * (T)5;
+    Z.ly_minus_lr = lz - P.lr;
+    return Z;
+}
+
+// Kernel_lo x dipole at one (z, theta) node; sh2 = sin^2(theta/2).
+template <typename T>
+__device__ __forceinline__ T k1_point(const SplineView<T>& s, const K1Parent<T>& P, const K1Z<T>& Z,
+                                      const Phys<T>& ph, T sh2)
+{
+    const T r = P.r, z = Z.z;
+    const T Xsq = (r - z) * (r - z) + (T)4 * r * z * sh2;
+    if (!(Xsq >= M<T>::tiny_square())) return (T)0;
+    const T lXsq = M<T>::log_fast(Xsq);
+    const T lX = (T)0.5 * lXsq;
+    const T alpha_X = alpha_of_log(lX, ph);
+    // X^2 - Y^2 = r (r - 2 z cos theta), cos theta = 1 - 2 sin^2(theta/2)
+    const T XmY = r * (r - (T)2 * z * ((T)1 - (T)2 * sh2));
+    T dalpha;
+    if (ph.fixed) {
+        dalpha = (T)0;
+    } else if (ph.alpha_cap > (T)0) {
+        dalpha = Z.alpha_Y - alpha_X;
+    } else {
+        // alpha_Y - alpha_X = alpha_X alpha_Y b0 c (lae_X - lae_Y)
+        const T delta = -(T)5 * M<T>::log1p(M<T>::div(XmY, Z.Ysq));
+        dalpha = alpha_X * Z.alpha_Y * ph.b0c * lae_difference(ph.left, Z.right_Y, delta);
+    }
+    // r^2/(X^2Y^2) + (aY/aX - 1)/Y^2 + (aX/aY - 1)/X^2
+    const T inv_XY = M<T>::rcp(Xsq * Z.Ysq);
+    const T bracket = (P.r2 + dalpha * M<T>::div(Z.alpha_Y * XmY + Z.Ysq * dalpha, alpha_X * Z.alpha_Y)) * inv_XY;
+    const T pref = ph.nc * (T)(1.0 / (2.0 * kPi * kPi));
+    T lo = pref * P.alpha_r * bracket;
+    if (!M<T>::finite(lo)) lo = (T)0;
+    // double-log resummation (k1.py:109-119), alpha at the smallest size (RESUM_RC_SMALLEST)
+    const T lmin = M<T>::fmin(M<T>::fmin(lX, Z.lz), P.lr);
+    const T alpha_min = alpha_of_log(lmin, ph);
+    const T xarg = (T)4 * (lX - P.lr) * Z.ly_minus_lr;
+    const T abar = alpha_min * ph.nc * (T)(1.0 / kPi);
+    const T as_x = M<T>::sqrt(abar * M<T>::fabs(xarg));
+    T dlog = (T)1;
+    if (as_x != (T)0) {
+        const T bes = xarg >= (T)0 ? M<T>::j1((T)2 * as_x) : M<T>::i1((T)2 * as_x);
+        dlog = M<T>::div(bes, as_x);
+    }
+    if (!(r > (T)1.01 * ph.minr)) dlog = (T)1;
+    if (!M<T>::finite(dlog)) return (T)0;
+    // single-log resummation (k1.py:121-132): exp(-abar A1 |log(ksub (r/minxy)^2)|)
+    const T lminxy = M<T>::fmin(lX, Z.lz);
+    const T slog_exp = -abar * (T)(11.0 / 12.0) * M<T>::fabs(ph.log_ksub + (T)2 * (P.lr - lminxy));
+    const T slog = M<T>::exp_fast(slog_exp);
+    const T lo_single = pref * P.alpha_r * P.r2 * inv_XY;
+    const T k1fin = lo * P.alpha_r * ph.nc * (T)(1.0 / (4.0 * kPi)) *
+                    ((T)(67.0 / 9.0 - kPi * kPi / 3.0) - (T)(10.0 / 9.0) * ph.nf_over_nc);
+    // dipole N_X + N_Y - N_r - N_X N_Y = S_r (N_Y + D_X) - D_X D_Y  (or with X and Y exchanged)
+    T NX, DX;
+    k1_amplitude(s, P, lX, NX, DX);
+    const T base = Z.NY <= NX ? Z.NY + DX : NX + Z.DY;
+    const T dipole = P.Sr * base - DX * Z.DY;
+    const T result = (dlog * slog * lo - lo_single * slog_exp + k1fin) * dipole;
+    return M<T>::finite(result) ? result : (T)0;
+}
+
+template <typename T>
+__device__ __forceinline__ K1Parent<T> k1_parent(const SplineView<T>& s, const Phys<T>& ph, double r, int knot)
+{
+    K1Parent<T> P;
+    P.r = (T)r;
+    P.lr = s.x[knot];
+    P.r2 = P.r * P.r;
+    P.alpha_r = alpha_of_log(P.lr, ph);
+    P.knot = knot;
+    P.pr = s.coef[4 * (knot < s.n - 1 ? knot : s.n - 2)];
+    if (knot == s.n - 1) {
+        const T* c = s.coef + 4 * (s.n - 2);
+        const T h = s.x[s.n - 1] - s.x[s.n - 2];
+        P.pr = c[0] + h * (c[1] + h * (c[2] + h * c[3]));
+    }
+    const T e = M<T>::exp_fast(P.pr);
+    P.Nr = e < (T)1 ? e : (T)1;
+    P.Sr = P.pr < (T)0 ? -M<T>::expm1(P.pr) : (T)0;
+    return P;
+}
+
+struct K1Consts {
+    K1Rule rule;
+    double sh2[24];  // sin^2(theta_j / 2), theta_j = pi v_j^2
+    double aw[24];   // w_j pi v_j
+};
+
+// TF: arithmetic of the regular intervals (float in the mixed build).
+template <typename TF>
+__global__ void __launch_bounds__(kK1Threads) k1_kernel(Phys<TF> phf, Phys<double> phd, K1Consts consts,
+                                                        const double* __restrict__ r_grid, int n,
+                                                        const double* __restrict__ spline,
+                                                        const int32_t* __restrict__ active,
+                                                        const int32_t* __restrict__ count, double* __restrict__ out)
+{
+    const int slot = blockIdx.x;
+    if (slot >= *count) return;
+    const int knot = active[slot];
+    extern __shared__ __align__(16) unsigned char k1_smem[];
+    double* x64 = reinterpret_cast<double*>(k1_smem);
+    double* c64 = x64 + n;
+    TF* xf = reinterpret_cast<TF*>(c64 + 4 * (n - 1));
+    TF* cf = xf + n;
+    __shared__ double warp_sum[kK1Threads / 32];
+    __shared__ TF sh2f[24], awf[24];
+    const double* src_coef = spline + n;  // log N block
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        x64[i] = spline[i];
+        xf[i] = (TF)spline[i];
+    }
+    for (int i = threadIdx.x; i < 4 * (n - 1); i += blockDim.x) {
+        c64[i] = src_coef[i];
+        cf[i] = (TF)src_coef[i];
+    }
+    if (threadIdx.x < 24) {
+        sh2f[threadIdx.x] = (TF)consts.sh2[threadIdx.x];
+        awf[threadIdx.x] = (TF)consts.aw[threadIdx.x];
+    }
+    __syncthreads();
+    SplineView<double> sd;
+    sd.x = x64; sd.coef = c64; sd.n = n; sd.x0 = x64[0];
+    sd.inv_h = (double)(n - 1) / (x64[n - 1] - x64[0]);
+    SplineView<TF> sf;
+    sf.x = xf; sf.coef = cf; sf.n = n; sf.x0 = xf[0];
+    sf.inv_h = (TF)((double)(n - 1) / (x64[n - 1] - x64[0]));
+    const double r = r_grid[knot];
+    const K1Parent<TF> Pf = k1_parent<TF>(sf, phf, r, knot);
+    const K1Parent<double> Pd = k1_parent<double>(sd, phd, r, knot);
+
+    double total = 0.0;
+    const int nodes = (n - 1) * 8;
+    for (int k = threadIdx.x; k < nodes; k += blockDim.x) {
+        const int iv = k >> 3, m = k & 7;
+        const double center = 0.5 * (x64[iv] + x64[iv + 1]);
+        const double hw = 0.5 * (x64[iv + 1] - x64[iv]);
+        const double lz = center + hw * consts.rule.x8[m];
+        const double rw = hw * consts.rule.w8[m];
+        double node_sum;
+        if (iv == knot - 1 || iv == knot) {
+            // the two intervals adjacent to the parent knot in FP64
+            const K1Z<double> Z = k1_prepare_z<double>(sd, Pd, phd, lz);
+            double acc = 0.0;
+#pragma unroll 4
+            for (int j = 0; j < 24; ++j) acc += k1_point<double>(sd, Pd, Z, phd, consts.sh2[j]) * consts.aw[j];
+            node_sum = acc * (2.0 * Z.z * Z.z) * rw;
+        } else {
+            const K1Z<TF> Z = k1_prepare_z<TF>(sf, Pf, phf, (TF)lz);
+            TF acc = (TF)0;
+#pragma unroll 4
+            for (int j = 0; j < 24; ++j) acc += k1_point<TF>(sf, Pf, Z, phf, sh2f[j]) * awf[j];
+            node_sum = (double)acc * (2.0 * (double)Z.z * (double)Z.z) * rw;
+        }
+        total += node_sum;
+    }
+    // deterministic block reduction
+    for (int o = 16; o > 0; o >>= 1) total += __shfl_down_sync(0xffffffffu, total, o);
+    if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = total;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < kK1Threads / 32; ++w) s += warp_sum[w];
+        out[knot] = s;
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_k1(const nlo_bk_params& p, const double* r, int points, const double* spline,
+                      const int32_t* active, const int32_t* count, double* out, cudaStream_t stream)
+{
+    K1Consts consts;
+    consts.rule = k1_rule();
+    for (int j = 0; j < 24; ++j) {
+        const double v = 0.5 * (consts.rule.x24[j] + 1.0);
+        const double theta = kPi * v * v;
+        const double sh = std::sin(0.5 * theta);
+        consts.sh2[j] = sh * sh;
+        consts.aw[j] = consts.rule.w24[j] * kPi * v;
+    }
+    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(double) * (size_t)points, stream);
+    if (e != cudaSuccess) return e;
+    const Phys<double> phd = make_phys<double>(p);
+    if (p.precision == NLO_PRECISION_FP64) {
+        const size_t smem = (sizeof(double) * 2) * (size_t)(points + 4 * (points - 1));
+        e = cudaFuncSetAttribute(k1_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        k1_kernel<double><<<points, kK1Threads, smem, stream>>>(phd, phd, consts, r, points, spline, active, count,
+                                                                out);
+    } else {
+        const size_t smem = (sizeof(double) + sizeof(float)) * (size_t)(points + 4 * (points - 1));
+        e = cudaFuncSetAttribute(k1_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        k1_kernel<float><<<points, kK1Threads, smem, stream>>>(make_phys<float>(p), phd, consts, r, points, spline,
+                                                               active, count, out);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace nlo

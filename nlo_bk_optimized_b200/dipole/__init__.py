@@ -1,0 +1,5 @@
+"""Dipole tables and the legacy BK text format."""
+
+from nlo_bk_optimized_b200.dipole.table import DipoleTable, load_bk_table, save_bk_table
+
+__all__ = ["DipoleTable", "load_bk_table", "save_bk_table"]

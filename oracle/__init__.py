@@ -1,0 +1,380 @@
+"""CPU FP64 oracle for the NLO BK hot path -- TEST INFRASTRUCTURE ONLY.
+
+This package is the checker: ``tests/``, ``__graft_entry__.smoke()`` and the
+CPU-baseline leg of ``bench.py`` import it to compute reference values on the
+same inputs the CUDA product consumes.  The product package
+``nlo_bk_optimized_b200`` never imports it.
+
+The numerics live in ``nlo_oracle.c`` (a plain-C restatement of the reference
+``torch_nlo_clean/src/nlo_torch`` BK path; see its header for the file:line map).
+This module wraps it with ctypes and adds the Python-level orchestration of
+the reference's evolution driver:
+
+* ``derivative``   -- dN/dY assembly, bk/evolution.py:329-351 and 354-488
+                      (K1 by the fixed rule of custom_kernels/bk/k1/kernel.cu:2040-2092,
+                      K2+Kf by quasi-Monte Carlo on fixed Sobol points)
+* ``evolve``       -- stepping loop bk/evolution.py:85-159 with the Euler
+                      (:110-122), Kutta RK3 (:190-236) or classical RK4 stepper
+* ``r_grid``       -- bk/evolution.py:584-592
+* ``mv_amplitude`` -- bk/initial_conditions.py:29-35
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from oracle import build as _build
+
+_lib = None
+
+
+class Physics(ctypes.Structure):
+    _fields_ = [
+        ("nc", ctypes.c_double),
+        ("nf", ctypes.c_double),
+        ("lambda_qcd", ctypes.c_double),
+        ("c2", ctypes.c_double),
+        ("minr", ctypes.c_double),
+        ("ksub", ctypes.c_double),
+        ("symmetrize", ctypes.c_int),
+        ("fixed_coupling", ctypes.c_int),
+        ("fixed_alpha_s", ctypes.c_double),
+        ("alpha_cap", ctypes.c_double),
+    ]
+
+
+class _Spline(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_int),
+        ("x", ctypes.POINTER(ctypes.c_double)),
+        ("a", ctypes.POINTER(ctypes.c_double)),
+        ("b", ctypes.POINTER(ctypes.c_double)),
+        ("c", ctypes.POINTER(ctypes.c_double)),
+        ("d", ctypes.POINTER(ctypes.c_double)),
+        ("rmin", ctypes.c_double),
+        ("rmax", ctypes.c_double),
+    ]
+
+
+def _dp(array: np.ndarray):
+    return array.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        path = _build.build()
+        handle = ctypes.CDLL(str(path))
+        D, I, P = ctypes.c_double, ctypes.c_int, ctypes.POINTER
+        DP = P(D)
+        handle.or_alpha_s.restype = D
+        handle.or_alpha_s.argtypes = [D, P(Physics)]
+        handle.or_natural_spline.argtypes = [DP, DP, I, DP, DP, DP, DP]
+        handle.or_loglog_knots.argtypes = [DP, I, I, I, DP]
+        handle.or_n_from_nspline.restype = D
+        handle.or_n_from_nspline.argtypes = [P(_Spline), D]
+        handle.or_n_from_sspline.restype = D
+        handle.or_n_from_sspline.argtypes = [P(_Spline), D]
+        handle.or_k1_integrand.restype = D
+        handle.or_k1_integrand.argtypes = [D, D, D, P(_Spline), P(Physics)]
+        handle.or_bessel_i1.restype = D
+        handle.or_bessel_i1.argtypes = [D]
+        handle.or_k1_fixed_many.argtypes = [DP, I, P(_Spline), P(Physics), DP, DP, DP, DP, DP]
+        handle.or_nlo_kernels.argtypes = [D, D, D, D, D, D, D, DP]
+        handle.or_k2kf_integrand.argtypes = [D, DP, P(_Spline), P(Physics), DP]
+        handle.or_k2kf_sums.argtypes = [DP, I, DP, ctypes.c_long, DP, DP, I, P(_Spline), P(Physics), DP]
+        handle.or_sobol.argtypes = [
+            P(ctypes.c_int64), P(ctypes.c_int64), I, ctypes.c_long, ctypes.c_long, I, DP
+        ]
+        handle.or_nlo_kernels_literal_q.argtypes = [D, D, D, D, D, D, D, DP]
+        handle.or_lo_kernel_literal_q.restype = D
+        handle.or_lo_kernel_literal_q.argtypes = [D, D, D, P(Physics)]
+        handle.or_lo_kernel.restype = D
+        handle.or_lo_kernel.argtypes = [D, D, D, P(Physics)]
+        handle.or_k1_dipole.restype = D
+        handle.or_k1_dipole.argtypes = [P(_Spline), D, D, D]
+        handle.or_k1_dipole_literal_q.restype = D
+        handle.or_k1_dipole_literal_q.argtypes = [P(_Spline), D, D, D]
+        handle.or_k2_dipoles.argtypes = [P(_Spline), D, DP, DP, DP]
+        handle.or_num_threads.restype = I
+        _lib = handle
+    return _lib
+
+
+def physics(config) -> Physics:
+    """Physics constants from any object with BKConfig's field names."""
+
+    fixed = getattr(config, "RC_LO", None)
+    fixed_coupling = bool(fixed is not None and getattr(fixed, "name", "") == "FIXED_LO")
+    return Physics(
+        float(config.NC),
+        float(config.NF),
+        float(config.LambdaQCD),
+        float(config.C2),
+        float(config.MINR),
+        float(config.KSUB),
+        int(bool(config.SYMMETRIZE_Z_Z2_INTEGRATION)),
+        int(fixed_coupling),
+        float(config.FIXED_AS),
+        float(getattr(config, "ALPHA_S_CAP", 0.0) or 0.0),
+    )
+
+
+@dataclass
+class Spline:
+    """Natural cubic spline of a log-log table over the r grid."""
+
+    x: np.ndarray
+    a: np.ndarray
+    b: np.ndarray
+    c: np.ndarray
+    d: np.ndarray
+    rmin: float
+    rmax: float
+
+    def struct(self) -> _Spline:
+        s = _Spline()
+        s.n = self.x.size
+        s.x, s.a, s.b, s.c, s.d = (_dp(v) for v in (self.x, self.a, self.b, self.c, self.d))
+        s.rmin, s.rmax = self.rmin, self.rmax
+        self._keep = s
+        return s
+
+
+def r_grid(minr: float, maxr: float, rpoints: int) -> np.ndarray:
+    """bk/evolution.py:584-592, float64 (torch.pow per index, as the reference)."""
+
+    import torch
+
+    rind = torch.arange(rpoints + 1, dtype=torch.float64)
+    step = (maxr / minr) ** (1 / rpoints)
+    return (minr * torch.pow(rind.new_tensor(step), rind)).numpy().copy()
+
+
+def mv_amplitude(r: np.ndarray, qs0sqr: float, ec: float = 1.0, lambdaqcd: float = 0.241,
+                 gamma: float = 1.0) -> np.ndarray:
+    """bk/initial_conditions.py:29-35."""
+
+    exponent = np.power(r * r * qs0sqr, gamma) / 4 * np.log(1 / (r * lambdaqcd) + ec * 2.7182818)
+    return np.where(exponent < 1e-5, exponent, 1 - np.exp(-exponent))
+
+
+def loglog_spline(r: np.ndarray, N: np.ndarray, kind: int, force_positive: bool = True) -> Spline:
+    """kind 0: log N spline (K1); kind 1: log S spline (K2+Kf)."""
+
+    r = np.ascontiguousarray(r, dtype=np.float64)
+    N = np.ascontiguousarray(N, dtype=np.float64)
+    n = r.size
+    x = np.log(r)
+    y = np.empty(n)
+    lib().or_loglog_knots(_dp(N), n, kind, int(force_positive), _dp(y))
+    a, b, c, d = (np.empty(n - 1) for _ in range(4))
+    lib().or_natural_spline(_dp(x), _dp(y), n, _dp(a), _dp(b), _dp(c), _dp(d))
+    return Spline(x, a, b, c, d, float(r[0]), float(r[-1]))
+
+
+def natural_spline(x: np.ndarray, y: np.ndarray):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    n = x.size
+    a, b, c, d = (np.empty(n - 1) for _ in range(4))
+    lib().or_natural_spline(_dp(x), _dp(y), n, _dp(a), _dp(b), _dp(c), _dp(d))
+    return a, b, c, d
+
+
+def gauss_legendre(order: int) -> tuple[np.ndarray, np.ndarray]:
+    x, w = np.polynomial.legendre.leggauss(order)
+    return np.ascontiguousarray(x), np.ascontiguousarray(w)
+
+
+def k1_fixed(rpar: np.ndarray, nspline: Spline, phys: Physics) -> np.ndarray:
+    rpar = np.ascontiguousarray(rpar, dtype=np.float64)
+    x8, w8 = gauss_legendre(8)
+    x24, w24 = gauss_legendre(24)
+    out = np.empty(rpar.size)
+    lib().or_k1_fixed_many(_dp(rpar), rpar.size, ctypes.byref(nspline.struct()), ctypes.byref(phys),
+                           _dp(x8), _dp(w8), _dp(x24), _dp(w24), _dp(out))
+    return out
+
+
+def k1_integrand(r: float, z: float, theta: float, nspline: Spline, phys: Physics) -> float:
+    return lib().or_k1_integrand(r, z, theta, ctypes.byref(nspline.struct()), ctypes.byref(phys))
+
+
+def k2kf_integrand(r: float, x: np.ndarray, sspline: Spline, phys: Physics) -> tuple[float, float]:
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    out = np.empty(2)
+    lib().or_k2kf_integrand(r, _dp(x), ctypes.byref(sspline.struct()), ctypes.byref(phys), _dp(out))
+    return float(out[0]), float(out[1])
+
+
+def k2kf_sums(rpar: np.ndarray, points: np.ndarray, lower: np.ndarray, width: np.ndarray, map_f32: bool,
+              sspline: Spline, phys: Physics) -> np.ndarray:
+    """Per-parent [sum K2 w, sum Kf w, sum (K2+Kf)^2 w^2] over unit-cube points [n,4]."""
+
+    rpar = np.ascontiguousarray(rpar, dtype=np.float64)
+    points = np.ascontiguousarray(points, dtype=np.float64)
+    lower = np.ascontiguousarray(lower, dtype=np.float64)
+    width = np.ascontiguousarray(width, dtype=np.float64)
+    out = np.empty((rpar.size, 3))
+    lib().or_k2kf_sums(_dp(rpar), rpar.size, _dp(points), points.shape[0], _dp(lower), _dp(width),
+                       int(map_f32), ctypes.byref(sspline.struct()), ctypes.byref(phys), _dp(out))
+    return out
+
+
+def sobol(state: np.ndarray, shift: np.ndarray, offset: int, n: int, as_f32: bool) -> np.ndarray:
+    state = np.ascontiguousarray(state, dtype=np.int64)
+    shift = np.ascontiguousarray(shift, dtype=np.int64)
+    dims = shift.size
+    out = np.empty((n, dims))
+    lib().or_sobol(state.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                   shift.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), dims, offset, n, int(as_f32),
+                   _dp(out))
+    return out
+
+
+def sobol_state(dims: int, seed: int) -> tuple[np.ndarray, np.ndarray]:
+    """Scrambled direction numbers and shift of SobolEngine(dims, scramble=True, seed)."""
+
+    import torch
+
+    engine = torch.quasirandom.SobolEngine(dims, scramble=True, seed=seed)
+    return engine.sobolstate.numpy().copy(), engine.shift.numpy().copy()
+
+
+def nlo_kernels(r, lz, lz2, th, th2, nf=3.0, nc=3.0) -> np.ndarray:
+    out = np.empty(3)
+    lib().or_nlo_kernels(r, lz, lz2, th, th2, nf, nc, _dp(out))
+    return out
+
+
+def nlo_kernels_literal_quad(r, lz, lz2, th, th2, nf=3.0, nc=3.0) -> np.ndarray:
+    out = np.empty(3)
+    lib().or_nlo_kernels_literal_q(r, lz, lz2, th, th2, nf, nc, _dp(out))
+    return out
+
+
+def lo_kernel(r, z, theta, phys: Physics) -> float:
+    return lib().or_lo_kernel(r, z, theta, ctypes.byref(phys))
+
+
+def lo_kernel_literal_quad(r, z, theta, phys: Physics) -> float:
+    return lib().or_lo_kernel_literal_q(r, z, theta, ctypes.byref(phys))
+
+
+def k1_dipole(nspline: Spline, r: float, z: float, theta: float) -> tuple[float, float]:
+    """(stable FP64, quad literal) K1 dipole factor."""
+
+    st = nspline.struct()
+    return (lib().or_k1_dipole(ctypes.byref(st), r, z, theta),
+            lib().or_k1_dipole_literal_q(ctypes.byref(st), r, z, theta))
+
+
+def k2_dipoles(sspline: Spline, r: float, x: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """(stable FP64, quad literal) [dipole, dipole_swap, fermion factor] of the K2+Kf integrand."""
+
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    out, out_q = np.empty(3), np.empty(3)
+    lib().or_k2_dipoles(ctypes.byref(sspline.struct()), r, _dp(x), _dp(out), _dp(out_q))
+    return out, out_q
+
+
+def bessel_i1(x: float) -> float:
+    return lib().or_bessel_i1(x)
+
+
+def alpha_s(r: float, phys: Physics) -> float:
+    return lib().or_alpha_s(r, ctypes.byref(phys))
+
+
+def num_threads() -> int:
+    return lib().or_num_threads()
+
+
+def nlo_box(r: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """bk/derivatives.py:424-431: [log(r0/2), log(2 r_max)]^2 x [0, 2 pi]^2 as (lower, width)."""
+
+    lo = math.log(0.5 * r[0])
+    hi = math.log(2 * r[-1])
+    lower = np.array([lo, lo, 0.0, 0.0])
+    width = np.array([hi - lo, hi - lo, 2 * math.pi, 2 * math.pi])
+    return lower, width
+
+
+@dataclass
+class Derivative:
+    dNdy: np.ndarray
+    K1: np.ndarray
+    K2: np.ndarray
+    Kf: np.ndarray
+    sq: np.ndarray
+
+
+def derivative(N: np.ndarray, r: np.ndarray, phys: Physics, points: np.ndarray, map_f32: bool,
+               force_positive: bool = True) -> Derivative:
+    """dN/dY = K1 + (K2+Kf) at active parents (index > 0 and N <= 0.99999), else 0;
+    non-finite values become 0 (bk/evolution.py:329-351, 501)."""
+
+    nspl = loglog_spline(r, N, 0, force_positive)
+    sspl = loglog_spline(r, N, 1, force_positive)
+    active = np.nonzero((np.arange(r.size) > 0) & (N <= 0.99999))[0]
+    K1 = np.zeros_like(N)
+    K2 = np.zeros_like(N)
+    Kf = np.zeros_like(N)
+    sq = np.zeros_like(N)
+    if active.size:
+        K1[active] = k1_fixed(r[active], nspl, phys)
+        lower, width = nlo_box(r)
+        sums = k2kf_sums(r[active], points, lower, width, map_f32, sspl, phys)
+        n = points.shape[0]
+        K2[active] = sums[:, 0] / n
+        Kf[active] = sums[:, 1] / n
+        sq[active] = sums[:, 2]
+    dNdy = K1 + K2 + Kf
+    dNdy = np.where(np.isfinite(dNdy), dNdy, 0.0)
+    return Derivative(dNdy, K1, K2, Kf, sq)
+
+
+def evolve(N0: np.ndarray, r: np.ndarray, phys: Physics, points: np.ndarray, map_f32: bool, step: float,
+           maxy: float, stepper: str = "rk4", force_positive: bool = True):
+    """Rapidity stepping (bk/evolution.py:85-159); returns (y[steps+1], N[steps+1, R])."""
+
+    ys = [0.0]
+    Ns = [np.array(N0, dtype=np.float64)]
+    N = Ns[0].copy()
+    y = 0.0
+
+    def f(state):
+        return derivative(state, r, phys, points, map_f32, force_positive).dNdy
+
+    while True:
+        h = step
+        if stepper == "euler":
+            N = N + h * f(N)
+        elif stepper == "rk3":
+            k1 = f(N)
+            k2 = f(N + 0.5 * h * k1)
+            k3 = f(N + h * (-k1 + 2.0 * k2))
+            N = N + h * (k1 + 4.0 * k2 + k3) / 6.0
+        elif stepper == "rk4":
+            k1 = f(N)
+            k2 = f(N + 0.5 * h * k1)
+            k3 = f(N + 0.5 * h * k2)
+            k4 = f(N + h * k3)
+            N = N + h * (k1 + 2.0 * k2 + 2.0 * k3 + k4) / 6.0
+        else:
+            raise ValueError(stepper)
+        y = y + step
+        if force_positive:
+            N = np.clip(N, 0.0, 1.0)
+        if not np.all(np.isfinite(N)):
+            raise FloatingPointError(f"non-finite BK amplitude after rapidity step y={y}")
+        ys.append(y)
+        Ns.append(N.copy())
+        if y >= maxy - 1e-12 * max(1.0, abs(maxy), abs(step)):
+            break
+    return np.array(ys), np.stack(Ns)

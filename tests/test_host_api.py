@@ -1,0 +1,134 @@
+"""Host-side behaviour that needs no GPU: configuration, table I/O, stepping
+counts, initial conditions, and the C-ABI library's exports."""
+
+from __future__ import annotations
+
+import ctypes
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+from golden_data import bk_table_mc50w
+from nlo_bk_optimized_b200 import _native
+from nlo_bk_optimized_b200.bk.config import BKConfig, IntegrationMethod, RunningCouplingLO, device_supported
+from nlo_bk_optimized_b200.bk.evolution import _r_grid, _steps_to, nlo_box, solve_bk
+from nlo_bk_optimized_b200.bk.initial_conditions import MV, ICDataFile
+from nlo_bk_optimized_b200.dipole.table import DipoleTable, load_bk_table, save_bk_table
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def test_config_defaults_and_validation():
+    config = BKConfig()
+    assert config.NC == 3.0 and config.NF == 3 and config.RPOINTS == 100
+    assert config.INTMETHOD_NLO is IntegrationMethod.SOBOL
+    assert config.stepper == "rk4"
+    assert BKConfig(EULER_METHOD=True).stepper == "euler"
+    with pytest.raises(ValueError):
+        BKConfig(NF=4)
+    with pytest.raises(ValueError):
+        BKConfig(MINR=1.0, MAXR=0.5)
+    with pytest.raises(ValueError):
+        BKConfig(RC_LO=RunningCouplingLO.FIXED_LO)  # needs FIXED_NLO too (bk/config.py:119-122)
+    with pytest.raises(ValueError):
+        BKConfig(STEPPER="rk45")
+    with pytest.raises(ValueError):
+        BKConfig(KINEMATICAL_CONSTRAINT=True)
+    assert device_supported(config) is None
+    assert "VEGAS" not in (device_supported(BKConfig(INTMETHOD_NLO=IntegrationMethod.VEGAS)) or "VEGAS")
+
+
+def test_r_grid_matches_reference_construction():
+    config = BKConfig(RPOINTS=399, MINR=1e-7, MAXR=1e2)
+    r = _r_grid(config, device="cpu", dtype=torch.float64)
+    assert r.numel() == 400
+    assert r[0].item() == pytest.approx(1e-7, rel=1e-15)
+    assert r[-1].item() == pytest.approx(1e2, rel=1e-12)
+    lower, width = nlo_box(float(r[0]), float(r[-1]))
+    assert lower[0] == pytest.approx(np.log(0.5e-7))
+    assert lower[0] + width[0] == pytest.approx(np.log(200.0))
+    assert width[2] == pytest.approx(2 * np.pi)
+
+
+def test_step_count_follows_reference_accumulation():
+    ys = _steps_to(0.0, 10.0, 0.1)
+    assert len(ys) == 100
+    assert ys[-1] == pytest.approx(10.0)
+    assert len(_steps_to(0.0, 4.0, 0.2)) == 20
+    assert len(_steps_to(0.0, 0.0, 0.2)) == 1  # the reference always takes one step
+
+
+def test_cpu_device_is_rejected_without_fallback():
+    with pytest.raises((ValueError, RuntimeError)):
+        solve_bk(MV(qs0sqr=0.2), 0.2, BKConfig(RPOINTS=10), device="cpu")
+
+
+def test_table_round_trip_and_legacy_format(tmp_path):
+    golden = bk_table_mc50w()
+    r = torch.tensor(golden["r"])
+    table = DipoleTable(r=r, y=torch.tensor(golden["y"]), N=torch.tensor(golden["N"]), x0=float(golden["x0"][0]))
+    path = tmp_path / "table.dat"
+    save_bk_table(path, table)
+    loaded = load_bk_table(path)
+    torch.testing.assert_close(loaded.r, table.r, rtol=1e-14, atol=0)
+    torch.testing.assert_close(loaded.y, table.y, rtol=0, atol=1e-15)
+    torch.testing.assert_close(loaded.N, table.N, rtol=1e-14, atol=1e-300)
+    assert loaded.x0 == table.x0
+    # the C++ table: 101 r points from 1e-5, multiplier 1.16083692085089, x0 = 0.01
+    assert r.numel() == 101 and r[0].item() == pytest.approx(1e-5)
+    assert float(golden["x0"][0]) == pytest.approx(0.01)
+
+
+def test_table_validation():
+    r = torch.logspace(-3, 1, 8, dtype=torch.float64)
+    with pytest.raises(ValueError):
+        DipoleTable(r=r, y=torch.zeros(1, dtype=torch.float64), N=torch.zeros((2, 8), dtype=torch.float64), x0=0.01)
+    with pytest.raises(ValueError):
+        DipoleTable(r=r.flip(0), y=torch.zeros(1, dtype=torch.float64), N=torch.zeros((1, 8), dtype=torch.float64),
+                    x0=0.01)
+
+
+def test_initial_conditions(tmp_path):
+    r = torch.logspace(-7, 2, 50, dtype=torch.float64)
+    mv = MV(qs0sqr=0.2).dipole_amplitude(r)
+    assert bool(((mv >= 0) & (mv <= 1)).all())
+    head = bk_table_mc50w()["ic_head"]
+    path = tmp_path / "ic.dat"
+    np.savetxt(path, head)
+    ic = ICDataFile(path, x0=0.01)
+    torch.testing.assert_close(ic.dipole_amplitude(ic.r), ic.N, rtol=1e-12, atol=1e-30)
+    assert ic.dipole_amplitude(torch.tensor([1e-12], dtype=torch.float64)).item() == 0.0
+    assert ic.dipole_amplitude(torch.tensor([1e6], dtype=torch.float64)).item() == 1.0
+    short = tmp_path / "short.dat"
+    np.savetxt(short, head[:5])
+    with pytest.raises(ValueError):
+        ICDataFile(short)
+
+
+def test_library_exports_every_declared_symbol():
+    header = (ROOT / "include" / "nlo_b200.h").read_text()
+    declared = set(re.findall(r"^\s*(?:const\s+)?\w+\*?\s+\*?(nlo_\w+)\(", header, flags=re.M))
+    assert declared, "no declarations parsed"
+    lib = ctypes.CDLL(str(_native.LIBRARY_PATH))
+    missing = [name for name in sorted(declared) if not hasattr(lib, name)]
+    assert not missing, missing
+    assert set(_native.EXPORTED) <= declared
+
+
+def test_library_rejects_bad_arguments_without_a_gpu():
+    lib = _native.load()
+    assert lib.nlo_abi_version() == 1
+    dirs = _native.sobol_dirs(4, 0)
+    # invalid precision and NULL buffers are rejected on the host before any launch
+    assert lib.nlo_sobol_draw(dirs, 0, 16, 7, None, None) == 1
+    assert lib.nlo_bk_splines(None, None, 2, 1, None, None) == 1
+    assert b"spline" in lib.nlo_last_error()
+    params = _native.BKParams()
+    params.nc, params.nf, params.lambda_qcd, params.c2, params.ksub = 3.0, 4.0, 0.241, 1.0, 0.65
+    assert lib.nlo_bk_k1(params, None, 10, None, None, None, None, None) == 1
+    assert b"NF" in lib.nlo_last_error()
+    assert lib.nlo_bk_k2kf_workspace_bytes(400) > 0
+    assert lib.nlo_bk_spline_doubles(400) == 400 + 8 * 399

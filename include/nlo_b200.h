@@ -84,7 +84,8 @@ int nlo_sobol_draw(const nlo_sobol_dirs* dirs, int64_t offset, int64_t n, int32_
 
 /* Spline buffer size in doubles for a grid of `points` knots:
  * x[points] (log r) followed by the log N and log S coefficient blocks,
- * each [points-1][4] (a, b, c, d). */
+ * each [points-1][4] (a, b, c, d), then 2*points doubles of scratch for the
+ * tridiagonal factorisation. */
 size_t nlo_bk_spline_doubles(int32_t points);
 
 /* Natural-cubic log N and log S splines of an amplitude row (FP64).

@@ -95,23 +95,24 @@ SobolDirsArg to_arg(const nlo_sobol_dirs* d)
 size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
 
 // Workspace layout of one right-hand-side evaluation.
-size_t rhs_bytes(int points, size_t* offsets /*[6] or NULL*/)
+size_t rhs_bytes(int points, size_t* offsets /*[7] or NULL*/)
 {
     size_t o = 0;
-    size_t off[6];
+    size_t off[7];
     off[0] = o; o = align_up(o + sizeof(double) * spline_doubles(points));
     off[1] = o; o = align_up(o + sizeof(int32_t) * (size_t)points);
     off[2] = o; o = align_up(o + sizeof(int32_t) * 4);
     off[3] = o; o = align_up(o + sizeof(double) * (size_t)points);
     off[4] = o; o = align_up(o + sizeof(double) * 3 * (size_t)points);
     off[5] = o; o = align_up(o + sizeof(double) * 3 * (size_t)points * (size_t)k2kf_max_blocks());
+    off[6] = o; o = align_up(o + sizeof(double) * 2 * (size_t)points);
     if (offsets) std::memcpy(offsets, off, sizeof(off));
     return o;
 }
 
 RhsBuffers carve(void* ws, int points)
 {
-    size_t off[6];
+    size_t off[7];
     rhs_bytes(points, off);
     char* base = static_cast<char*>(ws);
     RhsBuffers b;
@@ -121,16 +122,18 @@ RhsBuffers carve(void* ws, int points)
     b.k1 = reinterpret_cast<double*>(base + off[3]);
     b.k2kf = reinterpret_cast<double*>(base + off[4]);
     b.partial = reinterpret_cast<double*>(base + off[5]);
+    b.factor = reinterpret_cast<double*>(base + off[6]);
     b.k2kf_blocks = k2kf_max_blocks();
     return b;
 }
 
 int run_rhs(const nlo_bk_params& p, const double* r, const double* N, int points, const SobolDirsArg& dirs,
             uint64_t samples, const nlo_bk_box& box, double* dndy, double* k1_out, double* k2kf_out,
-            const RhsBuffers& b, cudaStream_t stream)
+            const RhsBuffers& b, bool factor_ready, cudaStream_t stream)
 {
     cudaError_t e;
-    if ((e = launch_splines(r, N, points, p.force_positive, b.spline, stream)) != cudaSuccess)
+    if ((e = launch_splines(r, N, points, p.force_positive, b.factor, factor_ready ? 0 : 1, b.spline, stream)) !=
+        cudaSuccess)
         return cuda_fail(e, "splines");
     if ((e = launch_active(N, points, b.active, b.count, stream)) != cudaSuccess) return cuda_fail(e, "active");
     if ((e = launch_k1(p, r, points, b.spline, b.active, b.count, b.k1, stream)) != cudaSuccess)
@@ -164,6 +167,9 @@ const K1Rule& k1_rule()
 
 size_t spline_doubles(int points) { return (size_t)points + 8 * (size_t)(points - 1); }
 
+// buffer size a caller provides to nlo_bk_splines: coefficients plus factorisation scratch
+size_t spline_buffer_doubles(int points) { return spline_doubles(points) + 2 * (size_t)points; }
+
 int k2kf_max_blocks()
 {
     static int blocks = [] {
@@ -196,13 +202,15 @@ int nlo_sobol_draw(const nlo_sobol_dirs* dirs, int64_t offset, int64_t n, int32_
     return e == cudaSuccess ? NLO_OK : cuda_fail(e, "sobol");
 }
 
-size_t nlo_bk_spline_doubles(int32_t points) { return points >= 2 ? spline_doubles(points) : 0; }
+size_t nlo_bk_spline_doubles(int32_t points) { return points >= 2 ? spline_buffer_doubles(points) : 0; }
 
 int nlo_bk_splines(const double* r, const double* N, int32_t points, int32_t force_positive, double* spline, void* stream)
 {
     if (points < 3 || points > 4096) return fail(NLO_ERR_INVALID, "a cubic spline requires 3..4096 points");
     if (!r || !N || !spline) return fail(NLO_ERR_INVALID, "NULL buffer");
-    cudaError_t e = launch_splines(r, N, points, force_positive, spline, (cudaStream_t)stream);
+    // the factorisation scratch is the tail of the caller's spline buffer (nlo_bk_spline_doubles)
+    double* factor = spline + spline_doubles(points);
+    cudaError_t e = launch_splines(r, N, points, force_positive, factor, 1, spline, (cudaStream_t)stream);
     return e == cudaSuccess ? NLO_OK : cuda_fail(e, "splines");
 }
 
@@ -271,7 +279,7 @@ int nlo_bk_rhs(const nlo_bk_params* params, const double* r, const double* N, in
     if (!workspace || workspace_bytes < nlo_bk_rhs_workspace_bytes(points))
         return fail(NLO_ERR_WORKSPACE, "workspace too small for nlo_bk_rhs");
     const RhsBuffers b = carve(workspace, points);
-    return run_rhs(*params, r, N, points, to_arg(dirs), (uint64_t)samples, *box, dndy, k1, k2kf, b,
+    return run_rhs(*params, r, N, points, to_arg(dirs), (uint64_t)samples, *box, dndy, k1, k2kf, b, false,
                    (cudaStream_t)stream);
 }
 
@@ -304,8 +312,13 @@ int nlo_bk_evolve(const nlo_bk_params* params, const double* r, int32_t points, 
         const double* N = table + (size_t)it * points;
         double* next = table + (size_t)(it + 1) * points;
         int rc;
+        // the spline factorisation depends on the grid only: form it on the first stage
+        bool factor_ready = it > 0;
         auto f = [&](const double* in, double* out) {
-            return run_rhs(*params, r, in, points, dirs_arg, (uint64_t)samples, *box, out, nullptr, nullptr, b, s);
+            const int code = run_rhs(*params, r, in, points, dirs_arg, (uint64_t)samples, *box, out, nullptr,
+                                     nullptr, b, factor_ready, s);
+            factor_ready = true;
+            return code;
         };
         if (stepper == NLO_STEPPER_EULER) {
             if ((rc = f(N, kk[0])) != NLO_OK) return rc;

@@ -39,7 +39,7 @@ struct M<float> {
     static __device__ __forceinline__ float exp_acc(float x) { return expf(x); }
     static __device__ __forceinline__ float expm1(float x) { return expm1f(x); }
     static __device__ __forceinline__ float log1p(float x) { return log1pf(x); }
-    static __device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
+    static __device__ __forceinline__ float rcp(float x) { return __fdividef(1.0f, x); }
     static __device__ __forceinline__ float div(float a, float b) { return __fdividef(a, b); }
     static __device__ __forceinline__ float sqrt(float x) { return sqrtf(x); }
     static __device__ __forceinline__ float sin(float x) { return sinf(x); }
@@ -205,6 +205,41 @@ __device__ __forceinline__ T ndiff_s(const NS<T>& A, const NS<T>& B)
 {
     if (A.edge == 0 && B.edge == 0) return A.S * M<T>::expm1(B.p - A.p);
     if (A.N < (T)0.5 && B.N < (T)0.5) return A.N - B.N;
+    return B.S - A.S;
+}
+
+// Per-evaluation variant without N: p and S only; N = -expm1(p) is formed in
+// ndiff_ps only when one side is clamped to an edge value.
+template <typename T>
+struct PS {
+    T p, S;
+    int edge;
+};
+
+template <typename T>
+__device__ __forceinline__ PS<T> eval_s_ps(const SplineView<T>& s, T log_r)
+{
+    PS<T> v;
+    if (log_r < s.x[0]) { v.p = (T)0; v.S = (T)1; v.edge = -1; return v; }
+    if (log_r > s.x[s.n - 1]) { v.p = (T)0; v.S = (T)0; v.edge = 1; return v; }
+    v.edge = 0;
+    v.p = spline_poly(s, log_r);
+    v.S = M<T>::exp_fast(v.p);
+    return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T n_of(const PS<T>& v)
+{
+    return v.edge < 0 ? (T)0 : (v.edge > 0 ? (T)1 : -M<T>::expm1(v.p));
+}
+
+template <typename T>
+__device__ __forceinline__ T ndiff_ps(const PS<T>& A, const PS<T>& B)
+{
+    if (A.edge == 0 && B.edge == 0) return A.S * M<T>::expm1(B.p - A.p);
+    const T NA = n_of(A), NB = n_of(B);
+    if (NA < (T)0.5 && NB < (T)0.5) return NA - NB;
     return B.S - A.S;
 }
 

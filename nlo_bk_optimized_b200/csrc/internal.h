@@ -32,14 +32,15 @@ struct RhsBuffers {
     double* k1;       // [points]
     double* k2kf;     // [points][3]
     double* partial;  // [k2kf_blocks][points][3]
+    double* factor;   // [2][points] spline factorisation (grid only)
     int k2kf_blocks;
 };
 
 size_t spline_doubles(int points);
 int k2kf_max_blocks();
 
-cudaError_t launch_splines(const double* r, const double* N, int n, int force_positive, double* out,
-                           cudaStream_t stream);
+cudaError_t launch_splines(const double* r, const double* N, int n, int force_positive, double* factor,
+                           int compute_factor, double* out, cudaStream_t stream);
 cudaError_t launch_active(const double* N, int n, int32_t* active, int32_t* count, cudaStream_t stream);
 cudaError_t launch_sobol(const SobolDirsArg& dirs, uint64_t offset, uint64_t n, int precision, void* out,
                          cudaStream_t stream);

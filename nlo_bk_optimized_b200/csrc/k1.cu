@@ -11,20 +11,32 @@
 // the two intervals adjacent to the parent knot (z -> x, where X -> 0 and the
 // dipole N_Y - N_r cancels), which run in FP64.
 
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include "common.cuh"
 #include "internal.h"
+
+namespace cg = cooperative_groups;
 
 namespace nlo {
 
 namespace {
 
 constexpr int kK1Threads = 256;
+// Each parent's interval range is split over a cluster of CTAs; their partial
+// sums are combined through distributed shared memory in rank order.
+constexpr int kK1Split = 4;
 
+// Log coordinates inside the kernel are measured from the parent knot: the spline
+// knots are stored as x_j - log r (formed in FP64), and every distance enters as
+// log(d/r).  In FP32 this keeps full relative precision of the amplitudes even where
+// |log r| ~ 16, whose absolute FP32 spacing (2e-6) would otherwise become a 2e-6
+// relative error of N.
 template <typename T>
 struct K1Parent {
-    T r, lr, r2;
+    T r, r2;
+    T lr_abs;      // log r (absolute), for the coupling
     T alpha_r;
     T Nr, Sr, pr;  // amplitude at the knot and its log value
     int knot;
@@ -48,26 +60,40 @@ __device__ __forceinline__ void k1_amplitude(const SplineView<T>& s, const K1Par
 // Per radial node (r-dependent but theta-independent) data.
 template <typename T>
 struct K1Z {
-    T z, lz, Ysq;
+    T z, Ysq, inv_Ysq;
+    T rho;        // z / r
+    T dY;         // log(z / r)
     T NY, DY;
     T alpha_Y;
-    T right_Y;  // (log_sc - 2 log z) / 0.2
-    T ly_minus_lr;
+    T sigma, sigma_c;  // e^t/(e^c + e^t) and e^c/(e^c + e^t) at t = (log_sc - 2 log z)/0.2
 };
 
+// dlz = log z - log r (formed in FP64 by the caller), lz_abs = log z.
 template <typename T>
 __device__ __forceinline__ K1Z<T> k1_prepare_z(const SplineView<T>& s, const K1Parent<T>& P, const Phys<T>& ph,
-                                              T lz)
+                                              double dlz, double lz_abs)
 {
     K1Z<T> Z;
-    Z.lz = lz;
-    Z.z = M<T>::exp_acc(lz);
+    Z.dY = (T)dlz;
+    Z.z = (T)::exp(lz_abs);
+    Z.rho = (T)::exp(dlz);
     Z.Ysq = Z.z * Z.z;
-    k1_amplitude(s, P, lz, Z.NY, Z.DY);
-    Z.alpha_Y = alpha_of_log(lz, ph);
-    Z.right_Y = (ph.log_sc - (T)2 * lz) * (T)5;
-    Z.ly_minus_lr = lz - P.lr;
+    Z.inv_Ysq = M<T>::rcp(Z.Ysq);
+    k1_amplitude(s, P, Z.dY, Z.NY, Z.DY);
+    Z.alpha_Y = alpha_of_log((T)lz_abs, ph);
+    const T right_Y = (ph.log_sc - (T)2 * (T)lz_abs) * (T)5;
+    Z.sigma = M<T>::rcp((T)1 + M<T>::exp_fast(ph.left - right_Y));
+    Z.sigma_c = M<T>::rcp((T)1 + M<T>::exp_fast(right_Y - ph.left));
     return Z;
+}
+
+// logaddexp(c, t + delta) - logaddexp(c, t) with the sigmoids of t precomputed.
+template <typename T>
+__device__ __forceinline__ T lae_shift(const K1Z<T>& Z, T delta)
+{
+    const T v = Z.sigma * M<T>::expm1(delta);
+    if (v > (T)-0.5) return M<T>::log1p(v);
+    return M<T>::log_acc(Z.sigma_c + Z.sigma * M<T>::exp_fast(delta));
 }
 
 // Kernel_lo x dipole at one (z, theta) node; sh2 = sin^2(theta/2).
@@ -78,9 +104,10 @@ __device__ __forceinline__ T k1_point(const SplineView<T>& s, const K1Parent<T>&
     const T r = P.r, z = Z.z;
     const T Xsq = (r - z) * (r - z) + (T)4 * r * z * sh2;
     if (!(Xsq >= M<T>::tiny_square())) return (T)0;
-    const T lXsq = M<T>::log_fast(Xsq);
-    const T lX = (T)0.5 * lXsq;
-    const T alpha_X = alpha_of_log(lX, ph);
+    // log(X/r) from (X/r)^2 = (1 - z/r)^2 + 4 (z/r) sin^2(theta/2)
+    const T xr2 = ((T)1 - Z.rho) * ((T)1 - Z.rho) + (T)4 * Z.rho * sh2;
+    const T dX = (T)0.5 * M<T>::log_fast(xr2);
+    const T alpha_X = alpha_of_log(P.lr_abs + dX, ph);
     // X^2 - Y^2 = r (r - 2 z cos theta), cos theta = 1 - 2 sin^2(theta/2)
     const T XmY = r * (r - (T)2 * z * ((T)1 - (T)2 * sh2));
     T dalpha;
@@ -90,8 +117,8 @@ __device__ __forceinline__ T k1_point(const SplineView<T>& s, const K1Parent<T>&
         dalpha = Z.alpha_Y - alpha_X;
     } else {
         // alpha_Y - alpha_X = alpha_X alpha_Y b0 c (lae_X - lae_Y)
-        const T delta = -(T)5 * M<T>::log1p(M<T>::div(XmY, Z.Ysq));
-        dalpha = alpha_X * Z.alpha_Y * ph.b0c * lae_difference(ph.left, Z.right_Y, delta);
+        const T delta = -(T)5 * M<T>::log1p(XmY * Z.inv_Ysq);
+        dalpha = alpha_X * Z.alpha_Y * ph.b0c * lae_shift(Z, delta);
     }
     // r^2/(X^2Y^2) + (aY/aX - 1)/Y^2 + (aX/aY - 1)/X^2
     const T inv_XY = M<T>::rcp(Xsq * Z.Ysq);
@@ -100,9 +127,9 @@ __device__ __forceinline__ T k1_point(const SplineView<T>& s, const K1Parent<T>&
     T lo = pref * P.alpha_r * bracket;
     if (!M<T>::finite(lo)) lo = (T)0;
     // double-log resummation (k1.py:109-119), alpha at the smallest size (RESUM_RC_SMALLEST)
-    const T lmin = M<T>::fmin(M<T>::fmin(lX, Z.lz), P.lr);
-    const T alpha_min = alpha_of_log(lmin, ph);
-    const T xarg = (T)4 * (lX - P.lr) * Z.ly_minus_lr;
+    // alpha at min(X, Y, r): reuse alpha_X, alpha_Y or alpha_r
+    const T alpha_min = (dX <= Z.dY && dX <= (T)0) ? alpha_X : (Z.dY <= (T)0 ? Z.alpha_Y : P.alpha_r);
+    const T xarg = (T)4 * dX * Z.dY;
     const T abar = alpha_min * ph.nc * (T)(1.0 / kPi);
     const T as_x = M<T>::sqrt(abar * M<T>::fabs(xarg));
     T dlog = (T)1;
@@ -113,15 +140,15 @@ __device__ __forceinline__ T k1_point(const SplineView<T>& s, const K1Parent<T>&
     if (!(r > (T)1.01 * ph.minr)) dlog = (T)1;
     if (!M<T>::finite(dlog)) return (T)0;
     // single-log resummation (k1.py:121-132): exp(-abar A1 |log(ksub (r/minxy)^2)|)
-    const T lminxy = M<T>::fmin(lX, Z.lz);
-    const T slog_exp = -abar * (T)(11.0 / 12.0) * M<T>::fabs(ph.log_ksub + (T)2 * (P.lr - lminxy));
+    const T dminxy = M<T>::fmin(dX, Z.dY);
+    const T slog_exp = -abar * (T)(11.0 / 12.0) * M<T>::fabs(ph.log_ksub - (T)2 * dminxy);
     const T slog = M<T>::exp_fast(slog_exp);
     const T lo_single = pref * P.alpha_r * P.r2 * inv_XY;
     const T k1fin = lo * P.alpha_r * ph.nc * (T)(1.0 / (4.0 * kPi)) *
                     ((T)(67.0 / 9.0 - kPi * kPi / 3.0) - (T)(10.0 / 9.0) * ph.nf_over_nc);
     // dipole N_X + N_Y - N_r - N_X N_Y = S_r (N_Y + D_X) - D_X D_Y  (or with X and Y exchanged)
     T NX, DX;
-    k1_amplitude(s, P, lX, NX, DX);
+    k1_amplitude(s, P, dX, NX, DX);
     const T base = Z.NY <= NX ? Z.NY + DX : NX + Z.DY;
     const T dipole = P.Sr * base - DX * Z.DY;
     const T result = (dlog * slog * lo - lo_single * slog_exp + k1fin) * dipole;
@@ -133,9 +160,9 @@ __device__ __forceinline__ K1Parent<T> k1_parent(const SplineView<T>& s, const P
 {
     K1Parent<T> P;
     P.r = (T)r;
-    P.lr = s.x[knot];
+    P.lr_abs = (T)::log(r);
     P.r2 = P.r * P.r;
-    P.alpha_r = alpha_of_log(P.lr, ph);
+    P.alpha_r = alpha_of_log(P.lr_abs, ph);
     P.knot = knot;
     P.pr = s.coef[4 * (knot < s.n - 1 ? knot : s.n - 2)];
     if (knot == s.n - 1) {
@@ -157,7 +184,8 @@ struct K1Consts {
 
 // TF: arithmetic of the regular intervals (float in the mixed build).
 template <typename TF>
-__global__ void __launch_bounds__(kK1Threads) k1_kernel(Phys<TF> phf, Phys<double> phd, K1Consts consts,
+__global__ void __cluster_dims__(1, kK1Split, 1) __launch_bounds__(kK1Threads)
+    k1_kernel(Phys<TF> phf, Phys<double> phd, K1Consts consts,
                                                         const double* __restrict__ r_grid, int n,
                                                         const double* __restrict__ spline,
                                                         const int32_t* __restrict__ active,
@@ -174,9 +202,10 @@ __global__ void __launch_bounds__(kK1Threads) k1_kernel(Phys<TF> phf, Phys<doubl
     __shared__ double warp_sum[kK1Threads / 32];
     __shared__ TF sh2f[24], awf[24];
     const double* src_coef = spline + n;  // log N block
+    const double x_knot = spline[knot];
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        x64[i] = spline[i];
-        xf[i] = (TF)spline[i];
+        x64[i] = spline[i] - x_knot;
+        xf[i] = (TF)(spline[i] - x_knot);
     }
     for (int i = threadIdx.x; i < 4 * (n - 1); i += blockDim.x) {
         c64[i] = src_coef[i];
@@ -193,28 +222,38 @@ __global__ void __launch_bounds__(kK1Threads) k1_kernel(Phys<TF> phf, Phys<doubl
     SplineView<TF> sf;
     sf.x = xf; sf.coef = cf; sf.n = n; sf.x0 = xf[0];
     sf.inv_h = (TF)((double)(n - 1) / (x64[n - 1] - x64[0]));
+    const double lr_abs = ::log(r_grid[knot]);
     const double r = r_grid[knot];
     const K1Parent<TF> Pf = k1_parent<TF>(sf, phf, r, knot);
     const K1Parent<double> Pd = k1_parent<double>(sd, phd, r, knot);
 
     double total = 0.0;
     const int nodes = (n - 1) * 8;
-    for (int k = threadIdx.x; k < nodes; k += blockDim.x) {
+    // this CTA's share of the radial nodes (contiguous interval ranges)
+    const int split = blockIdx.y;
+    const int per_split = ((n - 1 + kK1Split - 1) / kK1Split) * 8;
+    const int k_begin = split * per_split;
+    const int k_end = min(nodes, k_begin + per_split);
+    for (int k = k_begin + threadIdx.x; k < k_end; k += blockDim.x) {
         const int iv = k >> 3, m = k & 7;
-        const double center = 0.5 * (x64[iv] + x64[iv + 1]);
-        const double hw = 0.5 * (x64[iv + 1] - x64[iv]);
+        // node positions from the absolute knots (as the reference rule), then relative to log r
+        const double xa = spline[iv], xb = spline[iv + 1];
+        const double center = 0.5 * (xa + xb);
+        const double hw = 0.5 * (xb - xa);
         const double lz = center + hw * consts.rule.x8[m];
+        const double dlz = lz - x_knot;
         const double rw = hw * consts.rule.w8[m];
         double node_sum;
+        (void)lr_abs;
         if (iv == knot - 1 || iv == knot) {
             // the two intervals adjacent to the parent knot in FP64
-            const K1Z<double> Z = k1_prepare_z<double>(sd, Pd, phd, lz);
+            const K1Z<double> Z = k1_prepare_z<double>(sd, Pd, phd, dlz, lz);
             double acc = 0.0;
 #pragma unroll 4
             for (int j = 0; j < 24; ++j) acc += k1_point<double>(sd, Pd, Z, phd, consts.sh2[j]) * consts.aw[j];
             node_sum = acc * (2.0 * Z.z * Z.z) * rw;
         } else {
-            const K1Z<TF> Z = k1_prepare_z<TF>(sf, Pf, phf, (TF)lz);
+            const K1Z<TF> Z = k1_prepare_z<TF>(sf, Pf, phf, dlz, lz);
             TF acc = (TF)0;
 #pragma unroll 4
             for (int j = 0; j < 24; ++j) acc += k1_point<TF>(sf, Pf, Z, phf, sh2f[j]) * awf[j];
@@ -222,15 +261,24 @@ __global__ void __launch_bounds__(kK1Threads) k1_kernel(Phys<TF> phf, Phys<doubl
         }
         total += node_sum;
     }
-    // deterministic block reduction
+    // deterministic block reduction, then the cluster's partials in rank order
+    __shared__ double cta_total;
     for (int o = 16; o > 0; o >>= 1) total += __shfl_down_sync(0xffffffffu, total, o);
     if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = total;
     __syncthreads();
     if (threadIdx.x == 0) {
         double s = 0.0;
         for (int w = 0; w < kK1Threads / 32; ++w) s += warp_sum[w];
+        cta_total = s;
+    }
+    cg::cluster_group cluster = cg::this_cluster();
+    cluster.sync();
+    if (cluster.block_rank() == 0 && threadIdx.x == 0) {
+        double s = 0.0;
+        for (int q = 0; q < kK1Split; ++q) s += *cluster.map_shared_rank(&cta_total, q);
         out[knot] = s;
     }
+    cluster.sync();  // keep every CTA's shared memory alive until rank 0 has read it
 }
 
 }  // namespace
@@ -254,14 +302,14 @@ cudaError_t launch_k1(const nlo_bk_params& p, const double* r, int points, const
         const size_t smem = (sizeof(double) * 2) * (size_t)(points + 4 * (points - 1));
         e = cudaFuncSetAttribute(k1_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        k1_kernel<double><<<points, kK1Threads, smem, stream>>>(phd, phd, consts, r, points, spline, active, count,
-                                                                out);
+        k1_kernel<double><<<dim3(points, kK1Split), kK1Threads, smem, stream>>>(phd, phd, consts, r, points, spline,
+                                                                                active, count, out);
     } else {
         const size_t smem = (sizeof(double) + sizeof(float)) * (size_t)(points + 4 * (points - 1));
         e = cudaFuncSetAttribute(k1_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        k1_kernel<float><<<points, kK1Threads, smem, stream>>>(make_phys<float>(p), phd, consts, r, points, spline,
-                                                               active, count, out);
+        k1_kernel<float><<<dim3(points, kK1Split), kK1Threads, smem, stream>>>(make_phys<float>(p), phd, consts, r,
+                                                                               points, spline, active, count, out);
     }
     return cudaGetLastError();
 }

@@ -42,28 +42,22 @@ struct K2Box {
     T cpt_scale;  // volume * Nc^2 / (8 pi^4)
 };
 
-// atanh(t)/t - 1 = t^2 sum_{k>=1} t^{2k-2}/(2k+1); 14 terms reach FP32 (and, with
-// |t| < 0.5, ~1e-9 relative in FP64 -- the FP64 build uses more terms).
+// atanh(t)/t - 1 = t^2 g(t^2), g(x) = sum_{k>=0} x^k/(2k+3), for t^2 < 1/4.
+// FP32: degree-6 polynomial fitted to g on [0, 1/4] in relative error (least
+// squares at Chebyshev nodes); 8e-8 relative in FP32 Horner, i.e. FP32 rounding.
 template <typename T>
 __device__ __forceinline__ T atanh_ratio_m1(T t2);
 
 template <>
 __device__ __forceinline__ float atanh_ratio_m1<float>(float t2)
 {
-    float s = 1.0f / 29.0f;
-    s = fmaf(s, t2, 1.0f / 27.0f);
-    s = fmaf(s, t2, 1.0f / 25.0f);
-    s = fmaf(s, t2, 1.0f / 23.0f);
-    s = fmaf(s, t2, 1.0f / 21.0f);
-    s = fmaf(s, t2, 1.0f / 19.0f);
-    s = fmaf(s, t2, 1.0f / 17.0f);
-    s = fmaf(s, t2, 1.0f / 15.0f);
-    s = fmaf(s, t2, 1.0f / 13.0f);
-    s = fmaf(s, t2, 1.0f / 11.0f);
-    s = fmaf(s, t2, 1.0f / 9.0f);
-    s = fmaf(s, t2, 1.0f / 7.0f);
-    s = fmaf(s, t2, 1.0f / 5.0f);
-    s = fmaf(s, t2, 1.0f / 3.0f);
+    float s = 0.15609439065092748f;
+    s = fmaf(s, t2, 0.04106302733766397f);
+    s = fmaf(s, t2, 0.09747851219255123f);
+    s = fmaf(s, t2, 0.11051354325642386f);
+    s = fmaf(s, t2, 0.1428825580061165f);
+    s = fmaf(s, t2, 0.19999959971627077f);
+    s = fmaf(s, t2, 0.33333333435159396f);
     return s * t2;
 }
 
@@ -127,8 +121,8 @@ struct K2Parent {
 };
 
 // K2 and Kf contributions of one sample to one parent (already weighted).
-template <typename T, bool SYM>
-__device__ __forceinline__ void k2_point(const SplineView<T>& s, const Phys<T>& ph, const K2Parent<T>& P,
+template <typename T, bool SYM, typename EvalSpline>
+__device__ __forceinline__ void k2_point(const EvalSpline& s, const Phys<T>& ph, const K2Parent<T>& P,
                                          const T* __restrict__ rec, T& k2w, T& kfw)
 {
     const T r = P.r;
@@ -137,7 +131,7 @@ __device__ __forceinline__ void k2_point(const SplineView<T>& s, const Phys<T>& 
     const T X2sq = (r - z2) * (r - z2) + (T)4 * r * z2 * rec[kS2];
     const bool valid = Xsq >= M<T>::tiny_square() && X2sq >= M<T>::tiny_square();
     const T lXs = M<T>::log_fast(Xsq), lX2s = M<T>::log_fast(X2sq);
-    const NS<T> vX = eval_s_log(s, (T)0.5 * lXs), vX2 = eval_s_log(s, (T)0.5 * lX2s);
+    const PS<T> vX = eval_s_ps(s, (T)0.5 * lXs), vX2 = eval_s_ps(s, (T)0.5 * lX2s);
     // kernels (k2.py, kf.py) in the stable form
     const T a = Xsq * rec[kZ2sq], b = X2sq * rec[kZsq];
     const T sab = a + b;
@@ -169,7 +163,7 @@ __device__ __forceinline__ void k2_point(const SplineView<T>& s, const Phys<T>& 
     T dips = vX2.S * rec[kD2];
     if (M<T>::fabs(k2) > (T)1e10 && M<T>::fabs(dip) < (T)1e-10) { k2 = (T)0; dip = (T)0; }
     if (M<T>::fabs(k2s) > (T)1e10 && M<T>::fabs(dips) < (T)1e-10) { k2s = (T)0; dips = (T)0; }
-    const T dNX = ndiff_s(vX, vX2);
+    const T dNX = ndiff_ps(vX, vX2);
     T k2part, fermion;
     if (SYM) {
         k2part = (T)0.5 * (k2 * dip + k2s * dips);
@@ -188,7 +182,171 @@ __device__ __forceinline__ void k2_point(const SplineView<T>& s, const Phys<T>& 
     if (!valid || !M<T>::finite(kfw)) kfw = (T)0;
 }
 
-template <typename T, bool SYM>
+// ---------------------------------------------------------------------------
+// FP32 evaluation tuned for instruction count (the kernel is issue-bound).
+// Spline values are carried in log2 units; the log S coefficients are stored
+// pre-scaled to the unit interval, (a, b h, c h^2, d h^3) * log2(e), so that the
+// position u = (log X - x0)/h gives the piece i = floor(u) and t = u - i directly.
+// Amplitudes outside the grid are encoded as p2 = 0 (S = 1, below r_min) and
+// p2 = -150 (S = 0, above r_max), which lets one branch-free difference formula
+// serve every case:  N_A - N_B = S_A (2^(pB-pA) - 1) if pB <= pA, else -S_B (2^(pA-pB) - 1).
+__device__ __forceinline__ float ex2_approx(float x)
+{
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float lg2_approx(float x)
+{
+    float y;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float rcp_approx(float x)
+{
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// 2^x - 1 for x <= 0: degree-5 polynomial in x times x on [-1/2, 0] (fitted to
+// (2^x - 1)/x in relative error; 1.2e-7 in FP32), 2^x - 1 directly below.
+__device__ __forceinline__ float exp2m1_nonpositive(float x)
+{
+    float q = 0.0001327910803141678f;
+    q = fmaf(q, x, 0.001321632968973654f);
+    q = fmaf(q, x, 0.009615099576281485f);
+    q = fmaf(q, x, 0.05550375169709732f);
+    q = fmaf(q, x, 0.24022649146109623f);
+    q = fmaf(q, x, 0.6931471804499034f);
+    const float poly = q * x;
+    const float direct = ex2_approx(x) - 1.0f;
+    return x > -0.5f ? poly : direct;
+}
+
+struct FastSpline {
+    const float4* coef;  // [n-1] pre-scaled (see above)
+    float u_scale;       // (ln 2 / 2) / h : u from log2(X^2)
+    float u_off;         // -x0 / h
+    float u_max;         // n - 1
+    int last;            // n - 2
+};
+
+struct P2S {
+    float p2, S;
+};
+
+// log2(X^2) -> (log2 S, S) with the edge encoding
+__device__ __forceinline__ P2S fast_amplitude(const FastSpline& s, float l2sq)
+{
+    const float u = fmaf(l2sq, s.u_scale, s.u_off);
+    const float uc = fminf(fmaxf(u, 0.0f), s.u_max);
+    const int i = min((int)uc, s.last);
+    const float t = uc - (float)i;
+    const float4 c = s.coef[i];
+    float p2 = fmaf(t, fmaf(t, fmaf(t, c.w, c.z), c.y), c.x);
+    p2 = u < 0.0f ? 0.0f : p2;
+    p2 = u > s.u_max ? -150.0f : p2;
+    return {p2, ex2_approx(p2)};
+}
+
+// N_A - N_B from log2 S values
+__device__ __forceinline__ float fast_ndiff(const P2S& A, const P2S& B)
+{
+    const float d = B.p2 - A.p2;
+    const float e = exp2m1_nonpositive(-fabsf(d));
+    return d <= 0.0f ? A.S * e : -B.S * e;
+}
+
+struct K2ParentF {
+    float r, r2, lr, two_r, four_r;
+};
+
+// COUPLING: 0 smooth freeze, 1 smooth freeze capped at alpha_cap, 2 fixed.
+template <bool SYM, int COUPLING>
+__device__ __forceinline__ void k2_point_fast(const FastSpline& s, const Phys<float>& ph, const K2ParentF& P,
+                                              const float4* __restrict__ rec4, float& k2w, float& kfw)
+{
+    constexpr float LN2 = 0.69314718055994531f;
+    constexpr float L2E = 1.4426950408889634f;
+    const float4 q0 = rec4[0], q1 = rec4[1], q2 = rec4[2], q3 = rec4[3], q4 = rec4[4];
+    // record layout (enum Rec): z z2 s1 s2 | P1 P2 U1 V1 | U2 V2 q D1 | D2 dN SY Lmin | Cpt Dl zsq z2sq
+    const float z = q0.x, z2 = q0.y, s1 = q0.z, s2 = q0.w;
+    const float P1 = q1.x, P2 = q1.y, U1 = q1.z, V1 = q1.w;
+    const float U2 = q2.x, V2 = q2.y, q = q2.z, D1 = q2.w;
+    const float D2 = q3.x, dN = q3.y, SY = q3.z, Lmin = q3.w;
+    const float cpt = q4.x, Dl = q4.y, zsq = q4.z, z2sq = q4.w;
+    const float r = P.r;
+    const float rz = r - z, rz2 = r - z2;
+    const float Xsq = fmaf(P.four_r * z, s1, rz * rz);
+    const float X2sq = fmaf(P.four_r * z2, s2, rz2 * rz2);
+    const bool valid = Xsq >= 1e-38f && X2sq >= 1e-38f;
+    const float L2X = lg2_approx(Xsq), L2X2 = lg2_approx(X2sq);
+    const P2S vX = fast_amplitude(s, L2X), vX2 = fast_amplitude(s, L2X2);
+    // kernels
+    const float a = Xsq * z2sq, b = X2sq * zsq;
+    const float rs = rcp_approx(a + b);
+    const float d = r * fmaf(r, P1, -P2);
+    const float t = d * rs;
+    const float t2 = t * t;
+    float g = 0.15609439065092748f;
+    g = fmaf(g, t2, 0.04106302733766397f);
+    g = fmaf(g, t2, 0.09747851219255123f);
+    g = fmaf(g, t2, 0.11051354325642386f);
+    g = fmaf(g, t2, 0.1428825580061165f);
+    g = fmaf(g, t2, 0.19999959971627077f);
+    g = fmaf(g, t2, 0.33333333435159396f);
+    const float hm1_series = g * t2;
+    const float Ld = fmaf(LN2, L2X - L2X2, Dl);  // log(a/b)
+    const float hm1_log = fmaf(Ld, 0.5f * rcp_approx(t), -1.0f);
+    const float hm1 = t2 < 0.25f ? hm1_series : hm1_log;
+    const float rs2 = rs + rs;
+    const float L = fmaf(hm1, rs2, rs2);
+    const float r2Lq = P.r2 * L * q;
+    const float fq2 = (hm1 + hm1) * (q * q);
+    const float C0 = fmaf(-4.0f, r2Lq, fq2);
+    const float B1 = fmaf(r, U1, V1), B2 = fmaf(r, U2, V2);
+    const float w = r2Lq * P.two_r;
+    float k2 = fmaf(w * B1, rcp_approx(Xsq * z2), C0);
+    float k2s = fmaf(w * B2, rcp_approx(X2sq * z), C0);
+    const float kf = (r2Lq - fq2) * ph.nf_over_nc;
+    float dip = vX.S * D1, dips = vX2.S * D2;
+    const bool cut = fabsf(k2) > 1e10f && fabsf(dip) < 1e-10f;
+    const bool cut_s = fabsf(k2s) > 1e10f && fabsf(dips) < 1e-10f;
+    k2 = cut ? 0.0f : k2;
+    dip = cut ? 0.0f : dip;
+    k2s = cut_s ? 0.0f : k2s;
+    dips = cut_s ? 0.0f : dips;
+    const float dNX = fast_ndiff(vX, vX2);
+    float k2part, fermion;
+    if (SYM) {  // the factor 1/2 of the symmetrisation is folded into cpt
+        k2part = fmaf(k2, dip, k2s * dips);
+        fermion = kf * dNX * dN;
+    } else {
+        k2part = k2 * dip;
+        fermion = kf * SY * dNX;
+    }
+    float alpha;
+    if (COUPLING == 2) {
+        alpha = ph.fixed_as;
+    } else {
+        const float lmin = fminf(fminf(Lmin, P.lr), (0.5f * LN2) * fminf(L2X, L2X2));
+        const float right = fmaf(-10.0f, lmin, 5.0f * ph.log_sc);
+        const float m = fmaxf(ph.left, right);
+        const float e = ex2_approx(-fabsf(ph.left - right) * L2E);
+        const float lae = fmaf(LN2, lg2_approx(1.0f + e), m);
+        alpha = rcp_approx(ph.b0c * lae);
+        if (COUPLING == 1) alpha = fminf(alpha, ph.alpha_cap);
+    }
+    const float scale = alpha * alpha * cpt;
+    k2w = k2part * scale;
+    kfw = -fermion * scale;
+    const bool ok = valid && fabsf(k2w + kfw) < INFINITY;
+    k2w = ok ? k2w : 0.0f;
+    kfw = ok ? kfw : 0.0f;
+}
+
+template <typename T, bool SYM, int COUPLING>
 __global__ void __launch_bounds__(1024) k2kf_kernel(Phys<T> ph, K2Box<T> box, SobolDirsArg dirs,
                                                     const double* __restrict__ r_grid, int n,
                                                     const double* __restrict__ spline,
@@ -197,13 +355,23 @@ __global__ void __launch_bounds__(1024) k2kf_kernel(Phys<T> ph, K2Box<T> box, So
                                                     uint64_t samples, double* __restrict__ partial)
 {
     extern __shared__ __align__(16) unsigned char k2_smem[];
-    K2Rec<T>* recs = reinterpret_cast<K2Rec<T>*>(k2_smem);  // [blockDim.x]
-    T* xs = reinterpret_cast<T*>(recs + blockDim.x);
-    T* cs = xs + n;
-    uint32_t* st = reinterpret_cast<uint32_t*>(cs + 4 * (n - 1));  // [4][30] + shift[4]
+    K2Rec<T>* recs = reinterpret_cast<K2Rec<T>*>(k2_smem);  // [blockDim.x], 16-byte aligned rows
+    T* cs = reinterpret_cast<T*>(recs + blockDim.x);          // [n-1][4] natural units, 16-byte aligned
+    float4* cs2 = reinterpret_cast<float4*>(cs + 4 * (n - 1)); // [n-1] pre-scaled (FP32 path)
+    T* xs = reinterpret_cast<T*>(cs2 + (sizeof(T) == sizeof(float) ? n - 1 : 0));
+    uint32_t* st = reinterpret_cast<uint32_t*>(xs + n);         // [4][30] + shift[4]
     const double* src_coef = spline + n + 4 * (size_t)(n - 1);     // log S block
+    const double h64 = (spline[n - 1] - spline[0]) / (double)(n - 1);
     for (int i = threadIdx.x; i < n; i += blockDim.x) xs[i] = (T)spline[i];
     for (int i = threadIdx.x; i < 4 * (n - 1); i += blockDim.x) cs[i] = (T)src_coef[i];
+    if (sizeof(T) == sizeof(float)) {
+        const double l2e = 1.4426950408889634;
+        for (int i = threadIdx.x; i < n - 1; i += blockDim.x) {
+            const double* c = src_coef + 4 * (size_t)i;
+            cs2[i] = make_float4((float)(c[0] * l2e), (float)(c[1] * h64 * l2e), (float)(c[2] * h64 * h64 * l2e),
+                                 (float)(c[3] * h64 * h64 * h64 * l2e));
+        }
+    }
     for (int i = threadIdx.x; i < 120; i += blockDim.x) st[i] = dirs.state[i / 30][i % 30];
     if (threadIdx.x < 4) st[120 + threadIdx.x] = dirs.shift[threadIdx.x];
     __syncthreads();
@@ -214,16 +382,31 @@ __global__ void __launch_bounds__(1024) k2kf_kernel(Phys<T> ph, K2Box<T> box, So
     s.x0 = xs[0];
     s.inv_h = (T)((double)(n - 1) / (spline[n - 1] - spline[0]));
 
+    // per-evaluation spline: uniform-grid FP32 form in the mixed build, the exact
+    // knot search in the FP64 build
+    FastSpline fs;
+    fs.coef = cs2;
+    fs.u_scale = (float)(0.5 * 0.69314718055994531 / h64);
+    fs.u_off = (float)(-spline[0] / h64);
+    fs.u_max = (float)(n - 1);
+    fs.last = n - 2;
+
     const int n_active = *count;
     const int slot = blockIdx.y * blockDim.x + threadIdx.x;
     const bool has_parent = slot < n_active;
     K2Parent<T> P;
+    K2ParentF PF;
     {
         const double r = has_parent ? r_grid[active[slot]] : 1.0;
         P.r = (T)r;
         P.r2 = P.r * P.r;
         P.lr = (T)log(r);
         P.two_r = (T)2 * P.r;
+        PF.r = (float)r;
+        PF.r2 = (float)(r * r);
+        PF.lr = (float)log(r);
+        PF.two_r = (float)(2.0 * r);
+        PF.four_r = (float)(4.0 * r);
     }
     double acc_k2 = 0.0, acc_kf = 0.0, acc_sq = 0.0;
     const uint64_t tile = blockDim.x;
@@ -241,16 +424,22 @@ __global__ void __launch_bounds__(1024) k2kf_kernel(Phys<T> ph, K2Box<T> box, So
                 Kahan<T> sk2, skf;
                 sk2.reset();
                 skf.reset();
+                T sq = (T)0;  // variance estimate only: plain sum per tile
                 for (int j = 0; j < count_here; ++j) {
                     T k2w, kfw;
-                    k2_point<T, SYM>(s, ph, P, recs[j].v, k2w, kfw);
+                    if constexpr (sizeof(T) == sizeof(float))
+                        k2_point_fast<SYM, COUPLING>(fs, ph, PF, reinterpret_cast<const float4*>(recs[j].v), k2w,
+                                                     kfw);
+                    else
+                        k2_point<T, SYM>(s, ph, P, recs[j].v, k2w, kfw);
                     sk2.add(k2w);
                     skf.add(kfw);
-                    const double tot = (double)k2w + (double)kfw;
-                    acc_sq = fma(tot, tot, acc_sq);
+                    const T tot = k2w + kfw;
+                    sq += tot * tot;
                 }
                 acc_k2 += (double)sk2.sum - (double)sk2.comp;
                 acc_kf += (double)skf.sum - (double)skf.comp;
+                acc_sq += (double)sq;
             }
             __syncthreads();
         }
@@ -263,38 +452,50 @@ __global__ void __launch_bounds__(1024) k2kf_kernel(Phys<T> ph, K2Box<T> box, So
     }
 }
 
-__global__ void k2kf_finalize_kernel(const double* __restrict__ partial, int blocks, int n,
-                                     const int32_t* __restrict__ active, const int32_t* __restrict__ count,
-                                     double* __restrict__ out)
+// One warp per active parent: lanes add strided CTA partials, then a fixed
+// shuffle tree combines them (the order does not depend on timing).
+__global__ void __launch_bounds__(256) k2kf_finalize_kernel(const double* __restrict__ partial, int blocks, int n,
+                                                            const int32_t* __restrict__ active,
+                                                            const int32_t* __restrict__ count,
+                                                            double* __restrict__ out)
 {
-    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot >= *count || slot >= n) return;
+    const int slot = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (slot >= n || slot >= *count) return;
     double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-    for (int c = 0; c < blocks; ++c) {
+    for (int c = lane; c < blocks; c += 32) {
         const double* p = partial + ((size_t)c * n + slot) * 3;
         s0 += p[0];
         s1 += p[1];
         s2 += p[2];
     }
-    double* o = out + 3 * (size_t)active[slot];
-    o[0] = s0;
-    o[1] = s1;
-    o[2] = s2;
+    for (int o = 16; o > 0; o >>= 1) {
+        s0 += __shfl_down_sync(0xffffffffu, s0, o);
+        s1 += __shfl_down_sync(0xffffffffu, s1, o);
+        s2 += __shfl_down_sync(0xffffffffu, s2, o);
+    }
+    if (lane == 0) {
+        double* o = out + 3 * (size_t)active[slot];
+        o[0] = s0;
+        o[1] = s1;
+        o[2] = s2;
+    }
 }
 
-template <typename T, bool SYM>
+template <typename T, bool SYM, int COUPLING>
 cudaError_t launch_typed(const nlo_bk_params& p, const double* r, int points, const double* spline,
                          const int32_t* active, const int32_t* count, const SobolDirsArg& dirs, uint64_t offset,
                          uint64_t samples, const nlo_bk_box& box, double* partial, int max_blocks, int threads,
                          int parent_tiles, int* used_blocks, cudaStream_t stream)
 {
     const size_t smem = sizeof(K2Rec<T>) * threads + sizeof(T) * (size_t)(points + 4 * (points - 1)) +
+                        (sizeof(T) == sizeof(float) ? sizeof(float4) * (size_t)(points - 1) : 0) +
                         sizeof(uint32_t) * 124;
-    cudaError_t e = cudaFuncSetAttribute(k2kf_kernel<T, SYM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(k2kf_kernel<T, SYM, COUPLING>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k2kf_kernel<T, SYM>, threads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k2kf_kernel<T, SYM, COUPLING>, threads, smem);
     if (e != cudaSuccess) return e;
     int device = 0, sms = 0;
     cudaGetDevice(&device);
@@ -319,10 +520,12 @@ cudaError_t launch_typed(const nlo_bk_params& p, const double* r, int points, co
     } else {
         volume = box.width[0] * box.width[1] * box.width[2] * box.width[3];
     }
-    kb.cpt_scale = (T)(volume * p.nc * p.nc / (8.0 * kPi * kPi * kPi * kPi));
+    // the FP32 path folds the symmetrisation's 1/2 into the per-sample weight
+    const double half = (sizeof(T) == sizeof(float) && SYM) ? 0.5 : 1.0;
+    kb.cpt_scale = (T)(half * volume * p.nc * p.nc / (8.0 * kPi * kPi * kPi * kPi));
     dim3 grid((unsigned)blocks, (unsigned)parent_tiles);
-    k2kf_kernel<T, SYM><<<grid, threads, smem, stream>>>(make_phys<T>(p), kb, dirs, r, points, spline, active, count,
-                                                        offset, samples, partial);
+    k2kf_kernel<T, SYM, COUPLING><<<grid, threads, smem, stream>>>(make_phys<T>(p), kb, dirs, r, points, spline,
+                                                                  active, count, offset, samples, partial);
     return cudaGetLastError();
 }
 
@@ -342,20 +545,21 @@ cudaError_t launch_k2kf(const nlo_bk_params& p, const double* r, int points, con
     int used = 0;
     const bool fp64 = p.precision == NLO_PRECISION_FP64;
     const bool sym = p.symmetrize != 0;
-    if (fp64 && sym)
-        e = launch_typed<double, true>(p, r, points, spline, active, count, dirs, offset, samples, box, partial,
-                                       max_blocks, threads, parent_tiles, &used, stream);
-    else if (fp64)
-        e = launch_typed<double, false>(p, r, points, spline, active, count, dirs, offset, samples, box, partial,
-                                        max_blocks, threads, parent_tiles, &used, stream);
-    else if (sym)
-        e = launch_typed<float, true>(p, r, points, spline, active, count, dirs, offset, samples, box, partial,
-                                      max_blocks, threads, parent_tiles, &used, stream);
+    const int coupling = p.fixed_coupling ? 2 : (p.alpha_cap > 0.0 ? 1 : 0);
+#define NLO_K2_LAUNCH(T, S, C)                                                                                  \
+    launch_typed<T, S, C>(p, r, points, spline, active, count, dirs, offset, samples, box, partial, max_blocks, \
+                          threads, parent_tiles, &used, stream)
+    if (fp64)
+        e = sym ? NLO_K2_LAUNCH(double, true, 0) : NLO_K2_LAUNCH(double, false, 0);
+    else if (coupling == 0)
+        e = sym ? NLO_K2_LAUNCH(float, true, 0) : NLO_K2_LAUNCH(float, false, 0);
+    else if (coupling == 1)
+        e = sym ? NLO_K2_LAUNCH(float, true, 1) : NLO_K2_LAUNCH(float, false, 1);
     else
-        e = launch_typed<float, false>(p, r, points, spline, active, count, dirs, offset, samples, box, partial,
-                                       max_blocks, threads, parent_tiles, &used, stream);
+        e = sym ? NLO_K2_LAUNCH(float, true, 2) : NLO_K2_LAUNCH(float, false, 2);
+#undef NLO_K2_LAUNCH
     if (e != cudaSuccess) return e;
-    k2kf_finalize_kernel<<<(points + 127) / 128, 128, 0, stream>>>(partial, used, points, active, count, out);
+    k2kf_finalize_kernel<<<(points * 32 + 255) / 256, 256, 0, stream>>>(partial, used, points, active, count, out);
     return cudaGetLastError();
 }
 

@@ -16,19 +16,25 @@
 
 namespace nlo {
 
+// factor: [2][n] = 1/denominator and upper coefficient of the Thomas sweep for
+// the natural-spline system on the knots log r (it depends on the grid only).
+// With compute_factor set, thread 0 forms it first (and stores it for later calls).
 __global__ void __launch_bounds__(256) splines_kernel(const double* __restrict__ r, const double* __restrict__ N,
-                                                      int n, int force_positive, double* __restrict__ out)
+                                                      int n, int force_positive, double* __restrict__ factor,
+                                                      int compute_factor, double* __restrict__ out)
 {
     extern __shared__ double smem[];
-    double* x = smem;            // [n]
-    double* y = x + n;           // [2][n]
-    double* up = y + 2 * n;      // [2][n]
-    double* sol = up + 2 * n;    // [2][n]
+    double* x = smem;             // [n]
+    double* y = x + n;            // [2][n]
+    double* rhs = y + 2 * n;      // [2][n]
+    double* sol = rhs + 2 * n;    // [2][n]
+    double* inv_den = sol + 2 * n;  // [n]
+    double* up = inv_den + n;       // [n]
     const int m = n - 2;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         x[i] = log(r[i]);
         out[i] = x[i];
-        double v = N[i];
+        const double v = N[i];
         // log N row: N > 1 -> 1; force_positive: N < 0 -> 0
         double vn = v > 1.0 ? 1.0 : v;
         if (force_positive && vn < 0.0) vn = 0.0;
@@ -39,29 +45,44 @@ __global__ void __launch_bounds__(256) splines_kernel(const double* __restrict__
         y[n + i] = ns < 1.0 ? log1p(-ns) : kMinLog;
     }
     __syncthreads();
-    // Thomas algorithm (interpolation.py:124-149); warp 0 solves row 0, warp 1 row 1.
-    if ((threadIdx.x & 31) == 0 && threadIdx.x < 64) {
-        const int row = threadIdx.x >> 5;
+    for (int item = threadIdx.x; item < 2 * m; item += blockDim.x) {
+        const int row = item / m, i = item - row * m;
         const double* yy = y + row * n;
-        double* u = up + row * n;
+        rhs[row * n + i] =
+            6.0 * ((yy[i + 2] - yy[i + 1]) / (x[i + 2] - x[i + 1]) - (yy[i + 1] - yy[i]) / (x[i + 1] - x[i]));
+    }
+    if (compute_factor && threadIdx.x == 0 && m >= 1) {
+        // denominators of the forward sweep (interpolation.py:124-149)
+        double d = 2.0 * ((x[1] - x[0]) + (x[2] - x[1]));
+        factor[0] = 1.0 / d;
+        for (int i = 1; i < m; ++i) {
+            const double upper_prev = (x[i + 1] - x[i]) * factor[i - 1];
+            factor[n + i - 1] = upper_prev;
+            d = 2.0 * ((x[i + 1] - x[i]) + (x[i + 2] - x[i + 1])) - (x[i + 1] - x[i]) * upper_prev;
+            factor[i] = 1.0 / d;
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        inv_den[i] = factor[i];
+        up[i] = i < m - 1 ? factor[n + i] : 0.0;
+    }
+    __syncthreads();
+    // forward and back substitution; warp 0 solves row 0, warp 1 row 1
+    if ((threadIdx.x & 31) == 0 && threadIdx.x < 64 && m >= 1) {
+        const int row = threadIdx.x >> 5;
+        const double* b = rhs + row * n;
         double* s = sol + row * n;
-        if (m == 1) {
-            const double rhs = 6.0 * ((yy[2] - yy[1]) / (x[2] - x[1]) - (yy[1] - yy[0]) / (x[1] - x[0]));
-            s[0] = rhs / (2.0 * ((x[1] - x[0]) + (x[2] - x[1])));
-        } else if (m > 1) {
-            const double h0 = x[1] - x[0], h1 = x[2] - x[1];
-            const double diag = 2.0 * (h0 + h1);
-            u[0] = h1 / diag;
-            s[0] = 6.0 * ((yy[2] - yy[1]) / h1 - (yy[1] - yy[0]) / h0) / diag;
-            for (int i = 1; i < m; ++i) {
-                const double hi = x[i + 1] - x[i];
-                const double hi1 = x[i + 2] - x[i + 1];
-                const double denom = 2.0 * (hi + hi1) - hi * u[i - 1];
-                if (i < m - 1) u[i] = hi1 / denom;
-                const double rhs = 6.0 * ((yy[i + 2] - yy[i + 1]) / hi1 - (yy[i + 1] - yy[i]) / hi);
-                s[i] = (rhs - hi * s[i - 1]) / denom;
-            }
-            for (int i = m - 2; i >= 0; --i) s[i] -= u[i] * s[i + 1];
+        double prev = b[0] * inv_den[0];
+        s[0] = prev;
+        for (int i = 1; i < m; ++i) {
+            prev = fma(-(x[i + 1] - x[i]), prev, b[i]) * inv_den[i];
+            s[i] = prev;
+        }
+        double next = s[m - 1];
+        for (int i = m - 2; i >= 0; --i) {
+            next = fma(-up[i], next, s[i]);
+            s[i] = next;
         }
     }
     __syncthreads();
@@ -124,15 +145,15 @@ __global__ void sobol_draw_kernel(SobolDirsArg dirs, uint64_t offset, uint64_t n
     }
 }
 
-cudaError_t launch_splines(const double* r, const double* N, int n, int force_positive, double* out,
-                           cudaStream_t stream)
+cudaError_t launch_splines(const double* r, const double* N, int n, int force_positive, double* factor,
+                           int compute_factor, double* out, cudaStream_t stream)
 {
-    const size_t smem = sizeof(double) * 7 * (size_t)n;
+    const size_t smem = sizeof(double) * 9 * (size_t)n;
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(splines_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
-    splines_kernel<<<1, 256, smem, stream>>>(r, N, n, force_positive, out);
+    splines_kernel<<<1, 256, smem, stream>>>(r, N, n, force_positive, factor, compute_factor, out);
     return cudaGetLastError();
 }
 

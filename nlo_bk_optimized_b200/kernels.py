@@ -40,7 +40,7 @@ def splines(r: torch.Tensor, N: torch.Tensor, *, force_positive: bool = True) ->
     with torch.cuda.device(r.device):
         _native.check(lib.nlo_bk_splines(r64.data_ptr(), N64.data_ptr(), n, int(force_positive), out.data_ptr(),
                                          _native.stream_handle(r.device)))
-    coef = out[n:].view(2, n - 1, 4)
+    coef = out[n:n + 8 * (n - 1)].view(2, n - 1, 4)
     return {"x": out[:n], "n": coef[0], "s": coef[1], "raw": out}
 
 

@@ -131,4 +131,4 @@ def test_library_rejects_bad_arguments_without_a_gpu():
     assert lib.nlo_bk_k1(params, None, 10, None, None, None, None, None) == 1
     assert b"NF" in lib.nlo_last_error()
     assert lib.nlo_bk_k2kf_workspace_bytes(400) > 0
-    assert lib.nlo_bk_spline_doubles(400) == 400 + 8 * 399
+    assert lib.nlo_bk_spline_doubles(400) == 400 + 8 * 399 + 2 * 400

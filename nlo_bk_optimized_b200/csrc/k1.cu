@@ -194,11 +194,29 @@ __global__ void __cluster_dims__(1, kK1Split, 1) __launch_bounds__(kK1Threads)
     const int slot = blockIdx.x;
     if (slot >= *count) return;
     const int knot = active[slot];
+    // this CTA's share of the radial nodes (contiguous interval ranges)
+    const int nodes = (n - 1) * 8;
+    const int split = blockIdx.y;
+    const int per_split = ((n - 1 + kK1Split - 1) / kK1Split) * 8;
+    const int k_begin = split * per_split;
+    const int k_end = min(nodes, k_begin + per_split);
+    const int k_count = max(0, k_end - k_begin);
+
     extern __shared__ __align__(16) unsigned char k1_smem[];
-    double* x64 = reinterpret_cast<double*>(k1_smem);
-    double* c64 = x64 + n;
-    TF* xf = reinterpret_cast<TF*>(c64 + 4 * (n - 1));
-    TF* cf = xf + n;
+    unsigned char* cursor = k1_smem;
+    auto carve = [&](size_t bytes) {
+        unsigned char* p = cursor;
+        cursor += (bytes + 15) & ~(size_t)15;
+        return p;
+    };
+    double* x64 = reinterpret_cast<double*>(carve(sizeof(double) * n));
+    double* c64 = reinterpret_cast<double*>(carve(sizeof(double) * 4 * (n - 1)));
+    TF* xf = reinterpret_cast<TF*>(carve(sizeof(TF) * n));
+    TF* cf = reinterpret_cast<TF*>(carve(sizeof(TF) * 4 * (n - 1)));
+    K1Z<TF>* zt = reinterpret_cast<K1Z<TF>*>(carve(sizeof(K1Z<TF>) * per_split));
+    double* zw = reinterpret_cast<double*>(carve(sizeof(double) * per_split));
+    K1Z<double>* zd = reinterpret_cast<K1Z<double>*>(carve(sizeof(K1Z<double>) * 16));
+    double* zdw = reinterpret_cast<double*>(carve(sizeof(double) * 16));
     __shared__ double warp_sum[kK1Threads / 32];
     __shared__ TF sh2f[24], awf[24];
     const double* src_coef = spline + n;  // log N block
@@ -215,6 +233,7 @@ __global__ void __cluster_dims__(1, kK1Split, 1) __launch_bounds__(kK1Threads)
         sh2f[threadIdx.x] = (TF)consts.sh2[threadIdx.x];
         awf[threadIdx.x] = (TF)consts.aw[threadIdx.x];
     }
+    if (threadIdx.x < 16) zdw[threadIdx.x] = 0.0;
     __syncthreads();
     SplineView<double> sd;
     sd.x = x64; sd.coef = c64; sd.n = n; sd.x0 = x64[0];
@@ -222,44 +241,46 @@ __global__ void __cluster_dims__(1, kK1Split, 1) __launch_bounds__(kK1Threads)
     SplineView<TF> sf;
     sf.x = xf; sf.coef = cf; sf.n = n; sf.x0 = xf[0];
     sf.inv_h = (TF)((double)(n - 1) / (x64[n - 1] - x64[0]));
-    const double lr_abs = ::log(r_grid[knot]);
     const double r = r_grid[knot];
     const K1Parent<TF> Pf = k1_parent<TF>(sf, phf, r, knot);
     const K1Parent<double> Pd = k1_parent<double>(sd, phd, r, knot);
 
-    double total = 0.0;
-    const int nodes = (n - 1) * 8;
-    // this CTA's share of the radial nodes (contiguous interval ranges)
-    const int split = blockIdx.y;
-    const int per_split = ((n - 1 + kK1Split - 1) / kK1Split) * 8;
-    const int k_begin = split * per_split;
-    const int k_end = min(nodes, k_begin + per_split);
-    for (int k = k_begin + threadIdx.x; k < k_end; k += blockDim.x) {
+    // phase 1: per-node data of this CTA's range; the two intervals adjacent to the
+    // parent knot (z -> x) go to the FP64 table
+    for (int L = threadIdx.x; L < k_count; L += blockDim.x) {
+        const int k = k_begin + L;
         const int iv = k >> 3, m = k & 7;
-        // node positions from the absolute knots (as the reference rule), then relative to log r
+        // node positions from the absolute knots (the reference rule), then relative to log r
         const double xa = spline[iv], xb = spline[iv + 1];
-        const double center = 0.5 * (xa + xb);
         const double hw = 0.5 * (xb - xa);
-        const double lz = center + hw * consts.rule.x8[m];
+        const double lz = 0.5 * (xa + xb) + hw * consts.rule.x8[m];
         const double dlz = lz - x_knot;
         const double rw = hw * consts.rule.w8[m];
-        double node_sum;
-        (void)lr_abs;
         if (iv == knot - 1 || iv == knot) {
-            // the two intervals adjacent to the parent knot in FP64
-            const K1Z<double> Z = k1_prepare_z<double>(sd, Pd, phd, dlz, lz);
-            double acc = 0.0;
-#pragma unroll 4
-            for (int j = 0; j < 24; ++j) acc += k1_point<double>(sd, Pd, Z, phd, consts.sh2[j]) * consts.aw[j];
-            node_sum = acc * (2.0 * Z.z * Z.z) * rw;
+            const int idx = (iv - (knot - 1)) * 8 + m;
+            zd[idx] = k1_prepare_z<double>(sd, Pd, phd, dlz, lz);
+            zdw[idx] = 2.0 * zd[idx].z * zd[idx].z * rw;
+            zw[L] = 0.0;
         } else {
-            const K1Z<TF> Z = k1_prepare_z<TF>(sf, Pf, phf, dlz, lz);
-            TF acc = (TF)0;
-#pragma unroll 4
-            for (int j = 0; j < 24; ++j) acc += k1_point<TF>(sf, Pf, Z, phf, sh2f[j]) * awf[j];
-            node_sum = (double)acc * (2.0 * (double)Z.z * (double)Z.z) * rw;
+            zt[L] = k1_prepare_z<TF>(sf, Pf, phf, dlz, lz);
+            const double z = (double)zt[L].z;
+            zw[L] = 2.0 * z * z * rw;
         }
-        total += node_sum;
+    }
+    __syncthreads();
+
+    // phase 2: the flattened (node, angle) evaluations, an equal share per thread
+    double total = 0.0;
+    for (int e = threadIdx.x; e < k_count * 24; e += blockDim.x) {
+        const int L = e / 24, j = e - 24 * (e / 24);
+        const double w = zw[L];
+        if (w != 0.0) total += (double)(k1_point<TF>(sf, Pf, zt[L], phf, sh2f[j]) * awf[j]) * w;
+    }
+    // phase 3: FP64 evaluations of the panel nodes this CTA owns
+    for (int e = threadIdx.x; e < 16 * 24; e += blockDim.x) {
+        const int idx = e / 24, j = e - 24 * (e / 24);
+        const double w = zdw[idx];
+        if (w != 0.0) total += k1_point<double>(sd, Pd, zd[idx], phd, consts.sh2[j]) * consts.aw[j] * w;
     }
     // deterministic block reduction, then the cluster's partials in rank order
     __shared__ double cta_total;
@@ -298,14 +319,21 @@ cudaError_t launch_k1(const nlo_bk_params& p, const double* r, int points, const
     cudaError_t e = cudaMemsetAsync(out, 0, sizeof(double) * (size_t)points, stream);
     if (e != cudaSuccess) return e;
     const Phys<double> phd = make_phys<double>(p);
+    const size_t per_split = (size_t)((points - 1 + kK1Split - 1) / kK1Split) * 8;
+    auto smem_for = [&](size_t tf) {
+        auto a16 = [](size_t v) { return (v + 15) & ~(size_t)15; };
+        return a16(8 * (size_t)points) + a16(8 * 4 * (size_t)(points - 1)) + a16(tf * (size_t)points) +
+               a16(tf * 4 * (size_t)(points - 1)) + a16((tf == 4 ? sizeof(K1Z<float>) : sizeof(K1Z<double>)) * per_split) +
+               a16(8 * per_split) + a16(sizeof(K1Z<double>) * 16) + a16(8 * 16);
+    };
     if (p.precision == NLO_PRECISION_FP64) {
-        const size_t smem = (sizeof(double) * 2) * (size_t)(points + 4 * (points - 1));
+        const size_t smem = smem_for(8);
         e = cudaFuncSetAttribute(k1_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         k1_kernel<double><<<dim3(points, kK1Split), kK1Threads, smem, stream>>>(phd, phd, consts, r, points, spline,
                                                                                 active, count, out);
     } else {
-        const size_t smem = (sizeof(double) + sizeof(float)) * (size_t)(points + 4 * (points - 1));
+        const size_t smem = smem_for(4);
         e = cudaFuncSetAttribute(k1_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         k1_kernel<float><<<dim3(points, kK1Split), kK1Threads, smem, stream>>>(make_phys<float>(p), phd, consts, r,

@@ -120,6 +120,20 @@ int nlo_bk_k2kf(const nlo_bk_params* params, const double* r, int32_t points, co
                 int64_t samples, const nlo_bk_box* box, double* out, void* workspace, size_t workspace_bytes,
                 void* stream);
 
+/* The same K2+Kf sums as nlo_bk_k2kf for callers that cannot allocate device
+ * memory (a plugin inside a framework that owns the GPU's memory pool, a serving
+ * loop that must not pay cudaMalloc's latency and synchronisation): there is no
+ * workspace argument and nothing is allocated; the per-CTA partial sums live in a
+ * fixed device array of 296 x 512 x 3 doubles (3.6 MB) that every GPU loading the
+ * library holds until the process exits.  points must be <= 512 (larger grids are
+ * rejected with NLO_ERR_INVALID).  The first call on a device looks up the
+ * array's address with that device current; make it before any stream capture.
+ * All calls share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller.  This entry point has no counterpart in the reference. */
+int nlo_bk_k2kf_static(const nlo_bk_params* params, const double* r, int32_t points, const double* spline,
+                       const int32_t* active, const int32_t* count, const nlo_sobol_dirs* dirs, int64_t offset,
+                       int64_t samples, const nlo_bk_box* box, double* out, void* stream);
+
 /* Workspace bytes for nlo_bk_rhs / nlo_bk_evolve. */
 size_t nlo_bk_rhs_workspace_bytes(int32_t points);
 

@@ -62,6 +62,7 @@ EXPORTED = (
     "nlo_bk_k1",
     "nlo_bk_k2kf_workspace_bytes",
     "nlo_bk_k2kf",
+    "nlo_bk_k2kf_static",
     "nlo_bk_rhs_workspace_bytes",
     "nlo_bk_rhs",
     "nlo_bk_evolve",
@@ -92,6 +93,8 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.nlo_bk_k2kf_workspace_bytes.argtypes = [i32]
     lib.nlo_bk_k2kf.restype = ctypes.c_int
     lib.nlo_bk_k2kf.argtypes = [P(BKParams), vp, i32, vp, vp, vp, P(SobolDirs), i64, i64, P(Box), vp, vp, sz, vp]
+    lib.nlo_bk_k2kf_static.restype = ctypes.c_int
+    lib.nlo_bk_k2kf_static.argtypes = [P(BKParams), vp, i32, vp, vp, vp, P(SobolDirs), i64, i64, P(Box), vp, vp]
     lib.nlo_bk_rhs_workspace_bytes.restype = sz
     lib.nlo_bk_rhs_workspace_bytes.argtypes = [i32]
     lib.nlo_bk_rhs.restype = ctypes.c_int

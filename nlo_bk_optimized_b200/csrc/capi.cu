@@ -165,6 +165,8 @@ const K1Rule& k1_rule()
     return rule;
 }
 
+int set_last_error(int code, const char* message) { return fail(code, message); }
+
 size_t spline_doubles(int points) { return (size_t)points + 8 * (size_t)(points - 1); }
 
 // buffer size a caller provides to nlo_bk_splines: coefficients plus factorisation scratch

@@ -39,6 +39,9 @@ struct RhsBuffers {
 size_t spline_doubles(int points);
 int k2kf_max_blocks();
 
+// Records a message for nlo_last_error() and returns code.
+int set_last_error(int code, const char* message);
+
 cudaError_t launch_splines(const double* r, const double* N, int n, int force_positive, double* factor,
                            int compute_factor, double* out, cudaStream_t stream);
 cudaError_t launch_active(const double* N, int n, int32_t* active, int32_t* count, cudaStream_t stream);

@@ -412,6 +412,25 @@ def run_reference(args) -> None:
     print(json.dumps(line))
 
 
+def run_kernel_case() -> None:
+    """Small case for ncu captures: one K2+Kf launch (400 parents x 2^18 Sobol points)
+    and one K1 launch at the initial condition, twice."""
+
+    import torch
+
+    from nlo_bk_optimized_b200 import MV, kernels
+    from nlo_bk_optimized_b200.bk.evolution import _r_grid
+
+    config = workload_config()
+    r = _r_grid(config, device="cuda", dtype=torch.float64)
+    N = MV(qs0sqr=QS0SQR).dipole_amplitude(r)
+    for _ in range(2):
+        kernels.k2kf(r, N, config, samples=1 << 18)
+        kernels.k1(r, N, config)
+    torch.cuda.synchronize()
+    print("kernel case done")
+
+
 def main() -> None:
     parser = argparse.ArgumentParser()
     parser.add_argument("--gpus", type=int, default=1)
@@ -419,7 +438,12 @@ def main() -> None:
     parser.add_argument("--warmup", type=int, default=3)
     parser.add_argument("--impl", choices=["ours", "reference"], default="ours")
     parser.add_argument("--no-cpu-baseline", action="store_true")
+    parser.add_argument("--kernel-case", action="store_true",
+                        help="run only the small K2+Kf/K1 case used for ncu captures")
     args = parser.parse_args()
+    if args.kernel_case:
+        run_kernel_case()
+        return
     if args.warmup < 3 and args.impl == "ours":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
     if args.impl == "reference":

@@ -24,6 +24,7 @@ import argparse
 import json
 import math
 import os
+import re
 import statistics
 import subprocess
 import sys
@@ -279,12 +280,14 @@ def run_ours(args) -> None:
         "launch_ms": round(k2_ms, 4),
         "evals_per_s": round(evals / (k2_ms * 1e-3), 1),
     }
-    traffic_file = ROOT / "profiles" / "k2kf_traffic.json"
-    if traffic_file.exists():
-        try:
-            roofline["traffic"] = json.loads(traffic_file.read_text()).get("bytes_per_launch_full_workload")
-        except Exception:
-            pass
+    # DRAM bytes per K2+Kf launch from the committed ncu summary (constant in the
+    # number of Sobol points: the spline is staged into shared memory once per CTA)
+    summary = ROOT / "profiles" / "k2kf_k1_400r_kernel_case.md"
+    if summary.exists():
+        match = re.search(r"dram_bytes_per_launch_k2kf = (\d+)", summary.read_text())
+        if match:
+            roofline["traffic"] = int(match.group(1))
+            roofline["traffic_source"] = "profiles/k2kf_k1_400r_kernel_case.md"
 
     line = {
         "metric": METRIC,

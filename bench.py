@@ -434,6 +434,95 @@ def run_kernel_case() -> None:
     print("kernel case done")
 
 
+DIS_Q2 = (1.0, 50.0, 32)
+DIS_X = (1e-5, 1e-2, 16)
+DIS_SQRT_S = 318.0
+DIS_SIGMA0_HALF_MB = 16.0
+MB_TO_GEV2 = 2.56819
+DIS_BINS, DIS_ITERATIONS, DIS_SAMPLES = 50, 10, 1 << 18
+
+
+def run_dis(args) -> None:
+    """NLO DIS reduced cross section on an evolved BK table: 32 Q^2 log-spaced in [1, 50] GeV^2
+    x 16 x_Bj log-spaced in [1e-5, 1e-2], sqrt(s) = 318 GeV, light quarks (m = 0.14 GeV,
+    sum of charges^2 = 2/3), sigma_0/2 = 16 mb, Vegas 50 bins x 10 iterations x 2^18, seed 0.
+    The table is the headline BK workload (400 r, 2^20 Sobol points, RK4 h = 0.1) evolved to
+    Y = 16 (the qqbar-g terms reach Y = ln(Q^2/(x Q0^2)) = 15.4).  Timed: the batched
+    structure_functions call over all points (value) and single-point sigma_r calls on a
+    sample of points (the plain path)."""
+    import torch
+
+    from nlo_bk_optimized_b200 import MV, solve_bk
+    from nlo_bk_optimized_b200.dipole import BKDipole
+    from nlo_bk_optimized_b200.dis import DISConfig, DISOrder, Quark, QuarkType, sigma_r, structure_functions
+
+    device = torch.device("cuda", 0)
+    torch.cuda.set_device(device)
+    config_bk = workload_config()
+    table = solve_bk(MV(qs0sqr=QS0SQR), 16.0, config_bk, device=device, dtype=torch.float64, seed=0)
+    dipole = BKDipole(table)
+    Q2 = torch.logspace(math.log10(DIS_Q2[0]), math.log10(DIS_Q2[1]), DIS_Q2[2], dtype=torch.float64)
+    xs = torch.logspace(math.log10(DIS_X[0]), math.log10(DIS_X[1]), DIS_X[2], dtype=torch.float64)
+    Qg, Xg = torch.meshgrid(Q2, xs, indexing="ij")
+    Qg, Xg = Qg.reshape(-1), Xg.reshape(-1)
+    if args.dis_points:
+        Qg, Xg = Qg[: args.dis_points], Xg[: args.dis_points]
+    area = DIS_SIGMA0_HALF_MB * MB_TO_GEV2
+
+    def cfg(precision):
+        return DISConfig(order=DISOrder.NLO, quarks=(Quark(QuarkType.LIGHT, 0.14),), transverse_area=area,
+                         vegas_bins=DIS_BINS, precision=precision)
+
+    opts = dict(vegas_samples=DIS_SAMPLES, vegas_iterations=DIS_ITERATIONS, vegas_min_iterations=DIS_ITERATIONS)
+    # warm-up (compiles nothing; touches every kernel once)
+    structure_functions(Qg[:2], Xg[:2], dipole, cfg("mixed"), sqrt_s=DIS_SQRT_S, seed=0,
+                        vegas_samples=4096, vegas_iterations=2)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    batch = structure_functions(Qg, Xg, dipole, cfg("mixed"), sqrt_s=DIS_SQRT_S, seed=0, **opts)
+    stop.record()
+    torch.cuda.synchronize()
+    batch_s = start.elapsed_time(stop) / 1e3
+    wall_s = time.perf_counter() - t0
+    single_n = min(args.dis_single, Qg.numel())
+    t1 = time.perf_counter()
+    singles = []
+    for i in range(single_n):
+        r = sigma_r(Qg[i].to(device), Xg[i].to(device), dipole, cfg("mixed"), sqrt_s=DIS_SQRT_S, seed=0, **opts)
+        singles.append(float(r.value))
+    torch.cuda.synchronize()
+    single_s = (time.perf_counter() - t1) / max(single_n, 1)
+    # FP64 build on the first points with the same Sobol points and seeds
+    check_n = min(args.dis_check, Qg.numel())
+    fp64 = structure_functions(Qg[:check_n], Xg[:check_n], dipole, cfg("fp64"), sqrt_s=DIS_SQRT_S, seed=0, **opts)
+    rel = (batch["sigma_r"][:check_n] - fp64["sigma_r"]).abs() / fp64["sigma_r"].abs()
+    same = max(abs(singles[i] / float(batch["sigma_r"][i]) - 1) for i in range(single_n)) if single_n else None
+    line = {
+        "metric": "DIS sigma_r points/s (NLO, batched)",
+        "value": round(Qg.numel() / batch_s, 3),
+        "unit": "points/s",
+        "n_gpus": 1,
+        "higher_is_better": True,
+        "dtype": "f32+f64",
+        "data": "synthetic: BK table evolved from the MV initial condition on the device",
+        "config": {"workload": "NLO DIS sigma_r: 32 Q^2 in [1,50] x 16 x in [1e-5,1e-2], sqrt(s)=318, light quarks "
+                               "m=0.14, sigma0/2=16 mb, Vegas 50 bins x 10 it x 2^18, seed 0",
+                   "points": Qg.numel(), "integrals_per_point": 10},
+        "batched_s": round(batch_s, 4),
+        "batched_wall_s": round(wall_s, 4),
+        "single_point_s": round(single_s, 4),
+        "single_points_timed": single_n,
+        "speedup_batched_vs_single": round(single_s / (batch_s / Qg.numel()), 3),
+        "mixed_vs_fp64_max_rel": float(rel.max()) if check_n else None,
+        "single_vs_batched_max_rel": same,
+        "sigma_r_sample": [float(v) for v in batch["sigma_r"][:4]],
+        "sigma_r_error_sample": [float(v) for v in batch["sigma_r_error"][:4]],
+    }
+    print(json.dumps(line))
+
+
 def main() -> None:
     parser = argparse.ArgumentParser()
     parser.add_argument("--gpus", type=int, default=1)
@@ -443,7 +532,15 @@ def main() -> None:
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--kernel-case", action="store_true",
                         help="run only the small K2+Kf/K1 case used for ncu captures")
+    parser.add_argument("--workload", choices=["bk", "dis"], default="bk",
+                        help="bk: the NLO BK evolution (default); dis: NLO DIS sigma_r throughput")
+    parser.add_argument("--dis-points", type=int, default=0, help="DIS: first N of the 512 points (0 = all)")
+    parser.add_argument("--dis-single", type=int, default=4, help="DIS: points timed through single sigma_r calls")
+    parser.add_argument("--dis-check", type=int, default=4, help="DIS: points recomputed in FP64")
     args = parser.parse_args()
+    if args.workload == "dis":
+        run_dis(args)
+        return
     if args.kernel_case:
         run_kernel_case()
         return

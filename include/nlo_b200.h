@@ -153,6 +153,124 @@ int nlo_bk_evolve(const nlo_bk_params* params, const double* r, int32_t points, 
                   int32_t stepper, const nlo_sobol_dirs* dirs, int64_t samples, const nlo_bk_box* box,
                   double* table, uint32_t* status, void* workspace, size_t workspace_bytes, void* stream);
 
+/* ======================================================================== NLO DIS
+ * The NLO DIS cross-section integrands (dis/observables.py, dis/lo.py, dis/transverse.py,
+ * dis/longitudinal.py) with the GBW or BK-table dipole, their tensor Gauss-Legendre rule and
+ * the device Vegas integrator.  One "job" is one integral: a (Q^2, x_Bj) point, a quark, a
+ * polarisation and one term. */
+
+/* Integrand terms (the `contribution` strings of dis/observables.py:107-331). */
+#define NLO_DIS_TERM_LO 0   /* LO |Psi|^2 N 2 pi r maxr over (z, r/maxr), all LO quarks; dis/observables.py:352-359 */
+#define NLO_DIS_TERM_DIP0 1 /* T0 / Omega_L_const, 2D; dis/observables.py:107-172 */
+#define NLO_DIS_TERM_DIP1 2 /* T1 / ab, 3D */
+#define NLO_DIS_TERM_DIP2 3 /* T2 / cd, 4D */
+#define NLO_DIS_TERM_I1 4   /* qqbar-g I1, 5D; dis/observables.py:175-250 */
+#define NLO_DIS_TERM_I2 5   /* qqbar-g I2 with y_t explicit, 6D */
+#define NLO_DIS_TERM_I3 6   /* qqbar-g I3 with y_t1, y_t2 explicit, 7D */
+#define NLO_DIS_TERM_I2_NESTED 7 /* I2 with the inner rule, 5D; dis/observables.py:253-331 */
+#define NLO_DIS_TERM_I3_NESTED 8 /* I3 with the inner rule, 5D */
+
+#define NLO_DIPOLE_GBW 0   /* dipole/amplitude.py:23-45 */
+#define NLO_DIPOLE_TABLE 1 /* BKDipole, dipole/amplitude.py:48-252 */
+
+#define NLO_DIS_MAX_QUARKS 8
+
+/* Physics of one job: DISConfig (dis/config.py:103-145), the kinematic point and the quark. */
+typedef struct nlo_dis_kinematics {
+    double Q2;
+    double xbj;
+    double mf;                  /* quark mass of the dipole and qqbar-g terms */
+    int32_t n_quarks;           /* LO term: sum over these quarks */
+    double lo_mass[NLO_DIS_MAX_QUARKS];
+    double lo_charge2[NLO_DIS_MAX_QUARKS];
+    double maxr;                /* DISConfig.maxr */
+    int32_t transverse;         /* 1: Polarization.T, 0: Polarization.L */
+    int32_t finite_nc;          /* NcScheme.FiniteNC */
+    int32_t parent_coupling;    /* RunningCouplingScheme.PARENT (else SMALLEST) */
+    int32_t smooth_coupling;    /* RunningCouplingIRScheme.SMOOTH (else FREEZE) */
+    int32_t mass_dependent_x;   /* HeavyQuarkX.MassDependentX */
+    double c2_alpha;            /* DISConfig.C2_alpha */
+    double active_flavors;      /* DISConfig.active_flavors */
+    double max_alpha;           /* DISConfig.max_alpha_s_freeze */
+} nlo_dis_kinematics;
+
+/* The dipole amplitude: GBW parameters, or a BK table prepared by nlo_dis_table_prepare. */
+typedef struct nlo_dipole {
+    int32_t kind;               /* NLO_DIPOLE_* */
+    double qs0sqr, lambda, gamma, x0;  /* GBW(Qs0sqr, lambda_, gamma, x0) */
+    const double* table;        /* NLO_DIPOLE_TABLE: device buffer of nlo_dis_table_doubles(nr, ny) */
+    int32_t nr, ny;
+} nlo_dipole;
+
+/* Size in doubles of a prepared BK table with nr r points and ny rapidities. */
+size_t nlo_dis_table_doubles(int32_t nr, int32_t ny);
+
+/* Prepare a BK table for the device amplitude (BKDipole.__init__, dipole/amplitude.py:48-83):
+ * r: device double[nr] (logarithmic, increasing, nr >= 9), y: device double[ny] (increasing),
+ * N: device double[ny*nr] (row y), x0: DipoleTable.x0; table: device double[nlo_dis_table_doubles].
+ * The rapidities are stored as y + max(0, ln(1/x0)) like BKDipole.Y. */
+int nlo_dis_table_prepare(const double* r, const double* y, const double* N, int32_t nr, int32_t ny, double x0,
+                          double* table, void* stream);
+
+/* BKDipole.initialize_interpolation(Y) (dipole/amplitude.py:105-133, 254-272): fit the global
+ * spline at rapidity Y, which later evaluations at a matching Y use, and find maxr_interpolate.
+ * The caller checks 0 <= Y <= max rapidity of the table (the reference raises ValueError). */
+int nlo_dis_table_initialize(double* table, int32_t nr, int32_t ny, double Y, void* stream);
+
+/* dipole_amplitude(r, Y) of GBW (dipole/amplitude.py:37-42) or BKDipole (:135-170) at n points:
+ * r, Y, out: device double[n].  A BK table answers from its initialised global spline where Y
+ * matches the initialisation rapidity, from the local splines elsewhere. */
+int nlo_dis_dipole_amplitude(const nlo_dipole* dipole, const double* r, const double* Y, int64_t n, int32_t precision,
+                             double* out, void* stream);
+
+/* Evaluate one term at n unit-cube points (the reference's integrand_* functions and the
+ * dis_lo_integrand / dis_dipole_integrand operators, custom_kernels/dis/lo_dipole/kernel.cu):
+ * x: device double[n*dims(term)], out: device double[n].  inner_points: the inner rule of the
+ * nested terms (8..128, 48 in the reference).  precision: NLO_PRECISION_*. */
+int nlo_dis_integrand(const nlo_dis_kinematics* kin, int32_t term, const nlo_dipole* dipole, int32_t inner_points,
+                      int32_t precision, const double* x, int64_t n, double* out, void* stream);
+
+/* Tensor Gauss-Legendre integral of a 2D term (LO or DIP0) on the unit square for `jobs`
+ * kinematic points at once: out[2*j] = value with `points` nodes per axis, out[2*j+1] =
+ * |value - value with points/2 nodes| (numerics/integration.py:94-117,
+ * custom_kernels/quadrature.py:38-55).  kin: host array [jobs]; out: device double[2*jobs]. */
+int nlo_dis_gauss_legendre(const nlo_dis_kinematics* kin, int32_t jobs, int32_t term, const nlo_dipole* dipole,
+                           int32_t points, int32_t precision, double* out, void* workspace, size_t workspace_bytes,
+                           void* stream);
+size_t nlo_dis_gauss_legendre_workspace_bytes(int32_t jobs);
+
+/* Vegas options (numerics/integration.py:120-138). */
+typedef struct nlo_vegas_options {
+    int32_t bins;               /* bins per dimension (<= 256) */
+    int32_t max_iterations;
+    int32_t min_iterations;
+    int64_t samples_per_iteration;
+    int64_t warmup_samples;     /* 0 or >= 2: one extra adaptation-only round first */
+    double epsrel, epsabs;
+    int32_t inner_points;       /* nested terms */
+    int32_t precision;          /* NLO_PRECISION_* */
+    int32_t keep_edges;         /* 1: start from the edges already in `state` (VegasState reuse) */
+} nlo_vegas_options;
+
+/* Per-job Vegas state in doubles: edges[dims][bins+1], then value, error, n_eval, iterations,
+ * converged at offsets NLO_VEGAS_VALUE.. from the end of the edges. */
+#define NLO_VEGAS_VALUE 2
+#define NLO_VEGAS_ERROR 3
+#define NLO_VEGAS_EVALS 4
+#define NLO_VEGAS_ITERATIONS 5
+#define NLO_VEGAS_CONVERGED 6
+size_t nlo_dis_vegas_state_doubles(int32_t term, int32_t bins);
+size_t nlo_dis_vegas_workspace_bytes(int32_t jobs, int32_t term, const nlo_vegas_options* options);
+
+/* Vegas integration of one term for `jobs` kinematic points at once, all iterations on the
+ * device without host synchronisation (vegas, numerics/integration.py:120-589, with the grid
+ * re-binning of :804-866).  Samples are the scrambled Sobol points of dirs[j] (indices
+ * 0, 1, ... across the rounds), split into a bin and a fraction per dimension.
+ * kin, dirs: host arrays [jobs]; state: device double[jobs * nlo_dis_vegas_state_doubles]. */
+int nlo_dis_vegas(const nlo_dis_kinematics* kin, int32_t jobs, int32_t term, const nlo_dipole* dipole,
+                  const nlo_vegas_options* options, const nlo_sobol_dirs* dirs, double* state, void* workspace,
+                  size_t workspace_bytes, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

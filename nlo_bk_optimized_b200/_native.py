@@ -52,6 +52,63 @@ class Box(ctypes.Structure):
     _fields_ = [("lower", ctypes.c_double * 4), ("width", ctypes.c_double * 4)]
 
 
+MAX_QUARKS = 8
+
+DIS_TERMS = {"LO": 0, "DIP0": 1, "DIP1": 2, "DIP2": 3, "I1": 4, "I2": 5, "I3": 6, "I2N": 7, "I3N": 8}
+DIS_DIMS = {0: 2, 1: 2, 2: 3, 3: 4, 4: 5, 5: 6, 6: 7, 7: 5, 8: 5}
+DIPOLE_GBW = 0
+DIPOLE_TABLE = 1
+VEGAS_VALUE, VEGAS_ERROR, VEGAS_EVALS, VEGAS_ITERATIONS, VEGAS_CONVERGED = 2, 3, 4, 5, 6
+
+
+class DisKinematics(ctypes.Structure):
+    _fields_ = [
+        ("Q2", ctypes.c_double),
+        ("xbj", ctypes.c_double),
+        ("mf", ctypes.c_double),
+        ("n_quarks", ctypes.c_int32),
+        ("lo_mass", ctypes.c_double * MAX_QUARKS),
+        ("lo_charge2", ctypes.c_double * MAX_QUARKS),
+        ("maxr", ctypes.c_double),
+        ("transverse", ctypes.c_int32),
+        ("finite_nc", ctypes.c_int32),
+        ("parent_coupling", ctypes.c_int32),
+        ("smooth_coupling", ctypes.c_int32),
+        ("mass_dependent_x", ctypes.c_int32),
+        ("c2_alpha", ctypes.c_double),
+        ("active_flavors", ctypes.c_double),
+        ("max_alpha", ctypes.c_double),
+    ]
+
+
+class Dipole(ctypes.Structure):
+    _fields_ = [
+        ("kind", ctypes.c_int32),
+        ("qs0sqr", ctypes.c_double),
+        ("lambda_", ctypes.c_double),
+        ("gamma", ctypes.c_double),
+        ("x0", ctypes.c_double),
+        ("table", ctypes.c_void_p),
+        ("nr", ctypes.c_int32),
+        ("ny", ctypes.c_int32),
+    ]
+
+
+class VegasOptions(ctypes.Structure):
+    _fields_ = [
+        ("bins", ctypes.c_int32),
+        ("max_iterations", ctypes.c_int32),
+        ("min_iterations", ctypes.c_int32),
+        ("samples_per_iteration", ctypes.c_int64),
+        ("warmup_samples", ctypes.c_int64),
+        ("epsrel", ctypes.c_double),
+        ("epsabs", ctypes.c_double),
+        ("inner_points", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+        ("keep_edges", ctypes.c_int32),
+    ]
+
+
 EXPORTED = (
     "nlo_last_error",
     "nlo_abi_version",
@@ -66,6 +123,16 @@ EXPORTED = (
     "nlo_bk_rhs_workspace_bytes",
     "nlo_bk_rhs",
     "nlo_bk_evolve",
+    "nlo_dis_table_doubles",
+    "nlo_dis_table_prepare",
+    "nlo_dis_table_initialize",
+    "nlo_dis_dipole_amplitude",
+    "nlo_dis_integrand",
+    "nlo_dis_gauss_legendre_workspace_bytes",
+    "nlo_dis_gauss_legendre",
+    "nlo_dis_vegas_state_doubles",
+    "nlo_dis_vegas_workspace_bytes",
+    "nlo_dis_vegas",
 )
 
 _lock = threading.Lock()
@@ -101,6 +168,26 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.nlo_bk_rhs.argtypes = [P(BKParams), vp, vp, i32, P(SobolDirs), i64, P(Box), vp, vp, vp, vp, sz, vp]
     lib.nlo_bk_evolve.restype = ctypes.c_int
     lib.nlo_bk_evolve.argtypes = [P(BKParams), vp, i32, i32, d, i32, P(SobolDirs), i64, P(Box), vp, vp, vp, sz, vp]
+    lib.nlo_dis_table_doubles.restype = sz
+    lib.nlo_dis_table_doubles.argtypes = [i32, i32]
+    lib.nlo_dis_table_prepare.restype = ctypes.c_int
+    lib.nlo_dis_table_prepare.argtypes = [vp, vp, vp, i32, i32, d, vp, vp]
+    lib.nlo_dis_table_initialize.restype = ctypes.c_int
+    lib.nlo_dis_table_initialize.argtypes = [vp, i32, i32, d, vp]
+    lib.nlo_dis_dipole_amplitude.restype = ctypes.c_int
+    lib.nlo_dis_dipole_amplitude.argtypes = [P(Dipole), vp, vp, i64, i32, vp, vp]
+    lib.nlo_dis_integrand.restype = ctypes.c_int
+    lib.nlo_dis_integrand.argtypes = [P(DisKinematics), i32, P(Dipole), i32, i32, vp, i64, vp, vp]
+    lib.nlo_dis_gauss_legendre_workspace_bytes.restype = sz
+    lib.nlo_dis_gauss_legendre_workspace_bytes.argtypes = [i32]
+    lib.nlo_dis_gauss_legendre.restype = ctypes.c_int
+    lib.nlo_dis_gauss_legendre.argtypes = [P(DisKinematics), i32, i32, P(Dipole), i32, i32, vp, vp, sz, vp]
+    lib.nlo_dis_vegas_state_doubles.restype = sz
+    lib.nlo_dis_vegas_state_doubles.argtypes = [i32, i32]
+    lib.nlo_dis_vegas_workspace_bytes.restype = sz
+    lib.nlo_dis_vegas_workspace_bytes.argtypes = [i32, i32, P(VegasOptions)]
+    lib.nlo_dis_vegas.restype = ctypes.c_int
+    lib.nlo_dis_vegas.argtypes = [P(DisKinematics), i32, i32, P(Dipole), P(VegasOptions), P(SobolDirs), vp, vp, sz, vp]
 
 
 def load(path: Path | None = None) -> ctypes.CDLL:

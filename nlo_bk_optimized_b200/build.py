@@ -11,6 +11,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PACKAGE = Path(__file__).resolve().parent
@@ -42,11 +43,7 @@ def _stale() -> bool:
     return any(path.stat().st_mtime > built for path in inputs)
 
 
-def build(force: bool = False, verbose: bool = False) -> Path:
-    if not force and not _stale():
-        return LIBRARY
-    LIBDIR.mkdir(parents=True, exist_ok=True)
-    tmp = LIBRARY.with_suffix(".so.tmp")
+def _compile(source: Path, obj: Path, verbose: bool) -> tuple[int, str]:
     command = [
         _nvcc(),
         *ARCH_FLAGS,
@@ -55,21 +52,45 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         "-std=c++17",
         "-Xcompiler",
         "-fPIC",
-        "-shared",
         "--expt-relaxed-constexpr",
+        "-c",
+        str(source),
         "-o",
-        str(tmp),
-        *[str(s) for s in sources()],
-        "-lcudart",
+        str(obj),
     ]
     if verbose or os.environ.get("NLO_PTXAS_VERBOSE"):
         command.insert(1, "-Xptxas=-v")
     result = subprocess.run(command, capture_output=True, text=True)
+    return result.returncode, result.stdout + result.stderr
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    """Compile every csrc/*.cu for sm_100a (in parallel, one nvcc per file) and link
+    libnlo_b200.so."""
+    if not force and not _stale():
+        return LIBRARY
+    LIBDIR.mkdir(parents=True, exist_ok=True)
+    objdir = PACKAGE / "_build"
+    objdir.mkdir(parents=True, exist_ok=True)
+    srcs = sources()
+    objs = [objdir / (src.stem + ".o") for src in srcs]
+    workers = max(1, min(len(srcs), os.cpu_count() or 1))
+    with ThreadPoolExecutor(max_workers=workers) as pool:
+        results = list(pool.map(lambda pair: _compile(pair[0], pair[1], verbose), zip(srcs, objs)))
+    failed = [(src, out) for src, (code, out) in zip(srcs, results) if code != 0]
+    if verbose:
+        for src, (_, out) in zip(srcs, results):
+            sys.stderr.write(f"== {src.name}\n{out}")
+    if failed:
+        for src, out in failed:
+            sys.stderr.write(f"== {src.name}\n{out}")
+        raise RuntimeError("nvcc failed to build libnlo_b200.so")
+    tmp = LIBRARY.with_suffix(".so.tmp")
+    link = [_nvcc(), *ARCH_FLAGS, "-shared", "-o", str(tmp), *[str(o) for o in objs], "-lcudart"]
+    result = subprocess.run(link, capture_output=True, text=True)
     if result.returncode != 0:
         sys.stderr.write(result.stdout + result.stderr)
-        raise RuntimeError("nvcc failed to build libnlo_b200.so")
-    if verbose:
-        sys.stderr.write(result.stdout + result.stderr)
+        raise RuntimeError("nvcc failed to link libnlo_b200.so")
     tmp.replace(LIBRARY)
     return LIBRARY
 

@@ -167,6 +167,8 @@ const K1Rule& k1_rule()
 
 int set_last_error(int code, const char* message) { return fail(code, message); }
 
+void gauss_legendre_rule(int n, double* x, double* w) { gauss_legendre(n, x, w); }
+
 size_t spline_doubles(int points) { return (size_t)points + 8 * (size_t)(points - 1); }
 
 // buffer size a caller provides to nlo_bk_splines: coefficients plus factorisation scratch

@@ -1,0 +1,298 @@
+"""Parity of the device DIS path with the reference (golden vectors) and the oracle.
+
+FP64 build: pointwise 1e-10 relative (floor 1e-10 of the largest value of the sample set),
+Vegas value/error/grid 1e-10 against the oracle's Vegas on the same Sobol points.
+Mixed build (FP32 integrands): sums over the sample sets within 1e-4 relative of FP64.
+"""
+
+from __future__ import annotations
+
+import math
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import dis as od
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = np.load(Path(__file__).parent / "golden" / "dis_reference.npz")
+CASES = [str(c) for c in GOLDEN["cases"]]
+FP64_TOL = 1e-10
+MIXED_SUM_TOL = 1e-4
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from nlo_bk_optimized_b200 import _native
+
+    return _native.load()
+
+
+def dev(a):
+    return torch.as_tensor(np.asarray(a), dtype=torch.float64, device="cuda")
+
+
+def table_obj():
+    from nlo_bk_optimized_b200.dipole import BKDipole, DipoleTable
+
+    t = DipoleTable(dev(GOLDEN["table_r"]), dev(GOLDEN["table_y"]), dev(GOLDEN["table_N"]), 1.0)
+    return BKDipole(t)
+
+
+def gbw_obj():
+    from nlo_bk_optimized_b200.dipole import GBW
+
+    q, lam, g, x0 = GOLDEN["gbw_params"]
+    return GBW(Qs0sqr=float(q), lambda_=float(lam), gamma=float(g), x0=float(x0))
+
+
+def config_of(name):
+    from nlo_bk_optimized_b200.dis import (
+        DISConfig,
+        NcScheme,
+        Quark,
+        QuarkType,
+        RunningCouplingIRScheme,
+        RunningCouplingScheme,
+    )
+
+    k = GOLDEN[f"{name}/kin"]
+    quark = Quark(QuarkType.C if k[2] > 1 else QuarkType.LIGHT, float(k[2]))
+    config = DISConfig(
+        quarks=(quark,), maxr=float(k[5]),
+        nc_scheme=NcScheme.FiniteNC if k[6] else NcScheme.LargeNC,
+        rc_scheme=RunningCouplingScheme.PARENT if k[7] else RunningCouplingScheme.SMALLEST,
+        rc_ir_scheme=RunningCouplingIRScheme.SMOOTH if k[8] else RunningCouplingIRScheme.FREEZE,
+        C2_alpha=float(k[9]), max_alpha_s_freeze=float(k[11]))
+    return config, quark, float(k[0]), float(k[1]), bool(k[4])
+
+
+def oracle_kin(name):
+    k = GOLDEN[f"{name}/kin"]
+    return od.Kinematics(Q2=k[0], xbj=k[1], mf=k[2], transverse=bool(k[4]), maxr=k[5], finite_nc=bool(k[6]),
+                         parent_coupling=bool(k[7]), smooth_coupling=bool(k[8]), c2_alpha=k[9],
+                         active_flavors=int(k[10]), max_alpha=k[11])
+
+
+def oracle_dipole(name):
+    if name.endswith("bk") or "_bk_" in name:
+        return od.TableDipole(GOLDEN["table_r"], GOLDEN["table_y"], GOLDEN["table_N"])
+    q, lam, g, x0 = GOLDEN["gbw_params"]
+    return od.GBWDipole(qs0sqr=q, lam=lam, gamma=g, x0=x0)
+
+
+def device_dipole(name):
+    return table_obj() if name.endswith("bk") or "_bk_" in name else gbw_obj()
+
+
+def rel_err(got, ref):
+    got = np.asarray(got)
+    ref = np.asarray(ref)
+    floor = FP64_TOL * max(np.max(np.abs(ref)), 1e-300)
+    return float(np.max(np.abs(got - ref) / np.maximum(np.abs(ref), floor)))
+
+
+def pol_of(transverse):
+    from nlo_bk_optimized_b200.dis import Polarization
+
+    return Polarization.T if transverse else Polarization.L
+
+
+def evaluate(term, x, name, precision):
+    from nlo_bk_optimized_b200 import _native
+    from nlo_bk_optimized_b200.dis.observables import _integrand, kinematics
+
+    config, quark, Q2, xbj, transverse = config_of(name)
+    kin = kinematics(Q2, xbj, pol_of(transverse), config, None if term == "LO" else quark)
+    dipole = device_dipole(name)
+    if term == "LO":
+        dipole_init = dipole
+        if hasattr(dipole_init, "initialize_interpolation"):
+            dipole_init.initialize_interpolation(max(math.log(dipole.X0() / xbj), 0.0))
+    return _integrand(_native.DIS_TERMS[term], dev(x), kin, dipole, config, precision=precision).cpu().numpy()
+
+
+# ----------------------------------------------------------------------------- amplitudes
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_amplitudes(dtype):
+    r, Y = dev(GOLDEN["amp_r"]), dev(GOLDEN["amp_Y"])
+    tol = FP64_TOL if dtype == torch.float64 else 2e-5
+    gbw = gbw_obj().dipole_amplitude(r.to(dtype), Y.to(dtype)).double().cpu().numpy()
+    # 1 - exp(-a) in the reference loses ~1e-16 absolute for small a: allow that absolute slack
+    slack = 4e-16 if dtype == torch.float64 else 1e-9
+    assert np.all(np.abs(gbw - GOLDEN["gbw"]) <= tol * np.abs(GOLDEN["gbw"]) + slack)
+    tab = table_obj()
+    local = tab.dipole_amplitude(r, Y).cpu().numpy()
+    assert rel_err(local, GOLDEN["amp_local"]) < 1e-12
+    tab.initialize_interpolation(float(GOLDEN["amp_init_Y"][0]))
+    assert tab.maxr_interpolate == pytest.approx(float(GOLDEN["amp_init_maxr"][0]), rel=1e-12)
+    init = tab.dipole_amplitude(r, torch.full_like(r, float(GOLDEN["amp_init_Y"][0]))).cpu().numpy()
+    assert rel_err(init, GOLDEN["amp_init"]) < 1e-12
+
+
+# ----------------------------------------------------------------------------- integrands vs golden
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_lo_integrand(name):
+    from nlo_bk_optimized_b200 import _native
+
+    got = evaluate("LO", GOLDEN[f"{name}/lo_x"], name, _native.PRECISION_FP64)
+    # the golden LO values carry the case's single quark with charge^2 of its type
+    assert rel_err(got, GOLDEN[f"{name}/lo"]) < FP64_TOL
+    mixed = evaluate("LO", GOLDEN[f"{name}/lo_x"], name, _native.PRECISION_MIXED)
+    assert abs(mixed.sum() / got.sum() - 1) < MIXED_SUM_TOL
+
+
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("order", [0, 1, 2])
+def test_dipole_terms(name, order):
+    from nlo_bk_optimized_b200 import _native
+
+    x = GOLDEN[f"{name}/dip{order}_x"]
+    ref = GOLDEN[f"{name}/dip{order}"]
+    got = evaluate(f"DIP{order}", x, name, _native.PRECISION_FP64)
+    assert rel_err(got, ref) < 1e-9
+    mixed = evaluate(f"DIP{order}", x, name, _native.PRECISION_MIXED)
+    assert abs(mixed.sum() / got.sum() - 1) < MIXED_SUM_TOL
+
+
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("term", ["I1", "I2", "I3"])
+def test_qg_terms(name, term):
+    from nlo_bk_optimized_b200 import _native
+
+    x = GOLDEN[f"{name}/qg_{term}_x"]
+    ref = GOLDEN[f"{name}/qg_{term}"]
+    got = evaluate(term, x, name, _native.PRECISION_FP64)
+    assert rel_err(got, ref) < 1e-9
+    mixed = evaluate(term, x, name, _native.PRECISION_MIXED)
+    assert abs(mixed.sum() / got.sum() - 1) < MIXED_SUM_TOL
+
+
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("term", ["I2N", "I3N"])
+def test_nested_terms_vs_oracle(name, term):
+    from nlo_bk_optimized_b200 import _native
+
+    x = np.random.default_rng(11).uniform(0, 1, (128, 5))
+    ref = od.qg_integrand(x, oracle_kin(name), {"I2N": "I2n", "I3N": "I3n"}[term], oracle_dipole(name))
+    got = evaluate(term, x, name, _native.PRECISION_FP64)
+    assert rel_err(got, ref) < 1e-9
+    mixed = evaluate(term, x, name, _native.PRECISION_MIXED)
+    assert abs(mixed.sum() / got.sum() - 1) < MIXED_SUM_TOL
+
+
+# ----------------------------------------------------------------------------- integrals
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_sigma_lo_gauss_legendre(name):
+    from nlo_bk_optimized_b200.dis import DISConfig, photon_proton_cross_section_LO_d2b
+
+    config, quark, Q2, xbj, transverse = config_of(name)
+    config = DISConfig(**{**{f: getattr(config, f) for f in config.__dataclass_fields__}, "precision": "fp64"})
+    res = photon_proton_cross_section_LO_d2b(torch.tensor(Q2, dtype=torch.float64, device="cuda"),
+                                             torch.tensor(xbj, dtype=torch.float64, device="cuda"),
+                                             pol_of(transverse), device_dipole(name), config)
+    assert float(res.value) == pytest.approx(float(GOLDEN[f"{name}/sigma_lo"][0]), rel=1e-11)
+    assert float(res.error) == pytest.approx(float(GOLDEN[f"{name}/sigma_lo"][1]), rel=1e-6, abs=1e-14)
+
+
+@pytest.mark.parametrize("kind", ["gbw", "bk"])
+def test_lo_structure_functions(kind):
+    from nlo_bk_optimized_b200.dis import F2, FL, FT, DISConfig, Quark, QuarkType
+
+    config = DISConfig(quarks=(Quark(QuarkType.LIGHT, 0.14), Quark(QuarkType.C, 1.4)), precision="fp64")
+    dip = gbw_obj() if kind == "gbw" else table_obj()
+    Q2 = torch.tensor(7.5, dtype=torch.float64, device="cuda")
+    xbj = torch.tensor(2e-4, dtype=torch.float64, device="cuda")
+    ref = GOLDEN[f"lo_sf_{kind}"]
+    assert float(FT(Q2, xbj, dip, config).value) == pytest.approx(ref[0], rel=1e-11)
+    assert float(FL(Q2, xbj, dip, config).value) == pytest.approx(ref[1], rel=1e-11)
+    assert float(F2(Q2, xbj, dip, config).value) == pytest.approx(ref[2], rel=1e-11)
+    mixed = DISConfig(quarks=config.quarks)
+    assert float(F2(Q2, xbj, dip, mixed).value) == pytest.approx(ref[2], rel=MIXED_SUM_TOL)
+
+
+def sobol_points(dims, seed, n):
+    return torch.quasirandom.SobolEngine(dims, scramble=True, seed=seed).draw(n, dtype=torch.float64).numpy()
+
+
+@pytest.mark.parametrize("term,order,name", [("DIP1", 1, "light_T_bk"), ("DIP2", 2, "charm_L_gbw"),
+                                             ("I1", None, "light_T_bk"), ("I3N", None, "light_L_bk")])
+def test_vegas_matches_oracle(term, order, name):
+    """Device Vegas (FP64) vs the oracle's Vegas driver on the same Sobol points."""
+    from nlo_bk_optimized_b200 import _native
+    from nlo_bk_optimized_b200.dis.observables import kinematics
+    from nlo_bk_optimized_b200.numerics.integration import VegasOptions, state_results, vegas_terms
+
+    config, quark, Q2, xbj, transverse = config_of(name)
+    dims = _native.DIS_DIMS[_native.DIS_TERMS[term]]
+    n, iters, bins, seed = 2048 if term == "I3N" else 8192, 3, 50, 5
+    opts = VegasOptions(samples_per_iteration=n, max_iterations=iters, min_iterations=iters, bins=bins,
+                        epsrel=1e-12, inner_points=48)
+    kin = kinematics(Q2, xbj, pol_of(transverse), config, quark)
+    dip = device_dipole(name)
+    state = vegas_terms(_native.DIS_TERMS[term], [kin], dip.native(), opts, [seed],
+                        precision=_native.PRECISION_FP64, device=torch.device("cuda"))
+    res = state_results(state, _native.DIS_TERMS[term], bins)
+    pts = sobol_points(dims, seed, n * iters)
+    okin, odip = oracle_kin(name), oracle_dipole(name)
+    if order is not None:
+        f = lambda u: od.dip_integrand(u, okin, order, odip)  # noqa: E731
+    else:
+        f = lambda u: od.qg_integrand(u, okin, term, odip)  # noqa: E731
+    value, error, n_eval, converged, edges = od.vegas(
+        f, dims, lambda it, m: od.sobol_sampler(pts[it * m:(it + 1) * m], bins), samples=n, max_iterations=iters,
+        min_iterations=iters, bins=bins, epsrel=1e-12)
+    assert float(res["value"][0]) == pytest.approx(value, rel=1e-10)
+    assert float(res["error"][0]) == pytest.approx(error, rel=1e-8)
+    assert int(res["n_eval"][0]) == n_eval
+    assert np.max(np.abs(res["edges"][0].cpu().numpy() - edges)) < 1e-10
+    # mixed precision: one iteration on the uniform grid against the FP64 value
+    one = VegasOptions(samples_per_iteration=n, max_iterations=1, min_iterations=1, bins=bins, epsrel=1e-12)
+    vals = []
+    for precision in (_native.PRECISION_FP64, _native.PRECISION_MIXED):
+        st = vegas_terms(_native.DIS_TERMS[term], [kin], dip.native(), one, [seed], precision=precision,
+                         device=torch.device("cuda"))
+        vals.append(float(state_results(st, _native.DIS_TERMS[term], bins)["value"][0]))
+    assert vals[1] == pytest.approx(vals[0], rel=MIXED_SUM_TOL)
+
+
+def test_batch_matches_single_points():
+    """Every point of a batched structure-function run equals the same point run alone
+    (the batch changes only the CTA split of each integral's sums)."""
+    from nlo_bk_optimized_b200.dis import F2, DISConfig, DISOrder, Quark, QuarkType, structure_functions
+
+    config = DISConfig(order=DISOrder.NLO, quarks=(Quark(QuarkType.LIGHT, 0.14),), maxeval=4096,
+                       precision="fp64")
+    dip = gbw_obj()
+    Q2s = torch.tensor([2.0, 10.0, 40.0], dtype=torch.float64)
+    xs = torch.tensor([1e-3, 3e-4, 1e-2], dtype=torch.float64)
+    batch = structure_functions(Q2s, xs, dip, config, seed=3)
+    for i in range(3):
+        alone = F2(Q2s[i].cuda(), xs[i].cuda(), dip, config, seed=3)
+        assert float(batch["F2"][i]) == pytest.approx(float(alone.value), rel=1e-12)
+        assert float(batch["F2_error"][i]) == pytest.approx(float(alone.error), rel=1e-9)
+
+
+def test_vegas_is_deterministic():
+    from nlo_bk_optimized_b200 import _native
+    from nlo_bk_optimized_b200.dis.observables import kinematics
+    from nlo_bk_optimized_b200.numerics.integration import VegasOptions, vegas_terms
+
+    config, quark, Q2, xbj, transverse = config_of("light_T_bk")
+    kin = kinematics(Q2, xbj, pol_of(transverse), config, quark)
+    dip = table_obj()
+    opts = VegasOptions(samples_per_iteration=1 << 14, max_iterations=4, min_iterations=4, bins=50, epsrel=1e-12)
+    a = vegas_terms(_native.DIS_TERMS["I1"], [kin], dip.native(), opts, [0], precision=_native.PRECISION_MIXED,
+                    device=torch.device("cuda"))
+    b = vegas_terms(_native.DIS_TERMS["I1"], [kin], dip.native(), opts, [0], precision=_native.PRECISION_MIXED,
+                    device=torch.device("cuda"))
+    assert torch.equal(a, b)

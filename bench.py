@@ -53,6 +53,9 @@ FLOPS_PER_EVAL = 181
 LAUNCHES_PER_STEP = 4 * 6 + 4
 SM_COUNT = 148
 FP32_LANES_PER_SM = 128
+# CPU baseline sample (about 10 s of host work): K2+Kf points per parent and K1 parents
+CPU_K2_LOG2 = 19
+CPU_K1_PARENTS = 128
 
 
 def workload_config():
@@ -313,6 +316,9 @@ def run_ours(args) -> None:
     }
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(final_N.cpu().numpy(), r_host.numpy())
+    if not args.no_dis and world == 1:
+        # the second half of the metric: NLO DIS sigma_r points/s on an evolved table
+        line["dis"] = measure_dis(args.dis_points, args.dis_single, args.dis_check)
     print(json.dumps(line))
 
 
@@ -349,14 +355,14 @@ def _oracle_rates(N, r, k2_samples: int, k1_parents: int) -> dict:
 def cpu_baseline(N, r) -> dict:
     import oracle
 
-    rates = _oracle_rates(N, r, k2_samples=1 << 15, k1_parents=64)
+    rates = _oracle_rates(N, r, k2_samples=1 << CPU_K2_LOG2, k1_parents=CPU_K1_PARENTS)
     stages = 4 * MAXY / STEP
     return {
         "value": round(rates["stage_s"] * stages, 1),
         "unit": UNIT,
         "cores": oracle.num_threads(),
         "kind": "port",
-        "sample": (f"oracle (C, OpenMP) K2+Kf on {rates['active']} parents x 2^15 Sobol points and K1 on "
+        "sample": (f"oracle (C, OpenMP) K2+Kf on {rates['active']} parents x 2^{CPU_K2_LOG2} Sobol points and K1 on "
                    f"{rates['k1_parents']} parents at the final state; extrapolated to 400 stages x 2^20 points "
                    f"({rates['elapsed']:.1f} s measured)"),
         "k2kf_evals_per_s": round(rates["k2kf_evals_per_s"], 1),
@@ -442,7 +448,33 @@ MB_TO_GEV2 = 2.56819
 DIS_BINS, DIS_ITERATIONS, DIS_SAMPLES = 50, 10, 1 << 18
 
 
-def run_dis(args) -> None:
+def run_dis_kernel_case() -> None:
+    """Small DIS case for ncu captures: one (Q^2, x) point with the GBW dipole, one Vegas
+    round of 2^16 Sobol points for each of the qqbar-g terms I1, I2 and I3 (nested, 48 inner
+    nodes) in the mixed build, twice."""
+    import torch
+
+    from nlo_bk_optimized_b200 import _native
+    from nlo_bk_optimized_b200.dipole import GBW
+    from nlo_bk_optimized_b200.dis import DISConfig, Polarization, Quark, QuarkType
+    from nlo_bk_optimized_b200.dis.observables import kinematics
+    from nlo_bk_optimized_b200.numerics.integration import VegasOptions, vegas_terms
+
+    device = torch.device("cuda", 0)
+    config = DISConfig(quarks=(Quark(QuarkType.LIGHT, 0.14),))
+    kin = kinematics(10.0, 1e-3, Polarization.T, config, config.quarks[0])
+    dip = GBW(Qs0sqr=0.25, lambda_=0.29, gamma=1.0, x0=0.01).native()
+    opts = VegasOptions(samples_per_iteration=1 << 16, max_iterations=1, min_iterations=1, bins=DIS_BINS,
+                        epsrel=1e-12)
+    for _ in range(2):
+        for term in ("I1", "I2N", "I3N"):
+            vegas_terms(_native.DIS_TERMS[term], [kin], dip, opts, [0], precision=_native.PRECISION_MIXED,
+                        device=device)
+    torch.cuda.synchronize()
+    print("dis kernel case done")
+
+
+def measure_dis(points: int = 0, single: int = 4, check: int = 4) -> dict:
     """NLO DIS reduced cross section on an evolved BK table: 32 Q^2 log-spaced in [1, 50] GeV^2
     x 16 x_Bj log-spaced in [1e-5, 1e-2], sqrt(s) = 318 GeV, light quarks (m = 0.14 GeV,
     sum of charges^2 = 2/3), sigma_0/2 = 16 mb, Vegas 50 bins x 10 iterations x 2^18, seed 0.
@@ -465,8 +497,8 @@ def run_dis(args) -> None:
     xs = torch.logspace(math.log10(DIS_X[0]), math.log10(DIS_X[1]), DIS_X[2], dtype=torch.float64)
     Qg, Xg = torch.meshgrid(Q2, xs, indexing="ij")
     Qg, Xg = Qg.reshape(-1), Xg.reshape(-1)
-    if args.dis_points:
-        Qg, Xg = Qg[: args.dis_points], Xg[: args.dis_points]
+    if points:
+        Qg, Xg = Qg[:points], Xg[:points]
     area = DIS_SIGMA0_HALF_MB * MB_TO_GEV2
 
     def cfg(precision):
@@ -486,7 +518,7 @@ def run_dis(args) -> None:
     torch.cuda.synchronize()
     batch_s = start.elapsed_time(stop) / 1e3
     wall_s = time.perf_counter() - t0
-    single_n = min(args.dis_single, Qg.numel())
+    single_n = min(single, Qg.numel())
     t1 = time.perf_counter()
     singles = []
     for i in range(single_n):
@@ -495,7 +527,7 @@ def run_dis(args) -> None:
     torch.cuda.synchronize()
     single_s = (time.perf_counter() - t1) / max(single_n, 1)
     # FP64 build on the first points with the same Sobol points and seeds
-    check_n = min(args.dis_check, Qg.numel())
+    check_n = min(check, Qg.numel())
     fp64 = structure_functions(Qg[:check_n], Xg[:check_n], dipole, cfg("fp64"), sqrt_s=DIS_SQRT_S, seed=0, **opts)
     rel = (batch["sigma_r"][:check_n] - fp64["sigma_r"]).abs() / fp64["sigma_r"].abs()
     same = max(abs(singles[i] / float(batch["sigma_r"][i]) - 1) for i in range(single_n)) if single_n else None
@@ -520,7 +552,11 @@ def run_dis(args) -> None:
         "sigma_r_sample": [float(v) for v in batch["sigma_r"][:4]],
         "sigma_r_error_sample": [float(v) for v in batch["sigma_r_error"][:4]],
     }
-    print(json.dumps(line))
+    return line
+
+
+def run_dis(args) -> None:
+    print(json.dumps(measure_dis(args.dis_points, args.dis_single, args.dis_check)))
 
 
 def main() -> None:
@@ -534,12 +570,16 @@ def main() -> None:
                         help="run only the small K2+Kf/K1 case used for ncu captures")
     parser.add_argument("--workload", choices=["bk", "dis"], default="bk",
                         help="bk: the NLO BK evolution (default); dis: NLO DIS sigma_r throughput")
+    parser.add_argument("--no-dis", action="store_true", help="skip the DIS sigma_r measurement")
     parser.add_argument("--dis-points", type=int, default=0, help="DIS: first N of the 512 points (0 = all)")
     parser.add_argument("--dis-single", type=int, default=4, help="DIS: points timed through single sigma_r calls")
     parser.add_argument("--dis-check", type=int, default=4, help="DIS: points recomputed in FP64")
     args = parser.parse_args()
     if args.workload == "dis":
-        run_dis(args)
+        if args.kernel_case:
+            run_dis_kernel_case()
+        else:
+            run_dis(args)
         return
     if args.kernel_case:
         run_kernel_case()

@@ -144,6 +144,20 @@ int nlo_bk_rhs(const nlo_bk_params* params, const double* r, const double* N, in
                const nlo_sobol_dirs* dirs, int64_t samples, const nlo_bk_box* box, double* dndy, double* k1,
                double* k2kf, void* workspace, size_t workspace_bytes, void* stream);
 
+/* The right-hand side of nlo_bk_rhs restricted to the parents i with i % shards == shard
+ * (the others get 0), for evolutions sharded over several GPUs: the ranks sum their dndy rows
+ * with one all-reduce per stage (no counterpart in the reference, which runs on one GPU). */
+int nlo_bk_rhs_shard(const nlo_bk_params* params, const double* r, const double* N, int32_t points, int32_t shard,
+                     int32_t shards, const nlo_sobol_dirs* dirs, int64_t samples, const nlo_bk_box* box, double* dndy,
+                     void* workspace, size_t workspace_bytes, void* stream);
+
+/* One stepper stage: out = N + sum_j coef[j] k[j] (nk <= 4; k: host array of device
+ * pointers, coef: host array), clamped to [0, 1] when clamp != 0; status (optional device
+ * uint32[1]) gets bit 0 when a value is not finite.  The stage combinations of
+ * nlo_bk_evolve, for callers that drive the stepper themselves (bk/evolution.py:110-236). */
+int nlo_bk_stage(const double* N, const double* const* k, const double* coef, int32_t nk, int32_t points,
+                 int32_t clamp, double* out, uint32_t* status, void* stream);
+
 /* Rapidity evolution of one amplitude row through `steps` steps of size `step`
  * (_bk_steps, bk/evolution.py:85-159): each step applies the stepper, clamps N to
  * [0,1] when force_positive, and stores the row.  table: device double[(steps+1)*points]
@@ -270,6 +284,37 @@ size_t nlo_dis_vegas_workspace_bytes(int32_t jobs, int32_t term, const nlo_vegas
 int nlo_dis_vegas(const nlo_dis_kinematics* kin, int32_t jobs, int32_t term, const nlo_dipole* dipole,
                   const nlo_vegas_options* options, const nlo_sobol_dirs* dirs, double* state, void* workspace,
                   size_t workspace_bytes, void* stream);
+
+/* Fixed-Sobol options (dis/fixed_sobol.py:30-37 defaults in brackets). */
+typedef struct nlo_fixed_sobol_options {
+    int64_t training_samples;      /* [65536] power of two */
+    int32_t training_rounds;       /* [3] */
+    int64_t samples_per_replicate; /* [32768] power of two */
+    int32_t replicates;            /* [7] >= 2 */
+    int32_t bins;                  /* [32] */
+    int32_t fold_angle;            /* [1] fold the gluon angle onto [0, pi] */
+    double i1_weight;              /* [1.0] weight of I1 in the grid-training score */
+    int32_t inner_points;          /* [48] inner rule of I2 / I3 */
+    int32_t precision;             /* NLO_PRECISION_* */
+} nlo_fixed_sobol_options;
+
+/* Grid buffer of nlo_dis_fixed_sobol in doubles: edges[5][bins+1] then 16 scalars. */
+size_t nlo_dis_fixed_sobol_grid_doubles(int32_t bins);
+size_t nlo_dis_fixed_sobol_workspace_bytes(const nlo_fixed_sobol_options* options);
+
+/* The fixed-Sobol qqbar-g integration of one quark and polarisation (gbw_qg_fixed_sobol,
+ * dis/fixed_sobol.py:273-368): training rounds learn one importance grid from the score
+ * |I1|/<|I1|> + |I2|/<|I2|> + |I3|/<|I3|> over Sobol points split by the nearer dipole end
+ * (custom_kernels/dis/sampling/kernel.cu:15-84; learn_triple_importance_grid :161-211),
+ * then each replicate's means of I1, I2, I3 through the frozen grid
+ * (integrate_triple_fixed_sobol :214-270).  dirs: host array [training_rounds + replicates]
+ * of the direction numbers for seeds seed + r and seed + 10000 + j.  grid: device
+ * double[nlo_dis_fixed_sobol_grid_doubles(bins)] (out); estimates: device
+ * double[replicates][3] (out).  The caller forms the replicate mean and standard error.
+ * The reference runs this path for GBW only; the device accepts a BK table as well. */
+int nlo_dis_fixed_sobol(const nlo_dis_kinematics* kin, const nlo_dipole* dipole, const nlo_fixed_sobol_options* options,
+                        const nlo_sobol_dirs* dirs, double* grid, double* estimates, void* workspace,
+                        size_t workspace_bytes, void* stream);
 
 #ifdef __cplusplus
 }

@@ -109,6 +109,20 @@ class VegasOptions(ctypes.Structure):
     ]
 
 
+class FixedSobolOptions(ctypes.Structure):
+    _fields_ = [
+        ("training_samples", ctypes.c_int64),
+        ("training_rounds", ctypes.c_int32),
+        ("samples_per_replicate", ctypes.c_int64),
+        ("replicates", ctypes.c_int32),
+        ("bins", ctypes.c_int32),
+        ("fold_angle", ctypes.c_int32),
+        ("i1_weight", ctypes.c_double),
+        ("inner_points", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+    ]
+
+
 EXPORTED = (
     "nlo_last_error",
     "nlo_abi_version",
@@ -123,6 +137,8 @@ EXPORTED = (
     "nlo_bk_rhs_workspace_bytes",
     "nlo_bk_rhs",
     "nlo_bk_evolve",
+    "nlo_bk_rhs_shard",
+    "nlo_bk_stage",
     "nlo_dis_table_doubles",
     "nlo_dis_table_prepare",
     "nlo_dis_table_initialize",
@@ -133,6 +149,9 @@ EXPORTED = (
     "nlo_dis_vegas_state_doubles",
     "nlo_dis_vegas_workspace_bytes",
     "nlo_dis_vegas",
+    "nlo_dis_fixed_sobol_grid_doubles",
+    "nlo_dis_fixed_sobol_workspace_bytes",
+    "nlo_dis_fixed_sobol",
 )
 
 _lock = threading.Lock()
@@ -168,6 +187,10 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.nlo_bk_rhs.argtypes = [P(BKParams), vp, vp, i32, P(SobolDirs), i64, P(Box), vp, vp, vp, vp, sz, vp]
     lib.nlo_bk_evolve.restype = ctypes.c_int
     lib.nlo_bk_evolve.argtypes = [P(BKParams), vp, i32, i32, d, i32, P(SobolDirs), i64, P(Box), vp, vp, vp, sz, vp]
+    lib.nlo_bk_rhs_shard.restype = ctypes.c_int
+    lib.nlo_bk_rhs_shard.argtypes = [P(BKParams), vp, vp, i32, i32, i32, P(SobolDirs), i64, P(Box), vp, vp, sz, vp]
+    lib.nlo_bk_stage.restype = ctypes.c_int
+    lib.nlo_bk_stage.argtypes = [vp, P(vp), P(d), i32, i32, i32, vp, vp, vp]
     lib.nlo_dis_table_doubles.restype = sz
     lib.nlo_dis_table_doubles.argtypes = [i32, i32]
     lib.nlo_dis_table_prepare.restype = ctypes.c_int
@@ -188,6 +211,13 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.nlo_dis_vegas_workspace_bytes.argtypes = [i32, i32, P(VegasOptions)]
     lib.nlo_dis_vegas.restype = ctypes.c_int
     lib.nlo_dis_vegas.argtypes = [P(DisKinematics), i32, i32, P(Dipole), P(VegasOptions), P(SobolDirs), vp, vp, sz, vp]
+    lib.nlo_dis_fixed_sobol_grid_doubles.restype = sz
+    lib.nlo_dis_fixed_sobol_grid_doubles.argtypes = [i32]
+    lib.nlo_dis_fixed_sobol_workspace_bytes.restype = sz
+    lib.nlo_dis_fixed_sobol_workspace_bytes.argtypes = [P(FixedSobolOptions)]
+    lib.nlo_dis_fixed_sobol.restype = ctypes.c_int
+    lib.nlo_dis_fixed_sobol.argtypes = [P(DisKinematics), P(Dipole), P(FixedSobolOptions), P(SobolDirs), vp, vp, vp,
+                                        sz, vp]
 
 
 def load(path: Path | None = None) -> ctypes.CDLL:

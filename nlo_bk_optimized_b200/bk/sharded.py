@@ -1,0 +1,131 @@
+"""BK evolution sharded over the GPUs of one node (one process per GPU).
+
+The right-hand side is independent across parent sizes r: rank k computes dN/dY for the
+parents i with i % world == k (``nlo_bk_rhs_shard``; interleaving balances the saturated,
+inactive parents) and the ranks sum their rows with one all-reduce of R doubles per
+stage (3.2 KB at R = 400, over NCCL).  Every rank then holds the full derivative, forms
+the stage with ``nlo_bk_stage`` and refits the full spline itself, so the ranks carry
+identical amplitude rows.  The stage sequence is that of ``nlo_bk_evolve`` (Euler,
+Kutta RK3 of bk/evolution.py:190-236, classical RK4).
+
+``shard_steps`` is the device-independent driver: it takes the rank's partial
+right-hand side, the all-reduce and the stage combination as functions, which lets the
+multi-rank logic run in CPU processes over gloo as well.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from collections.abc import Callable
+
+import torch
+
+from nlo_bk_optimized_b200 import _native
+from nlo_bk_optimized_b200.bk.config import BKConfig
+from nlo_bk_optimized_b200.dipole.table import DipoleTable
+
+Rhs = Callable[[torch.Tensor], torch.Tensor]
+AllReduce = Callable[[torch.Tensor], None]
+Stage = Callable[[torch.Tensor, list, list, bool], torch.Tensor]
+
+
+def shard_steps(N0: torch.Tensor, steps: int, step: float, stepper: str, rhs: Rhs, all_reduce: AllReduce,
+                stage: Stage, clamp: bool) -> list[torch.Tensor]:
+    """Rows N(Y_0 .. Y_steps) of a stepper whose every derivative is the all-reduced sum of
+    the ranks' partial right-hand sides."""
+
+    def f(state: torch.Tensor) -> torch.Tensor:
+        k = rhs(state)
+        all_reduce(k)
+        return k
+
+    rows = [N0]
+    N = N0
+    h = step
+    for _ in range(steps):
+        if stepper == "euler":
+            k1 = f(N)
+            N = stage(N, [k1], [h], clamp)
+        elif stepper == "rk3":
+            k1 = f(N)
+            k2 = f(stage(N, [k1], [0.5 * h], False))
+            k3 = f(stage(N, [k1, k2], [-h, 2.0 * h], False))
+            N = stage(N, [k1, k2, k3], [h / 6.0, 4.0 * h / 6.0, h / 6.0], clamp)
+        elif stepper == "rk4":
+            k1 = f(N)
+            k2 = f(stage(N, [k1], [0.5 * h], False))
+            k3 = f(stage(N, [k2], [0.5 * h], False))
+            k4 = f(stage(N, [k3], [h], False))
+            N = stage(N, [k1, k2, k3, k4], [h / 6.0, 2.0 * h / 6.0, 2.0 * h / 6.0, h / 6.0], clamp)
+        else:
+            raise ValueError(f"unknown stepper {stepper}")
+        rows.append(N)
+    return rows
+
+
+def solve_bk_sharded(initial_condition, maxy: float, config: BKConfig = BKConfig(), *,
+                     device: torch.device | str | None = None, dtype: torch.dtype = torch.float32, seed: int = 0,
+                     group: "torch.distributed.ProcessGroup | None" = None) -> DipoleTable:
+    """``solve_bk`` across the ranks of ``group`` (torch.distributed, NCCL for CUDA)."""
+    import torch.distributed as dist
+
+    from nlo_bk_optimized_b200.bk.evolution import (
+        _r_grid,
+        _steps_to,
+        nlo_box,
+        params_of,
+        precision_of,
+        workspace,
+    )
+
+    rank = dist.get_rank(group) if dist.is_initialized() else 0
+    world = dist.get_world_size(group) if dist.is_initialized() else 1
+    device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    if device.type != "cuda":
+        raise ValueError("the sharded evolution runs on CUDA devices only")
+    lib = _native.load()
+    params = params_of(config, precision_of(config, dtype))
+    r_host = _r_grid(config, device="cpu", dtype=torch.float64)
+    N0 = initial_condition.dipole_amplitude(r_host).to(device=device, dtype=torch.float64).contiguous()
+    r = r_host.to(device)
+    points = r.numel()
+    lower, width = nlo_box(float(r_host[0]), float(r_host[-1]))
+    box = _native.box(lower, width)
+    dirs = _native.sobol_dirs(4, seed)
+    ws = workspace(device, points)
+    status = torch.zeros(1, dtype=torch.int32, device=device)
+    stream = _native.stream_handle(device)
+    ys = _steps_to(0.0, maxy, config.DE_SOLVER_STEP)
+    steps = len(ys)
+    clamp = bool(config.FORCE_POSITIVE_N)
+
+    def rhs(N: torch.Tensor) -> torch.Tensor:
+        out = torch.empty_like(N)
+        _native.check(lib.nlo_bk_rhs_shard(params, r.data_ptr(), N.data_ptr(), points, rank, world, dirs,
+                                           int(config.MCINTPOINTS), box, out.data_ptr(), ws.data_ptr(), ws.numel(),
+                                           stream))
+        return out
+
+    def all_reduce(k: torch.Tensor) -> None:
+        if world > 1:
+            dist.all_reduce(k, op=dist.ReduceOp.SUM, group=group)
+
+    def stage(N: torch.Tensor, ks: list, coefs: list, clamp_: bool) -> torch.Tensor:
+        out = torch.empty_like(N)
+        kp = (ctypes.c_void_p * len(ks))(*[k.data_ptr() for k in ks])
+        cf = (ctypes.c_double * len(coefs))(*coefs)
+        # like nlo_bk_evolve, only the completed step is clamped and checked
+        _native.check(lib.nlo_bk_stage(N.data_ptr(), kp, cf, len(ks), points, int(clamp_), out.data_ptr(),
+                                       status.data_ptr() if clamp_ else None, stream))
+        return out
+
+    with torch.cuda.device(device):
+        rows = shard_steps(N0, steps, config.DE_SOLVER_STEP, config.stepper, rhs, all_reduce, stage, clamp)
+        if int(status.item()) != 0:
+            raise FloatingPointError("non-finite BK amplitude during the rapidity evolution")
+    y = torch.tensor([0.0, *ys], dtype=dtype, device=device)
+    N = torch.stack(rows)
+    return DipoleTable(r=r.to(dtype), y=y, N=N.to(dtype), x0=initial_condition.x0)
+
+
+__all__ = ["shard_steps", "solve_bk_sharded"]

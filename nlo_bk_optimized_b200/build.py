@@ -43,6 +43,12 @@ def _stale() -> bool:
     return any(path.stat().st_mtime > built for path in inputs)
 
 
+# Per-file flags.  The DIS kernels' FP32 bodies use approximate single-precision
+# division and square root (about 2 ulp) and flush FP32 denormals; their FP64 template
+# instances and every other file keep IEEE arithmetic.
+FILE_FLAGS = {"dis.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]}
+
+
 def _compile(source: Path, obj: Path, verbose: bool) -> tuple[int, str]:
     command = [
         _nvcc(),
@@ -53,6 +59,7 @@ def _compile(source: Path, obj: Path, verbose: bool) -> tuple[int, str]:
         "-Xcompiler",
         "-fPIC",
         "--expt-relaxed-constexpr",
+        *FILE_FLAGS.get(source.name, []),
         "-c",
         str(source),
         "-o",

@@ -129,13 +129,14 @@ RhsBuffers carve(void* ws, int points)
 
 int run_rhs(const nlo_bk_params& p, const double* r, const double* N, int points, const SobolDirsArg& dirs,
             uint64_t samples, const nlo_bk_box& box, double* dndy, double* k1_out, double* k2kf_out,
-            const RhsBuffers& b, bool factor_ready, cudaStream_t stream)
+            const RhsBuffers& b, bool factor_ready, cudaStream_t stream, int shard = 0, int shards = 1)
 {
     cudaError_t e;
     if ((e = launch_splines(r, N, points, p.force_positive, b.factor, factor_ready ? 0 : 1, b.spline, stream)) !=
         cudaSuccess)
         return cuda_fail(e, "splines");
-    if ((e = launch_active(N, points, b.active, b.count, stream)) != cudaSuccess) return cuda_fail(e, "active");
+    if ((e = launch_active(N, points, shard, shards, b.active, b.count, stream)) != cudaSuccess)
+        return cuda_fail(e, "active");
     if ((e = launch_k1(p, r, points, b.spline, b.active, b.count, b.k1, stream)) != cudaSuccess)
         return cuda_fail(e, "k1");
     if ((e = launch_k2kf(p, r, points, b.spline, b.active, b.count, dirs, 0, samples, box, b.k2kf, b.partial,
@@ -222,7 +223,7 @@ int nlo_bk_active(const double* N, int32_t points, int32_t* active, int32_t* cou
 {
     if (points < 1) return fail(NLO_ERR_INVALID, "points must be positive");
     if (!N || !active || !count) return fail(NLO_ERR_INVALID, "NULL buffer");
-    cudaError_t e = launch_active(N, points, active, count, (cudaStream_t)stream);
+    cudaError_t e = launch_active(N, points, 0, 1, active, count, (cudaStream_t)stream);
     return e == cudaSuccess ? NLO_OK : cuda_fail(e, "active");
 }
 
@@ -285,6 +286,36 @@ int nlo_bk_rhs(const nlo_bk_params* params, const double* r, const double* N, in
     const RhsBuffers b = carve(workspace, points);
     return run_rhs(*params, r, N, points, to_arg(dirs), (uint64_t)samples, *box, dndy, k1, k2kf, b, false,
                    (cudaStream_t)stream);
+}
+
+int nlo_bk_rhs_shard(const nlo_bk_params* params, const double* r, const double* N, int32_t points, int32_t shard,
+                     int32_t shards, const nlo_sobol_dirs* dirs, int64_t samples, const nlo_bk_box* box, double* dndy,
+                     void* workspace, size_t workspace_bytes, void* stream)
+{
+    std::string why;
+    if (!check_params(params, why)) return fail(NLO_ERR_INVALID, why);
+    if (!check_dirs(dirs, 4, why)) return fail(NLO_ERR_INVALID, why);
+    if (shards < 1 || shard < 0 || shard >= shards) return fail(NLO_ERR_INVALID, "shard must lie in [0, shards)");
+    if (points < 3 || points > 4096) return fail(NLO_ERR_INVALID, "points must be 3..4096");
+    if (!r || !N || !dndy || !box) return fail(NLO_ERR_INVALID, "NULL buffer");
+    if (samples < 0 || samples > (int64_t(1) << 30)) return fail(NLO_ERR_INVALID, "samples out of range");
+    if (!workspace || workspace_bytes < nlo_bk_rhs_workspace_bytes(points))
+        return fail(NLO_ERR_WORKSPACE, "workspace too small for nlo_bk_rhs_shard");
+    const RhsBuffers b = carve(workspace, points);
+    return run_rhs(*params, r, N, points, to_arg(dirs), (uint64_t)samples, *box, dndy, nullptr, nullptr, b, false,
+                   (cudaStream_t)stream, shard, shards);
+}
+
+int nlo_bk_stage(const double* N, const double* const* k, const double* coef, int32_t nk, int32_t points,
+                 int32_t clamp, double* out, uint32_t* status, void* stream)
+{
+    if (!N || !k || !coef || !out) return fail(NLO_ERR_INVALID, "NULL buffer");
+    if (nk < 1 || nk > 4) return fail(NLO_ERR_INVALID, "nk must be 1..4");
+    if (points < 1) return fail(NLO_ERR_INVALID, "points must be positive");
+    for (int j = 0; j < nk; ++j)
+        if (!k[j]) return fail(NLO_ERR_INVALID, "NULL stage derivative");
+    cudaError_t e = launch_axpy_stage(N, k, coef, nk, points, out, clamp ? 1 : 0, status, (cudaStream_t)stream);
+    return e == cudaSuccess ? NLO_OK : cuda_fail(e, "stage");
 }
 
 int nlo_bk_evolve(const nlo_bk_params* params, const double* r, int32_t points, int32_t steps, double step,

@@ -254,7 +254,7 @@ __global__ void gauss_legendre_kernel(const DisArgs<T>* __restrict__ args, Inner
 // partial layout per (job, block): [total, total2, hist[D][bins]] doubles and
 // count[D][bins] int32 in a parallel array
 template <typename T, int TERM>
-__global__ void __launch_bounds__(kVegasThreads) vegas_iteration_kernel(
+__global__ void __launch_bounds__(kVegasThreads, 3) vegas_iteration_kernel(
     const DisArgs<T>* __restrict__ args, const SobolDirsArg* __restrict__ dirs, InnerRule rule,
     double* __restrict__ state, int state_stride, int bins, uint64_t offset, uint64_t samples, int blocks_per_job,
     double* __restrict__ partial, int32_t* __restrict__ counts)
@@ -347,7 +347,7 @@ __global__ void __launch_bounds__(kVegasThreads) vegas_iteration_kernel(
     __syncthreads();
     const size_t pstride = 2 + (size_t)D * bins;
     double* out = partial + ((size_t)job * blocks_per_job + blockIdx.x) * pstride;
-    int32_t* cout = counts + ((size_t)job * blocks_per_job + blockIdx.x) * (size_t)D * bins;
+    int32_t* cout = counts + (size_t)job * D * bins;  // per-job bin counts, integer atomics
     if (threadIdx.x == 0) {
         double s = 0.0, s2 = 0.0;
         for (int w = 0; w < warps; ++w) {
@@ -361,53 +361,65 @@ __global__ void __launch_bounds__(kVegasThreads) vegas_iteration_kernel(
         double h = 0.0;
         for (int w = 0; w < warps; ++w) h += whist[w * D * bins + k];
         out[2 + k] = h;
-        cout[k] = cnt[k];
+        if (cnt[k]) atomicAdd(&cout[k], cnt[k]);
     }
 }
 
-// One CTA per job: reduce partials, adapt the grid (numerics/integration.py:804-866),
-// update the combined estimate (:510-582).
+// Sum the per-CTA partials of every job in a fixed order: grid (key chunks, jobs), one
+// thread per key (the |w| histogram bins, then total and total^2), looping over the CTAs.
+__global__ void vegas_reduce_kernel(const double* __restrict__ partial, int keys, int blocks_per_job,
+                                    double* __restrict__ reduced)
+{
+    const int job = blockIdx.y;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;  // 0..keys-1 over [total, total2, hist...]
+    if (k >= keys) return;
+    const double* p = partial + (size_t)job * blocks_per_job * keys + k;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    int b = 0;
+    for (; b + 4 <= blocks_per_job; b += 4) {
+        a0 += p[(size_t)(b + 0) * keys];
+        a1 += p[(size_t)(b + 1) * keys];
+        a2 += p[(size_t)(b + 2) * keys];
+        a3 += p[(size_t)(b + 3) * keys];
+    }
+    for (; b < blocks_per_job; ++b) a0 += p[(size_t)b * keys];
+    reduced[(size_t)job * keys + k] = (a0 + a1) + (a2 + a3);
+}
+
+// One CTA per job: adapt the grid (numerics/integration.py:804-866) from the reduced
+// histogram and counts, update the combined estimate (:510-582), clear the counts.
 __global__ void vegas_finalize_kernel(double* __restrict__ state, int state_stride, int D, int bins,
-                                      uint64_t samples, int blocks_per_job, const double* __restrict__ partial,
-                                      const int32_t* __restrict__ counts, int warmup, int min_iterations,
+                                      uint64_t samples, const double* __restrict__ reduced,
+                                      int32_t* __restrict__ counts, int warmup, int min_iterations,
                                       double epsrel, double epsabs)
 {
     extern __shared__ double fsm[];
-    double* hist = fsm;                 // [D*bins]
-    double* cntd = hist + D * bins;     // [D*bins]
-    double* smooth = cntd + D * bins;   // [D*bins]
+    double* smooth = fsm;               // [D*bins]
     double* cum = smooth + D * bins;    // [D*(bins+1)]
     double* ne = cum + D * (bins + 1);  // [D*(bins+1)]
     const int job = blockIdx.x;
     double* st = state + (size_t)job * state_stride;
     double* sc = st + D * (bins + 1);
+    int32_t* c = counts + (size_t)job * D * bins;
     if (sc[kStConverged] != 0.0) return;
-    const size_t pstride = 2 + (size_t)D * bins;
-    const double* p = partial + (size_t)job * blocks_per_job * pstride;
-    const int32_t* c = counts + (size_t)job * blocks_per_job * (size_t)D * bins;
-    for (int k = threadIdx.x; k < D * bins; k += blockDim.x) {
-        double h = 0.0;
-        long long n = 0;
-        for (int b = 0; b < blocks_per_job; ++b) {
-            h += p[b * pstride + 2 + k];
-            n += c[(size_t)b * D * bins + k];
-        }
-        hist[k] = h;
-        cntd[k] = (double)n;
-    }
-    __syncthreads();
+    const int keys = 2 + D * bins;
+    const double* red = reduced + (size_t)job * keys;
+    const double* hist = red + 2;
     // smoothed importance (+ eps), per dimension
     for (int k = threadIdx.x; k < D * bins; k += blockDim.x) {
         const int d = k / bins, b = k % bins;
-        auto imp = [&](int q) { return hist[d * bins + q] / (cntd[d * bins + q] > 1.0 ? cntd[d * bins + q] : 1.0); };
-        double s;
+        auto imp = [&](int q) {
+            const int n = c[d * bins + q];
+            return hist[d * bins + q] / (double)(n > 1 ? n : 1);
+        };
+        double v;
         if (b == 0)
-            s = (imp(0) + imp(1)) / 2.0;
+            v = (imp(0) + imp(1)) / 2.0;
         else if (b == bins - 1)
-            s = (imp(bins - 2) + imp(bins - 1)) / 2.0;
+            v = (imp(bins - 2) + imp(bins - 1)) / 2.0;
         else
-            s = (imp(b - 1) + imp(b) + imp(b + 1)) / 3.0;
-        smooth[k] = s + 2.220446049250313e-16;
+            v = (imp(b - 1) + imp(b) + imp(b + 1)) / 3.0;
+        smooth[k] = v + 2.220446049250313e-16;
     }
     __syncthreads();
     if (threadIdx.x < D) {
@@ -419,35 +431,26 @@ __global__ void vegas_finalize_kernel(double* __restrict__ state, int state_stri
         double* out = ne + d * (bins + 1);
         const double total = cd[bins];
         const double step = total / bins;
+        int idx = 0;
         for (int k = 0; k <= bins; ++k) {
-            // torch.linspace(0, total, bins + 1)
+            // torch.linspace(0, total, bins + 1); the targets increase, so the
+            // searchsorted(right) - 1 index only moves forward
             const double target = k < (bins + 1) / 2 ? step * k : total - step * (bins - k);
-            int lo = 0, hi = bins + 1;  // searchsorted(right) - 1
-            while (lo < hi) {
-                const int mid = (lo + hi) >> 1;
-                if (cd[mid] <= target)
-                    lo = mid + 1;
-                else
-                    hi = mid;
-            }
-            int idx = lo - 1;
-            idx = idx < 0 ? 0 : (idx > bins - 1 ? bins - 1 : idx);
-            const double frac = (target - cd[idx]) / smooth[d * bins + idx];
-            out[k] = e[idx] + frac * (e[idx + 1] - e[idx]);
+            while (idx < bins && cd[idx + 1] <= target) ++idx;
+            const int i = idx > bins - 1 ? bins - 1 : idx;
+            const double frac = (target - cd[i]) / smooth[d * bins + i];
+            out[k] = e[i] + frac * (e[i + 1] - e[i]);
         }
         out[0] = 0.0;
         out[bins] = 1.0;
     }
     __syncthreads();
     for (int k = threadIdx.x; k < D * (bins + 1); k += blockDim.x) st[k] = ne[k];
+    for (int k = threadIdx.x; k < D * bins; k += blockDim.x) c[k] = 0;
     if (threadIdx.x == 0) {
         sc[kStEvals] += (double)samples;
         if (!warmup) {
-            double s = 0.0, s2 = 0.0;
-            for (int b = 0; b < blocks_per_job; ++b) {
-                s += p[b * pstride + 0];
-                s2 += p[b * pstride + 1];
-            }
+            const double s = red[0], s2 = red[1];
             const double n = (double)samples;
             const double est = s / n;
             double var = (s2 - s * s / n);
@@ -469,10 +472,12 @@ __global__ void vegas_finalize_kernel(double* __restrict__ state, int state_stri
     }
 }
 
-__global__ void vegas_init_kernel(double* state, int state_stride, int D, int bins, int jobs, int keep_edges)
+__global__ void vegas_init_kernel(double* state, int state_stride, int D, int bins, int jobs, int keep_edges,
+                                  int32_t* counts)
 {
     const int job = blockIdx.x;
     if (job >= jobs) return;
+    for (int k = threadIdx.x; k < D * bins; k += blockDim.x) counts[(size_t)job * D * bins + k] = 0;
     double* st = state + (size_t)job * state_stride;
     if (!keep_edges)
         for (int k = threadIdx.x; k < D * (bins + 1); k += blockDim.x) {
@@ -525,12 +530,16 @@ cudaError_t launch_vegas_round_t(const VegasLaunch& L, cudaStream_t stream)
                                                 L.partial, L.counts);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    const size_t fsmem = sizeof(double) * (3 * D * L.bins + 2 * D * (L.bins + 1));
+    const int keys = 2 + D * L.bins;
+    dim3 rgrid((keys + 127) / 128, L.jobs);
+    vegas_reduce_kernel<<<rgrid, 128, 0, stream>>>(L.partial, keys, L.blocks_per_job, L.reduced);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const size_t fsmem = sizeof(double) * (D * L.bins + 2 * D * (L.bins + 1));
     e = cudaFuncSetAttribute(vegas_finalize_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsmem);
     if (e != cudaSuccess) return e;
-    vegas_finalize_kernel<<<L.jobs, 64, fsmem, stream>>>(L.state, L.state_stride, D, L.bins, L.samples,
-                                                         L.blocks_per_job, L.partial, L.counts, L.warmup,
-                                                         L.min_iterations, L.epsrel, L.epsabs);
+    vegas_finalize_kernel<<<L.jobs, 128, fsmem, stream>>>(L.state, L.state_stride, D, L.bins, L.samples, L.reduced,
+                                                          L.counts, L.warmup, L.min_iterations, L.epsrel, L.epsabs);
     return cudaGetLastError();
 }
 
@@ -622,9 +631,27 @@ cudaError_t dis_launch_gl(int precision, int term, const void* args, int jobs, c
 }
 
 cudaError_t dis_launch_vegas_init(double* state, int state_stride, int D, int bins, int jobs, int keep_edges,
-                                  cudaStream_t stream)
+                                  int32_t* counts, cudaStream_t stream)
 {
-    dis::vegas_init_kernel<<<jobs, 128, 0, stream>>>(state, state_stride, D, bins, jobs, keep_edges);
+    dis::vegas_init_kernel<<<jobs, 128, 0, stream>>>(state, state_stride, D, bins, jobs, keep_edges, counts);
+    return cudaGetLastError();
+}
+
+cudaError_t dis_launch_reduce_finalize(int D, int bins, int jobs, int blocks_per_job, const double* partial,
+                                       double* reduced, int32_t* counts, double* state, int state_stride,
+                                       uint64_t samples, int warmup, int min_iterations, double epsrel, double epsabs,
+                                       cudaStream_t stream)
+{
+    const int keys = 2 + D * bins;
+    dim3 rgrid((keys + 127) / 128, jobs);
+    dis::vegas_reduce_kernel<<<rgrid, 128, 0, stream>>>(partial, keys, blocks_per_job, reduced);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const size_t fsmem = sizeof(double) * (D * bins + 2 * D * (bins + 1));
+    e = cudaFuncSetAttribute(dis::vegas_finalize_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsmem);
+    if (e != cudaSuccess) return e;
+    dis::vegas_finalize_kernel<<<jobs, 128, fsmem, stream>>>(state, state_stride, D, bins, samples, reduced, counts,
+                                                               warmup, min_iterations, epsrel, epsabs);
     return cudaGetLastError();
 }
 

@@ -153,13 +153,13 @@ int sm_count()
     return sms;
 }
 
-// CTAs per job per round: at least 4 samples per thread, and enough CTAs over all jobs
-// to give every SM several (a fixed function of the job count and the sample count, so
-// results do not depend on the device beyond its SM count)
+// CTAs per job per round: one sample per thread at most, and over all jobs about four
+// times the resident capacity (three 256-thread CTAs per SM), so that CTAs of uneven cost
+// even out (a fixed function of the job count, the sample count and the SM count)
 int vegas_blocks(int64_t samples, int jobs)
 {
-    const int64_t by_samples = (samples + 4 * dis::kVegasThreads - 1) / (4 * dis::kVegasThreads);
-    const int64_t want = (8 * (int64_t)sm_count() + jobs - 1) / jobs;
+    const int64_t by_samples = (samples + dis::kVegasThreads - 1) / dis::kVegasThreads;
+    const int64_t want = (4 * 3 * (int64_t)sm_count() + jobs - 1) / jobs;
     int64_t b = std::min(by_samples, want);
     return (int)std::max<int64_t>(1, std::min<int64_t>(b, 65535));
 }
@@ -167,7 +167,7 @@ int vegas_blocks(int64_t samples, int jobs)
 size_t state_doubles(int term, int bins) { return (size_t)dis::term_dims(term) * (bins + 1) + dis::kStSlots; }
 
 struct VegasCarve {
-    size_t args, dirs, partial, counts, total;
+    size_t args, dirs, partial, reduced, counts, total;
 };
 
 VegasCarve vegas_carve(int jobs, int term, const nlo_vegas_options& o)
@@ -179,8 +179,9 @@ VegasCarve vegas_carve(int jobs, int term, const nlo_vegas_options& o)
     c.args = 0;
     c.dirs = align_up(c.args + args_bytes(jobs));
     c.partial = align_up(c.dirs + sizeof(SobolDirsArg) * (size_t)jobs);
-    c.counts = align_up(c.partial + sizeof(double) * (size_t)jobs * blocks * (2 + (size_t)D * o.bins));
-    c.total = align_up(c.counts + sizeof(int32_t) * (size_t)jobs * blocks * (size_t)D * o.bins);
+    c.reduced = align_up(c.partial + sizeof(double) * (size_t)jobs * blocks * (2 + (size_t)D * o.bins));
+    c.counts = align_up(c.reduced + sizeof(double) * (size_t)jobs * (2 + (size_t)D * o.bins));
+    c.total = align_up(c.counts + sizeof(int32_t) * (size_t)jobs * (size_t)D * o.bins);
     return c;
 }
 
@@ -359,7 +360,8 @@ int nlo_dis_vegas(const nlo_dis_kinematics* kin, int32_t jobs, int32_t term, con
     cudaError_t e = cudaMemcpyAsync(ws + c.dirs, dirs, sizeof(nlo_sobol_dirs) * (size_t)jobs, cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return dcuda(e, "Sobol direction upload");
     const int stride = (int)state_doubles(term, options->bins);
-    e = dis_launch_vegas_init(state, stride, D, options->bins, jobs, options->keep_edges, s);
+    int32_t* counts = reinterpret_cast<int32_t*>(ws + c.counts);
+    e = dis_launch_vegas_init(state, stride, D, options->bins, jobs, options->keep_edges, counts, s);
     if (e != cudaSuccess) return dcuda(e, "Vegas init launch");
     dis::VegasLaunch L;
     L.args = ws + c.args;
@@ -370,7 +372,8 @@ int nlo_dis_vegas(const nlo_dis_kinematics* kin, int32_t jobs, int32_t term, con
     L.jobs = jobs;
     L.bins = options->bins;
     L.partial = reinterpret_cast<double*>(ws + c.partial);
-    L.counts = reinterpret_cast<int32_t*>(ws + c.counts);
+    L.reduced = reinterpret_cast<double*>(ws + c.reduced);
+    L.counts = counts;
     L.min_iterations = options->min_iterations;
     L.epsrel = options->epsrel;
     L.epsabs = options->epsabs;
@@ -387,6 +390,44 @@ int nlo_dis_vegas(const nlo_dis_kinematics* kin, int32_t jobs, int32_t term, con
         offset += L.samples;
     }
     return NLO_OK;
+}
+
+size_t nlo_dis_fixed_sobol_grid_doubles(int32_t bins)
+{
+    return bins < 2 ? 0 : (size_t)5 * (bins + 1) + dis::kStSlots;
+}
+
+size_t nlo_dis_fixed_sobol_workspace_bytes(const nlo_fixed_sobol_options* options)
+{
+    std::string why;
+    if (!dis_fixed_check(options, why)) return 0;
+    return dis_fixed_workspace_bytes(*options);
+}
+
+int nlo_dis_fixed_sobol(const nlo_dis_kinematics* kin, const nlo_dipole* dipole, const nlo_fixed_sobol_options* options,
+                        const nlo_sobol_dirs* dirs, double* grid, double* estimates, void* workspace,
+                        size_t workspace_bytes, void* stream)
+{
+    std::string why;
+    if (!kin || !dirs || !grid || !estimates) return dfail(NLO_ERR_INVALID, "nlo_dis_fixed_sobol: NULL argument");
+    if (!dis_fixed_check(options, why) || !check_dipole(dipole, why) || !check_kin(*kin, dis::kTermI1, why))
+        return dfail(NLO_ERR_INVALID, why);
+    const int rounds = options->training_rounds + options->replicates;
+    for (int j = 0; j < rounds; ++j)
+        if (dirs[j].dims < 5 || dirs[j].dims > 8) return dfail(NLO_ERR_INVALID, "fixed-Sobol needs 5-dimensional directions");
+    const size_t need = dis_fixed_workspace_bytes(*options);
+    if (!workspace || workspace_bytes < need) return dfail(NLO_ERR_WORKSPACE, "workspace missing or too small");
+    InnerRule rule;
+    if (!make_rule(dis::kTermI3N, options->inner_points, rule, why)) return dfail(NLO_ERR_INVALID, why);
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemcpyAsync(workspace, dirs, sizeof(nlo_sobol_dirs) * (size_t)rounds, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return dcuda(e, "Sobol direction upload");
+    if (options->precision == NLO_PRECISION_FP64) {
+        const DisArgs<double> a = make_args<double>(*kin, *dipole);
+        return dis_run_fixed(options->precision, &a, rule, *options, workspace, grid, estimates, s);
+    }
+    const DisArgs<float> a = make_args<float>(*kin, *dipole);
+    return dis_run_fixed(options->precision, &a, rule, *options, workspace, grid, estimates, s);
 }
 
 }  // extern "C"

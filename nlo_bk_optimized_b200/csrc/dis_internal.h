@@ -5,6 +5,8 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include <string>
+
 #include "internal.h"
 
 namespace nlo {
@@ -45,7 +47,8 @@ struct VegasLaunch {
     int jobs, bins, blocks_per_job;
     uint64_t offset, samples;
     double* partial;             // device [jobs][blocks][2 + D*bins]
-    int32_t* counts;             // device [jobs][blocks][D*bins]
+    double* reduced;             // device [jobs][2 + D*bins]
+    int32_t* counts;             // device [jobs][D*bins], integer sums over the CTAs
     int warmup, min_iterations;
     double epsrel, epsabs;
 };
@@ -62,8 +65,21 @@ cudaError_t dis_launch_amplitude(int precision, const void* args, const double* 
 cudaError_t dis_launch_gl(int precision, int term, const void* args, int jobs, const dis::InnerRule& rule,
                           const dis::GLRules& gl, double* out, cudaStream_t stream);
 cudaError_t dis_launch_vegas_init(double* state, int state_stride, int D, int bins, int jobs, int keep_edges,
-                                  cudaStream_t stream);
+                                  int32_t* counts, cudaStream_t stream);
 cudaError_t dis_launch_vegas_round(int precision, int term, const dis::VegasLaunch& L, cudaStream_t stream);
+// Reduce per-CTA partials [jobs][blocks][2 + D*bins] and run the grid adaptation and
+// estimate update of one Vegas round (warmup = adaptation only).
+cudaError_t dis_launch_reduce_finalize(int D, int bins, int jobs, int blocks_per_job, const double* partial,
+                                       double* reduced, int32_t* counts, double* state, int state_stride,
+                                       uint64_t samples, int warmup, int min_iterations, double epsrel, double epsabs,
+                                       cudaStream_t stream);
+
+// Fixed-Sobol qqbar-g integration (dis_fixed.cu).  The workspace starts with the
+// Sobol directions of the training rounds and replicates (SobolDirsArg each).
+bool dis_fixed_check(const nlo_fixed_sobol_options* o, std::string& why);
+size_t dis_fixed_workspace_bytes(const nlo_fixed_sobol_options& o);
+int dis_run_fixed(int precision, const void* args, const dis::InnerRule& rule, const nlo_fixed_sobol_options& o,
+                  void* workspace, double* grid_state, double* estimates, cudaStream_t s);
 
 // Gauss-Legendre nodes and weights on [-1, 1], ascending (capi.cu)
 void gauss_legendre_rule(int n, double* x, double* w);

@@ -813,6 +813,49 @@ __device__ T qg_term(const DisArgs<T>& a, const double* x, const InnerRule& rule
     return DM<T>::finite(out) ? out : (T)0;
 }
 
+// I1, and I2 and I3 with the inner rule, at one point: the map, the amplitudes, the
+// coupling and the tripole geometry are shared, and I2 and I3 use one moment set (the
+// combined evaluation of the fixed-Sobol path, dis/fixed_sobol.py:273-368).
+template <typename T>
+__device__ void qg_triple(const DisArgs<T>& a, const double* x, const InnerRule& rule, T out[3])
+{
+    out[0] = out[1] = out[2] = (T)0;
+    const double z2min = a.z2min;
+    if (z2min > 1.0) return;
+    const double z1 = (1.0 - z2min) * x[0];
+    const double z2 = (1.0 - z1 - z2min) * x[1] + z2min;
+    const double x01 = a.maxr * x[2];
+    const double x02 = a.maxr * x[3];
+    const double phi = 2.0 * kPi * x[4];
+    const double x01sq = x01 * x01, x02sq = x02 * x02;
+    double x21sq = x01sq + x02sq - 2.0 * x01 * x02 * ::cos(phi);
+    x21sq = x21sq > 0.0 ? x21sq : 0.0;
+    const double x21 = ::sqrt(x21sq);
+    const double jac = (1.0 - z2min) * (1.0 - z1 - z2min) * x01 * x02 * a.maxr * a.maxr * 2.0 * kPi;
+    const double Y = ::log(a.W2 * z2 / kQ0sqr);
+    if (!(Y >= 0.0)) return;
+    const T S01 = (T)1 - amplitude(a, x01, Y);
+    const T S02 = (T)1 - amplitude(a, x02, Y);
+    const T S12 = (T)1 - amplitude(a, x21, Y);
+    const T N012 = a.finite_nc ? (T)1 - (T)(kNc / (2.0 * kCF)) * (S02 * S12 - S01 / (T)(kNc * kNc))
+                               : (T)1 - S02 * S12;
+    const double ra = a.parent_coupling ? x01 : fmin(x01, fmin(x02, x21));
+    const T scale = alpha_bar(a, (T)ra) * (T)(jac / z2);
+    const Trip<T> t = make_trip<T>(a.Q2, a.mf, z1, z2, x01sq, x02sq, x21sq);
+    T uvsub, trip;
+    if (a.transverse)
+        t_i1(t, (T)x01sq, uvsub, trip);
+    else
+        l_i1(t, (T)x01sq, uvsub, trip);
+    const GSet<T> G = g_moments(t, rule);
+    const T i1 = (((T)1 - S01) * uvsub + N012 * trip) * scale;
+    const T i2 = N012 * (a.transverse ? t_i2(t, G) : l_i2(t, G)) * scale;
+    const T i3 = N012 * (a.transverse ? t_i3(t, G, G) : l_i3(t, G, G)) * scale;
+    out[0] = DM<T>::finite(i1) ? i1 : (T)0;
+    out[1] = DM<T>::finite(i2) ? i2 : (T)0;
+    out[2] = DM<T>::finite(i3) ? i3 : (T)0;
+}
+
 template <typename T, int TERM>
 __device__ __forceinline__ T term_value(const DisArgs<T>& a, const double* x, const InnerRule& rule)
 {

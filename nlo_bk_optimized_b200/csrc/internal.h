@@ -44,7 +44,9 @@ int set_last_error(int code, const char* message);
 
 cudaError_t launch_splines(const double* r, const double* N, int n, int force_positive, double* factor,
                            int compute_factor, double* out, cudaStream_t stream);
-cudaError_t launch_active(const double* N, int n, int32_t* active, int32_t* count, cudaStream_t stream);
+// active parents (index > 0, N <= 0.99999) with index % shards == shard
+cudaError_t launch_active(const double* N, int n, int shard, int shards, int32_t* active, int32_t* count,
+                          cudaStream_t stream);
 cudaError_t launch_sobol(const SobolDirsArg& dirs, uint64_t offset, uint64_t n, int precision, void* out,
                          cudaStream_t stream);
 cudaError_t launch_k1(const nlo_bk_params& p, const double* r, int points, const double* spline,

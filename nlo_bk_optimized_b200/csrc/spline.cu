@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(256) splines_kernel(const double* __restrict__
 
 // Active parents: index > 0 and N <= 0.99999 (bk/evolution.py:501), compacted in
 // index order by a single-CTA ballot scan.
-__global__ void __launch_bounds__(1024) active_kernel(const double* __restrict__ N, int n,
+__global__ void __launch_bounds__(1024) active_kernel(const double* __restrict__ N, int n, int shard, int shards,
                                                       int32_t* __restrict__ active, int32_t* __restrict__ count)
 {
     __shared__ int warp_counts[32];
@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(1024) active_kernel(const double* __restrict__
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int start = 0; start < n; start += blockDim.x) {
         const int i = start + threadIdx.x;
-        const bool on = i < n && i > 0 && N[i] <= 0.99999;
+        const bool on = i < n && i > 0 && N[i] <= 0.99999 && i % shards == shard;
         const unsigned mask = __ballot_sync(0xffffffffu, on);
         if (lane == 0) warp_counts[warp] = __popc(mask);
         __syncthreads();
@@ -157,9 +157,10 @@ cudaError_t launch_splines(const double* r, const double* N, int n, int force_po
     return cudaGetLastError();
 }
 
-cudaError_t launch_active(const double* N, int n, int32_t* active, int32_t* count, cudaStream_t stream)
+cudaError_t launch_active(const double* N, int n, int shard, int shards, int32_t* active, int32_t* count,
+                          cudaStream_t stream)
 {
-    active_kernel<<<1, 1024, 0, stream>>>(N, n, active, count);
+    active_kernel<<<1, 1024, 0, stream>>>(N, n, shard, shards, active, count);
     return cudaGetLastError();
 }
 

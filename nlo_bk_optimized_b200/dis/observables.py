@@ -138,6 +138,8 @@ class _Job:
     options: VegasOptions | None = None  # None: tensor Gauss-Legendre
     points: int = 24
     lo_Y: float | None = None            # LO jobs on a BK table: rapidity to initialise at
+    fixed: tuple | None = None           # fixed-Sobol qqbar-g job: (polarisation, quark)
+    done: bool = False
     value: float = 0.0
     error: float = 0.0
     n_eval: int = 0
@@ -159,11 +161,21 @@ class _Engine:
         precision = _precision(self.config)
         native = self.dipole.native()
         pending = []
+        todo = [j for j in self.jobs if not j.done]
+        for job in todo:
+            if job.fixed is not None:
+                from nlo_bk_optimized_b200.dis.fixed_sobol import FIXED_SOBOL_EVALUATIONS, fixed_sobol_device
+
+                pol, quark = job.fixed
+                _, est = fixed_sobol_device(job.kin.Q2, job.kin.xbj, pol, quark, self.dipole, self.config,
+                                            seed=job.seed, device=self.device, precision=precision)
+                pending.append(("fixed", [job], est))
+        todo = [j for j in todo if j.fixed is None]
         # Gauss-Legendre jobs first, grouped by the table rapidity they initialise at (the
         # reference initialises the BK table before each LO integral, and the later terms
         # see that state)
         gl_groups: dict[tuple, list[_Job]] = {}
-        for job in self.jobs:
+        for job in todo:
             if job.options is None:
                 gl_groups.setdefault((job.lo_Y if job.term == TERMS["LO"] else None, job.term, job.points),
                                      []).append(job)
@@ -180,7 +192,7 @@ class _Engine:
                                        device=self.device)
             pending.append(("gl", group, out))
         vegas_groups: dict[tuple, list[_Job]] = {}
-        for job in self.jobs:
+        for job in todo:
             if job.options is not None:
                 vegas_groups.setdefault((job.term, job.options), []).append(job)
         for (term, options), group in vegas_groups.items():
@@ -188,7 +200,17 @@ class _Engine:
                                 precision=precision, device=self.device)
             pending.append(("vegas", group, state_results(state, term, options.bins)))
         for kind, group, out in pending:
-            if kind == "gl":
+            for job in group:
+                job.done = True
+            if kind == "fixed":
+                est = out.cpu()
+                job = group[0]
+                totals = est.sum(dim=1)
+                job.value = float(totals.mean())
+                job.error = float(totals.std(unbiased=True) / math.sqrt(totals.numel()))
+                job.n_eval = FIXED_SOBOL_EVALUATIONS
+                job.converged = job.error <= self.config.epsrel * abs(job.value)
+            elif kind == "gl":
                 host = out.cpu()
                 for j, job in enumerate(group):
                     job.value = float(host[j, 0])
@@ -224,6 +246,36 @@ class _SigmaPlan:
     dip: list[list[_Job]]
     qg: list[list[_Job]]
     seed: int
+    qg_fixed: list[_Job] = field(default_factory=list)
+    Q2: float = 0.0
+    xbj: float = 0.0
+    pol: Polarization = Polarization.T
+    overrides: dict = field(default_factory=dict)
+
+
+def fixed_sobol_supported(dipole: Dipole, config: DISConfig, single_precision: bool) -> bool:
+    """_fixed_sobol_supported (dis/observables.py:644-660): GBW, nested 48-node inner rule,
+    a budget of at least FIXED_SOBOL_EVALUATIONS, and the single-precision (mixed) path."""
+    from nlo_bk_optimized_b200.dis.fixed_sobol import FIXED_SOBOL_EVALUATIONS
+
+    return (single_precision and config.cuda_fusion and config.cuda_nested and config.cuda_nested_points == 48
+            and isinstance(dipole, GBW) and config.maxeval >= FIXED_SOBOL_EVALUATIONS)
+
+
+def _plan_qg_vegas(engine: "_Engine", plan: _SigmaPlan) -> None:
+    config = engine.config
+    qg, offset = [], 0
+    qg_seed = plan.seed + 100
+    nested = config.cuda_nested
+    for quark in config.quarks:
+        kin = kinematics(plan.Q2, plan.xbj, plan.pol, config, quark)
+        opts = _vegas_options(config, config.maxeval, plan.overrides)
+        jobs = []
+        for term in ("I1", "I2N" if nested else "I2", "I3N" if nested else "I3"):
+            jobs.append(engine.add(_Job(TERMS[term], kin, seed=qg_seed + offset, options=opts)))
+            offset += 1
+        qg.append(jobs)
+    plan.qg = qg
 
 
 def _integration_overrides(options: dict) -> dict:
@@ -252,7 +304,7 @@ def _plan_lo(engine: _Engine, Q2: float, xbj: float, pol: Polarization, points: 
 
 
 def _plan_sigma(engine: _Engine, Q2: float, xbj: float, pol: Polarization, *, seed: int, points: int,
-                overrides: dict) -> _SigmaPlan:
+                overrides: dict, fixed: bool = False) -> _SigmaPlan:
     config, dipole = engine.config, engine.dipole
     if config.order is DISOrder.LO:
         return _SigmaPlan(_plan_lo(engine, Q2, xbj, pol, points), [], [], seed)
@@ -269,18 +321,26 @@ def _plan_sigma(engine: _Engine, Q2: float, xbj: float, pol: Polarization, *, se
             jobs.append(engine.add(_Job(TERMS[term], kin, seed=seed + offset, options=opts)))
             offset += 1
         dip.append(jobs)
-    qg, offset = [], 0
-    qg_seed = seed + 100
-    nested = config.cuda_nested
-    for quark in config.quarks:
-        kin = kinematics(Q2, xbj, pol, config, quark)
-        opts = _vegas_options(config, config.maxeval, overrides)
-        jobs = []
-        for term in ("I1", "I2N" if nested else "I2", "I3N" if nested else "I3"):
-            jobs.append(engine.add(_Job(TERMS[term], kin, seed=qg_seed + offset, options=opts)))
-            offset += 1
-        qg.append(jobs)
-    return _SigmaPlan(lo, dip, qg, seed)
+    plan = _SigmaPlan(lo, dip, [], seed, Q2=Q2, xbj=xbj, pol=pol, overrides=overrides)
+    if fixed and fixed_sobol_supported(dipole, config, True):
+        for index, quark in enumerate(config.quarks):
+            kin = kinematics(Q2, xbj, pol, config, quark)
+            plan.qg_fixed.append(engine.add(_Job(-1, kin, seed=seed + 100 + index, fixed=(pol, quark))))
+    else:
+        _plan_qg_vegas(engine, plan)
+    return plan
+
+
+def _run_with_fallback(engine: _Engine, plans: list[_SigmaPlan]) -> None:
+    """Run the engine; where a fixed-Sobol qqbar-g result did not converge, integrate that
+    plan's qqbar-g terms by Vegas instead (dis/observables.py:470-489)."""
+    engine.run()
+    retry = [p for p in plans if p.qg_fixed and not all(j.converged for j in p.qg_fixed)]
+    for plan in retry:
+        plan.qg_fixed = []
+        _plan_qg_vegas(engine, plan)
+    if retry:
+        engine.run()
 
 
 def _sigma_result(plan: _SigmaPlan, config: DISConfig, device: torch.device) -> IntegralResult:
@@ -291,8 +351,11 @@ def _sigma_result(plan: _SigmaPlan, config: DISConfig, device: torch.device) -> 
     per_quark = [_sum_results([_result(j, q.charge**2, device, None) for j in jobs], seed)
                  for q, jobs in zip(config.quarks, plan.dip)]
     dip = _scale_result(_sum_results(per_quark, seed), DIP_FACTOR)
-    per_quark = [_sum_results([_result(j, q.charge**2, device, None) for j in jobs], seed + 100)
-                 for q, jobs in zip(config.quarks, plan.qg)]
+    if plan.qg_fixed:
+        per_quark = [_result(j, q.charge**2, device, None) for q, j in zip(config.quarks, plan.qg_fixed)]
+    else:
+        per_quark = [_sum_results([_result(j, q.charge**2, device, None) for j in jobs], seed + 100)
+                     for q, jobs in zip(config.quarks, plan.qg)]
     qg = _scale_result(_sum_results(per_quark, seed + 100), QG_FACTOR)
     return _sum_results((lo, dip, qg), seed)
 
@@ -335,11 +398,14 @@ def sigma_qg_d2b(Q2: torch.Tensor, xbj: torch.Tensor, polarization: Polarization
     nlo = DISConfig(**{**{f: getattr(config, f) for f in config.__dataclass_fields__}, "order": DISOrder.NLO})
     engine = _Engine(dipole, nlo, _device(Q2))
     plan = _plan_sigma(engine, float(Q2), float(xbj), polarization, seed=seed - 100, points=24,
-                       overrides=_integration_overrides(options))
-    engine.jobs = [j for jobs in plan.qg for j in jobs]
-    engine.run()
-    per_quark = [_sum_results([_result(j, q.charge**2, engine.device, None) for j in jobs], seed)
-                 for q, jobs in zip(config.quarks, plan.qg)]
+                       overrides=_integration_overrides(options), fixed=Q2.dtype == torch.float32)
+    engine.jobs = list(plan.qg_fixed) + [j for jobs in plan.qg for j in jobs]
+    _run_with_fallback(engine, [plan])
+    if plan.qg_fixed:
+        per_quark = [_result(j, q.charge**2, engine.device, None) for q, j in zip(config.quarks, plan.qg_fixed)]
+    else:
+        per_quark = [_sum_results([_result(j, q.charge**2, engine.device, None) for j in jobs], seed)
+                     for q, jobs in zip(config.quarks, plan.qg)]
     return _scale_result(_sum_results(per_quark, seed), QG_FACTOR)
 
 
@@ -349,8 +415,8 @@ def photon_proton_cross_section_d2b(Q2: torch.Tensor, xbj: torch.Tensor, polariz
     _validate_kinematics(Q2, xbj)
     engine = _Engine(dipole, config, _device(Q2))
     plan = _plan_sigma(engine, float(Q2), float(xbj), polarization, seed=seed, points=quadrature_points,
-                       overrides=_integration_overrides(options))
-    engine.run()
+                       overrides=_integration_overrides(options), fixed=Q2.dtype == torch.float32)
+    _run_with_fallback(engine, [plan])
     return _sigma_result(plan, config, engine.device)
 
 
@@ -377,8 +443,9 @@ def _two_polarisations(Q2: torch.Tensor, xbj: torch.Tensor, dipole: Dipole, conf
     plans = []
     for pol, opts in ((Polarization.T, options_T), (Polarization.L, options_L)):
         plans.append(_plan_sigma(engine, float(Q2), float(xbj), pol, seed=opts.get("seed", 0),
-                                 points=opts.get("quadrature_points", 24), overrides=_integration_overrides(opts)))
-    engine.run()
+                                 points=opts.get("quadrature_points", 24), overrides=_integration_overrides(opts),
+                                 fixed=Q2.dtype == torch.float32))
+    _run_with_fallback(engine, plans)
     factor = _sf_factor(float(Q2), config)
     return tuple(_scale_result(_sigma_result(p, config, engine.device), factor) for p in plans)
 
@@ -407,7 +474,7 @@ def sigma_r(Q2: torch.Tensor, xbj: torch.Tensor, dipole: Dipole, config: DISConf
 
 def structure_functions(Q2: torch.Tensor, xbj: torch.Tensor, dipole: Dipole, config: DISConfig, *,
                         sqrt_s: float | None = None, seed: int = 0, quadrature_points: int = 24,
-                        **options) -> dict[str, torch.Tensor]:
+                        fixed_sobol: bool | None = None, **options) -> dict[str, torch.Tensor]:
     """F_T, F_L, F_2 (and sigma_r when sqrt_s is given) for many (Q^2, x_Bj) points in one
     batched device run.  Every point uses the single-point functions' seeds (F_T: seed,
     F_L: seed + 1000), so each entry equals F2(Q2[i], xbj[i], ..., seed=seed) run alone."""
@@ -420,14 +487,16 @@ def structure_functions(Q2: torch.Tensor, xbj: torch.Tensor, dipole: Dipole, con
     device = _device(Q2 if isinstance(Q2, torch.Tensor) else None)
     engine = _Engine(dipole, config, device)
     overrides = _integration_overrides(options)
+    # the fixed-Sobol qqbar-g path follows the single-point rule: GBW and the mixed build
+    fixed = (config.precision == "mixed") if fixed_sobol is None else fixed_sobol
     plans = []
     for i in range(Q2h.numel()):
         q2, x = float(Q2h[i]), float(xh[i])
         plans.append((_plan_sigma(engine, q2, x, Polarization.T, seed=seed, points=quadrature_points,
-                                  overrides=overrides),
+                                  overrides=overrides, fixed=fixed),
                       _plan_sigma(engine, q2, x, Polarization.L, seed=seed + 1000, points=quadrature_points,
-                                  overrides=overrides)))
-    engine.run()
+                                  overrides=overrides, fixed=fixed)))
+    _run_with_fallback(engine, [p for pair in plans for p in pair])
     out = {k: torch.empty(Q2h.numel(), dtype=torch.float64) for k in ("FT", "FL", "F2", "FT_error", "FL_error",
                                                                       "F2_error")}
     for i, (pt, pl) in enumerate(plans):

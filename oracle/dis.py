@@ -998,3 +998,88 @@ def structure_function_factor(Q2, transverse_area=1.0):
 def reduced_cross_section(F2, FL, Q2, xbj, sqrt_s):
     y = Q2 / (sqrt_s**2 * xbj)
     return F2 - y * y / (1 + (1 - y) ** 2) * FL
+
+
+# ----------------------------------------------------------------------------- fixed-Sobol qg path
+
+
+def map_importance_grid(points, edges):
+    """Unit points through the importance grid: source, inverse density and bins
+    (dis/fixed_sobol.py:100-112)."""
+    bins = edges.shape[1] - 1
+    scaled = points * bins
+    bi = np.minimum(np.floor(scaled).astype(np.int64), bins - 1)
+    frac = scaled - bi
+    d = np.arange(edges.shape[0])
+    left = edges[d, bi]
+    width = edges[d, bi + 1] - left
+    return left + width * frac, np.prod(bins * width, axis=1), bi
+
+
+def paired_endpoint_inputs(source, maxr, fold_angle=False):
+    """Split the gluon plane by the nearer dipole end (dis/fixed_sobol.py:115-158): the
+    two 5D inputs and their weights."""
+    parent = maxr * source[:, 2]
+    radial = source[:, 3]
+    af = 0.5 * source[:, 4] if fold_angle else source[:, 4]
+    angle = 2 * np.pi * af
+    c, s = np.cos(angle), np.sin(angle)
+    tiny = np.finfo(np.float64).tiny
+    with np.errstate(divide="ignore"):
+        closer = np.where(c > 0, parent / (2 * np.maximum(c, tiny)), np.inf)
+    first_limit = np.minimum(maxr, closer)
+    first = source.copy()
+    first[:, 3] = radial * first_limit / maxr
+    first[:, 4] = af
+    first_weight = first_limit / maxr
+    disk = parent * c + np.sqrt(np.maximum(maxr**2 - parent**2 * s**2, 0))
+    second_limit = np.maximum(np.minimum(disk, closer), 0)
+    sr = radial * second_limit
+    gx, gy = parent - sr * c, sr * s
+    gr = np.sqrt(gx**2 + gy**2)
+    second = source.copy()
+    second[:, 3] = gr / maxr
+    second[:, 4] = np.remainder(np.arctan2(gy, gx), 2 * np.pi) / (2 * np.pi)
+    second_weight = sr * second_limit / (np.maximum(gr, tiny) * maxr)
+    return first, first_weight, second, second_weight
+
+
+def qg_triple(x, kin: Kinematics, dipole, points=48):
+    """(I1, I2, I3) at x: the un-nested I1 and the nested I2, I3."""
+    return (qg_integrand(x, kin, "I1", dipole), qg_integrand(x, kin, "I2n", dipole, points),
+            qg_integrand(x, kin, "I3n", dipole, points))
+
+
+def fixed_sobol(triple, training, replicates, maxr, bins=32, fold_angle=True, i1_weight=1.0):
+    """learn_triple_importance_grid (dis/fixed_sobol.py:161-211) then the replicate
+    estimates of integrate_triple_fixed_sobol (:214-270).  Returns (edges, estimates
+    [replicates, 3])."""
+    dims = training[0].shape[1]
+    edges = np.tile(np.linspace(0, 1, bins + 1), (dims, 1))
+    tiny = np.finfo(np.float64).tiny
+    for pts in training:
+        source, inv, bi = map_importance_grid(pts, edges)
+        first, fw, second, sw = paired_endpoint_inputs(source, maxr, fold_angle)
+        v1, v2 = triple(first), triple(second)
+        weighted = [(a * fw + b * sw) * inv for a, b in zip(v1, v2)]
+        score = sum(w * np.abs(v) / max(np.abs(v).mean(), tiny)
+                    for w, v in zip((i1_weight, 1.0, 1.0), weighted))
+        hist = np.zeros((dims, bins))
+        count = np.zeros((dims, bins))
+        for d in range(dims):
+            hist[d] = np.bincount(bi[:, d], weights=score, minlength=bins)
+            count[d] = np.bincount(bi[:, d], minlength=bins)
+        edges = adapt_edges(edges, hist, count)
+    estimates = []
+    for pts in replicates:
+        source, inv, _ = map_importance_grid(pts, edges)
+        first, fw, second, sw = paired_endpoint_inputs(source, maxr, fold_angle)
+        v1, v2 = triple(first), triple(second)
+        estimates.append([float(np.mean((a * fw + b * sw) * inv)) for a, b in zip(v1, v2)])
+    return edges, np.array(estimates)
+
+
+def replicate_result(values):
+    """Mean and standard error of replicate estimates (dis/fixed_sobol.py:258-268)."""
+    values = np.asarray(values, dtype=np.float64)
+    return float(values.mean()), float(values.std(ddof=1) / math.sqrt(values.size))

@@ -17,7 +17,10 @@ what its own functions return for seeded inputs:
 * ``integrand_dip_massive`` for T0/T1/T2 and Omega_L/ab/cd (dis/observables.py:107-172);
 * ``integrand_qgunsub_massive`` for I1 (5D), I2 (6D) and I3 (7D) (dis/observables.py:175-250);
 * one ``vegas`` run on a dipole term (numerics/integration.py:120-589) with its final grid;
-* LO-order F_T, F_L, F_2 (dis/observables.py:581-624).
+* LO-order F_T, F_L, F_2 (dis/observables.py:581-624);
+* the fixed-Sobol sampling pieces ``map_importance_grid`` and ``paired_endpoint_inputs``
+  (dis/fixed_sobol.py:100-158) and one ``_adapt_vegas_edges`` re-binning
+  (numerics/integration.py:804-866) on float64 inputs.
 
 Unit-cube points come from numpy's default_rng(20260301); each case is listed in
 ``cases`` with its kinematics.
@@ -173,6 +176,29 @@ def main() -> None:
         out[f"lo_sf_{kind}"] = np.array([float(FT(Q2, xbj, dip, config).value),
                                          float(FL(Q2, xbj, dip, config).value),
                                          float(F2(Q2, xbj, dip, config).value)])
+    # fixed-Sobol sampling pieces (dis/fixed_sobol.py:100-158) and the grid re-binning
+    # (numerics/integration.py:804-866) on float64 inputs, with their own generator
+    from nlo_torch.dis.fixed_sobol import map_importance_grid, paired_endpoint_inputs
+    from nlo_torch.numerics.integration import _adapt_vegas_edges
+
+    frng = np.random.default_rng(777)
+    fs_points = frng.uniform(0, 1, (256, 5))
+    widths = frng.uniform(0.2, 1.0, (5, 32))
+    fs_edges = np.concatenate([np.zeros((5, 1)), np.cumsum(widths, axis=1) / widths.sum(axis=1, keepdims=True)],
+                              axis=1)
+    fs_edges[:, -1] = 1.0
+    src, inv, bi = map_importance_grid(T64(fs_points), T64(fs_edges))
+    out["fs_points"], out["fs_edges"] = fs_points, fs_edges
+    out["fs_source"], out["fs_inv"], out["fs_bins"] = src.numpy(), inv.numpy(), bi.numpy()
+    for fold in (False, True):
+        f, fw, sc, sw = paired_endpoint_inputs(src, 5.0, fold_angle=fold)
+        tag = "fold" if fold else "nofold"
+        out[f"fs_first_{tag}"], out[f"fs_fw_{tag}"] = f.numpy(), fw.numpy()
+        out[f"fs_second_{tag}"], out[f"fs_sw_{tag}"] = sc.numpy(), sw.numpy()
+    hist = frng.uniform(0, 3, (5, 32))
+    count = frng.integers(0, 9, (5, 32)).astype(np.float64)
+    out["adapt_hist"], out["adapt_count"] = hist, count
+    out["adapt_edges"] = _adapt_vegas_edges(T64(fs_edges), T64(hist), T64(count), cuda_fusion=False).numpy()
     out["cases"] = np.array(names)
     np.savez_compressed(OUT, **out)
     print("wrote", OUT, sum(v.nbytes for v in out.values()), "bytes")

@@ -296,3 +296,90 @@ def test_vegas_is_deterministic():
     b = vegas_terms(_native.DIS_TERMS["I1"], [kin], dip.native(), opts, [0], precision=_native.PRECISION_MIXED,
                     device=torch.device("cuda"))
     assert torch.equal(a, b)
+
+
+# ----------------------------------------------------------------------------- fixed-Sobol qqbar-g path
+
+
+def _fixed_points(dims, seed, n):
+    return torch.quasirandom.SobolEngine(dims, scramble=True, seed=seed).draw_base2(
+        int(math.log2(n)), dtype=torch.float32).double().numpy()
+
+
+@pytest.mark.parametrize("transverse", [True, False])
+def test_fixed_sobol_matches_oracle(transverse):
+    """Device fixed-Sobol flow (FP64) against the oracle's restatement on the same points:
+    grid after training and every replicate estimate."""
+    from nlo_bk_optimized_b200 import _native
+    from nlo_bk_optimized_b200.dis import DISConfig, Quark, QuarkType
+    from nlo_bk_optimized_b200.dis.fixed_sobol import fixed_sobol_device
+
+    config = DISConfig(quarks=(Quark(QuarkType.C, 1.4),), maxr=5.0, nf_alphas=1)
+    dip = gbw_obj()
+    Q2, xbj, seed = 9.0, 1e-3, 21
+    nt, rounds, nr, reps = 1024, 2, 512, 3
+    grid, est = fixed_sobol_device(Q2, xbj, pol_of(transverse), config.quarks[0], dip, config, seed=seed,
+                                   device=torch.device("cuda"), precision=_native.PRECISION_FP64,
+                                   training_samples=nt, training_rounds=rounds, samples_per_replicate=nr,
+                                   replicates=reps)
+    q, lam, g, x0 = GOLDEN["gbw_params"]
+    odip = od.GBWDipole(qs0sqr=q, lam=lam, gamma=g, x0=x0)
+    okin = od.Kinematics(Q2=Q2, xbj=xbj, mf=1.4, transverse=transverse, maxr=5.0, active_flavors=1)
+    training = [_fixed_points(5, seed + r, nt) for r in range(rounds)]
+    replicates = [_fixed_points(5, seed + 10_000 + j, nr) for j in range(reps)]
+    edges, ref = od.fixed_sobol(lambda x: od.qg_triple(x, okin, odip), training, replicates, 5.0, bins=32)
+    got_edges = grid[: 5 * 33].reshape(5, 33).cpu().numpy()
+    assert np.max(np.abs(got_edges - edges)) < 1e-10
+    assert rel_err(est.cpu().numpy(), ref) < 1e-9
+
+
+REFERENCE_CPP = {  # T/benchmarks/dis_fixed_sobol_all_qg.py:69-76: (value, standard error)
+    ("L", 0): (0.10206739088678346, 0.0002535000977528945),
+    ("L", 1): (-0.024439455902300525, 0.00004764427185133986),
+    ("L", 2): (0.009414936380564324, 0.000026852425497947778),
+    ("T", 0): (0.40263591173620866, 0.0017956984452001683),
+    ("T", 1): (-0.08719375357937224, 0.00026850014906050766),
+    ("T", 2): (0.04848797141670969, 0.00013338145018266037),
+}
+
+
+@pytest.mark.parametrize("transverse", [True, False])
+def test_fixed_sobol_agrees_with_reference_cpp_values(transverse):
+    """Statistical pin: the GBW charm workload of the reference's fixed-Sobol benchmark
+    (GBW(1, 0.3, 1, 1), m = 1.4, Q^2 = 9, x = 1e-3, maxr = 5, nf = 1, seed 3100) against the
+    C++ values it quotes; agreement within 5 combined standard errors."""
+    from nlo_bk_optimized_b200 import _native
+    from nlo_bk_optimized_b200.dipole import GBW
+    from nlo_bk_optimized_b200.dis import DISConfig, Quark, QuarkType
+    from nlo_bk_optimized_b200.dis.fixed_sobol import fixed_sobol_device
+
+    config = DISConfig(quarks=(Quark(QuarkType.C, 1.4),), maxr=5.0, nf_alphas=1, epsrel=0.001)
+    dip = GBW(Qs0sqr=1.0, lambda_=0.3, gamma=1.0, x0=1.0)
+    _, est = fixed_sobol_device(9.0, 1e-3, pol_of(transverse), config.quarks[0], dip, config, seed=3100,
+                                device=torch.device("cuda"), precision=_native.PRECISION_MIXED)
+    est = est.cpu().numpy()
+    tag = "T" if transverse else "L"
+    for k in range(3):
+        value, err = od.replicate_result(est[:, k])
+        ref, ref_err = REFERENCE_CPP[(tag, k)]
+        assert abs(value - ref) <= 5 * math.hypot(err, ref_err), (tag, k, value, err, ref, ref_err)
+
+
+def test_sigma_qg_dispatches_by_precision():
+    """float32 kinematics with GBW take the fixed-Sobol path (FIXED_SOBOL_EVALUATIONS
+    evaluations per quark); float64 takes Vegas."""
+    from nlo_bk_optimized_b200.dipole import GBW
+    from nlo_bk_optimized_b200.dis import FIXED_SOBOL_EVALUATIONS, DISConfig, Polarization, Quark, QuarkType
+    from nlo_bk_optimized_b200.dis import sigma_qg_d2b
+
+    config = DISConfig(quarks=(Quark(QuarkType.C, 1.4),), maxr=5.0, nf_alphas=1, epsrel=0.05)
+    dip = GBW(Qs0sqr=1.0, lambda_=0.3, gamma=1.0, x0=1.0)
+    r32 = sigma_qg_d2b(torch.tensor(9.0, device="cuda"), torch.tensor(1e-3, device="cuda"), Polarization.L, dip,
+                       config, seed=0)
+    assert r32.n_eval == FIXED_SOBOL_EVALUATIONS
+    small = DISConfig(quarks=config.quarks, maxr=5.0, nf_alphas=1, epsrel=0.05, maxeval=20_000)
+    r64 = sigma_qg_d2b(torch.tensor(9.0, dtype=torch.float64, device="cuda"),
+                       torch.tensor(1e-3, dtype=torch.float64, device="cuda"), Polarization.L, dip, small, seed=0)
+    assert r64.n_eval != FIXED_SOBOL_EVALUATIONS
+    diff = abs(float(r64.value) - float(r32.value))
+    assert diff <= 5 * math.hypot(float(r64.error), float(r32.error)) + 0.02 * abs(float(r32.value))

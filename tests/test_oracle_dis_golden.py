@@ -165,3 +165,29 @@ def test_lo_structure_functions(kind):
     assert out[0] == pytest.approx(FTv, rel=1e-12)
     assert out[1] == pytest.approx(FLv, rel=1e-12)
     assert out[0] + out[1] == pytest.approx(F2v, rel=1e-12)
+
+
+def test_fixed_sobol_sampling_pieces():
+    """map_importance_grid, paired_endpoint_inputs and the grid re-binning against the
+    reference's own functions."""
+    src, inv, bi = od.map_importance_grid(GOLDEN["fs_points"], GOLDEN["fs_edges"])
+    assert np.array_equal(bi, GOLDEN["fs_bins"])
+    assert rel(src, GOLDEN["fs_source"], 1e-300) < 1e-14
+    assert rel(inv, GOLDEN["fs_inv"], 1e-300) < 1e-13
+    for fold in (False, True):
+        tag = "fold" if fold else "nofold"
+        f, fw, s, sw = od.paired_endpoint_inputs(GOLDEN["fs_source"], 5.0, fold)
+        assert rel(f, GOLDEN[f"fs_first_{tag}"], 1e-300) < 1e-13
+        assert rel(fw, GOLDEN[f"fs_fw_{tag}"], 1e-300) < 1e-13
+        assert rel(s, GOLDEN[f"fs_second_{tag}"], 1e-12) < 1e-12
+        assert rel(sw, GOLDEN[f"fs_sw_{tag}"], 1e-300) < 1e-12
+    new = od.adapt_edges(GOLDEN["fs_edges"], GOLDEN["adapt_hist"], GOLDEN["adapt_count"])
+    assert np.max(np.abs(new - GOLDEN["adapt_edges"])) < 1e-15
+
+
+def test_fixed_sobol_replicate_statistics_known_answer():
+    """The correlated-replicate total of T/tests/test_dis_production.py:153-192: replicate
+    totals (0.7, 0.7, 0.65) give their mean and std/sqrt(3)."""
+    mean, err = od.replicate_result([0.7, 0.7, 0.65])
+    assert mean == pytest.approx(np.mean([0.7, 0.7, 0.65]), rel=1e-15)
+    assert err == pytest.approx(np.std([0.7, 0.7, 0.65], ddof=1) / math.sqrt(3), rel=1e-15)

@@ -13,6 +13,13 @@ A bench "step" is one RK4 step (four right-hand sides).  With the default
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
+With --gpus N > 1 (one process per GPU under torchrun) the parents are sharded over the
+ranks with one NCCL all-reduce of dN/dY per RK stage; the total work is fixed (strong
+scaling) and the value is the slowest rank's device time.
+
+The line also carries a "dis" object: NLO DIS sigma_r throughput on a BK table evolved by
+the same workload (see measure_dis); --workload dis prints that measurement alone.
+
 --impl reference times the reference algorithm on the host cores (the oracle's
 C restatement, all threads) on a bounded sample of every step and reports the
 same metric extrapolated to the full workload.
@@ -183,10 +190,37 @@ def run_ours(args) -> None:
     table = torch.empty((max(steps, warmup) + 1, points), dtype=torch.float64, device=device)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)
 
-    def rk4_step(row: int) -> None:
-        _native.check(lib.nlo_bk_evolve(params, r.data_ptr(), points, 1, STEP, _native.STEPPERS["rk4"], dirs,
-                                        SAMPLES, box, table[row].data_ptr(), status.data_ptr(), ws.data_ptr(),
-                                        ws.numel(), stream.cuda_stream))
+    if world == 1:
+        def rk4_step(row: int) -> None:
+            _native.check(lib.nlo_bk_evolve(params, r.data_ptr(), points, 1, STEP, _native.STEPPERS["rk4"], dirs,
+                                            SAMPLES, box, table[row].data_ptr(), status.data_ptr(), ws.data_ptr(),
+                                            ws.numel(), stream.cuda_stream))
+    else:
+        # parents sharded over the ranks (i % world == rank), one NCCL all-reduce of the
+        # R-point derivative per stage (nlo_bk_optimized_b200/bk/sharded.py)
+        import ctypes
+
+        from nlo_bk_optimized_b200.bk.sharded import shard_steps
+
+        def shard_rhs(N):
+            out = torch.empty_like(N)
+            _native.check(lib.nlo_bk_rhs_shard(params, r.data_ptr(), N.data_ptr(), points, rank, world, dirs,
+                                               SAMPLES, box, out.data_ptr(), ws.data_ptr(), ws.numel(),
+                                               stream.cuda_stream))
+            return out
+
+        def shard_stage(N, ks, coefs, clamp):
+            out = torch.empty_like(N)
+            kp = (ctypes.c_void_p * len(ks))(*[k.data_ptr() for k in ks])
+            cf = (ctypes.c_double * len(coefs))(*coefs)
+            _native.check(lib.nlo_bk_stage(N.data_ptr(), kp, cf, len(ks), points, int(clamp), out.data_ptr(),
+                                           status.data_ptr() if clamp else None, stream.cuda_stream))
+            return out
+
+        def rk4_step(row: int) -> None:
+            rows = shard_steps(table[row], 1, STEP, "rk4", shard_rhs,
+                               lambda k: dist.all_reduce(k, op=dist.ReduceOp.SUM), shard_stage, True)
+            table[row + 1].copy_(rows[1])
 
     # warm-up: W steps from the initial condition (discarded)
     table[0].copy_(N0_host.to(device))
@@ -247,7 +281,13 @@ def run_ours(args) -> None:
     if world > 1:
         dist.barrier()
     t0 = time.perf_counter()
-    result = solve_bk(MV(qs0sqr=QS0SQR), e2e_maxy, e2e_config, device=device, dtype=torch.float32, seed=0)
+    if world == 1:
+        result = solve_bk(MV(qs0sqr=QS0SQR), e2e_maxy, e2e_config, device=device, dtype=torch.float32, seed=0)
+    else:
+        from nlo_bk_optimized_b200.bk.sharded import solve_bk_sharded
+
+        result = solve_bk_sharded(MV(qs0sqr=QS0SQR), e2e_maxy, e2e_config, device=device, dtype=torch.float32,
+                                  seed=0)
     host_table = result.N.cpu()
     e2e_s = time.perf_counter() - t0
     h2d = 2 * points * 8
@@ -301,14 +341,18 @@ def run_ours(args) -> None:
         "warmup": warmup,
         "ms_per_step": round(step_ms, 4),
         "higher_is_better": False,
-        "scaling": "weak" if world > 1 else "strong",
+        "scaling": "strong",
         "vs_baseline": None,
         "dtype": "f32+f64",
         "data": "synthetic (MV initial condition)",
-        "config": workload_description({"parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+        "config": workload_description({"parallelism": (f"r parents sharded over {world} GPUs, one NCCL "
+                                                         "all-reduce of dN/dY per stage") if world > 1
+                                        else "single GPU",
                                         "active_parents_final": n_active}),
         "e2e": {"value": round(e2e_seconds, 4), "unit": UNIT, "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h, "api": "nlo_bk_optimized_b200.solve_bk + table.N.cpu()"},
+                "d2h_bytes_per_step": d2h,
+                "api": ("nlo_bk_optimized_b200.solve_bk" if world == 1 else
+                        "nlo_bk_optimized_b200.bk.sharded.solve_bk_sharded") + " + table.N.cpu()"},
         "gpu_launches": LAUNCHES_PER_STEP * steps,
         "roofline": roofline,
         "clocks": clocks,

@@ -61,7 +61,7 @@ LAUNCHES_PER_STEP = 4 * 6 + 4
 SM_COUNT = 148
 FP32_LANES_PER_SM = 128
 # CPU baseline sample (about 10 s of host work): K2+Kf points per parent and K1 parents
-CPU_K2_LOG2 = 19
+CPU_K2_LOG2 = 21
 CPU_K1_PARENTS = 128
 
 

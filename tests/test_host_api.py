@@ -159,3 +159,21 @@ def test_c_struct_layouts_match_ctypes(tmp_path):
           _native.DisKinematics.max_alpha.offset, ctypes.sizeof(_native.Dipole), _native.Dipole.table.offset,
           ctypes.sizeof(_native.VegasOptions), _native.VegasOptions.keep_edges.offset]
     assert c == py
+
+
+def test_serving_helpers():
+    """Rapidity range and Vegas settings of a served request, and the latency quantiles."""
+    import math
+
+    from nlo_bk_optimized_b200.serving import ServerStats, dis_options_for, maxy_for
+
+    assert maxy_for([(10.0, 1e-3)], step=0.2) >= math.log(10.0 / 1e-3)
+    assert abs(maxy_for([(10.0, 1e-3)], step=0.2) / 0.2 - round(maxy_for([(10.0, 1e-3)], step=0.2) / 0.2)) < 1e-9
+    assert dis_options_for(1 << 20)["vegas_samples"] == (1 << 20) // 16
+    assert dis_options_for(1 << 10)["vegas_samples"] == 4096
+    stats = ServerStats(latencies=[0.1 * k for k in range(1, 101)], points=300, requests=100, started=0.0,
+                        finished=10.0)
+    summary = stats.summary()
+    assert summary["p50_s"] == pytest.approx(5.0)
+    assert summary["p99_s"] == pytest.approx(9.9)
+    assert summary["points_per_s"] == pytest.approx(30.0)

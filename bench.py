@@ -603,6 +603,150 @@ def run_dis(args) -> None:
     print(json.dumps(measure_dis(args.dis_points, args.dis_single, args.dis_check)))
 
 
+# ---------------------------------------------------------------------------
+# Batched and served workloads: parameter sets drawn from a seeded generator
+# (Qs0^2 ~ U[0.05, 0.5], gamma ~ U[0.8, 1.3], e_c ~ logU[1, 100]), each evolved with the
+# 200-point grid in [1e-6, 1e2] (RK4, h = 0.2, frozen-coupling cap 0.7) and uneven Monte
+# Carlo budgets 2^U{16..20} Sobol points per r per stage.
+
+def _sets(n: int, seed: int = 0):
+    import torch
+
+    g = torch.Generator().manual_seed(seed)
+    u = torch.rand((n, 4), generator=g, dtype=torch.float64)
+    qs = 0.05 + 0.45 * u[:, 0]
+    gamma = 0.8 + 0.5 * u[:, 1]
+    ec = torch.exp(u[:, 2] * math.log(100.0))
+    budgets = (2 ** (16 + torch.floor(u[:, 3] * 5))).to(torch.int64)
+    return [(float(qs[i]), float(gamma[i]), float(ec[i]), int(budgets[i])) for i in range(n)]
+
+
+def _small_bk_config(samples: int = 1 << 16):
+    from nlo_bk_optimized_b200 import BKConfig
+
+    return BKConfig(RPOINTS=199, MINR=1e-6, MAXR=1e2, MCINTPOINTS=samples, DE_SOLVER_STEP=0.2, STEPPER="rk4",
+                    PRECISION="mixed", ALPHA_S_CAP=0.7)
+
+
+def run_batch(args) -> None:
+    """256 parameter sets evolved to Y = 8 (the rapidity 8 points of Q^2 in [1, 50], x in
+    [1e-3, 1e-2] reach is ln(Q^2/(x Q0^2)) <= 10.8; the sets stop at Y = 8 and the DIS points
+    of each set are drawn so that they stay inside its table) in one stream-parallel run,
+    against the same sets solved one after another on one stream (a sample of them)."""
+    import torch
+
+    from nlo_bk_optimized_b200 import MV
+    from nlo_bk_optimized_b200.bk.batch import evolve_batch, tune_streams
+    from nlo_bk_optimized_b200.bk.evolution import _r_grid, _steps_to
+
+    device = torch.device("cuda", 0)
+    torch.cuda.set_device(device)
+    sets = _sets(args.batch_sets)
+    config = _small_bk_config()
+    r_host = _r_grid(config, device="cpu", dtype=torch.float64)
+    N0 = torch.stack([MV(qs0sqr=q, gamma=g, ec=e).dipole_amplitude(r_host).to(torch.float64)
+                      for q, g, e, _ in sets]).to(device)
+    r = r_host.to(device)
+    budgets = [b for *_, b in sets]
+    steps = len(_steps_to(0.0, args.batch_maxy, 0.2))
+    streams = tune_streams(N0, r, config, budgets)
+    evolve_batch(N0[:2], r, 1, config, budgets[:2], streams=2)  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    evolve_batch(N0, r, steps, config, budgets, streams=streams)
+    torch.cuda.synchronize()
+    batched = time.perf_counter() - t0
+    sample = list(range(0, len(sets), max(1, len(sets) // 16)))[:16]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in sample:
+        evolve_batch(N0[i:i + 1], r, steps, config, budgets[i:i + 1], streams=1)
+    torch.cuda.synchronize()
+    single = (time.perf_counter() - t0) / len(sample)
+    evals = sum(budgets) * 200 * 4 * steps
+    line = {
+        "metric": "batched NLO BK evolutions per second",
+        "value": round(len(sets) / batched, 3),
+        "unit": "parameter sets/s",
+        "n_gpus": 1,
+        "higher_is_better": True,
+        "dtype": "f32+f64",
+        "data": "synthetic: MV parameter sets from torch.Generator().manual_seed(0)",
+        "config": {"workload": f"{len(sets)} MV sets, 200 r in [1e-6,1e2], RK4 h=0.2 to Y={args.batch_maxy}, "
+                               "budgets 2^U{16..20} per r per stage, alpha_s cap 0.7",
+                   "streams_chosen": streams, "k2kf_evaluations": evals},
+        "batched_s": round(batched, 4),
+        "single_set_s_mean": round(single, 5),
+        "speedup_vs_one_at_a_time": round(single * len(sets) / batched, 3),
+    }
+    print(json.dumps(line))
+
+
+def run_serve(args) -> None:
+    """Poisson arrivals: each request is one parameter set, 1-64 (Q^2, x) points of the
+    32 x 16 DIS grid restricted to x >= 1e-3 (table range), and its Monte Carlo budget; p50/p99
+    latency and points/s of the server against the same requests run one at a time."""
+    import random
+
+    import torch
+
+    from nlo_bk_optimized_b200.dis import DISConfig, DISOrder, Quark, QuarkType
+    from nlo_bk_optimized_b200.serving import Request, Server, run_alone
+
+    device = torch.device("cuda", 0)
+    torch.cuda.set_device(device)
+    rng = random.Random(0)
+    sets = _sets(4096, seed=1)
+    Q2s = [1.0 * (50.0 ** (k / 31)) for k in range(32)]
+    xs = [1e-3 * (10.0 ** (k / 15)) for k in range(16)]
+    grid = [(q, x) for q in Q2s for x in xs]
+    t, requests = 0.0, []
+    while t < args.serve_seconds:
+        t += rng.expovariate(args.serve_rate)
+        q, g, e, budget = sets[len(requests) % len(sets)]
+        pts = tuple(rng.sample(grid, rng.randint(1, 64)))
+        requests.append((t, Request(q, g, e, pts, budget, seed=len(requests))))
+    bk = _small_bk_config()
+    dis = DISConfig(order=DISOrder.NLO, quarks=(Quark(QuarkType.LIGHT, 0.14),), vegas_bins=32)
+    run_alone(requests[0][1], bk, dis)  # warm-up
+    server = Server(bk, dis, slots=args.serve_slots)
+    t0 = time.perf_counter()
+    futures = []
+    for at, req in requests:
+        delay = at - (time.perf_counter() - t0)
+        if delay > 0:
+            time.sleep(delay)
+        futures.append(server.submit(req))
+    for f in futures:
+        f.result()
+    server.close()
+    served = server.stats.summary()
+    sample = requests[: min(8, len(requests))]
+    t1 = time.perf_counter()
+    for _, req in sample:
+        run_alone(req, bk, dis)
+    alone = (time.perf_counter() - t1) / len(sample)
+    alone_pts = sum(len(r.points) for _, r in sample) / len(sample)
+    line = {
+        "metric": "served NLO BK + DIS requests: p50/p99 latency and points/s",
+        "value": round(served["points_per_s"], 3),
+        "unit": "points/s",
+        "n_gpus": 1,
+        "higher_is_better": True,
+        "dtype": "f32+f64",
+        "data": "synthetic Poisson arrivals, seeded",
+        "config": {"workload": f"Poisson {args.serve_rate}/s for {args.serve_seconds} s, 1-64 points per request, "
+                               "budgets 2^U{16..20}", "slots": args.serve_slots, "requests": len(requests)},
+        "p50_s": served["p50_s"],
+        "p99_s": served["p99_s"],
+        "requests_per_s": served["requests_per_s"],
+        "sequential_points_per_s": round(alone_pts / alone, 3),
+        "sequential_request_s_mean": round(alone, 4),
+        "speedup_vs_sequential": round(served["points_per_s"] / (alone_pts / alone), 3),
+    }
+    print(json.dumps(line))
+
+
 def main() -> None:
     parser = argparse.ArgumentParser()
     parser.add_argument("--gpus", type=int, default=1)
@@ -612,13 +756,25 @@ def main() -> None:
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--kernel-case", action="store_true",
                         help="run only the small K2+Kf/K1 case used for ncu captures")
-    parser.add_argument("--workload", choices=["bk", "dis"], default="bk",
-                        help="bk: the NLO BK evolution (default); dis: NLO DIS sigma_r throughput")
+    parser.add_argument("--workload", choices=["bk", "dis", "batch", "serve"], default="bk",
+                        help="bk: the NLO BK evolution (default); dis: NLO DIS sigma_r throughput; "
+                             "batch: many parameter sets at once; serve: the request loop under Poisson arrivals")
+    parser.add_argument("--batch-sets", type=int, default=256)
+    parser.add_argument("--batch-maxy", type=float, default=8.0)
+    parser.add_argument("--serve-rate", type=float, default=200.0)
+    parser.add_argument("--serve-seconds", type=float, default=1.0)
+    parser.add_argument("--serve-slots", type=int, default=8)
     parser.add_argument("--no-dis", action="store_true", help="skip the DIS sigma_r measurement")
     parser.add_argument("--dis-points", type=int, default=0, help="DIS: first N of the 512 points (0 = all)")
     parser.add_argument("--dis-single", type=int, default=4, help="DIS: points timed through single sigma_r calls")
     parser.add_argument("--dis-check", type=int, default=4, help="DIS: points recomputed in FP64")
     args = parser.parse_args()
+    if args.workload == "batch":
+        run_batch(args)
+        return
+    if args.workload == "serve":
+        run_serve(args)
+        return
     if args.workload == "dis":
         if args.kernel_case:
             run_dis_kernel_case()

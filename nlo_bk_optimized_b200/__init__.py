@@ -15,6 +15,8 @@ from nlo_bk_optimized_b200.bk import (
     compute_dndy,
     evolve_table,
     solve_bk,
+    solve_bk_batch,
+    solve_bk_sharded,
 )
 from nlo_bk_optimized_b200.dipole import DipoleTable, load_bk_table, save_bk_table
 
@@ -31,4 +33,6 @@ __all__ = [
     "load_bk_table",
     "save_bk_table",
     "solve_bk",
+    "solve_bk_batch",
+    "solve_bk_sharded",
 ]

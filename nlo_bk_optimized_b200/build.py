@@ -46,7 +46,7 @@ def _stale() -> bool:
 # Per-file flags.  The DIS kernels' FP32 bodies use approximate single-precision
 # division and square root (about 2 ulp) and flush FP32 denormals; their FP64 template
 # instances and every other file keep IEEE arithmetic.
-FILE_FLAGS = {"dis.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]}
+FILE_FLAGS = {name: ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"] for name in ("dis.cu", "dis_fixed.cu")}
 
 
 def _compile(source: Path, obj: Path, verbose: bool) -> tuple[int, str]:

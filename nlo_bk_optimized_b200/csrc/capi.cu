@@ -7,7 +7,10 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <utility>
 
 #include "common.cuh"
 #include "internal.h"
@@ -169,6 +172,25 @@ const K1Rule& k1_rule()
 int set_last_error(int code, const char* message) { return fail(code, message); }
 
 void gauss_legendre_rule(int n, double* x, double* w) { gauss_legendre(n, x, w); }
+
+cudaError_t raise_dynamic_smem(const void* func, size_t bytes)
+{
+    // The limit is a property of the kernel on the device, shared by every host thread:
+    // only ever raise it, so that a launch prepared by one thread is never invalidated by
+    // another thread lowering the limit for a smaller launch of the same kernel.
+    static std::mutex lock;
+    static std::map<std::pair<int, const void*>, size_t> limits;
+    if (bytes <= 48 * 1024) return cudaSuccess;  // within the default limit
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> guard(lock);
+    size_t& current = limits[{device, func}];
+    if (bytes <= current) return cudaSuccess;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) current = bytes;
+    return e;
+}
 
 size_t spline_doubles(int points) { return (size_t)points + 8 * (size_t)(points - 1); }
 

@@ -522,7 +522,7 @@ cudaError_t launch_vegas_round_t(const VegasLaunch& L, cudaStream_t stream)
     const size_t smem = sizeof(double) * (D * (L.bins + 1) + (kVegasThreads / 32) * D * L.bins) +
                         sizeof(int32_t) * D * L.bins;
     auto kern = vegas_iteration_kernel<T, TERM>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = raise_dynamic_smem((const void*)kern, smem);
     if (e != cudaSuccess) return e;
     dim3 grid(L.blocks_per_job, L.jobs);
     kern<<<grid, kVegasThreads, smem, stream>>>(static_cast<const DisArgs<T>*>(L.args), L.dirs, *L.rule, L.state,
@@ -536,7 +536,7 @@ cudaError_t launch_vegas_round_t(const VegasLaunch& L, cudaStream_t stream)
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const size_t fsmem = sizeof(double) * (D * L.bins + 2 * D * (L.bins + 1));
-    e = cudaFuncSetAttribute(vegas_finalize_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsmem);
+    e = raise_dynamic_smem((const void*)vegas_finalize_kernel, fsmem);
     if (e != cudaSuccess) return e;
     vegas_finalize_kernel<<<L.jobs, 128, fsmem, stream>>>(L.state, L.state_stride, D, L.bins, L.samples, L.reduced,
                                                           L.counts, L.warmup, L.min_iterations, L.epsrel, L.epsabs);
@@ -595,8 +595,7 @@ cudaError_t dis_launch_table_prepare(const double* r, const double* y, const dou
 cudaError_t dis_launch_table_initialize(double* table, int nr, int ny, double Y, cudaStream_t stream)
 {
     const size_t smem = sizeof(double) * 3 * (size_t)nr;
-    cudaError_t e = cudaFuncSetAttribute(dis::table_initialize_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    cudaError_t e = raise_dynamic_smem((const void*)dis::table_initialize_kernel, smem);
     if (e != cudaSuccess) return e;
     dis::table_initialize_kernel<<<1, 256, smem, stream>>>(table, nr, ny, Y);
     return cudaGetLastError();
@@ -648,7 +647,7 @@ cudaError_t dis_launch_reduce_finalize(int D, int bins, int jobs, int blocks_per
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const size_t fsmem = sizeof(double) * (D * bins + 2 * D * (bins + 1));
-    e = cudaFuncSetAttribute(dis::vegas_finalize_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsmem);
+    e = raise_dynamic_smem((const void*)dis::vegas_finalize_kernel, fsmem);
     if (e != cudaSuccess) return e;
     dis::vegas_finalize_kernel<<<jobs, 128, fsmem, stream>>>(state, state_stride, D, bins, samples, reduced, counts,
                                                                warmup, min_iterations, epsrel, epsabs);

@@ -312,7 +312,7 @@ int run_fixed(const dis::DisArgs<T>& args, const dis::InnerRule& rule, const nlo
     if (e != cudaSuccess) return fcuda(e, "fixed-Sobol init");
     const size_t hsmem =
         sizeof(double) * (kFixedThreads / 32) * kFixedDims * o.bins + sizeof(int32_t) * kFixedDims * o.bins;
-    e = cudaFuncSetAttribute(fixed_score_hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem);
+    e = raise_dynamic_smem((const void*)fixed_score_hist_kernel, hsmem);
     if (e != cudaSuccess) return fcuda(e, "fixed-Sobol histogram attribute");
     const uint64_t nt = (uint64_t)o.training_samples;
     const int tb = fixed_blocks(nt);

@@ -106,18 +106,45 @@ __device__ __forceinline__ K01<double> bessel_k01(double x)
     return out;
 }
 
+__device__ __forceinline__ float ex2_approx_f(float x)
+{
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+__device__ __forceinline__ float rcp_approx_f(float x)
+{
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// exp(-x) for x >= 0 from the hardware 2^x: x log2(e) is split into its rounded product
+// and the exact rounding error (one FMA) plus the low part of log2(e), and 2^(-lo) is taken
+// to first order; relative error about 3e-7 for every x up to the underflow.
+__device__ __forceinline__ float exp_neg_f(float x)
+{
+    constexpr float kLog2eHi = 1.44269502162933349609375f;  // float(log2 e)
+    constexpr float kLog2eLo = 1.925963033500011e-8f;        // log2 e - kLog2eHi
+    const float hi = x * kLog2eHi;
+    const float lo = fmaf(x, kLog2eHi, -hi) + x * kLog2eLo;
+    return ex2_approx_f(-hi) * fmaf(-lo, 0.69314718055994531f, 1.0f);
+}
+
 __device__ __forceinline__ K01<float> bessel_k01(float x)
 {
     using namespace nlo_special;
     K01<float> out;
+    const float rx = rcp_approx_f(x);
     if (x <= 2.0f) {
         const float t = 0.25f * x * x;
         const float L = logf(0.5f * x);
         out.k0 = fmaf(-L, horner(kI0SeriesF, t), horner(kQ0SeriesF, t));
-        out.k1 = __frcp_rn(x) + 0.5f * x * fmaf(L, horner(kI1SeriesF, t), -0.5f * horner(kQ1SeriesF, t));
+        out.k1 = rx + 0.5f * x * fmaf(L, horner(kI1SeriesF, t), -0.5f * horner(kQ1SeriesF, t));
     } else {
-        const float s = 2.0f * __frcp_rn(x);
-        const float e = expf(-x) * rsqrtf(x);
+        const float s = 2.0f * rx;
+        const float e = exp_neg_f(x) * rsqrtf(x);
         out.k0 = e * horner(kK0PolyF, s);
         out.k1 = e * horner(kK1PolyF, s);
     }

@@ -42,6 +42,10 @@ int k2kf_max_blocks();
 // Records a message for nlo_last_error() and returns code.
 int set_last_error(int code, const char* message);
 
+// Raise (never lower) a kernel's dynamic shared-memory limit on the current device to at
+// least `bytes`; safe when several host threads launch the same kernel with different sizes.
+cudaError_t raise_dynamic_smem(const void* func, size_t bytes);
+
 cudaError_t launch_splines(const double* r, const double* N, int n, int force_positive, double* factor,
                            int compute_factor, double* out, cudaStream_t stream);
 // active parents (index > 0, N <= 0.99999) with index % shards == shard

@@ -328,13 +328,13 @@ cudaError_t launch_k1(const nlo_bk_params& p, const double* r, int points, const
     };
     if (p.precision == NLO_PRECISION_FP64) {
         const size_t smem = smem_for(8);
-        e = cudaFuncSetAttribute(k1_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = raise_dynamic_smem((const void*)k1_kernel<double>, smem);
         if (e != cudaSuccess) return e;
         k1_kernel<double><<<dim3(points, kK1Split), kK1Threads, smem, stream>>>(phd, phd, consts, r, points, spline,
                                                                                 active, count, out);
     } else {
         const size_t smem = smem_for(4);
-        e = cudaFuncSetAttribute(k1_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = raise_dynamic_smem((const void*)k1_kernel<float>, smem);
         if (e != cudaSuccess) return e;
         k1_kernel<float><<<dim3(points, kK1Split), kK1Threads, smem, stream>>>(make_phys<float>(p), phd, consts, r,
                                                                                points, spline, active, count, out);

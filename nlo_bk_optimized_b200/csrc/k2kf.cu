@@ -491,8 +491,7 @@ cudaError_t launch_typed(const nlo_bk_params& p, const double* r, int points, co
     const size_t smem = sizeof(K2Rec<T>) * threads + sizeof(T) * (size_t)(points + 4 * (points - 1)) +
                         (sizeof(T) == sizeof(float) ? sizeof(float4) * (size_t)(points - 1) : 0) +
                         sizeof(uint32_t) * 124;
-    cudaError_t e = cudaFuncSetAttribute(k2kf_kernel<T, SYM, COUPLING>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = raise_dynamic_smem((const void*)k2kf_kernel<T, SYM, COUPLING>, smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k2kf_kernel<T, SYM, COUPLING>, threads, smem);

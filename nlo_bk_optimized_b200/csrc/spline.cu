@@ -150,7 +150,7 @@ cudaError_t launch_splines(const double* r, const double* N, int n, int force_po
 {
     const size_t smem = sizeof(double) * 9 * (size_t)n;
     if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(splines_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = raise_dynamic_smem((const void*)splines_kernel, smem);
         if (e != cudaSuccess) return e;
     }
     splines_kernel<<<1, 256, smem, stream>>>(r, N, n, force_positive, factor, compute_factor, out);

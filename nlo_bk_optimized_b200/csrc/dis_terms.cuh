@@ -737,9 +737,98 @@ __device__ T l_i3(const Trip<T>& t, const GSet<T>& G1, const GSet<T>& G2)
                      - (T)2 * c * a * G1.g11[0] * G2.g11[1]));
 }
 
+// FP32 form of the moment loop.  Per node y the reciprocal 1/y and sqrt(y) are shared by
+// the two sides; per side the quantities that do not depend on y (M2 = Qbar^2 + m^2, its
+// square root, lambda m^2, x3^2, omega x2^2) are formed once.  With q = sqrt(B/y):
+//   z0 = sqrt(M2) q,  z1 = sqrt(A1) q,  sqrt(A/B) = z sqrt(y)/B,  z1 - z0 = q delta/(sqrt(A1)+sqrt(M2)),
+// so each (node, side) needs two square roots and two reciprocals besides the Bessel pairs.
+__device__ __forceinline__ K01<float> bessel_k01_rcp(float x, float& rx)
+{
+    using namespace nlo_special;
+    K01<float> out;
+    rx = rcp_approx_f(x);
+    if (x <= 2.0f) {
+        const float t = 0.25f * x * x;
+        const float L = logf(0.5f * x);
+        out.k0 = fmaf(-L, horner(kI0SeriesF, t), horner(kQ0SeriesF, t));
+        out.k1 = rx + 0.5f * x * fmaf(L, horner(kI1SeriesF, t), -0.5f * horner(kQ1SeriesF, t));
+    } else {
+        const float e = exp_neg_f(x) * rsqrtf(x);
+        const float s = 2.0f * rx;
+        out.k0 = e * horner(kK0PolyF, s);
+        out.k1 = e * horner(kK1PolyF, s);
+    }
+    return out;
+}
+
+__device__ __forceinline__ GSet<float> g_moments_f32(const Trip<float>& t, const InnerRule& rule)
+{
+    GSet<float> m;
+    float M2[2], sM2[2], lm2[2], x3[2], wx2[2], om[2];
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+        m.g22[s] = m.g12[s] = m.g21[s] = m.g11[s] = 0.0f;
+        M2[s] = t.Qb2[s] + t.m2;
+        sM2[s] = sqrtf(M2[s]);
+        lm2[s] = t.lam[s] * t.m2;
+        x3[s] = t.x3sq[s];
+        wx2[s] = t.omega[s] * t.x2sq[s];
+        om[s] = t.omega[s];
+    }
+    for (int i = 0; i < rule.n; ++i) {
+        const float y = (float)rule.y[i];
+        const float w = (float)rule.w[i];
+        const float iy = rcp_approx_f(y);
+        const float sqy = sqrtf(y);
+        const float isqy = sqy * iy;  // 1/sqrt(y)
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+            const float B = fmaf(y, x3[s], wx2[s]);
+            const float iB = rcp_approx_f(B);
+            const float q = sqrtf(B * iy);
+            const float delta = y * lm2[s];
+            const float Al = delta + M2[s];
+            const float sAl = sqrtf(Al);
+            const float z1 = sAl * q, z0 = sM2[s] * q;
+            float r1, r0;
+            const K01<float> kl = bessel_k01_rcp(z1, r1);
+            const K01<float> k0 = bessel_k01_rcp(z0, r0);
+            const float sl = z1 * sqy * iB, s0 = z0 * sqy * iB;  // sqrt(A/B)
+            const float h = q * delta * rcp_approx_f(sAl + sM2[s]);
+            float g22b, g12b;
+            if (h < 0.3f && h < 0.1f * z0) {
+                // Euler-Maclaurin integral of dF/dz over [z0, z1] (see f_differences_em)
+                const float h2 = h * h;
+                const float e2 = h2 * (1.0f / 12.0f), e4 = h2 * h2 * (1.0f / 720.0f);
+                const float d1 = 0.5f * h * (-z0 * k0.k0 - z1 * kl.k0) -
+                                 e2 * ((z1 * kl.k1 - kl.k0) - (z0 * k0.k1 - k0.k0)) +
+                                 e4 * ((z1 * kl.k1 - 2.0f * kl.k0 - kl.k1 * r1) - (z0 * k0.k1 - 2.0f * k0.k0 - k0.k1 * r0));
+                const float d2 = 0.5f * h * (-z0 * z0 * k0.k1 - z1 * z1 * kl.k1) -
+                                 e2 * ((z1 * z1 * kl.k0 - z1 * kl.k1) - (z0 * z0 * k0.k0 - z0 * k0.k1)) +
+                                 e4 * (((3.0f + z1 * z1) * kl.k0 - 4.0f * z1 * kl.k1) -
+                                       ((3.0f + z0 * z0) * k0.k0 - 4.0f * z0 * k0.k1));
+                g12b = 4.0f * om[s] * iy * iB * d1;
+                g22b = 8.0f * om[s] * iB * iB * d2;
+            } else {
+                const float rl = Al * iB, rz = M2[s] * iB;
+                g22b = 8.0f * iy * om[s] * (rl * (kl.k0 + 2.0f * kl.k1 * r1) - rz * (k0.k0 + 2.0f * k0.k1 * r0));
+                g12b = 4.0f * iy * isqy * om[s] * (sl * kl.k1 - s0 * k0.k1);
+            }
+            const float g21 = 4.0f * isqy * sl * kl.k1;
+            const float g11 = 2.0f * iy * kl.k0;
+            m.g22[s] = fmaf(w, g22b, m.g22[s]);
+            m.g12[s] = fmaf(w, g12b, m.g12[s]);
+            m.g21[s] = fmaf(w, g21, m.g21[s]);
+            m.g11[s] = fmaf(w, g11, m.g11[s]);
+        }
+    }
+    return m;
+}
+
 template <typename T>
 __device__ __forceinline__ GSet<T> g_moments(const Trip<T>& t, const InnerRule& rule)
 {
+    if constexpr (sizeof(T) == 4) return g_moments_f32(t, rule);
     GSet<T> m;
 #pragma unroll
     for (int s = 0; s < 2; ++s) m.g22[s] = m.g12[s] = m.g21[s] = m.g11[s] = (T)0;

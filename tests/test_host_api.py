@@ -177,3 +177,33 @@ def test_serving_helpers():
     assert summary["p50_s"] == pytest.approx(5.0)
     assert summary["p99_s"] == pytest.approx(9.9)
     assert summary["points_per_s"] == pytest.approx(30.0)
+
+
+def test_dis_budget_split_and_seed_plan():
+    """The Vegas budget split of _vegas_with_budget (dis/observables.py:667-692) and the seed
+    offsets of sigma_dip_d2b / sigma_qg_d2b (dis/observables.py:387-532), planned on the host."""
+    from nlo_bk_optimized_b200.dipole import GBW
+    from nlo_bk_optimized_b200.dis import DISConfig, DISOrder, Polarization, Quark, QuarkType
+    from nlo_bk_optimized_b200.dis.observables import TERMS, _Engine, _plan_sigma
+    from nlo_bk_optimized_b200.numerics.integration import budget_options
+
+    o = budget_options(2_000_000, 1e-3)
+    assert (o.max_iterations, o.samples_per_iteration, o.min_iterations) == (8, 250_000, 3)
+    o = budget_options(5, 1e-3)
+    assert (o.max_iterations, o.samples_per_iteration, o.min_iterations) == (2, 2, 2)
+    with pytest.raises(ValueError):
+        budget_options(1, 1e-3)
+    config = DISConfig(order=DISOrder.NLO, quarks=(Quark(QuarkType.LIGHT, 0.14), Quark(QuarkType.C, 1.4)),
+                       maxeval=1000)
+    engine = _Engine(GBW(), config, torch.device("cpu"))
+    plan = _plan_sigma(engine, 10.0, 1e-3, Polarization.T, seed=7, points=24, overrides={})
+    dip_seeds = [j.seed for jobs in plan.dip for j in jobs if j.options is not None]
+    qg_seeds = [j.seed for jobs in plan.qg for j in jobs]
+    assert dip_seeds == [7, 8, 9, 10]
+    assert qg_seeds == [107, 108, 109, 110, 111, 112]
+    # light quarks get 10x the virtual-term budget
+    light, charm = plan.dip[0][1].options, plan.dip[1][1].options
+    assert light.samples_per_iteration * light.max_iterations == 10_000
+    assert charm.samples_per_iteration * charm.max_iterations == 1000
+    assert [j.term for j in plan.qg[0]] == [TERMS["I1"], TERMS["I2N"], TERMS["I3N"]]
+    assert plan.lo.kin.xbj == 1.0  # NLO: LO term at x_Bj = X0

@@ -226,6 +226,15 @@ size_t nlo_dis_table_doubles(int32_t nr, int32_t ny);
 int nlo_dis_table_prepare(const double* r, const double* y, const double* N, int32_t nr, int32_t ny, double x0,
                           double* table, void* stream);
 
+/* The same with the reference's interpolation choice (AmplitudeInterpolation,
+ * dipole/amplitude.py:15-17): NLO_INTERP_SPLINE_LINEAR (the default of BKDipole, what
+ * nlo_dis_table_prepare selects) or NLO_INTERP_LINEAR_LINEAR (bilinear in r and Y,
+ * dipole/amplitude.py:188-212; the reference's nlo-dis command line uses it). */
+#define NLO_INTERP_SPLINE_LINEAR 0
+#define NLO_INTERP_LINEAR_LINEAR 1
+int nlo_dis_table_prepare_interpolated(const double* r, const double* y, const double* N, int32_t nr, int32_t ny,
+                                       double x0, int32_t interpolation, double* table, void* stream);
+
 /* BKDipole.initialize_interpolation(Y) (dipole/amplitude.py:105-133, 254-272): fit the global
  * spline at rapidity Y, which later evaluations at a matching Y use, and find maxr_interpolate.
  * The caller checks 0 <= Y <= max rapidity of the table (the reference raises ValueError). */

@@ -141,6 +141,7 @@ EXPORTED = (
     "nlo_bk_stage",
     "nlo_dis_table_doubles",
     "nlo_dis_table_prepare",
+    "nlo_dis_table_prepare_interpolated",
     "nlo_dis_table_initialize",
     "nlo_dis_dipole_amplitude",
     "nlo_dis_integrand",
@@ -195,6 +196,8 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.nlo_dis_table_doubles.argtypes = [i32, i32]
     lib.nlo_dis_table_prepare.restype = ctypes.c_int
     lib.nlo_dis_table_prepare.argtypes = [vp, vp, vp, i32, i32, d, vp, vp]
+    lib.nlo_dis_table_prepare_interpolated.restype = ctypes.c_int
+    lib.nlo_dis_table_prepare_interpolated.argtypes = [vp, vp, vp, i32, i32, d, i32, vp, vp]
     lib.nlo_dis_table_initialize.restype = ctypes.c_int
     lib.nlo_dis_table_initialize.argtypes = [vp, i32, i32, d, vp]
     lib.nlo_dis_dipole_amplitude.restype = ctypes.c_int

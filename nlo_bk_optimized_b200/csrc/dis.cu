@@ -23,7 +23,8 @@ namespace dis {
 // Table preparation (dipole/amplitude.py:48-83, 215-252)
 
 __global__ void table_prepare_kernel(const double* __restrict__ r, const double* __restrict__ y,
-                                     const double* __restrict__ N, int nr, int ny, double y0, double* table)
+                                     const double* __restrict__ N, int nr, int ny, double y0, int interp,
+                                     double* table)
 {
     const TableView v = table_view(table, nr, ny);
     double* hdr = table;
@@ -49,6 +50,7 @@ __global__ void table_prepare_kernel(const double* __restrict__ r, const double*
         hdr[kHdrYmax] = y[ny - 1] + y0;
         hdr[kHdrLogR0] = ::log(r[0]);
         hdr[kHdrInvDlogR] = (nr - 1) / (::log(r[nr - 1]) - ::log(r[0]));
+        hdr[kHdrInterp] = interp;
     }
     // window weights: second derivatives of the natural spline through the 7/9 window
     // points as linear maps of the window values (one Thomas solve per unit vector)
@@ -584,11 +586,11 @@ cudaError_t launch_vegas_round_typed(int term, const VegasLaunch& L, cudaStream_
 }  // namespace dis
 
 cudaError_t dis_launch_table_prepare(const double* r, const double* y, const double* N, int nr, int ny, double y0,
-                                     double* table, cudaStream_t stream)
+                                     int interp, double* table, cudaStream_t stream)
 {
     int blocks = (nr * ny + 255) / 256;
     blocks = blocks > 1024 ? 1024 : (blocks < 1 ? 1 : blocks);
-    dis::table_prepare_kernel<<<blocks, 256, 0, stream>>>(r, y, N, nr, ny, y0, table);
+    dis::table_prepare_kernel<<<blocks, 256, 0, stream>>>(r, y, N, nr, ny, y0, interp, table);
     return cudaGetLastError();
 }
 

@@ -212,15 +212,24 @@ extern "C" {
 
 size_t nlo_dis_table_doubles(int32_t nr, int32_t ny) { return nr < 2 || ny < 1 ? 0 : dis::table_doubles(nr, ny); }
 
-int nlo_dis_table_prepare(const double* r, const double* y, const double* N, int32_t nr, int32_t ny, double x0,
-                          double* table, void* stream)
+int nlo_dis_table_prepare_interpolated(const double* r, const double* y, const double* N, int32_t nr, int32_t ny,
+                                       double x0, int32_t interpolation, double* table, void* stream)
 {
     if (!r || !y || !N || !table) return dfail(NLO_ERR_INVALID, "nlo_dis_table_prepare: NULL argument");
     if (nr < 9 || ny < 1) return dfail(NLO_ERR_INVALID, "BKDipole requires at least nine r points and one rapidity");
     if (!(x0 > 0) || !std::isfinite(x0)) return dfail(NLO_ERR_INVALID, "x0 must be positive and finite");
+    if (interpolation != NLO_INTERP_SPLINE_LINEAR && interpolation != NLO_INTERP_LINEAR_LINEAR)
+        return dfail(NLO_ERR_INVALID, "unknown table interpolation");
     const double y0 = std::fmax(0.0, std::log(1.0 / x0));
-    cudaError_t e = dis_launch_table_prepare(r, y, N, nr, ny, y0, table, static_cast<cudaStream_t>(stream));
+    cudaError_t e = dis_launch_table_prepare(r, y, N, nr, ny, y0, interpolation, table,
+                                             static_cast<cudaStream_t>(stream));
     return e == cudaSuccess ? NLO_OK : dcuda(e, "table prepare launch");
+}
+
+int nlo_dis_table_prepare(const double* r, const double* y, const double* N, int32_t nr, int32_t ny, double x0,
+                          double* table, void* stream)
+{
+    return nlo_dis_table_prepare_interpolated(r, y, N, nr, ny, x0, NLO_INTERP_SPLINE_LINEAR, table, stream);
 }
 
 int nlo_dis_table_initialize(double* table, int32_t nr, int32_t ny, double Y, void* stream)

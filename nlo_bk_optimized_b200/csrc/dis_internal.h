@@ -56,7 +56,7 @@ struct VegasLaunch {
 }  // namespace dis
 
 cudaError_t dis_launch_table_prepare(const double* r, const double* y, const double* N, int nr, int ny, double y0,
-                                     double* table, cudaStream_t stream);
+                                     int interp, double* table, cudaStream_t stream);
 cudaError_t dis_launch_table_initialize(double* table, int nr, int ny, double Y, cudaStream_t stream);
 cudaError_t dis_launch_points(int precision, int term, const void* args, const dis::InnerRule& rule, const double* x,
                               int64_t n, double* out, cudaStream_t stream);

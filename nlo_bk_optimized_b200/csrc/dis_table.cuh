@@ -12,6 +12,8 @@
 // Evaluation is then 9 Y-interpolated loads, two dot products and one cubic.
 // global[] holds the natural spline of the table at one fixed rapidity that
 // initialize_interpolation builds (dipole/amplitude.py:105-133, 177-184).
+// Header slot kHdrInterp selects the reference's LINEAR_LINEAR mode instead of the local
+// spline (1; dipole/amplitude.py:188-212): bilinear in (r, Y) on the stored rows.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -36,6 +38,7 @@ enum TableSlot {
     kHdrYmax = 8,
     kHdrLogR0 = 9,
     kHdrInvDlogR = 10,
+    kHdrInterp = 11,  // 0: SPLINE_LINEAR, 1: LINEAR_LINEAR
 };
 
 struct TableView {
@@ -124,6 +127,26 @@ __device__ __forceinline__ double table_local(const TableView& t, double r, doub
     return vj + dx * (b + dx * (c + dx * d));
 }
 
+// LINEAR_LINEAR (dipole/amplitude.py:188-212), the reference's expression order: the
+// last Y row interpolates in r only, and r on (or past) the last knot gives 1.
+__device__ __forceinline__ double table_bilinear(const TableView& t, double r, double Y, int rind)
+{
+    if (r >= t.r[t.nr - 1]) return 1.0;
+    int yind = table_y_index(t, Y);
+    yind = yind < 0 ? 0 : yind;
+    const int yind2 = yind + 1 < t.ny ? yind + 1 : t.ny - 1;
+    const double r1 = t.r[rind], r2 = t.r[rind + 1];
+    const double* lo = t.N + (size_t)yind * t.nr + rind;
+    const double N11 = lo[0], N12 = lo[1];
+    if (yind2 == yind) return N11 + (r - r1) / (r2 - r1) * (N12 - N11);
+    const double* hi = t.N + (size_t)yind2 * t.nr + rind;
+    const double N21 = hi[0], N22 = hi[1];
+    const double Y1 = t.Y[yind], Y2 = t.Y[yind2];
+    return (N11 * (r2 - r) * (Y2 - Y) + N12 * (r - r1) * (Y2 - Y) + N21 * (r2 - r) * (Y - Y1) +
+            N22 * (r - r1) * (Y - Y1)) /
+           ((r2 - r1) * (Y2 - Y1));
+}
+
 __device__ __forceinline__ bool table_initialized_at(const TableView& t, double Y)
 {
     if (t.hdr[kHdrInitialized] == 0.0) return false;
@@ -156,7 +179,9 @@ __device__ __forceinline__ double table_amplitude(const TableView& t, double r, 
     if (Y >= 0.0 && Y < ymin) Y = ymin;
     if (Y > ymax) Y = ymax;  // the host rejects requests that reach beyond the table
     const int rind = table_r_interval(t, r);
-    const double v = table_initialized_at(t, Y) ? table_global(t, r, rind) : table_local(t, r, Y, rind);
+    const double v = table_initialized_at(t, Y)       ? table_global(t, r, rind)
+                     : t.hdr[kHdrInterp] != 0.0 ? table_bilinear(t, r, Y, rind)
+                                                : table_local(t, r, Y, rind);
     return v < 0.0 ? 0.0 : (v > 1.0 ? 1.0 : v);
 }
 

@@ -1,8 +1,10 @@
 """GBW and BK-table dipole amplitudes (interface of the reference's
 dipole/amplitude.py:23-302), evaluated on the device by libnlo_b200.so.
 
-``BKDipole`` keeps the table prepared for the device (nlo_dis_table_prepare): the local
-7/9-point splines of every r interval are precomputed once, and
+``BKDipole`` keeps the table prepared for the device (nlo_dis_table_prepare_interpolated):
+with the default SPLINE_LINEAR interpolation the local 7/9-point splines of every r
+interval are precomputed once; LINEAR_LINEAR interpolates bilinearly in (r, Y)
+(dipole/amplitude.py:188-212).
 ``initialize_interpolation(Y)`` fits the global spline at one rapidity on the device,
 exactly as the reference's state machine does.  Evaluation needs CUDA tensors; there is
 no CPU path.
@@ -84,8 +86,8 @@ class BKDipole:
                                                               device=table.r.device))
         if not bool((torch.abs(expected / table.r - 1) <= 0.01).all()):
             raise ValueError("BKDipole requires a logarithmic r grid")
-        if interpolation is not AmplitudeInterpolation.SPLINE_LINEAR:
-            raise NotImplementedError("the device amplitude implements SPLINE_LINEAR interpolation")
+        if not isinstance(interpolation, AmplitudeInterpolation):
+            raise TypeError("interpolation must be an AmplitudeInterpolation")
         self.table = table
         self.interpolation = interpolation
         Y0 = max(0.0, math.log(1 / table.x0))
@@ -99,8 +101,10 @@ class BKDipole:
         y = table.y.to(device=device, dtype=torch.float64).contiguous()
         N = table.N.to(device=device, dtype=torch.float64).contiguous()
         with torch.cuda.device(device):
-            _native.check(lib.nlo_dis_table_prepare(r.data_ptr(), y.data_ptr(), N.data_ptr(), nr, ny, float(table.x0),
-                                                    self._buffer.data_ptr(), _native.stream_handle(device)))
+            mode = 1 if interpolation is AmplitudeInterpolation.LINEAR_LINEAR else 0
+            _native.check(lib.nlo_dis_table_prepare_interpolated(r.data_ptr(), y.data_ptr(), N.data_ptr(), nr, ny,
+                                                                 float(table.x0), mode, self._buffer.data_ptr(),
+                                                                 _native.stream_handle(device)))
         self._nr, self._ny = nr, ny
         self._min_Y = float(self.Y[0])
         self._max_Y = float(self.Y[-1])

@@ -515,6 +515,29 @@ def structure_functions(Q2: torch.Tensor, xbj: torch.Tensor, dipole: Dipole, con
     return {k: v.to(device) for k, v in out.items()}
 
 
+def structure_function_batch(points, dipole: Dipole, config: DISConfig, *, quadrature_points: int = 24,
+                             single_precision: bool = False, **options) -> list[IntegralResult]:
+    """F_T or F_L of many points in one batched device run.
+
+    ``points`` holds (Q^2, x_Bj, polarization, seed) tuples; entry i equals
+    ``FT(Q2, xbj, dipole, config, seed=seed)`` (``FL`` for Polarization.L) run alone, with
+    ``single_precision`` standing for float32 Q^2 (the fixed-Sobol qqbar-g path of
+    dis/observables.py:644-660).  All points share one engine, so every term of every point
+    is integrated by the same few batched launches."""
+    points = [(float(q2), float(x), pol, int(seed)) for q2, x, pol, seed in points]
+    for q2, x, _, _ in points:
+        if not q2 > 0 or not 0 < x <= 1:
+            raise ValueError("Q2 must be positive and xbj must lie in (0, 1]")
+    device = dipole.device if isinstance(dipole, BKDipole) else _device()
+    engine = _Engine(dipole, config, device)
+    overrides = _integration_overrides(options)
+    plans = [_plan_sigma(engine, q2, x, pol, seed=seed, points=quadrature_points, overrides=overrides,
+                         fixed=single_precision) for q2, x, pol, seed in points]
+    _run_with_fallback(engine, plans)
+    return [_scale_result(_sigma_result(plan, config, device), _sf_factor(q2, config))
+            for plan, (q2, _, _, _) in zip(plans, points)]
+
+
 # ----------------------------------------------------------------------------- integrands
 
 

@@ -190,9 +190,13 @@ def spline_eval(x, y, M, xe, interval):
 
 
 class TableDipole:
-    """BK-table dipole N(r, Y) of dipole/amplitude.py:48-252 (SPLINE_LINEAR)."""
+    """BK-table dipole N(r, Y) of dipole/amplitude.py:48-252; ``interpolation`` is
+    "spline_linear" (the default) or "linear_linear" (bilinear in r and Y, :188-212)."""
 
-    def __init__(self, r, y, N, x0=1.0):
+    def __init__(self, r, y, N, x0=1.0, interpolation="spline_linear"):
+        if interpolation not in ("spline_linear", "linear_linear"):
+            raise ValueError("interpolation is 'spline_linear' or 'linear_linear'")
+        self.interpolation = interpolation
         self.r = np.asarray(r, dtype=np.float64)
         self.Y = np.asarray(y, dtype=np.float64) + max(0.0, math.log(1 / x0))
         self.N = np.asarray(N, dtype=np.float64)
@@ -234,6 +238,31 @@ class TableDipole:
             interval = np.clip(rind[mask] - start, 0, points - 2)
             out[mask] = spline_eval(xs, vals, M, r[mask], interval)
         return out
+
+    def bilinear(self, r, Y):
+        """LINEAR_LINEAR amplitude (dipole/amplitude.py:188-212): bilinear in (r, Y) with the
+        same expression order; the last Y row interpolates in r only; r on the last knot
+        gives 1."""
+        r = np.asarray(r, dtype=np.float64)
+        Y = np.asarray(Y, dtype=np.float64)
+        nr, ny = self.r.size, self.Y.size
+        rind = np.searchsorted(self.r, r, side="right") - 1
+        yind = np.searchsorted(self.Y, Y, side="right") - 1
+        rind2 = np.minimum(rind + 1, nr - 1)
+        yind2 = np.minimum(yind + 1, ny - 1)
+        r1, r2 = self.r[rind], self.r[rind2]
+        Y1, Y2 = self.Y[yind], self.Y[yind2]
+        dr = np.where(rind2 != rind, r2 - r1, 1.0)
+        dY = np.where(yind2 != yind, Y2 - Y1, 1.0)
+        N11 = self.N[yind, rind]
+        N12 = self.N[yind, rind2]
+        N21 = self.N[yind2, rind]
+        N22 = self.N[yind2, rind2]
+        value = (N11 * (r2 - r) * (Y2 - Y) + N12 * (r - r1) * (Y2 - Y)
+                 + N21 * (r2 - r) * (Y - Y1) + N22 * (r - r1) * (Y - Y1)) / (dr * dY)
+        last_Y = N11 + (r - r1) / dr * (N12 - N11)
+        value = np.where(yind2 == yind, last_Y, value)
+        return np.where(rind2 == rind, 1.0, value)
 
     def _clamped(self, r, Y):
         r = np.where(r < self.min_r, self.min_r * 1.000001, r)
@@ -300,7 +329,8 @@ class TableDipole:
         if init.any():
             out[init] = self.global_spline(r[init])
         if (~init).any():
-            out[~init] = np.clip(self.local(r[~init], Y[~init]), 0, 1)
+            plain = self.bilinear if self.interpolation == "linear_linear" else self.local
+            out[~init] = np.clip(plain(r[~init], Y[~init]), 0, 1)
         return out
 
 

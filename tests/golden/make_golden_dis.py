@@ -20,7 +20,9 @@ what its own functions return for seeded inputs:
 * LO-order F_T, F_L, F_2 (dis/observables.py:581-624);
 * the fixed-Sobol sampling pieces ``map_importance_grid`` and ``paired_endpoint_inputs``
   (dis/fixed_sobol.py:100-158) and one ``_adapt_vegas_edges`` re-binning
-  (numerics/integration.py:804-866) on float64 inputs.
+  (numerics/integration.py:804-866) on float64 inputs;
+* the LINEAR_LINEAR table interpolation (dipole/amplitude.py:188-212): amplitudes on the
+  local and the initialised path, one dipole term and LO F_T, F_L with it.
 
 Unit-cube points come from numpy's default_rng(20260301); each case is listed in
 ``cases`` with its kinematics.
@@ -199,6 +201,35 @@ def main() -> None:
     count = frng.integers(0, 9, (5, 32)).astype(np.float64)
     out["adapt_hist"], out["adapt_count"] = hist, count
     out["adapt_edges"] = _adapt_vegas_edges(T64(fs_edges), T64(hist), T64(count), cuda_fusion=False).numpy()
+    # LINEAR_LINEAR table interpolation (dipole/amplitude.py:188-212), with its own
+    # generator: scattered (r, Y) plus the edges (r outside the table, on a knot and on the
+    # last knot; Y on a row and on the last row), the initialised spline, one dipole term
+    # and the LO structure functions
+    from nlo_torch.dipole.amplitude import AmplitudeInterpolation
+
+    brng = np.random.default_rng(4242)
+    b_r = np.concatenate([np.exp(brng.uniform(math.log(5e-7), math.log(80.0), 300)),
+                          [r_tab[0] * 0.5, r_tab[-1] * 2, r_tab[-1], r_tab[17], r_tab[0], 1.0, 3.0]])
+    b_Y = np.concatenate([brng.uniform(0.0, 14.0, 300), [3.0, 14.0, 14.0, 5.5, 0.0, 14.0, 7.25]])
+    linear = BKDipole(table, interpolation=AmplitudeInterpolation.LINEAR_LINEAR)
+    out["bilin_r"], out["bilin_Y"] = b_r, b_Y
+    out["bilin_amp"] = linear.dipole_amplitude(T64(b_r), T64(b_Y)).numpy()
+    linear.initialize_interpolation(4.7)
+    out["bilin_init"] = linear.dipole_amplitude(T64(b_r), torch.full((b_r.size,), 4.7)).numpy()
+    out["bilin_init_maxr"] = np.array([linear.maxr_interpolate])
+    config = DISConfig(quarks=(light,), cuda_fusion=False, cuda_nested=False)
+    x = brng.uniform(0, 1, (256, 3))
+    linear = BKDipole(table, interpolation=AmplitudeInterpolation.LINEAR_LINEAR)
+    out["bilin_dip1_x"] = x
+    out["bilin_dip1"] = integrand_dip_massive(T64(x), torch.tensor(10.0), torch.tensor(1e-3), Polarization.T,
+                                              light, "T1", linear, config).numpy()
+    config = DISConfig(quarks=(Quark(QuarkType.LIGHT, 0.14), Quark(QuarkType.C, 1.4)),
+                       cuda_fusion=False, cuda_nested=False)
+    Q2, xbj = torch.tensor(7.5), torch.tensor(2e-4)
+    out["bilin_lo_sf"] = np.array([
+        float(FT(Q2, xbj, BKDipole(table, interpolation=AmplitudeInterpolation.LINEAR_LINEAR), config).value),
+        float(FL(Q2, xbj, BKDipole(table, interpolation=AmplitudeInterpolation.LINEAR_LINEAR), config).value)])
+
     out["cases"] = np.array(names)
     np.savez_compressed(OUT, **out)
     print("wrote", OUT, sum(v.nbytes for v in out.values()), "bytes")

@@ -135,6 +135,44 @@ def test_amplitudes(dtype):
     assert rel_err(init, GOLDEN["amp_init"]) < 1e-12
 
 
+def bilinear_obj():
+    from nlo_bk_optimized_b200.dipole import AmplitudeInterpolation, BKDipole, DipoleTable
+
+    t = DipoleTable(dev(GOLDEN["table_r"]), dev(GOLDEN["table_y"]), dev(GOLDEN["table_N"]), 1.0)
+    return BKDipole(t, interpolation=AmplitudeInterpolation.LINEAR_LINEAR)
+
+
+def test_bilinear_table_interpolation():
+    """LINEAR_LINEAR tables (dipole/amplitude.py:188-212): amplitudes on the local and the
+    initialised path, edges included, a dipole term and LO F_T, F_L against the reference."""
+    from nlo_bk_optimized_b200 import _native
+    from nlo_bk_optimized_b200.dis import FL, FT, DISConfig, Quark, QuarkType
+    from nlo_bk_optimized_b200.dis.observables import _integrand, kinematics
+
+    r, Y = dev(GOLDEN["bilin_r"]), dev(GOLDEN["bilin_Y"])
+    tab = bilinear_obj()
+    assert rel_err(tab.dipole_amplitude(r, Y).cpu().numpy(), GOLDEN["bilin_amp"]) < 1e-12
+    tab.initialize_interpolation(4.7)
+    assert tab.maxr_interpolate == pytest.approx(float(GOLDEN["bilin_init_maxr"][0]), rel=1e-12)
+    init = tab.dipole_amplitude(r, torch.full_like(r, 4.7)).cpu().numpy()
+    assert rel_err(init, GOLDEN["bilin_init"]) < 1e-12
+
+    config, quark, Q2, xbj, transverse = config_of("light_T_bk")
+    kin = kinematics(Q2, xbj, pol_of(transverse), config, quark)
+    x = dev(GOLDEN["bilin_dip1_x"])
+    got = _integrand(_native.DIS_TERMS["DIP1"], x, kin, bilinear_obj(), config, precision=_native.PRECISION_FP64)
+    assert rel_err(got.cpu().numpy(), GOLDEN["bilin_dip1"]) < 1e-9
+    mixed = _integrand(_native.DIS_TERMS["DIP1"], x, kin, bilinear_obj(), config, precision=_native.PRECISION_MIXED)
+    assert abs(float(mixed.sum() / got.sum()) - 1) < MIXED_SUM_TOL
+
+    config = DISConfig(quarks=(Quark(QuarkType.LIGHT, 0.14), Quark(QuarkType.C, 1.4)), precision="fp64")
+    Q2t = torch.tensor(7.5, dtype=torch.float64, device="cuda")
+    xt = torch.tensor(2e-4, dtype=torch.float64, device="cuda")
+    ref = GOLDEN["bilin_lo_sf"]
+    assert float(FT(Q2t, xt, bilinear_obj(), config).value) == pytest.approx(ref[0], rel=1e-11)
+    assert float(FL(Q2t, xt, bilinear_obj(), config).value) == pytest.approx(ref[1], rel=1e-11)
+
+
 # ----------------------------------------------------------------------------- integrands vs golden
 
 

@@ -70,6 +70,36 @@ def test_amplitudes():
     assert rel(tab(r, np.full_like(r, GOLDEN["amp_init_Y"][0])), GOLDEN["amp_init"], 1e-12) < 1e-11
 
 
+def bilinear_dipole() -> od.TableDipole:
+    return od.TableDipole(GOLDEN["table_r"], GOLDEN["table_y"], GOLDEN["table_N"], interpolation="linear_linear")
+
+
+def test_bilinear_amplitudes():
+    r, Y = GOLDEN["bilin_r"], GOLDEN["bilin_Y"]
+    tab = bilinear_dipole()
+    assert rel(tab(r, Y), GOLDEN["bilin_amp"], 1e-12) < 1e-12
+    assert tab(np.array([GOLDEN["table_r"][-1]]), np.array([3.0]))[0] == 1.0  # the last knot
+    tab.initialize(4.7)
+    assert tab.maxr_interpolate == pytest.approx(float(GOLDEN["bilin_init_maxr"][0]), rel=1e-12)
+    assert rel(tab(r, np.full_like(r, 4.7)), GOLDEN["bilin_init"], 1e-12) < 1e-11
+
+
+def test_bilinear_dipole_term_and_lo():
+    kin, _ = kin_of("light_T_bk")  # Q2 = 10, x = 1e-3, light quark, default couplings
+    x = GOLDEN["bilin_dip1_x"]
+    ref = GOLDEN["bilin_dip1"]
+    got = od.dip_integrand(x, kin, 1, bilinear_dipole())
+    assert rel(got, ref, 1e-9 * np.max(np.abs(ref))) < 1e-9
+    Q2, xbj = 7.5, 2e-4
+    quarks = [(0.14, 2 / 3), (1.4, 4 / 9)]
+    dip = bilinear_dipole()
+    dip.initialize(max(math.log(dip.X0() / xbj), 0.0))
+    for transverse, want in zip((True, False), GOLDEN["bilin_lo_sf"]):
+        sigma = od.LO_FACTOR * od.gauss_legendre_tensor(
+            lambda u: od.lo_integrand(u, Q2, xbj, quarks, transverse, dip), 2, 24)
+        assert sigma * od.structure_function_factor(Q2) == pytest.approx(want, rel=1e-12)
+
+
 @pytest.mark.parametrize("name", CASES)
 def test_lo_integrand(name):
     kin, e2 = kin_of(name)

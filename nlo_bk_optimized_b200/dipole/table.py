@@ -117,14 +117,24 @@ def load_bk_table(
 
 
 def save_bk_table(path: str | Path, table: DipoleTable) -> None:
-    """Write the four-header format with 15-digit mantissas (table.py:121-144)."""
+    """Write the four-header format with 15-digit mantissas (table.py:121-144).
+
+    A float32 grid here is the float64 grid rounded once (solve_bk forms it in float64),
+    so r[1]/r[0] carries a rounding error that the 100th power turns into ~1e-5: the
+    multiplier of a float32 grid is taken from its end points in float64 instead, which
+    both passes the uniformity check and writes a header that reproduces the grid."""
 
     r = table.r.detach().cpu()
     y = table.y.detach().cpu()
     N = table.N.detach().cpu()
-    multiplier = r[1] / r[0]
+    if r.dtype == torch.float32:
+        r = r.double()
+        multiplier = (r[-1] / r[0]) ** (1.0 / (r.numel() - 1))
+        tolerance = 5e-6
+    else:
+        multiplier = r[1] / r[0]
+        tolerance = 2e-12
     expected = r[0] * torch.pow(multiplier, torch.arange(r.numel(), dtype=r.dtype))
-    tolerance = 5e-6 if r.dtype == torch.float32 else 2e-12
     if not bool(torch.allclose(r, expected, rtol=tolerance, atol=0)):
         raise ValueError("the legacy BK format requires a logarithmically uniform r grid")
     output = [

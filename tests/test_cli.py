@@ -6,6 +6,7 @@ from __future__ import annotations
 import math
 
 import pytest
+import torch
 
 from nlo_bk_optimized_b200.bk.config import (
     BKOrder,
@@ -105,3 +106,21 @@ def test_nlodis_points():
     assert len(grid) == 3 * per_Q2
     assert [q for q, _ in grid[::per_Q2]] == [4.5, 45.0, 100.0]
     assert grid[0][1] == 1e-5 and grid[per_Q2 - 1][1] <= 1e-2 < grid[per_Q2 - 1][1] * 1.5
+
+
+@pytest.mark.parametrize("dtype,tol", [(torch.float32, 5e-9), (torch.float64, 1e-13)])
+def test_legacy_table_round_trip_of_evolution_grids(tmp_path, dtype, tol):
+    """solve_bk's grid (float64, rounded once for float32 tables) survives the legacy
+    format: the header multiplier reproduces every r."""
+    from nlo_bk_optimized_b200.bk.config import BKConfig
+    from nlo_bk_optimized_b200.bk.evolution import _r_grid
+    from nlo_bk_optimized_b200.dipole.table import DipoleTable, load_bk_table, save_bk_table
+
+    r = _r_grid(BKConfig(RPOINTS=100, MINR=1e-6, MAXR=30.0), device="cpu", dtype=torch.float64)
+    N = torch.linspace(0, 1, 202, dtype=torch.float64).reshape(2, 101)
+    table = DipoleTable(r=r.to(dtype), y=torch.tensor([0.0, 0.2], dtype=dtype), N=N.to(dtype), x0=0.01)
+    save_bk_table(tmp_path / "t.dat", table)
+    back = load_bk_table(tmp_path / "t.dat")
+    assert float((back.r / r - 1).abs().max()) < tol
+    # 16 significant digits in the file: N comes back within 1e-15
+    assert torch.allclose(back.N, N.to(dtype).double(), rtol=1e-15, atol=1e-300) and back.x0 == 0.01

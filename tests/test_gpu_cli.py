@@ -52,7 +52,8 @@ def test_nlobk_writes_the_legacy_table(bk_table, capsys):
     assert float(table.y[-1]) == pytest.approx(7.0, rel=1e-12)
     N = table.N.numpy()
     assert np.all(np.isfinite(N)) and np.all(N >= 0) and np.all(N <= 1)
-    assert np.all(N[-1] >= N[0] - 1e-12)  # the amplitude grows with rapidity
+    mid = (N[0] > 0.01) & (N[0] < 0.9)  # away from the frozen, saturated parents and tiny N
+    assert mid.sum() > 10 and np.all(N[-1][mid] > N[0][mid])  # the amplitude grows with rapidity
 
 
 def _printed(out: str) -> list[list[str]]:

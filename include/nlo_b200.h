@@ -36,24 +36,55 @@ extern "C" {
 #define NLO_STEPPER_RK3 1   /* Kutta RK3, bk/evolution.py:190-236 (_fixed_rk23_step) */
 #define NLO_STEPPER_RK4 2   /* classical RK4 (no reference counterpart) */
 
+/* BKConfig.Order (bk/config.py:36-63).  The zero value is the production order. */
+#define NLO_ORDER_NLO_RESUM_DLOG_SLOG 0
+#define NLO_ORDER_NLO_RESUM_DLOG 1
+#define NLO_ORDER_NLO 2
+#define NLO_ORDER_LO_RESUM_DLOG_SLOG 3
+#define NLO_ORDER_LO_RESUM_DLOG 4
+#define NLO_ORDER_LO 5
+
+/* BKConfig.RC_LO, the form of Kernel_lo (bk_kernels/k1.py:37-94).  FIXED_LO is
+ * NLO_RC_LO_BALITSKY with fixed_coupling = 1. */
+#define NLO_RC_LO_BALITSKY 0
+#define NLO_RC_LO_PARENT 1
+#define NLO_RC_LO_SMALLEST 2
+#define NLO_RC_LO_FAC 3
+#define NLO_RC_LO_BEUF 4
+
+/* BKConfig.RESUM_RC, the coupling of the resummation factors (bk_kernels/k1.py:100-107). */
+#define NLO_RESUM_RC_SMALLEST 0
+#define NLO_RESUM_RC_PARENT 1
+#define NLO_RESUM_RC_FIXED 2
+
+/* BKConfig.RC_NLO, the coupling of K2 and Kf (bk/derivatives.py:615-632).  FIXED_NLO is
+ * fixed_coupling = 1. */
+#define NLO_RC_NLO_SMALLEST 0
+#define NLO_RC_NLO_PARENT 1
+
 /* Physics and numerical switches of BKConfig (bk/config.py:66-124) that the
- * right-hand side depends on.  Only the reference's production K1/K2 choices
- * are implemented on the device: RC_LO = BALITSKY_LO (or FIXED_LO),
- * RC_NLO = SMALLEST_NLO (or FIXED_NLO), RESUM_RC = RESUM_RC_SMALLEST,
- * Order = NLO_RESUM_DLOG_SLOG, NF <= 3 smooth-freeze coupling (coupling.py:81-97). */
+ * right-hand side depends on.  A zero-initialised tail (order, rc_lo, resum_rc, rc_nlo)
+ * selects the production choices.  The coupling is bk_alpha_s (coupling.py:10-46): the
+ * smooth freeze for NF <= 3, the heavy-flavour thresholds for NF = 5, a constant when
+ * fixed_coupling is set (RC_LO = FIXED_LO or RC_NLO = FIXED_NLO).  Orders without NLO
+ * kernels (NLO_ORDER_LO*) skip K2 + Kf. */
 typedef struct nlo_bk_params {
     double nc;            /* NC */
-    double nf;            /* NF */
+    double nf;            /* NF: 0, 3 or 5 */
     double lambda_qcd;    /* LambdaQCD */
     double c2;            /* C2 */
     double minr;          /* MINR (double-log resummation switch r > 1.01 MINR, k1.py:117) */
     double ksub;          /* KSUB */
-    double fixed_alpha_s; /* FIXED_AS, used when fixed_coupling != 0 */
+    double fixed_alpha_s; /* FIXED_AS: the fixed coupling, and the RESUM_RC_FIXED coupling */
     double alpha_cap;     /* > 0: alpha_s = min(alpha_s, alpha_cap) (frozen-coupling variant) */
     int32_t symmetrize;   /* SYMMETRIZE_Z_Z2_INTEGRATION */
     int32_t fixed_coupling;
     int32_t force_positive; /* FORCE_POSITIVE_N */
     int32_t precision;      /* NLO_PRECISION_* */
+    int32_t order;          /* NLO_ORDER_* */
+    int32_t rc_lo;          /* NLO_RC_LO_* */
+    int32_t resum_rc;       /* NLO_RESUM_RC_* */
+    int32_t rc_nlo;         /* NLO_RC_NLO_* */
 } nlo_bk_params;
 
 /* Scrambled Sobol direction numbers of torch.quasirandom.SobolEngine

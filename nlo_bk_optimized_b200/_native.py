@@ -37,6 +37,10 @@ class BKParams(ctypes.Structure):
         ("fixed_coupling", ctypes.c_int32),
         ("force_positive", ctypes.c_int32),
         ("precision", ctypes.c_int32),
+        ("order", ctypes.c_int32),
+        ("rc_lo", ctypes.c_int32),
+        ("resum_rc", ctypes.c_int32),
+        ("rc_nlo", ctypes.c_int32),
     ]
 
 

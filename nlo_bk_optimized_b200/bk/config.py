@@ -154,24 +154,51 @@ class BKConfig:
 
 
 def device_supported(config: BKConfig) -> str | None:
-    """Return why a configuration is outside the device kernels, or None."""
+    """Return why a configuration is outside the device kernels, or None.
 
-    if config.Order is not BKOrder.NLO_RESUM_DLOG_SLOG:
-        return "the device K1 implements Order = NLO_RESUM_DLOG_SLOG"
-    fixed = config.RC_LO is RunningCouplingLO.FIXED_LO
-    if not fixed and config.RC_LO is not RunningCouplingLO.BALITSKY_LO:
-        return "the device K1 implements RC_LO = BALITSKY_LO or FIXED_LO"
-    if not fixed and config.RC_NLO is not RunningCouplingNLO.SMALLEST_NLO:
-        return "the device K2+Kf implements RC_NLO = SMALLEST_NLO or FIXED_NLO"
-    if config.RESUM_RC is not ResummationCoupling.RESUM_RC_SMALLEST:
-        return "the device K1 implements RESUM_RC = RESUM_RC_SMALLEST"
-    if config.NF not in {0, 3}:
-        return "the device kernels implement NF = 0 or 3"
+    Every Order, RC_LO, RC_NLO, RESUM_RC and NF of BKConfig runs on the device; the K2+Kf
+    integral is always the fixed Sobol QMC estimate, and the kinematical constraint
+    (which needs the amplitude history) is not implemented."""
+
     if config.KINEMATICAL_CONSTRAINT:
         return "the kinematical constraint is not implemented on the device"
-    if config.INTMETHOD_NLO is not IntegrationMethod.SOBOL:
+    if config.Order.has_nlo_kernels and config.INTMETHOD_NLO is not IntegrationMethod.SOBOL:
         return "the device K2+Kf integrates with IntegrationMethod.SOBOL"
     return None
+
+
+ORDER_CODES = {
+    BKOrder.NLO_RESUM_DLOG_SLOG: 0,
+    BKOrder.NLO_RESUM_DLOG: 1,
+    BKOrder.NLO: 2,
+    BKOrder.LO_RESUM_DLOG_SLOG: 3,
+    BKOrder.LO_RESUM_DLOG: 4,
+    BKOrder.LO: 5,
+}
+RC_LO_CODES = {
+    RunningCouplingLO.BALITSKY_LO: 0,
+    RunningCouplingLO.FIXED_LO: 0,  # the Balitsky form with a constant coupling
+    RunningCouplingLO.PARENT_LO: 1,
+    RunningCouplingLO.SMALLEST_LO: 2,
+    RunningCouplingLO.FAC_LO: 3,
+    RunningCouplingLO.BEUF_LO: 4,
+}
+RESUM_RC_CODES = {
+    ResummationCoupling.RESUM_RC_SMALLEST: 0,
+    ResummationCoupling.RESUM_RC_PARENT: 1,
+    ResummationCoupling.RESUM_RC_FIXED: 2,
+}
+RC_NLO_CODES = {
+    RunningCouplingNLO.SMALLEST_NLO: 0,
+    RunningCouplingNLO.FIXED_NLO: 0,  # with the constant coupling
+    RunningCouplingNLO.PARENT_NLO: 1,
+}
+
+
+def fixed_coupling(config: BKConfig) -> bool:
+    """_alpha_s is the constant FIXED_AS when either coupling choice is fixed
+    (bk_kernels/k1.py:158-170, bk/derivatives.py:775-787)."""
+    return config.RC_LO is RunningCouplingLO.FIXED_LO or config.RC_NLO is RunningCouplingNLO.FIXED_NLO
 
 
 __all__ = [
@@ -182,4 +209,5 @@ __all__ = [
     "RunningCouplingLO",
     "RunningCouplingNLO",
     "device_supported",
+    "fixed_coupling",
 ]

@@ -17,7 +17,15 @@ from dataclasses import dataclass
 import torch
 
 from nlo_bk_optimized_b200 import _native
-from nlo_bk_optimized_b200.bk.config import BKConfig, RunningCouplingLO, device_supported
+from nlo_bk_optimized_b200.bk.config import (
+    ORDER_CODES,
+    RC_LO_CODES,
+    RC_NLO_CODES,
+    RESUM_RC_CODES,
+    BKConfig,
+    device_supported,
+    fixed_coupling,
+)
 from nlo_bk_optimized_b200.bk.initial_conditions import MV, ICDataFile
 from nlo_bk_optimized_b200.dipole.table import DipoleTable
 
@@ -65,9 +73,13 @@ def params_of(config: BKConfig, precision: int) -> _native.BKParams:
     p.fixed_alpha_s = float(config.FIXED_AS)
     p.alpha_cap = float(config.ALPHA_S_CAP)
     p.symmetrize = int(bool(config.SYMMETRIZE_Z_Z2_INTEGRATION))
-    p.fixed_coupling = int(config.RC_LO is RunningCouplingLO.FIXED_LO)
+    p.fixed_coupling = int(fixed_coupling(config))
     p.force_positive = int(bool(config.FORCE_POSITIVE_N))
     p.precision = int(precision)
+    p.order = ORDER_CODES[config.Order]
+    p.rc_lo = RC_LO_CODES[config.RC_LO]
+    p.resum_rc = RESUM_RC_CODES[config.RESUM_RC]
+    p.rc_nlo = RC_NLO_CODES[config.RC_NLO]
     return p
 
 

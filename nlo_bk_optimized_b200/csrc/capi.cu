@@ -67,7 +67,11 @@ bool check_params(const nlo_bk_params* p, std::string& why)
 {
     if (!p) { why = "params is NULL"; return false; }
     if (!(p->nc > 0)) { why = "NC must be positive"; return false; }
-    if (!(p->nf == 0.0 || p->nf == 3.0)) { why = "the device kernels implement NF = 0 or 3 (smooth coupling)"; return false; }
+    if (!(p->nf == 0.0 || p->nf == 3.0 || p->nf == 5.0)) { why = "NF must be 0, 3 or 5"; return false; }
+    if (p->order < NLO_ORDER_NLO_RESUM_DLOG_SLOG || p->order > NLO_ORDER_LO) { why = "unknown order"; return false; }
+    if (p->rc_lo < NLO_RC_LO_BALITSKY || p->rc_lo > NLO_RC_LO_BEUF) { why = "unknown RC_LO"; return false; }
+    if (p->resum_rc < NLO_RESUM_RC_SMALLEST || p->resum_rc > NLO_RESUM_RC_FIXED) { why = "unknown RESUM_RC"; return false; }
+    if (p->rc_nlo != NLO_RC_NLO_SMALLEST && p->rc_nlo != NLO_RC_NLO_PARENT) { why = "unknown RC_NLO"; return false; }
     if (!(p->lambda_qcd > 0) || !(p->c2 > 0) || !(p->ksub > 0)) { why = "LambdaQCD, C2 and KSUB must be positive"; return false; }
     if (p->precision != NLO_PRECISION_MIXED && p->precision != NLO_PRECISION_FP64) { why = "unknown precision"; return false; }
     return true;
@@ -142,11 +146,14 @@ int run_rhs(const nlo_bk_params& p, const double* r, const double* N, int points
         return cuda_fail(e, "active");
     if ((e = launch_k1(p, r, points, b.spline, b.active, b.count, b.k1, stream)) != cudaSuccess)
         return cuda_fail(e, "k1");
-    if ((e = launch_k2kf(p, r, points, b.spline, b.active, b.count, dirs, 0, samples, box, b.k2kf, b.partial,
+    // orders without NLO kernels (Order.has_nlo_kernels, bk/config.py:44-50) take no K2 + Kf:
+    // zero samples clear the sums and launch nothing
+    const uint64_t nlo_samples = order_has_nlo(p.order) ? samples : 0;
+    if ((e = launch_k2kf(p, r, points, b.spline, b.active, b.count, dirs, 0, nlo_samples, box, b.k2kf, b.partial,
                          b.k2kf_blocks, stream)) != cudaSuccess)
         return cuda_fail(e, "k2kf");
-    if ((e = launch_assemble(b.k1, b.k2kf, points, samples ? 1.0 / (double)samples : 0.0, dndy, k2kf_out, stream)) !=
-        cudaSuccess)
+    if ((e = launch_assemble(b.k1, b.k2kf, points, nlo_samples ? 1.0 / (double)nlo_samples : 0.0, dndy, k2kf_out,
+                             stream)) != cudaSuccess)
         return cuda_fail(e, "assemble");
     if (k1_out) {
         if ((e = cudaMemcpyAsync(k1_out, b.k1, sizeof(double) * points, cudaMemcpyDeviceToDevice, stream)) !=

@@ -88,13 +88,24 @@ struct Phys {
     T b0c;        // b0 * 0.2 with b0 = (11 Nc - 2 Nf)/(12 pi)          coupling.py:92-96
     T left;       // 2/0.2 * log(2.5)                                     coupling.py:92
     T log_sc;     // log(4 C2 / Lambda^2)                                 coupling.py:94
-    T fixed_as;   // fixed coupling value (if fixed)
+    T log_4c2;    // log(4 C2), the heavy-flavour threshold coupling      coupling.py:25-45
+    T fixed_as;   // fixed coupling value (if fixed), and the RESUM_RC_FIXED coupling
     T alpha_cap;  // > 0: cap
     T minr;
     T ksub, log_ksub;
     bool fixed;
+    bool thresholds;  // NF > 3: bk_alpha_s with flavour thresholds (coupling.py:25-45)
     bool symmetrize;
+    // BKConfig.Order / RC_LO / RESUM_RC / RC_NLO (nlo_bk_params)
+    bool nlo;          // Order.has_nlo_kernels
+    bool resum;        // Order.resum_dlog (k1.py:97-98: LO and NLO return the bare kernel)
+    bool slog;         // Order.resum_slog
+    int rc_lo;         // NLO_RC_LO_*
+    int resum_rc;      // NLO_RESUM_RC_*
+    bool nlo_parent;   // RC_NLO = PARENT_NLO
 };
+
+__host__ __device__ inline bool order_has_nlo(int order) { return order <= NLO_ORDER_NLO; }
 
 template <typename T>
 __host__ Phys<T> make_phys(const nlo_bk_params& p)
@@ -106,14 +117,46 @@ __host__ Phys<T> make_phys(const nlo_bk_params& p)
     q.b0c = (T)((11.0 * p.nc - 2.0 * p.nf) / (12.0 * kPi) * 0.2);
     q.left = (T)(2.0 / 0.2 * std::log(2.5));
     q.log_sc = (T)std::log(4.0 * p.c2 / (p.lambda_qcd * p.lambda_qcd));
+    q.log_4c2 = (T)std::log(4.0 * p.c2);
     q.fixed_as = (T)p.fixed_alpha_s;
     q.alpha_cap = (T)p.alpha_cap;
     q.minr = (T)p.minr;
     q.ksub = (T)p.ksub;
     q.log_ksub = (T)std::log(p.ksub);
     q.fixed = p.fixed_coupling != 0;
+    q.thresholds = !q.fixed && p.nf > 3.0;
     q.symmetrize = p.symmetrize != 0;
+    q.nlo = order_has_nlo(p.order);
+    q.resum = p.order != NLO_ORDER_NLO && p.order != NLO_ORDER_LO;
+    q.slog = p.order == NLO_ORDER_NLO_RESUM_DLOG_SLOG || p.order == NLO_ORDER_LO_RESUM_DLOG_SLOG;
+    q.rc_lo = p.rc_lo;
+    q.resum_rc = p.resum_rc;
+    q.nlo_parent = p.rc_nlo == NLO_RC_NLO_PARENT;
     return q;
+}
+
+// bk_alpha_s for NF > 3 (coupling.py:25-45): Nf = 3, 4, 5 below, between and above
+// the scales 1.3 and 4.5 GeV of 4 C2 / d^2, with Lambda_Nf fixed per flavour number;
+// 4 pi / (b0 log(4 C2 / (d^2 Lambda^2))), b0 = 11 - 2 Nf / 3, and 1 where the
+// logarithm is negative or the coupling exceeds 1.
+template <typename T>
+__device__ __forceinline__ T alpha_thresholds(T log_d, const Phys<T>& ph)
+{
+    const T log_scale = ph.log_4c2 - (T)2 * log_d;  // log(4 C2 / d^2)
+    T nf, log_lambda;
+    if (log_scale < (T)0.5247285289349821) {         // log(1.3^2)
+        nf = (T)3;
+        log_lambda = (T)-1.9230602087529778;          // log(0.146159)
+    } else if (log_scale < (T)3.0081547935525483) {  // log(4.5^2)
+        nf = (T)4;
+        log_lambda = (T)-2.0960263118360456;          // log(0.122944)
+    } else {
+        nf = (T)5;
+        log_lambda = (T)-2.4030807944061756;          // log(0.0904389)
+    }
+    const T log_arg = log_scale - (T)2 * log_lambda;
+    const T a = (T)(4.0 * kPi) * M<T>::rcp(((T)11 - (T)2 * nf / (T)3) * log_arg);
+    return (log_arg < (T)0 || !(a <= (T)1)) ? (T)1 : a;
 }
 
 // logaddexp(left, right) with right = (log_sc - 2 log d)/0.2   (coupling.py:81-97)
@@ -121,6 +164,7 @@ template <typename T>
 __device__ __forceinline__ T alpha_of_log(T log_d, const Phys<T>& ph)
 {
     if (ph.fixed) return ph.fixed_as;
+    if (ph.thresholds) return alpha_thresholds(log_d, ph);
     const T right = (ph.log_sc - (T)2 * log_d) * (T)5;
     const T m = M<T>::fmax(ph.left, right);
     const T lae = m + M<T>::log_fast((T)1 + M<T>::exp_fast(-M<T>::fabs(ph.left - right)));

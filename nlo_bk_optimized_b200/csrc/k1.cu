@@ -2,8 +2,8 @@
 // custom_kernels/bk/k1/kernel.cu:2040-2092 (per r-grid interval 8 Gauss-Legendre
 // nodes in log z times 24 nodes in v with theta = pi v^2, weight 2 z^2 * radial *
 // pi v * angular), with the integrand Kernel_lo x dipole of bk_kernels/k1.py:20-155
-// and bk/derivatives.py:434-468 for the production order NLO_RESUM_DLOG_SLOG,
-// RC_LO = BALITSKY_LO, RESUM_RC = RESUM_RC_SMALLEST.
+// and bk/derivatives.py:434-468, for every Order, RC_LO and RESUM_RC of BKConfig
+// (production: NLO_RESUM_DLOG_SLOG, BALITSKY_LO, RESUM_RC_SMALLEST).
 //
 // One CTA per active parent.  Threads own (interval, radial node) pairs and sweep
 // the 24 angular nodes; per-thread sums are FP64, the block reduction is a fixed
@@ -96,7 +96,9 @@ __device__ __forceinline__ T lae_shift(const K1Z<T>& Z, T delta)
     return M<T>::log_acc(Z.sigma_c + Z.sigma * M<T>::exp_fast(delta));
 }
 
-// Kernel_lo x dipole at one (z, theta) node; sh2 = sin^2(theta/2).
+// Kernel_lo x dipole at one (z, theta) node; sh2 = sin^2(theta/2).  The form of
+// Kernel_lo follows RC_LO (k1.py:37-94); orders without resummation stop at the bare
+// kernel (k1.py:97-98); the resummation coupling follows RESUM_RC (k1.py:100-107).
 template <typename T>
 __device__ __forceinline__ T k1_point(const SplineView<T>& s, const K1Parent<T>& P, const K1Z<T>& Z,
                                       const Phys<T>& ph, T sh2)
@@ -110,27 +112,62 @@ __device__ __forceinline__ T k1_point(const SplineView<T>& s, const K1Parent<T>&
     const T alpha_X = alpha_of_log(P.lr_abs + dX, ph);
     // X^2 - Y^2 = r (r - 2 z cos theta), cos theta = 1 - 2 sin^2(theta/2)
     const T XmY = r * (r - (T)2 * z * ((T)1 - (T)2 * sh2));
+    // alpha_Y - alpha_X: the smooth coupling's difference without cancellation, else direct
     T dalpha;
     if (ph.fixed) {
         dalpha = (T)0;
-    } else if (ph.alpha_cap > (T)0) {
+    } else if (ph.alpha_cap > (T)0 || ph.thresholds) {
         dalpha = Z.alpha_Y - alpha_X;
     } else {
         // alpha_Y - alpha_X = alpha_X alpha_Y b0 c (lae_X - lae_Y)
         const T delta = -(T)5 * M<T>::log1p(XmY * Z.inv_Ysq);
         dalpha = alpha_X * Z.alpha_Y * ph.b0c * lae_shift(Z, delta);
     }
-    // r^2/(X^2Y^2) + (aY/aX - 1)/Y^2 + (aX/aY - 1)/X^2
     const T inv_XY = M<T>::rcp(Xsq * Z.Ysq);
-    const T bracket = (P.r2 + dalpha * M<T>::div(Z.alpha_Y * XmY + Z.Ysq * dalpha, alpha_X * Z.alpha_Y)) * inv_XY;
     const T pref = ph.nc * (T)(1.0 / (2.0 * kPi * kPi));
-    T lo = pref * P.alpha_r * bracket;
-    if (!M<T>::finite(lo)) lo = (T)0;
-    // double-log resummation (k1.py:109-119), alpha at the smallest size (RESUM_RC_SMALLEST)
     // alpha at min(X, Y, r): reuse alpha_X, alpha_Y or alpha_r
     const T alpha_min = (dX <= Z.dY && dX <= (T)0) ? alpha_X : (Z.dY <= (T)0 ? Z.alpha_Y : P.alpha_r);
+    T lo, alpha_sc;  // Kernel_lo and the coupling at its scale (alphas_scale)
+    if (ph.rc_lo == NLO_RC_LO_PARENT) {
+        alpha_sc = P.alpha_r;
+        lo = pref * alpha_sc * P.r2 * inv_XY;
+    } else if (ph.rc_lo == NLO_RC_LO_SMALLEST) {
+        alpha_sc = alpha_min;
+        lo = pref * alpha_sc * P.r2 * inv_XY;
+    } else if (ph.rc_lo == NLO_RC_LO_FAC) {
+        // 1/(2 pi) / (1/abar_r + (X^2-Y^2)/r^2 (abar_X - abar_Y)/(abar_X abar_Y)) r^2/(X^2 Y^2)
+        //   = pref r^2/(X^2 Y^2) / (1/alpha_r - (X^2-Y^2)/r^2 (alpha_Y - alpha_X)/(alpha_X alpha_Y))
+        alpha_sc = P.alpha_r;
+        const T den = M<T>::rcp(P.alpha_r) - XmY * M<T>::rcp(P.r2) * M<T>::div(dalpha, alpha_X * Z.alpha_Y);
+        lo = pref * P.r2 * inv_XY * M<T>::rcp(den);
+    } else if (ph.rc_lo == NLO_RC_LO_BEUF) {
+        // r_eff^2 = r^2 (Y^2/X^2)^((X^2-Y^2)/r^2): log r_eff = log r - (X^2-Y^2)/(2 r^2) log(X^2/Y^2)
+        const T log_reff = P.lr_abs - (T)0.5 * XmY * M<T>::rcp(P.r2) * M<T>::log1p(XmY * Z.inv_Ysq);
+        alpha_sc = alpha_of_log(log_reff, ph);
+        lo = pref * alpha_sc * P.r2 * inv_XY;
+    } else {
+        // Balitsky: r^2/(X^2Y^2) + (aY/aX - 1)/Y^2 + (aX/aY - 1)/X^2
+        alpha_sc = P.alpha_r;
+        const T bracket =
+            (P.r2 + dalpha * M<T>::div(Z.alpha_Y * XmY + Z.Ysq * dalpha, alpha_X * Z.alpha_Y)) * inv_XY;
+        lo = pref * P.alpha_r * bracket;
+    }
+    if (!M<T>::finite(lo)) lo = (T)0;
+    // dipole N_X + N_Y - N_r - N_X N_Y = S_r (N_Y + D_X) - D_X D_Y  (or with X and Y exchanged)
+    T NX, DX;
+    k1_amplitude(s, P, dX, NX, DX);
+    const T base = Z.NY <= NX ? Z.NY + DX : NX + Z.DY;
+    const T dipole = P.Sr * base - DX * Z.DY;
+    if (!ph.resum) {
+        const T bare = lo * dipole;
+        return M<T>::finite(bare) ? bare : (T)0;
+    }
+    // double-log resummation (k1.py:109-119) with the RESUM_RC coupling
+    const T alpha_res = ph.resum_rc == NLO_RESUM_RC_PARENT
+                            ? P.alpha_r
+                            : (ph.resum_rc == NLO_RESUM_RC_FIXED ? ph.fixed_as : alpha_min);
     const T xarg = (T)4 * dX * Z.dY;
-    const T abar = alpha_min * ph.nc * (T)(1.0 / kPi);
+    const T abar = alpha_res * ph.nc * (T)(1.0 / kPi);
     const T as_x = M<T>::sqrt(abar * M<T>::fabs(xarg));
     T dlog = (T)1;
     if (as_x != (T)0) {
@@ -139,18 +176,17 @@ __device__ __forceinline__ T k1_point(const SplineView<T>& s, const K1Parent<T>&
     }
     if (!(r > (T)1.01 * ph.minr)) dlog = (T)1;
     if (!M<T>::finite(dlog)) return (T)0;
-    // single-log resummation (k1.py:121-132): exp(-abar A1 |log(ksub (r/minxy)^2)|)
-    const T dminxy = M<T>::fmin(dX, Z.dY);
-    const T slog_exp = -abar * (T)(11.0 / 12.0) * M<T>::fabs(ph.log_ksub - (T)2 * dminxy);
-    const T slog = M<T>::exp_fast(slog_exp);
-    const T lo_single = pref * P.alpha_r * P.r2 * inv_XY;
-    const T k1fin = lo * P.alpha_r * ph.nc * (T)(1.0 / (4.0 * kPi)) *
+    // single-log resummation (k1.py:121-132): exp(-abar A1 |log(ksub (r/minxy)^2)|) and its
+    // first-order expansion, subtracted with the kernel at one power of the coupling
+    T slog = (T)1, slog_exp = (T)0;
+    if (ph.slog) {
+        const T dminxy = M<T>::fmin(dX, Z.dY);
+        slog_exp = -abar * (T)(11.0 / 12.0) * M<T>::fabs(ph.log_ksub - (T)2 * dminxy);
+        slog = M<T>::exp_fast(slog_exp);
+    }
+    const T lo_single = pref * alpha_sc * P.r2 * inv_XY;
+    const T k1fin = lo * alpha_sc * ph.nc * (T)(1.0 / (4.0 * kPi)) *
                     ((T)(67.0 / 9.0 - kPi * kPi / 3.0) - (T)(10.0 / 9.0) * ph.nf_over_nc);
-    // dipole N_X + N_Y - N_r - N_X N_Y = S_r (N_Y + D_X) - D_X D_Y  (or with X and Y exchanged)
-    T NX, DX;
-    k1_amplitude(s, P, dX, NX, DX);
-    const T base = Z.NY <= NX ? Z.NY + DX : NX + Z.DY;
-    const T dipole = P.Sr * base - DX * Z.DY;
     const T result = (dlog * slog * lo - lo_single * slog_exp + k1fin) * dipole;
     return M<T>::finite(result) ? result : (T)0;
 }

@@ -118,6 +118,7 @@ __device__ __forceinline__ void k2_prepare(const SplineView<T>& s, const Phys<T>
 template <typename T>
 struct K2Parent {
     T r, r2, lr, two_r;
+    T alpha_r;  // the RC_NLO = PARENT_NLO coupling
 };
 
 // K2 and Kf contributions of one sample to one parent (already weighted).
@@ -174,7 +175,8 @@ __device__ __forceinline__ void k2_point(const EvalSpline& s, const Phys<T>& ph,
     }
     if (!(ph.nf > (T)0)) fermion = (T)0;
     const T lmin = M<T>::fmin(M<T>::fmin(rec[kLmin], P.lr), (T)0.5 * M<T>::fmin(lXs, lX2s));
-    const T alpha = alpha_of_log(lmin, ph);
+    // _nlo_alpha_s (bk/derivatives.py:615-632): the smallest of the six sizes, or the parent
+    const T alpha = ph.nlo_parent ? P.alpha_r : alpha_of_log(lmin, ph);
     const T scale = alpha * alpha * rec[kCpt];
     k2w = k2part * scale;
     kfw = -fermion * scale;
@@ -260,9 +262,11 @@ __device__ __forceinline__ float fast_ndiff(const P2S& A, const P2S& B)
 
 struct K2ParentF {
     float r, r2, lr, two_r, four_r;
+    float alpha_r;  // the RC_NLO = PARENT_NLO coupling
 };
 
-// COUPLING: 0 smooth freeze, 1 smooth freeze capped at alpha_cap, 2 fixed.
+// COUPLING: 0 smooth freeze, 1 smooth freeze capped at alpha_cap, 2 fixed, 3 any coupling
+// of alpha_of_log (flavour thresholds), 4 the parent's coupling (RC_NLO = PARENT_NLO).
 template <bool SYM, int COUPLING>
 __device__ __forceinline__ void k2_point_fast(const FastSpline& s, const Phys<float>& ph, const K2ParentF& P,
                                               const float4* __restrict__ rec4, float& k2w, float& kfw)
@@ -329,6 +333,10 @@ __device__ __forceinline__ void k2_point_fast(const FastSpline& s, const Phys<fl
     float alpha;
     if (COUPLING == 2) {
         alpha = ph.fixed_as;
+    } else if (COUPLING == 4) {
+        alpha = P.alpha_r;
+    } else if (COUPLING == 3) {
+        alpha = alpha_of_log(fminf(fminf(Lmin, P.lr), (0.5f * LN2) * fminf(L2X, L2X2)), ph);
     } else {
         const float lmin = fminf(fminf(Lmin, P.lr), (0.5f * LN2) * fminf(L2X, L2X2));
         const float right = fmaf(-10.0f, lmin, 5.0f * ph.log_sc);
@@ -407,6 +415,8 @@ __global__ void __launch_bounds__(1024) k2kf_kernel(Phys<T> ph, K2Box<T> box, So
         PF.lr = (float)log(r);
         PF.two_r = (float)(2.0 * r);
         PF.four_r = (float)(4.0 * r);
+        P.alpha_r = alpha_of_log(P.lr, ph);
+        PF.alpha_r = (float)P.alpha_r;
     }
     double acc_k2 = 0.0, acc_kf = 0.0, acc_sq = 0.0;
     const uint64_t tile = blockDim.x;
@@ -544,7 +554,11 @@ cudaError_t launch_k2kf(const nlo_bk_params& p, const double* r, int points, con
     int used = 0;
     const bool fp64 = p.precision == NLO_PRECISION_FP64;
     const bool sym = p.symmetrize != 0;
-    const int coupling = p.fixed_coupling ? 2 : (p.alpha_cap > 0.0 ? 1 : 0);
+    const int coupling = p.fixed_coupling                 ? 2
+                         : p.rc_nlo == NLO_RC_NLO_PARENT ? 4
+                         : p.nf > 3.0                    ? 3
+                         : p.alpha_cap > 0.0             ? 1
+                                                         : 0;
 #define NLO_K2_LAUNCH(T, S, C)                                                                                  \
     launch_typed<T, S, C>(p, r, points, spline, active, count, dirs, offset, samples, box, partial, max_blocks, \
                           threads, parent_tiles, &used, stream)
@@ -554,8 +568,12 @@ cudaError_t launch_k2kf(const nlo_bk_params& p, const double* r, int points, con
         e = sym ? NLO_K2_LAUNCH(float, true, 0) : NLO_K2_LAUNCH(float, false, 0);
     else if (coupling == 1)
         e = sym ? NLO_K2_LAUNCH(float, true, 1) : NLO_K2_LAUNCH(float, false, 1);
-    else
+    else if (coupling == 2)
         e = sym ? NLO_K2_LAUNCH(float, true, 2) : NLO_K2_LAUNCH(float, false, 2);
+    else if (coupling == 3)
+        e = sym ? NLO_K2_LAUNCH(float, true, 3) : NLO_K2_LAUNCH(float, false, 3);
+    else
+        e = sym ? NLO_K2_LAUNCH(float, true, 4) : NLO_K2_LAUNCH(float, false, 4);
 #undef NLO_K2_LAUNCH
     if (e != cudaSuccess) return e;
     k2kf_finalize_kernel<<<(points * 32 + 255) / 256, 256, 0, stream>>>(partial, used, points, active, count, out);

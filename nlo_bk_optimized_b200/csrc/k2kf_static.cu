@@ -76,8 +76,9 @@ extern "C" int nlo_bk_k2kf_static(const nlo_bk_params* params, const double* r, 
 {
     if (!params || !dirs || !box || !r || !spline || !active || !count || !out)
         return set_last_error(NLO_ERR_INVALID, "nlo_bk_k2kf_static: NULL argument");
-    if (!(params->nc > 0) || !(params->nf == 0.0 || params->nf == 3.0) || !(params->lambda_qcd > 0) ||
-        !(params->c2 > 0) || !(params->ksub > 0) ||
+    if (!(params->nc > 0) || !(params->nf == 0.0 || params->nf == 3.0 || params->nf == 5.0) ||
+        !(params->lambda_qcd > 0) || !(params->c2 > 0) || !(params->ksub > 0) ||
+        (params->rc_nlo != NLO_RC_NLO_SMALLEST && params->rc_nlo != NLO_RC_NLO_PARENT) ||
         (params->precision != NLO_PRECISION_MIXED && params->precision != NLO_PRECISION_FP64))
         return set_last_error(NLO_ERR_INVALID, "nlo_bk_k2kf_static: unsupported physics parameters");
     if (dirs->dims < 4 || dirs->dims > 8)

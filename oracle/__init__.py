@@ -44,7 +44,19 @@ class Physics(ctypes.Structure):
         ("fixed_coupling", ctypes.c_int),
         ("fixed_alpha_s", ctypes.c_double),
         ("alpha_cap", ctypes.c_double),
+        ("order", ctypes.c_int),
+        ("rc_lo", ctypes.c_int),
+        ("resum_rc", ctypes.c_int),
+        ("rc_nlo", ctypes.c_int),
     ]
+
+
+# enum codes of or_physics (nlo_oracle.c), by the reference's enum member names
+ORDER = {"NLO_RESUM_DLOG_SLOG": 0, "NLO_RESUM_DLOG": 1, "NLO": 2, "LO_RESUM_DLOG_SLOG": 3, "LO_RESUM_DLOG": 4,
+         "LO": 5}
+RC_LO = {"BALITSKY_LO": 0, "FIXED_LO": 0, "PARENT_LO": 1, "SMALLEST_LO": 2, "FAC_LO": 3, "BEUF_LO": 4}
+RESUM_RC = {"RESUM_RC_SMALLEST": 0, "RESUM_RC_PARENT": 1, "RESUM_RC_FIXED": 2}
+RC_NLO = {"SMALLEST_NLO": 0, "FIXED_NLO": 0, "PARENT_NLO": 1}
 
 
 class _Spline(ctypes.Structure):
@@ -106,10 +118,14 @@ def lib() -> ctypes.CDLL:
 
 
 def physics(config) -> Physics:
-    """Physics constants from any object with BKConfig's field names."""
+    """Physics constants and switches from any object with BKConfig's field names
+    (enum members are read by name, so the reference's own BKConfig works too)."""
 
-    fixed = getattr(config, "RC_LO", None)
-    fixed_coupling = bool(fixed is not None and getattr(fixed, "name", "") == "FIXED_LO")
+    def name(field, default):
+        value = getattr(config, field, None)
+        return getattr(value, "name", default)
+
+    fixed_coupling = name("RC_LO", "") == "FIXED_LO" or name("RC_NLO", "") == "FIXED_NLO"
     return Physics(
         float(config.NC),
         float(config.NF),
@@ -121,7 +137,16 @@ def physics(config) -> Physics:
         int(fixed_coupling),
         float(config.FIXED_AS),
         float(getattr(config, "ALPHA_S_CAP", 0.0) or 0.0),
+        ORDER[name("Order", "NLO_RESUM_DLOG_SLOG")],
+        RC_LO[name("RC_LO", "BALITSKY_LO")],
+        RESUM_RC[name("RESUM_RC", "RESUM_RC_SMALLEST")],
+        RC_NLO[name("RC_NLO", "SMALLEST_NLO")],
     )
+
+
+def has_nlo_kernels(phys: Physics) -> bool:
+    """Order.has_nlo_kernels (bk/config.py:44-50)."""
+    return phys.order <= ORDER["NLO"]
 
 
 @dataclass
@@ -328,12 +353,13 @@ def derivative(N: np.ndarray, r: np.ndarray, phys: Physics, points: np.ndarray, 
     sq = np.zeros_like(N)
     if active.size:
         K1[active] = k1_fixed(r[active], nspl, phys)
-        lower, width = nlo_box(r)
-        sums = k2kf_sums(r[active], points, lower, width, map_f32, sspl, phys)
-        n = points.shape[0]
-        K2[active] = sums[:, 0] / n
-        Kf[active] = sums[:, 1] / n
-        sq[active] = sums[:, 2]
+        if has_nlo_kernels(phys):  # LO orders take no K2 + Kf (bk/evolution.py:391, 473)
+            lower, width = nlo_box(r)
+            sums = k2kf_sums(r[active], points, lower, width, map_f32, sspl, phys)
+            n = points.shape[0]
+            K2[active] = sums[:, 0] / n
+            Kf[active] = sums[:, 1] / n
+            sq[active] = sums[:, 2]
     dNdy = K1 + K2 + Kf
     dNdy = np.where(np.isfinite(dNdy), dNdy, 0.0)
     return Derivative(dNdy, K1, K2, Kf, sq)

@@ -8,12 +8,14 @@
  * It restates, in plain C, the algorithm of the reference package
  * (HaowuDuan/nlo_bk_optimized, torch_nlo_clean/src/nlo_torch):
  *
- *   coupling              coupling.py:81-97            (_smooth_alpha_s)
+ *   coupling              coupling.py:10-46, 81-97     (bk_alpha_s: fixed, smooth
+ *                         freeze for NF <= 3, flavour thresholds for NF = 5)
  *   natural cubic spline  numerics/interpolation.py:10-92, 124-149
  *   log-log spline        numerics/interpolation.py:95-121
  *   edge rules            bk/derivatives.py:761-772     (_evaluate_loglog)
- *   K1 pointwise kernel   bk_kernels/k1.py:20-155       (Kernel_lo, production
- *                         order NLO_RESUM_DLOG_SLOG, BALITSKY_LO, RESUM_RC_SMALLEST)
+ *   K1 pointwise kernel   bk_kernels/k1.py:20-155       (Kernel_lo: every Order,
+ *                         RC_LO and RESUM_RC; production NLO_RESUM_DLOG_SLOG,
+ *                         BALITSKY_LO, RESUM_RC_SMALLEST)
  *   K1 integrand          bk/derivatives.py:434-468     (_lo_integrand)
  *   K1 fixed rule         custom_kernels/bk/k1/kernel.cu:2040-2092
  *                         (8 GL nodes in log z per r-grid interval x 24 GL nodes
@@ -22,6 +24,8 @@
  *   K2+Kf integrand       bk/derivatives.py:490-612     (_nlo_integrand) and the
  *                         log-variable Jacobian at bk/derivatives.py:322-335
  *   K2+Kf box             bk/derivatives.py:424-431     (nlo_vegas_bounds)
+ *   K2+Kf coupling        bk/derivatives.py:615-632     (_nlo_alpha_s: smallest
+ *                         size, or the parent for PARENT_NLO)
  *   dN/dY assembly        bk/evolution.py:329-351, 354-488
  *   steppers              bk/evolution.py:110-122 (Euler), 190-236 (Kutta RK3);
  *                         RK4 is the classical four-stage rule (no reference
@@ -71,6 +75,11 @@ typedef struct or_physics {
     int fixed_coupling;   /* RC_LO/RC_NLO FIXED */
     double fixed_alpha_s; /* BKConfig.FIXED_AS */
     double alpha_cap;     /* >0: cap alpha_s at this value (frozen variant) */
+    int order;            /* Order: 0 NLO_RESUM_DLOG_SLOG, 1 NLO_RESUM_DLOG, 2 NLO,
+                             3 LO_RESUM_DLOG_SLOG, 4 LO_RESUM_DLOG, 5 LO */
+    int rc_lo;            /* RC_LO: 0 BALITSKY (and FIXED), 1 PARENT, 2 SMALLEST, 3 FAC, 4 BEUF */
+    int resum_rc;         /* RESUM_RC: 0 SMALLEST, 1 PARENT, 2 FIXED */
+    int rc_nlo;           /* RC_NLO: 0 SMALLEST (and FIXED), 1 PARENT */
 } or_physics;
 
 /* One log-log spline over the r grid: knots x = log r, coefficients per interval. */
@@ -86,9 +95,22 @@ typedef struct or_spline {
 
 /* ------------------------------------------------------------------------ */
 /* coupling.py:81-97 (_smooth_alpha_s): 1/(b0 * c * logaddexp(2/c log mu0, log scale / c)) */
+static double alpha_thresholds(double r, const or_physics* p)
+{
+    /* coupling.py:25-45: Nf = 3/4/5 by 4 C2/r^2 against 1.3^2 and 4.5^2 */
+    const double dipolescale = 4.0 * p->c2 / (r * r);
+    const double nf = dipolescale < 1.3 * 1.3 ? 3.0 : (dipolescale < 4.5 * 4.5 ? 4.0 : 5.0);
+    const double lambda = nf == 3.0 ? 0.146159 : (nf == 4.0 ? 0.122944 : 0.0904389);
+    const double b0 = 11.0 - 2.0 * nf / 3.0;
+    const double log_arg = 4.0 * p->c2 / (r * r * lambda * lambda);
+    const double a = 4.0 * OR_PI / (b0 * log(log_arg));
+    return (log_arg < 1.0 || a > 1.0) ? 1.0 : a;
+}
+
 static double alpha_from_log_distance(double log_d, const or_physics* p)
 {
     if (p->fixed_coupling) return p->fixed_alpha_s;
+    if (p->nf > 3.0) return alpha_thresholds(exp(log_d), p);
     const double b0 = (11.0 * p->nc - 2.0 * p->nf) / (12.0 * OR_PI);
     const double c = 0.2;
     const double left = 2.0 / c * log(2.5);
@@ -311,9 +333,10 @@ static int knot_index(const or_spline* s, double r)
 }
 
 /* ------------------------------------------------------------------------ */
-/* K1: Kernel_lo (k1.py:20-155) x dipole (derivatives.py:452-468), stable form. */
-static double k1_integrand_at(double r, int knot, double z, double theta, const or_spline* nspl,
-                              const or_physics* p)
+/* K1: Kernel_lo (k1.py:20-155) x dipole (derivatives.py:452-468), stable form.
+ * RC_LO picks the kernel (k1.py:37-94); Order LO and NLO stop at the bare kernel
+ * (k1.py:97-98); RESUM_RC picks the resummation coupling (k1.py:100-107). */
+static double kernel_lo_value(double r, double z, double theta, const or_physics* p)
 {
     const double sh = sin(0.5 * theta);
     const double s2 = sh * sh;
@@ -324,19 +347,19 @@ static double k1_integrand_at(double r, int knot, double z, double theta, const 
     const double Ysq = z * z;
     const double nc = p->nc;
 
-    const double dipole = k1_dipole(nspl, knot, X, Y);
-
     const double log_r = log(r), log_X = 0.5 * log(Xsq), log_Y = log(z);
     const double alpha_r = alpha_from_log_distance(log_r, p);
     const double alpha_X = alpha_from_log_distance(log_X, p);
     const double alpha_Y = alpha_from_log_distance(log_Y, p);
+    const double log_min = fmin(fmin(log_X, log_Y), log_r);
+    const double alpha_min = alpha_from_log_distance(log_min, p);
 
     /* X^2 - Y^2 = r (r - 2 z cos theta), exact. */
     const double cos_t = 1.0 - 2.0 * s2;
     const double XmY = r * (r - 2.0 * z * cos_t);
-    /* alpha_Y - alpha_X without cancellation (fixed coupling: 0). */
+    /* alpha_Y - alpha_X without cancellation for the smooth coupling (fixed: 0). */
     double dalpha = 0.0;
-    if (!p->fixed_coupling && p->alpha_cap <= 0.0) {
+    if (!p->fixed_coupling && p->alpha_cap <= 0.0 && p->nf <= 3.0) {
         const double b0 = (11.0 * nc - 2.0 * p->nf) / (12.0 * OR_PI);
         const double c = 0.2;
         const double left = 2.0 / c * log(2.5);
@@ -346,21 +369,52 @@ static double k1_integrand_at(double r, int knot, double z, double theta, const 
         /* Lambda = c * lae; alpha = 1/(b0 Lambda):
            alpha_Y - alpha_X = alpha_X alpha_Y b0 c (lae_X - lae_Y) */
         dalpha = alpha_X * alpha_Y * b0 * c * lae_difference(left, right_Y, delta);
-    } else if (p->alpha_cap > 0.0) {
+    } else if (!p->fixed_coupling) {
         dalpha = alpha_Y - alpha_X;
     }
-    /* r^2/(X^2Y^2) + (aY/aX - 1)/Y^2 + (aX/aY - 1)/X^2
-       = [r^2 + dA (aY (X^2-Y^2) + Y^2 dA)/(aX aY)] / (X^2 Y^2) */
-    const double bracket = (r * r + dalpha * (alpha_Y * XmY + Ysq * dalpha) / (alpha_X * alpha_Y)) / (Xsq * Ysq);
-    double lo_kernel = nc / (2.0 * OR_PI * OR_PI) * alpha_r * bracket;
+    const double pref = nc / (2.0 * OR_PI * OR_PI);
+    const double rxy2 = r * r / (Xsq * Ysq);
+    double lo_kernel, alpha_scale;
+    switch (p->rc_lo) {
+    case 1: /* PARENT_LO */
+        alpha_scale = alpha_r;
+        lo_kernel = pref * alpha_r * rxy2;
+        break;
+    case 2: /* SMALLEST_LO */
+        alpha_scale = alpha_min;
+        lo_kernel = pref * alpha_min * rxy2;
+        break;
+    case 3: { /* FAC_LO: 1/(2pi) / (1/abar_r + (X^2-Y^2)/r^2 (abar_X - abar_Y)/(abar_X abar_Y)) r^2/(X^2Y^2)
+                 with (abar_X - abar_Y)/(abar_X abar_Y) = -(pi/Nc) (alpha_Y - alpha_X)/(alpha_X alpha_Y) */
+        alpha_scale = alpha_r;
+        const double den = 1.0 / alpha_r - XmY / (r * r) * dalpha / (alpha_X * alpha_Y);
+        lo_kernel = pref * rxy2 / den;
+        break;
+    }
+    case 4: { /* BEUF_LO: r_eff^2 = r^2 (Y^2/X^2)^((X^2-Y^2)/r^2) */
+        const double log_reff = log_r - 0.5 * XmY / (r * r) * log1p(XmY / Ysq);
+        alpha_scale = alpha_from_log_distance(log_reff, p);
+        lo_kernel = pref * alpha_scale * rxy2;
+        break;
+    }
+    default: { /* BALITSKY_LO (and FIXED_LO):
+                  r^2/(X^2Y^2) + (aY/aX - 1)/Y^2 + (aX/aY - 1)/X^2
+                  = [r^2 + dA (aY (X^2-Y^2) + Y^2 dA)/(aX aY)] / (X^2 Y^2) */
+        alpha_scale = alpha_r;
+        const double bracket =
+            (r * r + dalpha * (alpha_Y * XmY + Ysq * dalpha) / (alpha_X * alpha_Y)) / (Xsq * Ysq);
+        lo_kernel = pref * alpha_r * bracket;
+    }
+    }
     if (!isfinite(lo_kernel)) lo_kernel = 0.0;
+    const int resum = p->order != 2 && p->order != 5;
+    const int slog_on = p->order == 0 || p->order == 3;
+    if (!resum) return lo_kernel;
 
-    /* resummation (k1.py:100-155) with RESUM_RC_SMALLEST: alpha at min(X, Y, r) */
+    const double alpha_res = p->resum_rc == 1 ? alpha_r : (p->resum_rc == 2 ? p->fixed_alpha_s : alpha_min);
     const double min_xy = fmin(X, Y);
-    const double log_min = fmin(fmin(log_X, log_Y), log_r);
-    const double alpha_min = alpha_from_log_distance(log_min, p);
     const double xarg = 4.0 * (log_X - log_r) * (log_Y - log_r);
-    const double as_x = sqrt(alpha_min * nc / OR_PI * fabs(xarg));
+    const double as_x = sqrt(alpha_res * nc / OR_PI * fabs(xarg));
     double dlog;
     if (as_x == 0.0) {
         dlog = 1.0;
@@ -370,18 +424,30 @@ static double k1_integrand_at(double r, int knot, double z, double theta, const 
     if (!(r > 1.01 * p->minr)) dlog = 1.0;
     if (!isfinite(dlog)) return 0.0;
 
-    const double alphabar = alpha_min * nc / OR_PI;
+    const double alphabar = alpha_res * nc / OR_PI;
     const double A1 = 11.0 / 12.0;
     const double ratio = r / min_xy;
-    const double slog = exp(-alphabar * A1 * fabs(log(p->ksub * ratio * ratio)));
-    const double slog_exp = -alphabar * A1 * fabs(2.0 * log(sqrt(p->ksub) * r / min_xy));
-    const double rxy = r / (X * Y);
-    const double lo_single = alpha_r * nc / (2.0 * OR_PI * OR_PI) * rxy * rxy;
+    double slog = 1.0, slog_exp = 0.0;
+    if (slog_on) {
+        slog = exp(-alphabar * A1 * fabs(log(p->ksub * ratio * ratio)));
+        slog_exp = -alphabar * A1 * fabs(2.0 * log(sqrt(p->ksub) * r / min_xy));
+    }
+    const double lo_single = alpha_scale * pref * rxy2;
     const double subtract = lo_single * slog_exp;
-    const double k1fin = lo_kernel * alpha_r * nc / (4.0 * OR_PI) *
+    const double k1fin = lo_kernel * alpha_scale * nc / (4.0 * OR_PI) *
                          (67.0 / 9.0 - OR_PI * OR_PI / 3.0 - 10.0 / 9.0 * p->nf / nc);
-    const double result = (dlog * slog * lo_kernel - subtract + k1fin) * dipole;
+    const double result = dlog * slog * lo_kernel - subtract + k1fin;
     return isfinite(result) ? result : 0.0;
+}
+
+static double k1_integrand_at(double r, int knot, double z, double theta, const or_spline* nspl,
+                              const or_physics* p)
+{
+    const double sh = sin(0.5 * theta);
+    const double Xsq = (r - z) * (r - z) + 4.0 * r * z * sh * sh;
+    if (Xsq < 1e-40 || z < 1e-20 || r < 1e-20) return 0.0;
+    const double value = kernel_lo_value(r, z, theta, p) * k1_dipole(nspl, knot, sqrt(Xsq), z);
+    return isfinite(value) ? value : 0.0;
 }
 
 double or_k1_integrand(double r, double z, double theta, const or_spline* nspl, const or_physics* p)
@@ -556,7 +622,8 @@ static void k2_eval(double r, double log_r, const k2_point* pt, const or_spline*
         kfres = -fermion;
     }
     const double log_min = fmin(fmin(log_r, pt->log_min_pt), 0.5 * fmin(log(Xsq), log(X2sq)));
-    const double alpha = alpha_from_log_distance(log_min, p);
+    /* _nlo_alpha_s (bk/derivatives.py:615-632): smallest size, or the parent (PARENT_NLO) */
+    const double alpha = alpha_from_log_distance(p->rc_nlo == 1 ? log_r : log_min, p);
     const double scale = (alpha * p->nc) * (alpha * p->nc) / (8.0 * OR_PI * OR_PI * OR_PI * OR_PI) * pt->jac;
     k2res *= scale;
     kfres *= scale;
@@ -746,46 +813,7 @@ double or_lo_kernel_literal_q(double r_, double z_, double theta, const or_physi
 /* Stable lo-kernel alone (same as or_k1_integrand without the dipole), for tests. */
 double or_lo_kernel(double r, double z, double theta, const or_physics* p)
 {
-    /* Reproduce the kernel algebra of or_k1_integrand. */
-    const double sh = sin(0.5 * theta);
-    const double s2 = sh * sh;
-    const double Xsq = (r - z) * (r - z) + 4.0 * r * z * s2;
-    if (Xsq < 1e-40 || z < 1e-20 || r < 1e-20) return 0.0;
-    const double X = sqrt(Xsq), Y = z, Ysq = z * z, nc = p->nc;
-    const double log_r = log(r), log_X = 0.5 * log(Xsq), log_Y = log(z);
-    const double alpha_r = alpha_from_log_distance(log_r, p);
-    const double alpha_X = alpha_from_log_distance(log_X, p);
-    const double alpha_Y = alpha_from_log_distance(log_Y, p);
-    const double cos_t = 1.0 - 2.0 * s2;
-    const double XmY = r * (r - 2.0 * z * cos_t);
-    double dalpha = 0.0;
-    if (!p->fixed_coupling && p->alpha_cap <= 0.0) {
-        const double b0 = (11.0 * nc - 2.0 * p->nf) / (12.0 * OR_PI);
-        const double c = 0.2;
-        const double left = 2.0 / c * log(2.5);
-        const double right_Y = (log(4.0 * p->c2 / (p->lambda_qcd * p->lambda_qcd)) - 2.0 * log_Y) / c;
-        const double delta = -log1p(XmY / Ysq) / c;
-        dalpha = alpha_X * alpha_Y * b0 * c * lae_difference(left, right_Y, delta);
-    } else if (p->alpha_cap > 0.0) {
-        dalpha = alpha_Y - alpha_X;
-    }
-    const double bracket = (r * r + dalpha * (alpha_Y * XmY + Ysq * dalpha) / (alpha_X * alpha_Y)) / (Xsq * Ysq);
-    const double lo_kernel = nc / (2.0 * OR_PI * OR_PI) * alpha_r * bracket;
-    const double min_xy = fmin(X, Y);
-    const double alpha_min = alpha_from_log_distance(fmin(fmin(log_X, log_Y), log_r), p);
-    const double xarg = 4.0 * (log_X - log_r) * (log_Y - log_r);
-    const double as_x = sqrt(alpha_min * nc / OR_PI * fabs(xarg));
-    double dlog = as_x == 0.0 ? 1.0 : (xarg >= 0.0 ? j1(2.0 * as_x) : or_bessel_i1(2.0 * as_x)) / as_x;
-    if (!(r > 1.01 * p->minr)) dlog = 1.0;
-    const double alphabar = alpha_min * nc / OR_PI;
-    const double ratio = r / min_xy;
-    const double slog = exp(-alphabar * (11.0 / 12.0) * fabs(log(p->ksub * ratio * ratio)));
-    const double slog_exp = -alphabar * (11.0 / 12.0) * fabs(2.0 * log(sqrt(p->ksub) * r / min_xy));
-    const double rxy = r / (X * Y);
-    const double lo_single = alpha_r * nc / (2.0 * OR_PI * OR_PI) * rxy * rxy;
-    const double k1fin = lo_kernel * alpha_r * nc / (4.0 * OR_PI) *
-                         (67.0 / 9.0 - OR_PI * OR_PI / 3.0 - 10.0 / 9.0 * p->nf / nc);
-    return dlog * slog * lo_kernel - lo_single * slog_exp + k1fin;
+    return kernel_lo_value(r, z, theta, p);
 }
 
 int or_num_threads(void)

@@ -20,3 +20,29 @@ def bk_reference() -> dict[str, np.ndarray]:
 def bk_table_mc50w() -> dict[str, np.ndarray]:
     with np.load(GOLDEN / "bk_table_mc50w.npz") as data:
         return {key: data[key] for key in data.files}
+
+
+@lru_cache(maxsize=None)
+def bk_variants() -> dict[str, np.ndarray]:
+    with np.load(GOLDEN / "bk_variants.npz") as data:
+        return {key: data[key] for key in data.files}
+
+
+def variant_config(name: str):
+    """The package's BKConfig for a variant of bk_variants.npz (grid of make_golden.variants)."""
+    import ast
+
+    from nlo_bk_optimized_b200.bk import config as bkc
+
+    data = bk_variants()
+    names = [str(n) for n in data["names"]]
+    overrides = ast.literal_eval(str(data["overrides"][names.index(name)]))
+    kwargs = {}
+    for field, value in overrides.items():
+        if isinstance(value, str):
+            for enum in (bkc.BKOrder, bkc.RunningCouplingLO, bkc.RunningCouplingNLO, bkc.ResummationCoupling):
+                if value in enum.__members__:
+                    value = enum[value]
+                    break
+        kwargs[field] = value
+    return bkc.BKConfig(RPOINTS=99, MINR=1e-6, MAXR=1e2, **kwargs)

@@ -50,14 +50,29 @@ def test_nlobk_option_mapping():
 
 @pytest.mark.parametrize("argv,why", [
     (["--integration", "vegas"], "SOBOL"),
-    (["--order", "lo"], "NLO_RESUM_DLOG_SLOG"),
-    (["--rc-lo", "parent"], "RC_LO"),
-    (["--resum-rc", "fixed"], "RESUM_RC"),
-    (["--nf", "5"], "NF"),
+    (["--integration", "miser"], "SOBOL"),
+    (["--kinematical-constraint", "--euler"], "kinematical constraint"),
 ])
 def test_nlobk_switches_outside_the_device_kernels(argv, why):
     config = nlobk.config_from_args(nlobk._parser().parse_args(argv))
     assert why in device_supported(config)
+
+
+@pytest.mark.parametrize("argv", [
+    ["--order", "lo"], ["--order", "nlo"], ["--order", "lo_resum_dlog"], ["--order", "nlo_resum_dlog"],
+    ["--rc-lo", "parent"], ["--rc-lo", "smallest"], ["--rc-lo", "fac"], ["--rc-lo", "beuf"],
+    ["--resum-rc", "fixed"], ["--resum-rc", "parent"], ["--rc-nlo", "parent"], ["--nf", "5"], ["--nf", "0"],
+    # orders without NLO kernels never integrate K2 + Kf, so its method does not matter
+    ["--order", "lo", "--integration", "vegas"],
+])
+def test_nlobk_variants_run_on_the_device(argv):
+    from nlo_bk_optimized_b200.bk.evolution import params_of
+
+    config = nlobk.config_from_args(nlobk._parser().parse_args(argv))
+    assert device_supported(config) is None
+    params = params_of(config, 0)
+    assert (params.order, params.rc_lo, params.resum_rc, params.rc_nlo) != (0, 0, 0, 0) or argv == ["--nf", "5"] \
+        or argv == ["--nf", "0"]
 
 
 def test_nlobk_argument_errors(capsys):

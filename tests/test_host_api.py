@@ -135,7 +135,7 @@ def test_library_rejects_bad_arguments_without_a_gpu():
 
 
 def test_c_struct_layouts_match_ctypes(tmp_path):
-    """The ctypes mirrors of the DIS structs have the C header's sizes and offsets."""
+    """The ctypes mirrors of the C structs have the C header's sizes and offsets."""
     import ctypes
     import shutil
     import subprocess
@@ -149,15 +149,17 @@ def test_c_struct_layouts_match_ctypes(tmp_path):
     src = tmp_path / "layout.c"
     src.write_text(
         "#include <stdio.h>\n#include <stddef.h>\n#include \"nlo_b200.h\"\n"
-        "int main(void){printf(\"%zu %zu %zu %zu %zu %zu %zu\\n\", sizeof(nlo_dis_kinematics),"
+        "int main(void){printf(\"%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n\", sizeof(nlo_dis_kinematics),"
         " offsetof(nlo_dis_kinematics, maxr), offsetof(nlo_dis_kinematics, max_alpha), sizeof(nlo_dipole),"
-        " offsetof(nlo_dipole, table), sizeof(nlo_vegas_options), offsetof(nlo_vegas_options, keep_edges));return 0;}\n")
+        " offsetof(nlo_dipole, table), sizeof(nlo_vegas_options), offsetof(nlo_vegas_options, keep_edges),"
+        " sizeof(nlo_bk_params), offsetof(nlo_bk_params, order), offsetof(nlo_bk_params, rc_nlo));return 0;}\n")
     exe = tmp_path / "layout"
     subprocess.run([gcc, "-I", str(root / "include"), str(src), "-o", str(exe)], check=True)
     c = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     py = [ctypes.sizeof(_native.DisKinematics), _native.DisKinematics.maxr.offset,
           _native.DisKinematics.max_alpha.offset, ctypes.sizeof(_native.Dipole), _native.Dipole.table.offset,
-          ctypes.sizeof(_native.VegasOptions), _native.VegasOptions.keep_edges.offset]
+          ctypes.sizeof(_native.VegasOptions), _native.VegasOptions.keep_edges.offset,
+          ctypes.sizeof(_native.BKParams), _native.BKParams.order.offset, _native.BKParams.rc_nlo.offset]
     assert c == py
 
 

@@ -85,6 +85,8 @@ typedef struct nlo_bk_params {
     int32_t rc_lo;          /* NLO_RC_LO_* */
     int32_t resum_rc;       /* NLO_RESUM_RC_* */
     int32_t rc_nlo;         /* NLO_RC_NLO_* */
+    int32_t kinematical_constraint; /* KINEMATICAL_CONSTRAINT: K1 reads the amplitude history;
+                                       only nlo_bk_rhs_history / nlo_bk_evolve_history accept it */
 } nlo_bk_params;
 
 /* Scrambled Sobol direction numbers of torch.quasirandom.SobolEngine
@@ -197,6 +199,30 @@ int nlo_bk_stage(const double* N, const double* const* k, const double* coef, in
 int nlo_bk_evolve(const nlo_bk_params* params, const double* r, int32_t points, int32_t steps, double step,
                   int32_t stepper, const nlo_sobol_dirs* dirs, int64_t samples, const nlo_bk_box* box,
                   double* table, uint32_t* status, void* workspace, size_t workspace_bytes, void* stream);
+
+/* nlo_bk_rhs with the amplitude history that the kinematical constraint reads
+ * (bk/derivatives.py:469-487, 712-758; _derivative_components, bk/evolution.py:354-488):
+ * hist_N: device double[rows*points], rows >= 1, the last row the amplitude whose
+ * derivative is taken; hist_y: device double[rows], increasing, the last value the current
+ * rapidity.  Where min(X, Y) > r, K1 takes the daughters at the rapidity shifted by
+ * log(min(X^2, Y^2)/r^2), interpolated from the history (6-point natural splines in r,
+ * linear in y); where the shift is negative it contributes nothing.  Without
+ * params->kinematical_constraint the history beyond the last row is not read. */
+int nlo_bk_rhs_history(const nlo_bk_params* params, const double* r, int32_t points, const double* hist_y,
+                       const double* hist_N, int32_t rows, const nlo_sobol_dirs* dirs, int64_t samples,
+                       const nlo_bk_box* box, double* dndy, double* k1, double* k2kf, void* workspace,
+                       size_t workspace_bytes, void* stream);
+
+/* nlo_bk_evolve continued from a stored history (the loop of _bk_steps, bk/evolution.py:85-159,
+ * over a table that already holds rows 0..first): table: device double[(first+steps+1)*points],
+ * rows 0..first input (row `first` the current amplitude); y: device double[first+steps+1], the
+ * rapidities of all rows (y[k] = y[k-1] + step as the caller accumulates them).  Computes rows
+ * first+1..first+steps.  With params->kinematical_constraint each step reads the rows before
+ * it, and the stepper must be NLO_STEPPER_EULER (BKConfig requires EULER_METHOD). */
+int nlo_bk_evolve_history(const nlo_bk_params* params, const double* r, int32_t points, const double* y,
+                          int32_t first, int32_t steps, double step, int32_t stepper, const nlo_sobol_dirs* dirs,
+                          int64_t samples, const nlo_bk_box* box, double* table, uint32_t* status, void* workspace,
+                          size_t workspace_bytes, void* stream);
 
 /* ======================================================================== NLO DIS
  * The NLO DIS cross-section integrands (dis/observables.py, dis/lo.py, dis/transverse.py,

@@ -41,6 +41,7 @@ class BKParams(ctypes.Structure):
         ("rc_lo", ctypes.c_int32),
         ("resum_rc", ctypes.c_int32),
         ("rc_nlo", ctypes.c_int32),
+        ("kinematical_constraint", ctypes.c_int32),
     ]
 
 
@@ -141,6 +142,8 @@ EXPORTED = (
     "nlo_bk_rhs_workspace_bytes",
     "nlo_bk_rhs",
     "nlo_bk_evolve",
+    "nlo_bk_evolve_history",
+    "nlo_bk_rhs_history",
     "nlo_bk_rhs_shard",
     "nlo_bk_stage",
     "nlo_dis_table_doubles",
@@ -192,6 +195,12 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.nlo_bk_rhs.argtypes = [P(BKParams), vp, vp, i32, P(SobolDirs), i64, P(Box), vp, vp, vp, vp, sz, vp]
     lib.nlo_bk_evolve.restype = ctypes.c_int
     lib.nlo_bk_evolve.argtypes = [P(BKParams), vp, i32, i32, d, i32, P(SobolDirs), i64, P(Box), vp, vp, vp, sz, vp]
+    lib.nlo_bk_evolve_history.restype = ctypes.c_int
+    lib.nlo_bk_evolve_history.argtypes = [P(BKParams), vp, i32, vp, i32, i32, d, i32, P(SobolDirs), i64, P(Box), vp,
+                                          vp, vp, sz, vp]
+    lib.nlo_bk_rhs_history.restype = ctypes.c_int
+    lib.nlo_bk_rhs_history.argtypes = [P(BKParams), vp, i32, vp, vp, i32, P(SobolDirs), i64, P(Box), vp, vp, vp, vp,
+                                       sz, vp]
     lib.nlo_bk_rhs_shard.restype = ctypes.c_int
     lib.nlo_bk_rhs_shard.argtypes = [P(BKParams), vp, vp, i32, i32, i32, P(SobolDirs), i64, P(Box), vp, vp, sz, vp]
     lib.nlo_bk_stage.restype = ctypes.c_int

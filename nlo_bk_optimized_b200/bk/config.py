@@ -156,12 +156,10 @@ class BKConfig:
 def device_supported(config: BKConfig) -> str | None:
     """Return why a configuration is outside the device kernels, or None.
 
-    Every Order, RC_LO, RC_NLO, RESUM_RC and NF of BKConfig runs on the device; the K2+Kf
-    integral is always the fixed Sobol QMC estimate, and the kinematical constraint
-    (which needs the amplitude history) is not implemented."""
+    Every Order, RC_LO, RC_NLO, RESUM_RC and NF of BKConfig, and the kinematical
+    constraint, run on the device; the K2+Kf integral is always the fixed Sobol QMC
+    estimate."""
 
-    if config.KINEMATICAL_CONSTRAINT:
-        return "the kinematical constraint is not implemented on the device"
     if config.Order.has_nlo_kernels and config.INTMETHOD_NLO is not IntegrationMethod.SOBOL:
         return "the device K2+Kf integrates with IntegrationMethod.SOBOL"
     return None

@@ -80,6 +80,7 @@ def params_of(config: BKConfig, precision: int) -> _native.BKParams:
     p.rc_lo = RC_LO_CODES[config.RC_LO]
     p.resum_rc = RESUM_RC_CODES[config.RESUM_RC]
     p.rc_nlo = RC_NLO_CODES[config.RC_NLO]
+    p.kinematical_constraint = int(bool(config.KINEMATICAL_CONSTRAINT))
     return p
 
 
@@ -131,8 +132,13 @@ def rhs(
     *,
     seed: int | None = None,
     precision: int | None = None,
+    history: tuple[torch.Tensor, torch.Tensor] | None = None,
 ) -> tuple[torch.Tensor, torch.Tensor, torch.Tensor]:
-    """dN/dY, K1 and K2+Kf (each [R] float64) for one amplitude row (bk/evolution.py:329-488)."""
+    """dN/dY, K1 and K2+Kf (each [R] float64) for one amplitude row (bk/evolution.py:329-488).
+
+    ``history`` = (y [rows], N [rows, R]) is the amplitude history the kinematical
+    constraint reads (its last row the current amplitude; _derivative_components'
+    rapidity, history_y, history_N)."""
 
     device = _cuda_device(r.device)
     r64 = r.to(device=device, dtype=torch.float64).contiguous()
@@ -148,6 +154,22 @@ def rhs(
     k2kf = torch.empty_like(N64)
     ws = workspace(device, points)
     lib = _native.load()
+    if config.KINEMATICAL_CONSTRAINT:
+        if history is None:
+            raise ValueError("kinematical evolution requires rapidity and amplitude history")
+        hist_y = history[0].to(device=device, dtype=torch.float64).contiguous()
+        hist_N = history[1].to(device=device, dtype=torch.float64).contiguous()
+        if hist_N.ndim != 2 or hist_N.shape[1] != points or hist_y.numel() != hist_N.shape[0]:
+            raise ValueError("history must be (y [rows], N [rows, points])")
+        with torch.cuda.device(device):
+            _native.check(
+                lib.nlo_bk_rhs_history(
+                    params, r64.data_ptr(), points, hist_y.data_ptr(), hist_N.data_ptr(), hist_N.shape[0], dirs,
+                    int(config.MCINTPOINTS), box, dndy.data_ptr(), k1.data_ptr(), k2kf.data_ptr(), ws.data_ptr(),
+                    ws.numel(), _native.stream_handle(device),
+                )
+            )
+        return dndy, k1, k2kf
     with torch.cuda.device(device):
         _native.check(
             lib.nlo_bk_rhs(
@@ -166,11 +188,15 @@ def _evolve_rows(
     config: BKConfig,
     seed: int | None,
     precision: int,
+    *,
+    history_N: torch.Tensor | None = None,
+    y_all: list[float] | None = None,
 ) -> torch.Tensor:
+    """Rows [steps+1, R] from N0.  With the kinematical constraint the evolution reads
+    the history: ``history_N`` the rows before N0 (may be empty) and ``y_all`` the
+    rapidities of history, N0 and every new row."""
     device = r64.device
     points = r64.numel()
-    table = torch.empty((steps + 1, points), dtype=torch.float64, device=device)
-    table[0] = N0
     status = torch.zeros(1, dtype=torch.int32, device=device)
     params = params_of(config, precision)
     lower, width = nlo_box(float(r64[0]), float(r64[-1]))
@@ -178,6 +204,28 @@ def _evolve_rows(
     box = _native.box(lower, width)
     ws = workspace(device, points)
     lib = _native.load()
+    if config.KINEMATICAL_CONSTRAINT:
+        before = 0 if history_N is None else history_N.shape[0]
+        if y_all is None or len(y_all) != before + steps + 1:
+            raise ValueError("kinematical evolution requires the rapidities of every row")
+        table = torch.empty((before + steps + 1, points), dtype=torch.float64, device=device)
+        if before:
+            table[:before] = history_N.to(device=device, dtype=torch.float64)
+        table[before] = N0
+        y = torch.tensor(y_all, dtype=torch.float64, device=device)
+        with torch.cuda.device(device):
+            _native.check(
+                lib.nlo_bk_evolve_history(
+                    params, r64.data_ptr(), points, y.data_ptr(), before, steps, float(config.DE_SOLVER_STEP),
+                    _native.STEPPERS[config.stepper], dirs, int(config.MCINTPOINTS), box, table.data_ptr(),
+                    status.data_ptr(), ws.data_ptr(), ws.numel(), _native.stream_handle(device),
+                )
+            )
+        if int(status.item()) != 0:
+            raise FloatingPointError("non-finite BK amplitude during the rapidity evolution")
+        return table[before:]
+    table = torch.empty((steps + 1, points), dtype=torch.float64, device=device)
+    table[0] = N0
     with torch.cuda.device(device):
         _native.check(
             lib.nlo_bk_evolve(
@@ -216,7 +264,7 @@ def solve_bk(
     r64 = r_host.to(device, non_blocking=True)
     N0 = N_host.to(device, non_blocking=True)
     ys = _steps_to(0.0, maxy, config.DE_SOLVER_STEP)
-    table = _evolve_rows(N0, r64, len(ys), config, seed, precision_of(config, dtype))
+    table = _evolve_rows(N0, r64, len(ys), config, seed, precision_of(config, dtype), y_all=[0.0, *ys])
     y = torch.tensor([0.0, *ys], dtype=dtype, device=device)
     return DipoleTable(r=r64.to(dtype), y=y, N=table.to(dtype), x0=initial_condition.x0)
 
@@ -235,8 +283,10 @@ def evolve_table(
     r64 = table.r.to(torch.float64)
     start = float(table.y[-1].item())
     ys = _steps_to(start, maxy, config.DE_SOLVER_STEP)
+    history = table.N[:-1] if config.KINEMATICAL_CONSTRAINT else None
     rows = _evolve_rows(table.N[-1].to(torch.float64), r64, len(ys), config, seed,
-                        precision_of(config, table.r.dtype))
+                        precision_of(config, table.r.dtype), history_N=history,
+                        y_all=[float(v) for v in table.y.double().tolist()] + list(ys))
     y = torch.cat((table.y, torch.tensor(ys, dtype=table.y.dtype, device=device)))
     N = torch.cat((table.N, rows[1:].to(table.N.dtype)), dim=0)
     return DipoleTable(r=table.r, y=y, N=N, x0=table.x0)
@@ -268,7 +318,9 @@ def compute_dndy(
     device = _cuda_device(device)
     r64 = _r_grid(config, device=device, dtype=torch.float64)
     N = initial_condition.dipole_amplitude(r64).to(torch.float64)
-    _, K1, K2_Kf = rhs(N, r64, config, seed=seed, precision=precision_of(config, dtype))
+    # the history of the initial rapidity alone (bk/evolution.py:76-79)
+    history = (torch.zeros(1, dtype=torch.float64, device=device), N.unsqueeze(0))
+    _, K1, K2_Kf = rhs(N, r64, config, seed=seed, precision=precision_of(config, dtype), history=history)
     keep = (torch.arange(r64.numel(), device=device) > 0) & (N <= 0.99999)
     return DNDYResult(r=r64[keep].to(dtype), K1=K1[keep].to(dtype), K2_Kf=K2_Kf[keep].to(dtype),
                       N=N[keep].to(dtype))

@@ -102,10 +102,10 @@ SobolDirsArg to_arg(const nlo_sobol_dirs* d)
 size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
 
 // Workspace layout of one right-hand-side evaluation.
-size_t rhs_bytes(int points, size_t* offsets /*[7] or NULL*/)
+size_t rhs_bytes(int points, size_t* offsets /*[8] or NULL*/)
 {
     size_t o = 0;
-    size_t off[7];
+    size_t off[8];
     off[0] = o; o = align_up(o + sizeof(double) * spline_doubles(points));
     off[1] = o; o = align_up(o + sizeof(int32_t) * (size_t)points);
     off[2] = o; o = align_up(o + sizeof(int32_t) * 4);
@@ -113,13 +113,14 @@ size_t rhs_bytes(int points, size_t* offsets /*[7] or NULL*/)
     off[4] = o; o = align_up(o + sizeof(double) * 3 * (size_t)points);
     off[5] = o; o = align_up(o + sizeof(double) * 3 * (size_t)points * (size_t)k2kf_max_blocks());
     off[6] = o; o = align_up(o + sizeof(double) * 2 * (size_t)points);
+    off[7] = o; o = align_up(o + sizeof(double) * kc_weights_doubles(points));
     if (offsets) std::memcpy(offsets, off, sizeof(off));
     return o;
 }
 
 RhsBuffers carve(void* ws, int points)
 {
-    size_t off[7];
+    size_t off[8];
     rhs_bytes(points, off);
     char* base = static_cast<char*>(ws);
     RhsBuffers b;
@@ -130,21 +131,32 @@ RhsBuffers carve(void* ws, int points)
     b.k2kf = reinterpret_cast<double*>(base + off[4]);
     b.partial = reinterpret_cast<double*>(base + off[5]);
     b.factor = reinterpret_cast<double*>(base + off[6]);
+    b.kc = reinterpret_cast<double*>(base + off[7]);
     b.k2kf_blocks = k2kf_max_blocks();
     return b;
 }
 
 int run_rhs(const nlo_bk_params& p, const double* r, const double* N, int points, const SobolDirsArg& dirs,
             uint64_t samples, const nlo_bk_box& box, double* dndy, double* k1_out, double* k2kf_out,
-            const RhsBuffers& b, bool factor_ready, cudaStream_t stream, int shard = 0, int shards = 1)
+            const RhsBuffers& b, bool factor_ready, cudaStream_t stream, int shard = 0, int shards = 1,
+            const double* hist_y = nullptr, const double* hist_N = nullptr, int rows = 0)
 {
     cudaError_t e;
+    K1History history;
+    if (p.kinematical_constraint) {
+        if ((e = launch_kc_weights(r, points, b.kc, stream)) != cudaSuccess) return cuda_fail(e, "kc weights");
+        history.N = hist_N;
+        history.y = hist_y;
+        history.weights = b.kc;
+        history.rows = rows;
+        history.on = true;
+    }
     if ((e = launch_splines(r, N, points, p.force_positive, b.factor, factor_ready ? 0 : 1, b.spline, stream)) !=
         cudaSuccess)
         return cuda_fail(e, "splines");
     if ((e = launch_active(N, points, shard, shards, b.active, b.count, stream)) != cudaSuccess)
         return cuda_fail(e, "active");
-    if ((e = launch_k1(p, r, points, b.spline, b.active, b.count, b.k1, stream)) != cudaSuccess)
+    if ((e = launch_k1(p, r, points, b.spline, b.active, b.count, b.k1, stream, history)) != cudaSuccess)
         return cuda_fail(e, "k1");
     // orders without NLO kernels (Order.has_nlo_kernels, bk/config.py:44-50) take no K2 + Kf:
     // zero samples clear the sums and launch nothing
@@ -261,6 +273,9 @@ int nlo_bk_k1(const nlo_bk_params* params, const double* r, int32_t points, cons
 {
     std::string why;
     if (!check_params(params, why)) return fail(NLO_ERR_INVALID, why);
+    if (params->kinematical_constraint)
+        return fail(NLO_ERR_INVALID, "the kinematical constraint reads the amplitude history: use nlo_bk_rhs_history "
+                                     "or nlo_bk_evolve_history");
     if (points < 3 || points > 4096) return fail(NLO_ERR_INVALID, "points must be 3..4096");
     if (!r || !spline || !active || !count || !out) return fail(NLO_ERR_INVALID, "NULL buffer");
     cudaError_t e = launch_k1(*params, r, points, spline, active, count, out, (cudaStream_t)stream);
@@ -306,6 +321,9 @@ int nlo_bk_rhs(const nlo_bk_params* params, const double* r, const double* N, in
 {
     std::string why;
     if (!check_params(params, why)) return fail(NLO_ERR_INVALID, why);
+    if (params->kinematical_constraint)
+        return fail(NLO_ERR_INVALID, "the kinematical constraint reads the amplitude history: use nlo_bk_rhs_history "
+                                     "or nlo_bk_evolve_history");
     if (!check_dirs(dirs, 4, why)) return fail(NLO_ERR_INVALID, why);
     if (points < 3 || points > 4096) return fail(NLO_ERR_INVALID, "points must be 3..4096");
     if (!r || !N || !dndy || !box) return fail(NLO_ERR_INVALID, "NULL buffer");
@@ -323,6 +341,9 @@ int nlo_bk_rhs_shard(const nlo_bk_params* params, const double* r, const double*
 {
     std::string why;
     if (!check_params(params, why)) return fail(NLO_ERR_INVALID, why);
+    if (params->kinematical_constraint)
+        return fail(NLO_ERR_INVALID, "the kinematical constraint reads the amplitude history: use nlo_bk_rhs_history "
+                                     "or nlo_bk_evolve_history");
     if (!check_dirs(dirs, 4, why)) return fail(NLO_ERR_INVALID, why);
     if (shards < 1 || shard < 0 || shard >= shards) return fail(NLO_ERR_INVALID, "shard must lie in [0, shards)");
     if (points < 3 || points > 4096) return fail(NLO_ERR_INVALID, "points must be 3..4096");
@@ -347,18 +368,45 @@ int nlo_bk_stage(const double* N, const double* const* k, const double* coef, in
     return e == cudaSuccess ? NLO_OK : cuda_fail(e, "stage");
 }
 
-int nlo_bk_evolve(const nlo_bk_params* params, const double* r, int32_t points, int32_t steps, double step,
-                  int32_t stepper, const nlo_sobol_dirs* dirs, int64_t samples, const nlo_bk_box* box,
-                  double* table, uint32_t* status, void* workspace, size_t workspace_bytes, void* stream)
+int nlo_bk_rhs_history(const nlo_bk_params* params, const double* r, int32_t points, const double* hist_y,
+                       const double* hist_N, int32_t rows, const nlo_sobol_dirs* dirs, int64_t samples,
+                       const nlo_bk_box* box, double* dndy, double* k1, double* k2kf, void* workspace,
+                       size_t workspace_bytes, void* stream)
 {
     std::string why;
     if (!check_params(params, why)) return fail(NLO_ERR_INVALID, why);
     if (!check_dirs(dirs, 4, why)) return fail(NLO_ERR_INVALID, why);
     if (points < 3 || points > 4096) return fail(NLO_ERR_INVALID, "points must be 3..4096");
-    if (steps < 0) return fail(NLO_ERR_INVALID, "steps must be non-negative");
+    if (rows < 1) return fail(NLO_ERR_INVALID, "the history needs at least one row");
+    if (!r || !hist_y || !hist_N || !dndy || !box) return fail(NLO_ERR_INVALID, "NULL buffer");
+    if (samples < 0 || samples > (int64_t(1) << 30)) return fail(NLO_ERR_INVALID, "samples out of range");
+    if (!workspace || workspace_bytes < nlo_bk_rhs_workspace_bytes(points))
+        return fail(NLO_ERR_WORKSPACE, "workspace too small for nlo_bk_rhs_history");
+    const RhsBuffers b = carve(workspace, points);
+    const double* N = hist_N + (size_t)(rows - 1) * points;
+    return run_rhs(*params, r, N, points, to_arg(dirs), (uint64_t)samples, *box, dndy, k1, k2kf, b, false,
+                   (cudaStream_t)stream, 0, 1, hist_y, hist_N, rows);
+}
+
+// Rows first+1..first+steps of `table` from row `first` (the loop of _bk_steps,
+// bk/evolution.py:85-159).  y (device, may be NULL without the kinematical constraint):
+// the rapidities of all rows, read as the constraint's history.
+static int evolve_rows(const nlo_bk_params* params, const double* r, int32_t points, const double* y, int32_t first,
+                int32_t steps, double step, int32_t stepper, const nlo_sobol_dirs* dirs, int64_t samples,
+                const nlo_bk_box* box, double* table, uint32_t* status, void* workspace, size_t workspace_bytes,
+                void* stream)
+{
+    std::string why;
+    if (!check_params(params, why)) return fail(NLO_ERR_INVALID, why);
+    if (!check_dirs(dirs, 4, why)) return fail(NLO_ERR_INVALID, why);
+    if (points < 3 || points > 4096) return fail(NLO_ERR_INVALID, "points must be 3..4096");
+    if (steps < 0 || first < 0) return fail(NLO_ERR_INVALID, "steps and first must be non-negative");
     if (!(step > 0) || !std::isfinite(step)) return fail(NLO_ERR_INVALID, "step must be positive");
     if (stepper != NLO_STEPPER_EULER && stepper != NLO_STEPPER_RK3 && stepper != NLO_STEPPER_RK4)
         return fail(NLO_ERR_INVALID, "unknown stepper");
+    if (params->kinematical_constraint && stepper != NLO_STEPPER_EULER)
+        return fail(NLO_ERR_INVALID, "the kinematical constraint requires the Euler stepper");
+    if (params->kinematical_constraint && !y) return fail(NLO_ERR_INVALID, "the kinematical constraint needs y");
     if (!r || !table || !status || !box) return fail(NLO_ERR_INVALID, "NULL buffer");
     if (samples < 0 || samples > (int64_t(1) << 30)) return fail(NLO_ERR_INVALID, "samples out of range");
     if (!workspace || workspace_bytes < nlo_bk_rhs_workspace_bytes(points))
@@ -372,15 +420,15 @@ int nlo_bk_evolve(const nlo_bk_params* params, const double* r, int32_t points, 
     cudaError_t e = cudaMemsetAsync(status, 0, sizeof(uint32_t), s);
     if (e != cudaSuccess) return cuda_fail(e, "status reset");
     const int clamp = params->force_positive ? 1 : 0;
-    for (int it = 0; it < steps; ++it) {
+    for (int it = first; it < first + steps; ++it) {
         const double* N = table + (size_t)it * points;
         double* next = table + (size_t)(it + 1) * points;
         int rc;
         // the spline factorisation depends on the grid only: form it on the first stage
-        bool factor_ready = it > 0;
+        bool factor_ready = it > first;
         auto f = [&](const double* in, double* out) {
             const int code = run_rhs(*params, r, in, points, dirs_arg, (uint64_t)samples, *box, out, nullptr,
-                                     nullptr, b, factor_ready, s);
+                                     nullptr, b, factor_ready, s, 0, 1, y, table, it + 1);
             factor_ready = true;
             return code;
         };
@@ -420,6 +468,27 @@ int nlo_bk_evolve(const nlo_bk_params* params, const double* r, int32_t points, 
         }
     }
     return NLO_OK;
+}
+
+int nlo_bk_evolve(const nlo_bk_params* params, const double* r, int32_t points, int32_t steps, double step,
+                  int32_t stepper, const nlo_sobol_dirs* dirs, int64_t samples, const nlo_bk_box* box,
+                  double* table, uint32_t* status, void* workspace, size_t workspace_bytes, void* stream)
+{
+    if (params && params->kinematical_constraint)
+        return fail(NLO_ERR_INVALID, "the kinematical constraint reads the amplitude history: use "
+                                     "nlo_bk_evolve_history");
+    return evolve_rows(params, r, points, nullptr, 0, steps, step, stepper, dirs, samples, box, table, status,
+                       workspace, workspace_bytes, stream);
+}
+
+int nlo_bk_evolve_history(const nlo_bk_params* params, const double* r, int32_t points, const double* y,
+                          int32_t first, int32_t steps, double step, int32_t stepper, const nlo_sobol_dirs* dirs,
+                          int64_t samples, const nlo_bk_box* box, double* table, uint32_t* status, void* workspace,
+                          size_t workspace_bytes, void* stream)
+{
+    if (!y) return fail(NLO_ERR_INVALID, "NULL buffer");
+    return evolve_rows(params, r, points, y, first, steps, step, stepper, dirs, samples, box, table, status,
+                       workspace, workspace_bytes, stream);
 }
 
 }  // extern "C"

@@ -33,6 +33,7 @@ struct RhsBuffers {
     double* k2kf;     // [points][3]
     double* partial;  // [k2kf_blocks][points][3]
     double* factor;   // [2][points] spline factorisation (grid only)
+    double* kc;       // kc_weights_doubles(points): kinematical-constraint window weights
     int k2kf_blocks;
 };
 
@@ -53,8 +54,23 @@ cudaError_t launch_active(const double* N, int n, int shard, int shards, int32_t
                           cudaStream_t stream);
 cudaError_t launch_sobol(const SobolDirsArg& dirs, uint64_t offset, uint64_t n, int precision, void* out,
                          cudaStream_t stream);
+// Amplitude history of the kinematical constraint (bk/derivatives.py:469-487, 712-758):
+// rows N[rows][points] at rapidities y[rows], the last row the current amplitude, and
+// the per-interval weights of the 6-point natural splines in r (kc_weights_doubles).
+struct K1History {
+    const double* N = nullptr;
+    const double* y = nullptr;
+    const double* weights = nullptr;
+    int rows = 0;
+    bool on = false;
+};
+constexpr int kKcStride = 14;  // per r interval: start, local interval, 2 x 6 weights
+inline size_t kc_weights_doubles(int points) { return (size_t)(points - 1) * kKcStride; }
+cudaError_t launch_kc_weights(const double* r, int points, double* weights, cudaStream_t stream);
+
 cudaError_t launch_k1(const nlo_bk_params& p, const double* r, int points, const double* spline,
-                      const int32_t* active, const int32_t* count, double* out, cudaStream_t stream);
+                      const int32_t* active, const int32_t* count, double* out, cudaStream_t stream,
+                      const K1History& history = K1History());
 cudaError_t launch_k2kf(const nlo_bk_params& p, const double* r, int points, const double* spline,
                         const int32_t* active, const int32_t* count, const SobolDirsArg& dirs, uint64_t offset,
                         uint64_t samples, const nlo_bk_box& box, double* out, double* partial, int max_blocks,

@@ -12,6 +12,7 @@
 // dipole N_Y - N_r cancels), which run in FP64.
 
 #include <cooperative_groups.h>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -96,12 +97,57 @@ __device__ __forceinline__ T lae_shift(const K1Z<T>& Z, T delta)
     return M<T>::log_acc(Z.sigma_c + Z.sigma * M<T>::exp_fast(delta));
 }
 
+// Kinematical constraint (bk/derivatives.py:469-487): the amplitude at distance d and the
+// shifted rapidity y' from the stored history (_interpolate_history_N, :712-758).  Rows
+// k and k+1 with y_k <= y' < y_{k+1} are each interpolated in r by the natural cubic
+// spline through the 6 grid points starting at max(i-3, 0) (i the grid interval of d;
+// d below the grid is moved to r_0 * 1.00001; a window past the grid gives 1), then
+// linearly in y'; the result is clamped to [0, 1].  The spline's second derivatives
+// are linear in the 6 values: kc_weights_kernel stores, per interval, the rows of that
+// map for the two second derivatives the interval needs.
+template <typename T>
+__device__ __forceinline__ T kc_row_value(const double* row, const double* w, T h, T dx)
+{
+    T m0 = (T)0, m1 = (T)0, vj = (T)0, vj1 = (T)0;
+    const int start = (int)w[0], j = (int)w[1];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        const T v = (T)row[start + k];
+        m0 += (T)w[2 + k] * v;
+        m1 += (T)w[8 + k] * v;
+        if (k == j) vj = v;
+        if (k == j + 1) vj1 = v;
+    }
+    const T b = (vj1 - vj) / h - h * ((T)2 * m0 + m1) / (T)6;
+    return vj + dx * (b + dx * (m0 / (T)2 + dx * (m1 - m0) / ((T)6 * h)));
+}
+
+// lx = log(d / r_parent) in the spline's coordinates (knots relative to the parent)
+template <typename T>
+__device__ __forceinline__ T kc_history_amplitude(const SplineView<T>& s, const K1History& H, const double* r_grid,
+                                                  int n, T lx, int yind, T frac)
+{
+    if (lx >= s.x[n - 1]) return (T)1;  // rind = n-1: the window runs past the grid
+    const bool below = lx < s.x[0];
+    const int i = below ? 0 : spline_interval(s, lx);
+    const double* w = H.weights + (size_t)i * kKcStride;
+    if (w[0] < 0.0) return (T)1;
+    const int node = (int)w[0] + (int)w[1];
+    const double rj = r_grid[node];
+    const T h = (T)(r_grid[node + 1] - rj);
+    const T dx = below ? (T)(rj * 1.00001 - rj) : (T)rj * M<T>::expm1(lx - s.x[node]);
+    const T lo = kc_row_value<T>(H.N + (size_t)yind * n, w, h, dx);
+    const T hi = kc_row_value<T>(H.N + (size_t)(yind + 1) * n, w, h, dx);
+    const T v = lo + frac * (hi - lo);
+    return v < (T)0 ? (T)0 : (v > (T)1 ? (T)1 : v);
+}
+
 // Kernel_lo x dipole at one (z, theta) node; sh2 = sin^2(theta/2).  The form of
 // Kernel_lo follows RC_LO (k1.py:37-94); orders without resummation stop at the bare
 // kernel (k1.py:97-98); the resummation coupling follows RESUM_RC (k1.py:100-107).
-template <typename T>
+template <typename T, bool KC>
 __device__ __forceinline__ T k1_point(const SplineView<T>& s, const K1Parent<T>& P, const K1Z<T>& Z,
-                                      const Phys<T>& ph, T sh2)
+                                      const Phys<T>& ph, T sh2, const K1History& H, const double* r_grid)
 {
     const T r = P.r, z = Z.z;
     const T Xsq = (r - z) * (r - z) + (T)4 * r * z * sh2;
@@ -153,11 +199,40 @@ __device__ __forceinline__ T k1_point(const SplineView<T>& s, const K1Parent<T>&
         lo = pref * P.alpha_r * bracket;
     }
     if (!M<T>::finite(lo)) lo = (T)0;
-    // dipole N_X + N_Y - N_r - N_X N_Y = S_r (N_Y + D_X) - D_X D_Y  (or with X and Y exchanged)
-    T NX, DX;
-    k1_amplitude(s, P, dX, NX, DX);
-    const T base = Z.NY <= NX ? Z.NY + DX : NX + Z.DY;
-    const T dipole = P.Sr * base - DX * Z.DY;
+    T dipole;
+    // kinematical constraint: where min(X, Y) > r the daughters are taken at the shifted
+    // rapidity y - log(min(X^2, Y^2)/r^2) from the history (zero when it is negative);
+    // elsewhere the shift vanishes and the current amplitude is used
+    const T dmin = M<T>::fmin(dX, Z.dY);
+    if (KC && dmin > (T)0) {
+        const double rapidity = H.y[H.rows - 1];
+        const double shifted = rapidity - (double)((T)2 * dmin);
+        if (shifted < 0.0) return (T)0;
+        int lo = 0, hi = H.rows;  // yind = searchsorted(y, shifted, right) - 1
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (H.y[mid] <= shifted) lo = mid + 1; else hi = mid;
+        }
+        const int yind = lo - 1 < 0 ? 0 : lo - 1;
+        if (yind >= H.rows - 1) {
+            T NX, DX;  // at the current rapidity: the current amplitude
+            k1_amplitude(s, P, dX, NX, DX);
+            const T base = Z.NY <= NX ? Z.NY + DX : NX + Z.DY;
+            dipole = P.Sr * base - DX * Z.DY;
+        } else {
+            const T frac = (T)((shifted - H.y[yind]) / (H.y[yind + 1] - H.y[yind]));
+            const T NXh = kc_history_amplitude<T>(s, H, r_grid, s.n, dX, yind, frac);
+            const T NYh = kc_history_amplitude<T>(s, H, r_grid, s.n, Z.dY, yind, frac);
+            // (1 - N_r) - (1 - N_X')(1 - N_Y') without forming the 1 - N
+            dipole = NXh + NYh - P.Nr - NXh * NYh;
+        }
+    } else {
+        // dipole N_X + N_Y - N_r - N_X N_Y = S_r (N_Y + D_X) - D_X D_Y  (or with X and Y exchanged)
+        T NX, DX;
+        k1_amplitude(s, P, dX, NX, DX);
+        const T base = Z.NY <= NX ? Z.NY + DX : NX + Z.DY;
+        dipole = P.Sr * base - DX * Z.DY;
+    }
     if (!ph.resum) {
         const T bare = lo * dipole;
         return M<T>::finite(bare) ? bare : (T)0;
@@ -218,10 +293,12 @@ struct K1Consts {
     double aw[24];   // w_j pi v_j
 };
 
-// TF: arithmetic of the regular intervals (float in the mixed build).
-template <typename TF>
+// TF: arithmetic of the regular intervals (float in the mixed build); KC: the
+// kinematical constraint (a separate instantiation keeps the history code out of the
+// production kernel's registers).
+template <typename TF, bool KC>
 __global__ void __cluster_dims__(1, kK1Split, 1) __launch_bounds__(kK1Threads)
-    k1_kernel(Phys<TF> phf, Phys<double> phd, K1Consts consts,
+    k1_kernel(Phys<TF> phf, Phys<double> phd, K1Consts consts, K1History history,
                                                         const double* __restrict__ r_grid, int n,
                                                         const double* __restrict__ spline,
                                                         const int32_t* __restrict__ active,
@@ -310,13 +387,14 @@ __global__ void __cluster_dims__(1, kK1Split, 1) __launch_bounds__(kK1Threads)
     for (int e = threadIdx.x; e < k_count * 24; e += blockDim.x) {
         const int L = e / 24, j = e - 24 * (e / 24);
         const double w = zw[L];
-        if (w != 0.0) total += (double)(k1_point<TF>(sf, Pf, zt[L], phf, sh2f[j]) * awf[j]) * w;
+        if (w != 0.0) total += (double)(k1_point<TF, KC>(sf, Pf, zt[L], phf, sh2f[j], history, r_grid) * awf[j]) * w;
     }
     // phase 3: FP64 evaluations of the panel nodes this CTA owns
     for (int e = threadIdx.x; e < 16 * 24; e += blockDim.x) {
         const int idx = e / 24, j = e - 24 * (e / 24);
         const double w = zdw[idx];
-        if (w != 0.0) total += k1_point<double>(sd, Pd, zd[idx], phd, consts.sh2[j]) * consts.aw[j] * w;
+        if (w != 0.0)
+            total += k1_point<double, KC>(sd, Pd, zd[idx], phd, consts.sh2[j], history, r_grid) * consts.aw[j] * w;
     }
     // deterministic block reduction, then the cluster's partials in rank order
     __shared__ double cta_total;
@@ -338,10 +416,60 @@ __global__ void __cluster_dims__(1, kK1Split, 1) __launch_bounds__(kK1Threads)
     cluster.sync();  // keep every CTA's shared memory alive until rank 0 has read it
 }
 
+// Per r-grid interval i: the window start max(i-3, 0) (-1 when the 6-point window runs
+// past the grid), the local interval, and the rows of the linear maps y -> M_j, M_{j+1}
+// of the natural spline through the window (one Thomas solve per unit vector, the
+// tridiagonal system of numerics/interpolation.py:13-50).
+__global__ void kc_weights_kernel(const double* __restrict__ r, int n, double* __restrict__ weights)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    double* w = weights + (size_t)i * kKcStride;
+    const int start = i - 3 < 0 ? 0 : i - 3;
+    for (int k = 0; k < kKcStride; ++k) w[k] = 0.0;
+    if (start + 6 > n) {
+        w[0] = -1.0;
+        return;
+    }
+    const int j = i - start;
+    w[0] = start;
+    w[1] = j;
+    double h[5];
+    for (int k = 0; k < 5; ++k) h[k] = r[start + k + 1] - r[start + k];
+    for (int e = 0; e < 6; ++e) {
+        // right-hand side 6 ((y2-y1)/h1 - (y1-y0)/h0) of unit vector e, interior rows 1..4
+        double rhs[4], cp[4], dp[4], M[6];
+        for (int q = 0; q < 4; ++q) {
+            const double y0 = e == q ? 1.0 : 0.0, y1 = e == q + 1 ? 1.0 : 0.0, y2 = e == q + 2 ? 1.0 : 0.0;
+            rhs[q] = 6.0 * ((y2 - y1) / h[q + 1] - (y1 - y0) / h[q]);
+        }
+        for (int q = 0; q < 4; ++q) {
+            const double diag = 2.0 * (h[q] + h[q + 1]);
+            const double sub = q > 0 ? h[q] : 0.0;
+            const double den = diag - (q > 0 ? sub * cp[q - 1] : 0.0);
+            cp[q] = q < 3 ? h[q + 1] / den : 0.0;
+            dp[q] = (rhs[q] - (q > 0 ? sub * dp[q - 1] : 0.0)) / den;
+        }
+        M[0] = 0.0;
+        M[5] = 0.0;
+        M[4] = dp[3];
+        for (int q = 2; q >= 0; --q) M[q + 1] = dp[q] - cp[q] * M[q + 2];
+        w[2 + e] = M[j];
+        w[8 + e] = M[j + 1];
+    }
+}
+
 }  // namespace
 
+cudaError_t launch_kc_weights(const double* r, int points, double* weights, cudaStream_t stream)
+{
+    kc_weights_kernel<<<(points + 127) / 128, 128, 0, stream>>>(r, points, weights);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_k1(const nlo_bk_params& p, const double* r, int points, const double* spline,
-                      const int32_t* active, const int32_t* count, double* out, cudaStream_t stream)
+                      const int32_t* active, const int32_t* count, double* out, cudaStream_t stream,
+                      const K1History& history)
 {
     K1Consts consts;
     consts.rule = k1_rule();
@@ -362,20 +490,22 @@ cudaError_t launch_k1(const nlo_bk_params& p, const double* r, int points, const
                a16(tf * 4 * (size_t)(points - 1)) + a16((tf == 4 ? sizeof(K1Z<float>) : sizeof(K1Z<double>)) * per_split) +
                a16(8 * per_split) + a16(sizeof(K1Z<double>) * 16) + a16(8 * 16);
     };
-    if (p.precision == NLO_PRECISION_FP64) {
-        const size_t smem = smem_for(8);
-        e = raise_dynamic_smem((const void*)k1_kernel<double>, smem);
-        if (e != cudaSuccess) return e;
-        k1_kernel<double><<<dim3(points, kK1Split), kK1Threads, smem, stream>>>(phd, phd, consts, r, points, spline,
-                                                                                active, count, out);
-    } else {
-        const size_t smem = smem_for(4);
-        e = raise_dynamic_smem((const void*)k1_kernel<float>, smem);
-        if (e != cudaSuccess) return e;
-        k1_kernel<float><<<dim3(points, kK1Split), kK1Threads, smem, stream>>>(make_phys<float>(p), phd, consts, r,
-                                                                               points, spline, active, count, out);
-    }
-    return cudaGetLastError();
+    auto launch = [&](auto tag, auto kc) -> cudaError_t {
+        using TF = decltype(tag);
+        constexpr bool KC = decltype(kc)::value;
+        const size_t smem = smem_for(sizeof(TF));
+        const void* fn = (const void*)k1_kernel<TF, KC>;
+        cudaError_t err = raise_dynamic_smem(fn, smem);
+        if (err != cudaSuccess) return err;
+        k1_kernel<TF, KC><<<dim3(points, kK1Split), kK1Threads, smem, stream>>>(make_phys<TF>(p), phd, consts, history,
+                                                                               r, points, spline, active, count, out);
+        return cudaGetLastError();
+    };
+    using On = std::true_type;
+    using Off = std::false_type;
+    if (p.precision == NLO_PRECISION_FP64)
+        return history.on ? launch(double(), On()) : launch(double(), Off());
+    return history.on ? launch(float(), On()) : launch(float(), Off());
 }
 
 }  // namespace nlo

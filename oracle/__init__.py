@@ -96,6 +96,10 @@ def lib() -> ctypes.CDLL:
         handle.or_bessel_i1.restype = D
         handle.or_bessel_i1.argtypes = [D]
         handle.or_k1_fixed_many.argtypes = [DP, I, P(_Spline), P(Physics), DP, DP, DP, DP, DP]
+        handle.or_k1_fixed_history_many.argtypes = [DP, I, P(_Spline), P(Physics), DP, DP, DP, DP, DP, I, DP, DP, I,
+                                                    DP]
+        handle.or_k1_integrand_history.restype = D
+        handle.or_k1_integrand_history.argtypes = [D, D, D, P(_Spline), P(Physics), DP, I, DP, DP, I]
         handle.or_nlo_kernels.argtypes = [D, D, D, D, D, D, D, DP]
         handle.or_k2kf_integrand.argtypes = [D, DP, P(_Spline), P(Physics), DP]
         handle.or_k2kf_sums.argtypes = [DP, I, DP, ctypes.c_long, DP, DP, I, P(_Spline), P(Physics), DP]
@@ -216,18 +220,40 @@ def gauss_legendre(order: int) -> tuple[np.ndarray, np.ndarray]:
     return np.ascontiguousarray(x), np.ascontiguousarray(w)
 
 
-def k1_fixed(rpar: np.ndarray, nspline: Spline, phys: Physics) -> np.ndarray:
+def _history_arrays(r: np.ndarray, history) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    hy = np.ascontiguousarray(history[0], dtype=np.float64)
+    hN = np.ascontiguousarray(history[1], dtype=np.float64)
+    rg = np.ascontiguousarray(r, dtype=np.float64)
+    if hN.ndim != 2 or hN.shape != (hy.size, rg.size):
+        raise ValueError("history must be (y [rows], N [rows, R])")
+    return rg, hy, hN
+
+
+def k1_fixed(rpar: np.ndarray, nspline: Spline, phys: Physics, history=None, r_grid=None) -> np.ndarray:
+    """The fixed K1 rule at the parents rpar; with ``history`` = (y [rows], N [rows, R]) on
+    ``r_grid``, the kinematical constraint's K1 (the last row the current amplitude)."""
     rpar = np.ascontiguousarray(rpar, dtype=np.float64)
     x8, w8 = gauss_legendre(8)
     x24, w24 = gauss_legendre(24)
     out = np.empty(rpar.size)
-    lib().or_k1_fixed_many(_dp(rpar), rpar.size, ctypes.byref(nspline.struct()), ctypes.byref(phys),
-                           _dp(x8), _dp(w8), _dp(x24), _dp(w24), _dp(out))
+    if history is None:
+        lib().or_k1_fixed_many(_dp(rpar), rpar.size, ctypes.byref(nspline.struct()), ctypes.byref(phys),
+                               _dp(x8), _dp(w8), _dp(x24), _dp(w24), _dp(out))
+        return out
+    rg, hy, hN = _history_arrays(r_grid, history)
+    lib().or_k1_fixed_history_many(_dp(rpar), rpar.size, ctypes.byref(nspline.struct()), ctypes.byref(phys),
+                                   _dp(x8), _dp(w8), _dp(x24), _dp(w24), _dp(rg), rg.size, _dp(hy), _dp(hN),
+                                   hy.size, _dp(out))
     return out
 
 
-def k1_integrand(r: float, z: float, theta: float, nspline: Spline, phys: Physics) -> float:
-    return lib().or_k1_integrand(r, z, theta, ctypes.byref(nspline.struct()), ctypes.byref(phys))
+def k1_integrand(r: float, z: float, theta: float, nspline: Spline, phys: Physics, history=None,
+                 r_grid=None) -> float:
+    if history is None:
+        return lib().or_k1_integrand(r, z, theta, ctypes.byref(nspline.struct()), ctypes.byref(phys))
+    rg, hy, hN = _history_arrays(r_grid, history)
+    return lib().or_k1_integrand_history(r, z, theta, ctypes.byref(nspline.struct()), ctypes.byref(phys), _dp(rg),
+                                         rg.size, _dp(hy), _dp(hN), hy.size)
 
 
 def k2kf_integrand(r: float, x: np.ndarray, sspline: Spline, phys: Physics) -> tuple[float, float]:
@@ -340,9 +366,10 @@ class Derivative:
 
 
 def derivative(N: np.ndarray, r: np.ndarray, phys: Physics, points: np.ndarray, map_f32: bool,
-               force_positive: bool = True) -> Derivative:
+               force_positive: bool = True, history=None) -> Derivative:
     """dN/dY = K1 + (K2+Kf) at active parents (index > 0 and N <= 0.99999), else 0;
-    non-finite values become 0 (bk/evolution.py:329-351, 501)."""
+    non-finite values become 0 (bk/evolution.py:329-351, 501).  ``history`` = (y, N rows)
+    gives K1 the kinematical constraint (its last row is N)."""
 
     nspl = loglog_spline(r, N, 0, force_positive)
     sspl = loglog_spline(r, N, 1, force_positive)
@@ -352,7 +379,7 @@ def derivative(N: np.ndarray, r: np.ndarray, phys: Physics, points: np.ndarray, 
     Kf = np.zeros_like(N)
     sq = np.zeros_like(N)
     if active.size:
-        K1[active] = k1_fixed(r[active], nspl, phys)
+        K1[active] = k1_fixed(r[active], nspl, phys, history=history, r_grid=r)
         if has_nlo_kernels(phys):  # LO orders take no K2 + Kf (bk/evolution.py:391, 473)
             lower, width = nlo_box(r)
             sums = k2kf_sums(r[active], points, lower, width, map_f32, sspl, phys)
@@ -366,16 +393,20 @@ def derivative(N: np.ndarray, r: np.ndarray, phys: Physics, points: np.ndarray, 
 
 
 def evolve(N0: np.ndarray, r: np.ndarray, phys: Physics, points: np.ndarray, map_f32: bool, step: float,
-           maxy: float, stepper: str = "rk4", force_positive: bool = True):
-    """Rapidity stepping (bk/evolution.py:85-159); returns (y[steps+1], N[steps+1, R])."""
+           maxy: float, stepper: str = "rk4", force_positive: bool = True, kinematical_constraint: bool = False):
+    """Rapidity stepping (bk/evolution.py:85-159); returns (y[steps+1], N[steps+1, R]).
+    With the kinematical constraint (Euler only) each step's K1 reads the rows so far."""
 
     ys = [0.0]
     Ns = [np.array(N0, dtype=np.float64)]
     N = Ns[0].copy()
     y = 0.0
+    if kinematical_constraint and stepper != "euler":
+        raise ValueError("the kinematical constraint requires the Euler stepper")
 
     def f(state):
-        return derivative(state, r, phys, points, map_f32, force_positive).dNdy
+        history = (np.array(ys), np.stack(Ns)) if kinematical_constraint else None
+        return derivative(state, r, phys, points, map_f32, force_positive, history=history).dNdy
 
     while True:
         h = step

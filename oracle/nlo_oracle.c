@@ -17,6 +17,9 @@
  *                         RC_LO and RESUM_RC; production NLO_RESUM_DLOG_SLOG,
  *                         BALITSKY_LO, RESUM_RC_SMALLEST)
  *   K1 integrand          bk/derivatives.py:434-468     (_lo_integrand)
+ *   kinematical constr.   bk/derivatives.py:469-487, 712-758 (shifted rapidity,
+ *                         6-point natural splines of the history rows in r,
+ *                         linear in y)
  *   K1 fixed rule         custom_kernels/bk/k1/kernel.cu:2040-2092
  *                         (8 GL nodes in log z per r-grid interval x 24 GL nodes
  *                          in v with theta = pi v^2)
@@ -448,6 +451,122 @@ static double k1_integrand_at(double r, int knot, double z, double theta, const 
     if (Xsq < 1e-40 || z < 1e-20 || r < 1e-20) return 0.0;
     const double value = kernel_lo_value(r, z, theta, p) * k1_dipole(nspl, knot, sqrt(Xsq), z);
     return isfinite(value) ? value : 0.0;
+}
+
+/* Amplitude history for the kinematical constraint: rows hN[rows][n] at rapidities hy[rows]
+ * on the grid rg[n] (the last row the current amplitude). */
+typedef struct or_history {
+    const double* rg;
+    const double* hy;
+    const double* hN;
+    int n, rows;
+} or_history;
+
+/* _interpolate_history_N (bk/derivatives.py:712-758) at one distance d and rapidity yv,
+ * for yind < rows - 1: natural spline through the 6 grid points from max(rind-3, 0)
+ * of rows yind and yind+1 (1 when that window runs past the grid), linear in y. */
+static double history_amplitude(const or_history* H, double d, double yv, int yind)
+{
+    int lo = 0, hi = H->n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (d >= H->rg[mid]) lo = mid + 1; else hi = mid;
+    }
+    const int rind = lo - 1;
+    const int start = rind - 3 < 0 ? 0 : rind - 3;
+    if (start + 6 > H->n) return 1.0;
+    const double* x = H->rg + start;
+    double ev = d;
+    if (ev < x[0]) ev = x[0] * 1.00001;
+    if (ev > x[5]) ev = x[5] * 0.999999;
+    int j = 0;
+    while (j < 4 && ev >= x[j + 1]) ++j;
+    double v[2];
+    for (int k = 0; k < 2; ++k) {
+        double a[5], b[5], c[5], dd[5];
+        or_natural_spline(x, H->hN + (size_t)(yind + k) * H->n + start, 6, a, b, c, dd);
+        const double dx = ev - x[j];
+        v[k] = a[j] + dx * (b[j] + dx * (c[j] + dx * dd[j]));
+    }
+    const double frac = (yv - H->hy[yind]) / (H->hy[yind + 1] - H->hy[yind]);
+    const double out = v[0] + frac * (v[1] - v[0]);
+    return out < 0.0 ? 0.0 : (out > 1.0 ? 1.0 : out);
+}
+
+/* _lo_integrand with KINEMATICAL_CONSTRAINT (bk/derivatives.py:469-487): where
+ * min(X, Y) > r the daughters are taken at y - log(min(X^2, Y^2)/r^2) from the history
+ * (no contribution when that is negative); the dipole (1 - N_r) - (1 - N_X')(1 - N_Y')
+ * is formed as N_X' + N_Y' - N_r - N_X' N_Y'. */
+static double k1_integrand_history(double r, int knot, double z, double theta, const or_spline* nspl,
+                                   const or_physics* p, const or_history* H)
+{
+    const double sh = sin(0.5 * theta);
+    const double Xsq = (r - z) * (r - z) + 4.0 * r * z * sh * sh;
+    if (Xsq < 1e-40 || z < 1e-20 || r < 1e-20) return 0.0;
+    const double X = sqrt(Xsq);
+    const double rapidity = H->hy[H->rows - 1];
+    const double dmin = fmin(0.5 * log(Xsq), log(z)) - log(r);
+    double dipole;
+    if (dmin > 0.0) {
+        const double shifted = rapidity - 2.0 * dmin;
+        if (shifted < 0.0) return 0.0;
+        int lo = 0, hi = H->rows;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (H->hy[mid] <= shifted) lo = mid + 1; else hi = mid;
+        }
+        const int yind = lo - 1 < 0 ? 0 : lo - 1;
+        if (yind >= H->rows - 1) {
+            dipole = k1_dipole(nspl, knot, X, z);
+        } else {
+            const double NX = history_amplitude(H, X, shifted, yind);
+            const double NY = history_amplitude(H, z, shifted, yind);
+            const double Nr = or_n_from_nspline(nspl, r);
+            dipole = NX + NY - Nr - NX * NY;
+        }
+    } else {
+        dipole = k1_dipole(nspl, knot, X, z);
+    }
+    const double value = kernel_lo_value(r, z, theta, p) * dipole;
+    return isfinite(value) ? value : 0.0;
+}
+
+double or_k1_integrand_history(double r, double z, double theta, const or_spline* nspl, const or_physics* p,
+                               const double* rg, int n, const double* hy, const double* hN, int rows)
+{
+    const or_history H = {rg, hy, hN, n, rows};
+    return k1_integrand_history(r, knot_index(nspl, r), z, theta, nspl, p, &H);
+}
+
+/* The fixed K1 rule (k1/kernel.cu:2040-2092 nodes) with the kinematical constraint,
+ * for many parents. */
+void or_k1_fixed_history_many(const double* rpar, int nr, const or_spline* nspl, const or_physics* p,
+                              const double* x8, const double* w8, const double* x24, const double* w24,
+                              const double* rg, int n, const double* hy, const double* hN, int rows, double* out)
+{
+    const or_history H = {rg, hy, hN, n, rows};
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int q = 0; q < nr; ++q) {
+        const double r = rpar[q];
+        const int knot = knot_index(nspl, r);
+        double total = 0.0;
+        for (int i = 0; i < nspl->n - 1; ++i) {
+            const double lower = nspl->x[i], upper = nspl->x[i + 1];
+            const double center = 0.5 * (lower + upper), hw = 0.5 * (upper - lower);
+            for (int k = 0; k < 8; ++k) {
+                const double lz = center + hw * x8[k];
+                const double z = exp(lz);
+                const double rw = hw * w8[k];
+                for (int j = 0; j < 24; ++j) {
+                    const double v = 0.5 * (x24[j] + 1.0);
+                    const double theta = OR_PI * v * v;
+                    const double aw = w24[j] * OR_PI * v;
+                    total += k1_integrand_history(r, knot, z, theta, nspl, p, &H) * (2.0 * z * z) * rw * aw;
+                }
+            }
+        }
+        out[q] = total;
+    }
 }
 
 double or_k1_integrand(double r, double z, double theta, const or_spline* nspl, const or_physics* p)

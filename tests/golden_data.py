@@ -36,7 +36,11 @@ def variant_config(name: str):
 
     data = bk_variants()
     names = [str(n) for n in data["names"]]
-    overrides = ast.literal_eval(str(data["overrides"][names.index(name)]))
+    kc_names = [str(n) for n in data["kc_names"]]
+    if name in names:
+        overrides = ast.literal_eval(str(data["overrides"][names.index(name)]))
+    else:
+        overrides = ast.literal_eval(str(data["kc_overrides"][kc_names.index(name)]))
     kwargs = {}
     for field, value in overrides.items():
         if isinstance(value, str):

@@ -103,3 +103,89 @@ def test_short_variant_evolution_matches_oracle(name):
     assert got.shape == ref.shape
     err = float(np.max(np.abs(got[-1] - ref[-1]) / np.maximum(np.abs(ref[-1]), 1e-300)))
     assert err <= 1e-10, f"{name}: N(Y=0.6) max relative error {err:.3e}"
+
+
+# ----------------------------------------------------------------------------- kinematical constraint
+def _kc_history(config):
+    g = bk_variants()
+    r = _r_grid(config, device="cuda", dtype=torch.float64)
+    assert np.allclose(r.cpu().numpy(), g["r"], rtol=1e-15)
+    return r, g["kc_history_y"], g["kc_history_N"]
+
+
+@pytest.mark.parametrize("name", [str(n) for n in bk_variants()["kc_names"]])
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_kinematical_constraint_rhs_matches_oracle(name, precision):
+    from dataclasses import replace
+
+    config = replace(variant_config(name), MCINTPOINTS=1024)
+    r, hy, hN = _kc_history(config)
+    rn = r.cpu().numpy()
+    N = torch.tensor(hN[-1], device="cuda")
+    history = (torch.tensor(hy, device="cuda"), torch.tensor(hN, device="cuda"))
+    dndy, k1, k2kf = rhs(N, r, config, seed=0, precision=precision, history=history)
+    f32 = precision == _native.PRECISION_MIXED
+    ref = oracle.derivative(hN[-1], rn, oracle.physics(config), _sobol(1024, f32), f32, history=(hy, hN))
+    active = ref.dNdy != 0
+    assert _rel_err(k1.cpu().numpy()[active], ref.K1[active]) <= TOL[precision]
+    # dN/dY = K1 + (K2+Kf) cancels at some parents: measure its error against the parts
+    parts = np.abs(ref.K1) + np.abs(ref.K2 + ref.Kf)
+    err = np.abs(dndy.cpu().numpy() - ref.dNdy)[active] / parts[active]
+    assert float(err.max()) <= TOL[precision]
+    with pytest.raises(ValueError):
+        rhs(N, r, config, seed=0, precision=precision)  # the constraint needs the history
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_kinematical_constraint_evolution_matches_oracle(precision):
+    from dataclasses import replace
+
+    config = replace(variant_config("kc"), RPOINTS=59, MCINTPOINTS=1024, DE_SOLVER_STEP=0.2, PRECISION=precision)
+    r = _r_grid(config, device="cuda", dtype=torch.float64)
+    rn = r.cpu().numpy()
+    N0 = MV(qs0sqr=0.2).dipole_amplitude(r).cpu().numpy()
+    table = solve_bk(MV(qs0sqr=0.2), 0.8, config, device="cuda", dtype=torch.float64, seed=0)
+    f32 = precision == "mixed"
+    ys, ref = oracle.evolve(N0, rn, oracle.physics(config), _sobol(1024, f32), f32, 0.2, 0.8, stepper="euler",
+                            kinematical_constraint=True)
+    got = table.N.cpu().numpy()
+    assert got.shape == ref.shape
+    tol = 1e-4 if f32 else 1e-10
+    err = float(np.max(np.abs(got[-1] - ref[-1]) / np.maximum(np.abs(ref[-1]), 1e-300)))
+    assert err <= tol, f"N(Y=0.8) max relative error {err:.3e}"
+    # the constraint changes the evolution
+    _, plain = oracle.evolve(N0, rn, oracle.physics(replace(config, KINEMATICAL_CONSTRAINT=False)),
+                             _sobol(1024, f32), f32, 0.2, 0.8, stepper="euler")
+    assert np.max(np.abs(plain[-1] - ref[-1]) / np.maximum(np.abs(ref[-1]), 1e-300)) > 1e-3
+
+
+def test_kinematical_constraint_continuation_equals_one_run():
+    """evolve_table carries the stored rows as the constraint's history."""
+    from dataclasses import replace
+
+    from nlo_bk_optimized_b200.bk.evolution import evolve_table
+
+    config = replace(variant_config("kc"), RPOINTS=49, MCINTPOINTS=512, DE_SOLVER_STEP=0.2, PRECISION="fp64")
+    whole = solve_bk(MV(qs0sqr=0.2), 0.8, config, device="cuda", dtype=torch.float64, seed=0)
+    part = solve_bk(MV(qs0sqr=0.2), 0.4, config, device="cuda", dtype=torch.float64, seed=0)
+    resumed = evolve_table(part, 0.8, config, seed=0)
+    np.testing.assert_array_equal(resumed.y.cpu().numpy(), whole.y.cpu().numpy())
+    np.testing.assert_array_equal(resumed.N.cpu().numpy(), whole.N.cpu().numpy())
+
+
+def test_kinematical_constraint_dndy_at_the_initial_rapidity():
+    """At y = 0 the shifted rapidity is negative wherever min(X, Y) > r: only the rest of
+    the K1 integral remains (bk/evolution.py:76-79)."""
+    from dataclasses import replace
+
+    from nlo_bk_optimized_b200 import compute_dndy
+
+    config = replace(variant_config("kc"), MCINTPOINTS=512)
+    res = compute_dndy(MV(qs0sqr=0.2), config, device="cuda", dtype=torch.float64, seed=0)
+    r = _r_grid(config, device="cuda", dtype=torch.float64)
+    rn = r.cpu().numpy()
+    N0 = MV(qs0sqr=0.2).dipole_amplitude(r).cpu().numpy()
+    active = (np.arange(rn.size) > 0) & (N0 <= 0.99999)
+    ref = oracle.k1_fixed(rn[active], oracle.loglog_spline(rn, N0, 0), oracle.physics(config),
+                          history=(np.zeros(1), N0[None]), r_grid=rn)
+    assert _rel_err(res.K1.cpu().numpy(), ref) <= 1e-10

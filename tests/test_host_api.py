@@ -209,3 +209,29 @@ def test_dis_budget_split_and_seed_plan():
     assert charm.samples_per_iteration * charm.max_iterations == 1000
     assert [j.term for j in plan.qg[0]] == [TERMS["I1"], TERMS["I2N"], TERMS["I3N"]]
     assert plan.lo.kin.xbj == 1.0  # NLO: LO term at x_Bj = X0
+
+
+def test_kinematical_constraint_entry_points_validate_on_the_host():
+    """The constraint reads the amplitude history: the entry points without one refuse it,
+    and the history evolution refuses steppers other than Euler, before anything launches."""
+    import ctypes
+
+    from nlo_bk_optimized_b200 import _native
+    from nlo_bk_optimized_b200.bk.config import BKConfig
+    from nlo_bk_optimized_b200.bk.evolution import params_of
+
+    lib = _native.load()
+    config = BKConfig(KINEMATICAL_CONSTRAINT=True, EULER_METHOD=True)
+    params = params_of(config, _native.PRECISION_FP64)
+    assert params.kinematical_constraint == 1
+    dirs = _native.sobol_dirs(4, 0)
+    box = _native.box([0.0] * 4, [1.0] * 4)
+    fake = ctypes.c_void_p(16)  # never dereferenced: validation fails first
+    rc = lib.nlo_bk_evolve(params, fake, 32, 1, 0.2, _native.STEPPERS["euler"], dirs, 16, box, fake, fake, fake,
+                           1 << 30, None)
+    assert rc == 1 and b"history" in lib.nlo_last_error()
+    rc = lib.nlo_bk_rhs(params, fake, fake, 32, dirs, 16, box, fake, None, None, fake, 1 << 30, None)
+    assert rc == 1 and b"history" in lib.nlo_last_error()
+    rc = lib.nlo_bk_evolve_history(params, fake, 32, fake, 0, 1, 0.2, _native.STEPPERS["rk4"], dirs, 16, box, fake,
+                                   fake, fake, 1 << 30, None)
+    assert rc == 1 and b"Euler" in lib.nlo_last_error()

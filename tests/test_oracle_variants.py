@@ -74,3 +74,50 @@ def test_variants_change_what_they_should():
     assert not np.allclose(g["rc_nlo_parent/k2kf"], g["rc_parent/k2kf"], rtol=1e-6)
     # the RC_LO choice does not reach K2 + Kf
     np.testing.assert_array_equal(g["rc_fac/k2kf"], g["rc_parent/k2kf"])
+
+
+KC_NAMES = [str(n) for n in bk_variants()["kc_names"]]
+
+
+@pytest.mark.parametrize("name", KC_NAMES)
+def test_kinematical_constraint_integrand_and_sums(name):
+    """The kinematical constraint reads a four-row history (y = 0, 0.25, 0.5, 0.75)."""
+    g = bk_variants()
+    r = g["r"]
+    history = (g["kc_history_y"], g["kc_history_N"])
+    nspl = oracle.loglog_spline(r, g["kc_history_N"][-1], 0)
+    phys = oracle.physics(variant_config(name))
+    for row, index in enumerate(g["k1_parents"]):
+        ref = g[f"{name}/k1"][row]
+        mine = np.array([oracle.k1_integrand(float(r[index]), float(z), float(t), nspl, phys, history=history,
+                                             r_grid=r) for z, t in zip(g["z"], g["theta"])])
+        # the reference forms the dipole as (1 - N_r) - (1 - N_X')(1 - N_Y'), whose rounding is
+        # a few 1e-16 absolute, i.e. ~1e-16 |Kernel_lo| in the integrand where the dipole is
+        # small; the oracle forms N_X' + N_Y' - N_r - N_X' N_Y' (and log-spline differences)
+        kern = np.array([oracle.lo_kernel(float(r[index]), float(z), float(t), phys)
+                         for z, t in zip(g["z"], g["theta"])])
+        allowed = 1e-8 * np.abs(ref).max() + 4e-16 * np.abs(kern)
+        assert np.all(np.abs(mine - ref) <= allowed), (name, index)
+    mine = oracle.k1_fixed(r[g["k1_parents"]], nspl, phys, history=history, r_grid=r)
+    np.testing.assert_allclose(mine, g[f"{name}/k1_fixed"], rtol=1e-7, atol=0)
+
+
+def test_kinematical_constraint_fixed_rule_near_adaptive():
+    g = bk_variants()
+    r = g["r"]
+    nspl = oracle.loglog_spline(r, g["kc_history_N"][-1], 0)
+    phys = oracle.physics(variant_config("kc"))
+    fixed = oracle.k1_fixed(r[60:61], nspl, phys, history=(g["kc_history_y"], g["kc_history_N"]), r_grid=r)[0]
+    value, error = g["kc_adaptive_r60"]
+    # the adaptive reference targets 1e-3 relative accuracy (BKConfig.INTACCURACY)
+    assert abs(fixed - value) <= max(5 * error, 2e-3 * abs(value))
+
+
+def test_kinematical_constraint_changes_k1():
+    g = bk_variants()
+    r = g["r"]
+    nspl = oracle.loglog_spline(r, g["kc_history_N"][-1], 0)
+    phys = oracle.physics(variant_config("kc"))
+    with_kc = g["kc/k1_fixed"]
+    without = oracle.k1_fixed(r[g["k1_parents"]], nspl, phys)
+    assert np.all(np.abs(with_kc / without - 1) > 1e-3)

@@ -167,6 +167,16 @@ int nlo_bk_k2kf_static(const nlo_bk_params* params, const double* r, int32_t poi
                        const int32_t* active, const int32_t* count, const nlo_sobol_dirs* dirs, int64_t offset,
                        int64_t samples, const nlo_bk_box* box, double* out, void* stream);
 
+/* Tabulated initial condition (ICDataFile, bk/initial_conditions.py:38-91) on the device.
+ * nlo_ic_spline fits the natural cubic spline through n >= 3 rows (r: device double[n],
+ * strictly increasing; N: device double[n]) into spline: device double[nlo_ic_spline_doubles(n)],
+ * with the reference's FP64 operations (NaturalCubicSpline, numerics/interpolation.py:13-48,
+ * 124-149), so the coefficients equal the reference's.  nlo_ic_evaluate is
+ * ICDataFile.dipole_amplitude (:86-90) at m points: 0 below the first r, 1 above the last. */
+size_t nlo_ic_spline_doubles(int32_t n);
+int nlo_ic_spline(const double* r, const double* N, int32_t n, double* spline, void* stream);
+int nlo_ic_evaluate(const double* spline, int32_t n, const double* r, int64_t m, double* out, void* stream);
+
 /* Workspace bytes for nlo_bk_rhs / nlo_bk_evolve. */
 size_t nlo_bk_rhs_workspace_bytes(int32_t points);
 

@@ -144,6 +144,9 @@ EXPORTED = (
     "nlo_bk_evolve",
     "nlo_bk_evolve_history",
     "nlo_bk_rhs_history",
+    "nlo_ic_spline_doubles",
+    "nlo_ic_spline",
+    "nlo_ic_evaluate",
     "nlo_bk_rhs_shard",
     "nlo_bk_stage",
     "nlo_dis_table_doubles",
@@ -198,6 +201,12 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.nlo_bk_evolve_history.restype = ctypes.c_int
     lib.nlo_bk_evolve_history.argtypes = [P(BKParams), vp, i32, vp, i32, i32, d, i32, P(SobolDirs), i64, P(Box), vp,
                                           vp, vp, sz, vp]
+    lib.nlo_ic_spline_doubles.restype = sz
+    lib.nlo_ic_spline_doubles.argtypes = [i32]
+    lib.nlo_ic_spline.restype = ctypes.c_int
+    lib.nlo_ic_spline.argtypes = [vp, vp, i32, vp, vp]
+    lib.nlo_ic_evaluate.restype = ctypes.c_int
+    lib.nlo_ic_evaluate.argtypes = [vp, i32, vp, i64, vp, vp]
     lib.nlo_bk_rhs_history.restype = ctypes.c_int
     lib.nlo_bk_rhs_history.argtypes = [P(BKParams), vp, i32, vp, vp, i32, P(SobolDirs), i64, P(Box), vp, vp, vp, vp,
                                        sz, vp]

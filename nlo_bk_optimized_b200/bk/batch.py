@@ -104,14 +104,14 @@ def solve_bk_batch(initial_conditions: Sequence, maxy: float, config: BKConfig =
                    dtype: torch.dtype = torch.float32, seed: int = 0, streams: int | None = None) -> list[DipoleTable]:
     """``solve_bk`` for many initial conditions; ``samples[i]`` overrides MCINTPOINTS of set i.
     ``streams=None`` lets ``tune_streams`` choose the concurrency."""
-    from nlo_bk_optimized_b200.bk.evolution import _cuda_device, _r_grid, _steps_to, precision_of
+    from nlo_bk_optimized_b200.bk.evolution import _cuda_device, _r_grid, _steps_to, initial_row, precision_of
 
     device = _cuda_device(device)
     if not initial_conditions:
         return []
     budgets = list(samples) if samples is not None else [int(config.MCINTPOINTS)] * len(initial_conditions)
     r_host = _r_grid(config, device="cpu", dtype=torch.float64)
-    N0 = torch.stack([ic.dipole_amplitude(r_host).to(torch.float64) for ic in initial_conditions]).to(device)
+    N0 = torch.stack([initial_row(ic, r_host, device) for ic in initial_conditions])
     r = r_host.to(device)
     ys = _steps_to(0.0, maxy, config.DE_SOLVER_STEP)
     precision = precision_of(config, dtype)

@@ -112,6 +112,15 @@ def _cuda_device(device: torch.device | str) -> torch.device:
     return device
 
 
+def initial_row(initial_condition: MV | ICDataFile, r_host: torch.Tensor, device: torch.device) -> torch.Tensor:
+    """The initial amplitude row (float64) on the device: a tabulated initial condition is
+    fitted and evaluated there (nlo_ic_spline / nlo_ic_evaluate), MV is evaluated on the
+    host grid (initial_conditions.py:29-35) and copied in."""
+    if isinstance(initial_condition, ICDataFile):
+        return initial_condition.device_amplitude(r_host.to(device=device, dtype=torch.float64))
+    return initial_condition.dipole_amplitude(r_host.to(torch.float64)).to(torch.float64).to(device)
+
+
 def _steps_to(y_start: float, maxy: float, step: float) -> list[float]:
     """Rapidities after each step, as bk/evolution.py:108-159 accumulates them."""
 
@@ -257,12 +266,11 @@ def solve_bk(
     device = _cuda_device(device)
     # the grid and the initial row are formed on the host in float64 and copied in
     r_host = _r_grid(config, device="cpu", dtype=torch.float64)
-    if isinstance(initial_condition, ICDataFile):
-        N_host = initial_condition.dipole_amplitude(r_host.to(initial_condition.r.device)).to("cpu", torch.float64)
-    else:
-        N_host = initial_condition.dipole_amplitude(r_host).to(torch.float64)
     r64 = r_host.to(device, non_blocking=True)
-    N0 = N_host.to(device, non_blocking=True)
+    if isinstance(initial_condition, ICDataFile):
+        N0 = initial_condition.device_amplitude(r64)  # the tabulated IC's spline on the device
+    else:
+        N0 = initial_condition.dipole_amplitude(r_host).to(torch.float64).to(device, non_blocking=True)
     ys = _steps_to(0.0, maxy, config.DE_SOLVER_STEP)
     table = _evolve_rows(N0, r64, len(ys), config, seed, precision_of(config, dtype), y_all=[0.0, *ys])
     y = torch.tensor([0.0, *ys], dtype=dtype, device=device)
@@ -317,7 +325,10 @@ def compute_dndy(
         dtype = initial_condition.r.dtype
     device = _cuda_device(device)
     r64 = _r_grid(config, device=device, dtype=torch.float64)
-    N = initial_condition.dipole_amplitude(r64).to(torch.float64)
+    if isinstance(initial_condition, ICDataFile):
+        N = initial_condition.device_amplitude(r64)
+    else:
+        N = initial_condition.dipole_amplitude(r64).to(torch.float64)
     # the history of the initial rapidity alone (bk/evolution.py:76-79)
     history = (torch.zeros(1, dtype=torch.float64, device=device), N.unsqueeze(0))
     _, K1, K2_Kf = rhs(N, r64, config, seed=seed, precision=precision_of(config, dtype), history=history)

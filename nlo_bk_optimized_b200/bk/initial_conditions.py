@@ -1,7 +1,10 @@
 """Initial conditions (mirrors torch_nlo_clean/src/nlo_torch/bk/initial_conditions.py:13-91).
 
-They are evaluated once, on the host or the device, before the evolution; the
-evolution kernels only see the resulting amplitude row.
+They are evaluated once before the evolution; the evolution kernels only see the
+resulting amplitude row.  A tabulated initial condition (``ICDataFile``) is fitted and
+evaluated on the device (nlo_ic_spline / nlo_ic_evaluate) for CUDA tensors, which is the
+path solve_bk and compute_dndy take; CPU tensors get the same spline on the host, as the
+reference's own API allows.
 """
 
 from __future__ import annotations
@@ -73,9 +76,17 @@ class ICDataFile:
                 raise ValueError(f"{self.path}:{line_number} contains a non-numeric r or N") from error
         if len(N_values) < 10:
             raise ValueError(f"{self.path} contains {len(N_values)} points; at least 10 are required")
-        self.r = torch.tensor(r_values, dtype=dtype, device=device)
-        self.N = torch.tensor(N_values, dtype=dtype, device=device)
-        self._interpolator = NaturalCubicSpline(self.r, self.N)
+        r64 = torch.tensor(r_values, dtype=torch.float64)
+        N64 = torch.tensor(N_values, dtype=torch.float64)
+        if not bool(torch.isfinite(r64).all()) or not bool(torch.isfinite(N64).all()):
+            raise ValueError("x and y must contain only finite values")
+        if not bool((r64[1:] > r64[:-1]).all()):
+            raise ValueError("x must be strictly increasing")
+        self._r64, self._N64 = r64, N64  # the file's values, the device fit's input
+        self.r = r64.to(dtype=dtype, device=device)
+        self.N = N64.to(dtype=dtype, device=device)
+        self._host_spline: NaturalCubicSpline | None = None
+        self._device_splines: dict[int, torch.Tensor] = {}
 
     @property
     def min_r(self) -> float:
@@ -85,10 +96,50 @@ class ICDataFile:
     def max_r(self) -> float:
         return float(self.r[-1].item())
 
+    def device_spline(self, device: torch.device | str) -> torch.Tensor:
+        """The spline buffer fitted on a CUDA device (nlo_ic_spline), cached per device."""
+        from nlo_bk_optimized_b200 import _native
+
+        device = torch.device(device)
+        index = device.index if device.index is not None else torch.cuda.current_device()
+        buffer = self._device_splines.get(index)
+        if buffer is None:
+            lib = _native.load()
+            n = self._r64.numel()
+            dev = torch.device("cuda", index)
+            r = self._r64.to(dev)
+            N = self._N64.to(dev)
+            buffer = torch.empty(int(lib.nlo_ic_spline_doubles(n)), dtype=torch.float64, device=dev)
+            with torch.cuda.device(dev):
+                _native.check(lib.nlo_ic_spline(r.data_ptr(), N.data_ptr(), n, buffer.data_ptr(),
+                                                _native.stream_handle(dev)))
+            self._device_splines[index] = buffer
+        return buffer
+
+    def device_amplitude(self, r: torch.Tensor) -> torch.Tensor:
+        """N at CUDA points r, in float64 (nlo_ic_evaluate)."""
+        from nlo_bk_optimized_b200 import _native
+
+        r = r.contiguous()
+        _native.require_cuda(r, "r")
+        spline = self.device_spline(r.device)
+        r64 = r.to(torch.float64).contiguous()
+        out = torch.empty_like(r64)
+        lib = _native.load()
+        with torch.cuda.device(r.device):
+            _native.check(lib.nlo_ic_evaluate(spline.data_ptr(), self._r64.numel(), r64.data_ptr(), r64.numel(),
+                                              out.data_ptr(), _native.stream_handle(r.device)))
+        return out
+
     def dipole_amplitude(self, r: torch.Tensor) -> torch.Tensor:
-        value = self._interpolator(r.to(self.r.dtype))
-        value = torch.where(r < self.r[0], torch.zeros_like(value), value)
-        return torch.where(r > self.r[-1], torch.ones_like(value), value)
+        if r.is_cuda:
+            return self.device_amplitude(r).to(self.r.dtype)
+        if self._host_spline is None:
+            self._host_spline = NaturalCubicSpline(self._r64.to(self.r.dtype), self._N64.to(self.r.dtype))
+        rr = r.to(self.r.dtype)
+        value = self._host_spline(rr)
+        value = torch.where(rr < self._host_spline.x[0], torch.zeros_like(value), value)
+        return torch.where(rr > self._host_spline.x[-1], torch.ones_like(value), value)
 
 
 __all__ = ["ICDataFile", "MV"]

@@ -72,6 +72,7 @@ def solve_bk_sharded(initial_condition, maxy: float, config: BKConfig = BKConfig
     from nlo_bk_optimized_b200.bk.evolution import (
         _r_grid,
         _steps_to,
+        initial_row,
         nlo_box,
         params_of,
         precision_of,
@@ -86,7 +87,7 @@ def solve_bk_sharded(initial_condition, maxy: float, config: BKConfig = BKConfig
     lib = _native.load()
     params = params_of(config, precision_of(config, dtype))
     r_host = _r_grid(config, device="cpu", dtype=torch.float64)
-    N0 = initial_condition.dipole_amplitude(r_host).to(device=device, dtype=torch.float64).contiguous()
+    N0 = initial_row(initial_condition, r_host, device).contiguous()
     r = r_host.to(device)
     points = r.numel()
     lower, width = nlo_box(float(r_host[0]), float(r_host[-1]))

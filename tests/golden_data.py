@@ -50,3 +50,25 @@ def variant_config(name: str):
                     break
         kwargs[field] = value
     return bkc.BKConfig(RPOINTS=99, MINR=1e-6, MAXR=1e2, **kwargs)
+
+
+@lru_cache(maxsize=None)
+def bk_ic() -> dict[str, np.ndarray]:
+    with np.load(GOLDEN / "bk_ic.npz") as data:
+        return {key: data[key] for key in data.files}
+
+
+def synthetic_ic() -> tuple[np.ndarray, np.ndarray]:
+    """A 30,000-row tabulated initial condition on the grid of the reference's shipped
+    xb_001.dat (log-uniform from 1e-7 to 500): N = 1 - exp(-(r^2 Qs^2)^1.1/4 log(1/(r
+    Lambda) + e)) with Qs^2 = 0.104.  bk_ic.npz holds the SHA-256 of its bytes."""
+    i = np.arange(30000, dtype=np.float64)
+    r = 1e-7 * np.exp(i * (np.log(500.0 / 1e-7) / 29999.0))
+    exponent = (r * r * 0.104) ** 1.1 / 4 * np.log(1 / (r * 0.241) + np.e)
+    N = -np.expm1(-exponent)
+    return r, N
+
+
+def write_synthetic_ic(path) -> None:
+    r, N = synthetic_ic()
+    np.savetxt(path, np.stack((r, N), axis=1), fmt="%.17e")

@@ -232,24 +232,41 @@ struct FastSpline {
     float u_off;         // -x0 / h
     float u_max;         // n - 1
     int last;            // n - 2
+    float last_f;        // n - 2
 };
 
 struct P2S {
     float p2, S;
 };
 
-// log2(X^2) -> (log2 S, S) with the edge encoding
-__device__ __forceinline__ P2S fast_amplitude(const FastSpline& s, float l2sq)
+// floor(uc) for 0 <= uc < 2^23, clamped to `last`, without the XU conversions: adding
+// 2^23 rounded down leaves floor(uc) in the low mantissa bits.
+__device__ __forceinline__ float floor_clamped(float uc, float last)
 {
-    const float u = fmaf(l2sq, s.u_scale, s.u_off);
+    return fminf(__fadd_rd(uc, 8388608.0f) - 8388608.0f, last);
+}
+__device__ __forceinline__ int small_float_to_int(float integral)
+{
+    return __float_as_int(integral + 8388608.0f) - 0x4B000000;
+}
+
+// spline position u = (log X - x0)/h -> (log2 S, S) with the edge encoding
+__device__ __forceinline__ P2S fast_amplitude_at(const FastSpline& s, float u)
+{
     const float uc = fminf(fmaxf(u, 0.0f), s.u_max);
-    const int i = min((int)uc, s.last);
-    const float t = uc - (float)i;
-    const float4 c = s.coef[i];
+    const float fl = floor_clamped(uc, s.last_f);
+    const float t = uc - fl;
+    const float4 c = s.coef[small_float_to_int(fl)];
     float p2 = fmaf(t, fmaf(t, fmaf(t, c.w, c.z), c.y), c.x);
     p2 = u < 0.0f ? 0.0f : p2;
     p2 = u > s.u_max ? -150.0f : p2;
     return {p2, ex2_approx(p2)};
+}
+
+// log2(X^2) -> (log2 S, S) with the edge encoding
+__device__ __forceinline__ P2S fast_amplitude(const FastSpline& s, float l2sq)
+{
+    return fast_amplitude_at(s, fmaf(l2sq, s.u_scale, s.u_off));
 }
 
 // N_A - N_B from log2 S values
@@ -354,6 +371,154 @@ __device__ __forceinline__ void k2_point_fast(const FastSpline& s, const Phys<fl
     kfw = ok ? kfw : 0.0f;
 }
 
+// ---------------------------------------------------------------------------
+// Two samples per call on the packed FP32x2 pipe of sm_100 (FFMA2/FADD2/FMUL2): the
+// per-evaluation arithmetic of k2_point_fast, component x for sample 2p and y for 2p+1
+// of a pair record (every field of the two samples side by side), so each packed
+// instruction does the work of two.  MUFU operations, compares and selects stay scalar.
+using f2 = float2;
+__device__ __forceinline__ f2 bc2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ f2 add2(f2 a, f2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ f2 sub2(f2 a, f2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ f2 mul2(f2 a, f2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ f2 rcp2(f2 a) { return make_float2(rcp_approx(a.x), rcp_approx(a.y)); }
+__device__ __forceinline__ f2 lg22(f2 a) { return make_float2(lg2_approx(a.x), lg2_approx(a.y)); }
+__device__ __forceinline__ f2 sel2(bool cx, bool cy, f2 a, f2 b) { return make_float2(cx ? a.x : b.x, cy ? a.y : b.y); }
+
+// N_A - N_B from log2 S values, for a pair
+__device__ __forceinline__ f2 fast_ndiff2(const P2S& Ax, const P2S& Ay, const P2S& Bx, const P2S& By)
+{
+    const f2 d = make_float2(Bx.p2 - Ax.p2, By.p2 - Ay.p2);
+    const f2 x = make_float2(-fabsf(d.x), -fabsf(d.y));
+    f2 q = fma2(bc2(0.0001327910803141678f), x, bc2(0.001321632968973654f));
+    q = fma2(q, x, bc2(0.009615099576281485f));
+    q = fma2(q, x, bc2(0.05550375169709732f));
+    q = fma2(q, x, bc2(0.24022649146109623f));
+    q = fma2(q, x, bc2(0.6931471804499034f));
+    const f2 poly = mul2(q, x);
+    const f2 e = make_float2(x.x > -0.5f ? poly.x : ex2_approx(x.x) - 1.0f,
+                             x.y > -0.5f ? poly.y : ex2_approx(x.y) - 1.0f);
+    const f2 S = make_float2(d.x <= 0.0f ? Ax.S : -Bx.S, d.y <= 0.0f ? Ay.S : -By.S);
+    return mul2(S, e);
+}
+
+template <bool SYM, int COUPLING>
+__device__ __forceinline__ void k2_pair_fast(const FastSpline& s, const Phys<float>& ph, const K2ParentF& P,
+                                             const float4* __restrict__ rec4, f2& k2w, f2& kfw)
+{
+    constexpr float LN2 = 0.69314718055994531f;
+    constexpr float L2E = 1.4426950408889634f;
+    // pair layout: float4 k holds fields 2k and 2k+1 of (sample x, sample y)
+    const float4 w0 = rec4[0], w1 = rec4[1], w2 = rec4[2], w3 = rec4[3], w4 = rec4[4];
+    const float4 w5 = rec4[5], w6 = rec4[6], w7 = rec4[7], w8 = rec4[8], w9 = rec4[9];
+    const f2 z = make_float2(w0.x, w0.y), z2 = make_float2(w0.z, w0.w);
+    const f2 s1 = make_float2(w1.x, w1.y), s2 = make_float2(w1.z, w1.w);
+    const f2 P1 = make_float2(w2.x, w2.y), P2 = make_float2(w2.z, w2.w);
+    const f2 U1 = make_float2(w3.x, w3.y), V1 = make_float2(w3.z, w3.w);
+    const f2 U2 = make_float2(w4.x, w4.y), V2 = make_float2(w4.z, w4.w);
+    const f2 q = make_float2(w5.x, w5.y), D1 = make_float2(w5.z, w5.w);
+    const f2 D2 = make_float2(w6.x, w6.y), dN = make_float2(w6.z, w6.w);
+    const f2 SY = make_float2(w7.x, w7.y), Lmin = make_float2(w7.z, w7.w);
+    const f2 cpt = make_float2(w8.x, w8.y), Dl = make_float2(w8.z, w8.w);
+    const f2 zsq = make_float2(w9.x, w9.y), z2sq = make_float2(w9.z, w9.w);
+    const f2 r = bc2(P.r);
+    const f2 rz = sub2(r, z), rz2 = sub2(r, z2);
+    const f2 Xsq = fma2(mul2(bc2(P.four_r), z), s1, mul2(rz, rz));
+    const f2 X2sq = fma2(mul2(bc2(P.four_r), z2), s2, mul2(rz2, rz2));
+    const bool valid_x = Xsq.x >= 1e-38f && X2sq.x >= 1e-38f;
+    const bool valid_y = Xsq.y >= 1e-38f && X2sq.y >= 1e-38f;
+    const f2 L2X = lg22(Xsq), L2X2 = lg22(X2sq);
+    const f2 uX = fma2(L2X, bc2(s.u_scale), bc2(s.u_off)), uX2 = fma2(L2X2, bc2(s.u_scale), bc2(s.u_off));
+    const P2S vXx = fast_amplitude_at(s, uX.x), vXy = fast_amplitude_at(s, uX.y);
+    const P2S vX2x = fast_amplitude_at(s, uX2.x), vX2y = fast_amplitude_at(s, uX2.y);
+    // kernels
+    const f2 a = mul2(Xsq, z2sq), b = mul2(X2sq, zsq);
+    const f2 rs = rcp2(add2(a, b));
+    const f2 d = mul2(r, fma2(r, P1, make_float2(-P2.x, -P2.y)));
+    const f2 t = mul2(d, rs);
+    const f2 t2 = mul2(t, t);
+    f2 g = fma2(bc2(0.15609439065092748f), t2, bc2(0.04106302733766397f));
+    g = fma2(g, t2, bc2(0.09747851219255123f));
+    g = fma2(g, t2, bc2(0.11051354325642386f));
+    g = fma2(g, t2, bc2(0.1428825580061165f));
+    g = fma2(g, t2, bc2(0.19999959971627077f));
+    g = fma2(g, t2, bc2(0.33333333435159396f));
+    const f2 hm1_series = mul2(g, t2);
+    const f2 Ld = fma2(bc2(LN2), sub2(L2X, L2X2), Dl);  // log(a/b)
+    const f2 hm1_log = fma2(Ld, mul2(bc2(0.5f), rcp2(t)), bc2(-1.0f));
+    const f2 hm1 = sel2(t2.x < 0.25f, t2.y < 0.25f, hm1_series, hm1_log);
+    const f2 rs2 = add2(rs, rs);
+    const f2 L = fma2(hm1, rs2, rs2);
+    const f2 r2Lq = mul2(mul2(bc2(P.r2), L), q);
+    const f2 fq2 = mul2(add2(hm1, hm1), mul2(q, q));
+    const f2 C0 = fma2(bc2(-4.0f), r2Lq, fq2);
+    const f2 B1 = fma2(r, U1, V1), B2 = fma2(r, U2, V2);
+    const f2 w = mul2(r2Lq, bc2(P.two_r));
+    f2 k2 = fma2(mul2(w, B1), rcp2(mul2(Xsq, z2)), C0);
+    f2 k2s = fma2(mul2(w, B2), rcp2(mul2(X2sq, z)), C0);
+    const f2 kf = mul2(sub2(r2Lq, fq2), bc2(ph.nf_over_nc));
+    f2 dip = mul2(make_float2(vXx.S, vXy.S), D1), dips = mul2(make_float2(vX2x.S, vX2y.S), D2);
+    const bool cut_x = fabsf(k2.x) > 1e10f && fabsf(dip.x) < 1e-10f;
+    const bool cut_y = fabsf(k2.y) > 1e10f && fabsf(dip.y) < 1e-10f;
+    const bool cuts_x = fabsf(k2s.x) > 1e10f && fabsf(dips.x) < 1e-10f;
+    const bool cuts_y = fabsf(k2s.y) > 1e10f && fabsf(dips.y) < 1e-10f;
+    k2 = sel2(cut_x, cut_y, bc2(0.0f), k2);
+    dip = sel2(cut_x, cut_y, bc2(0.0f), dip);
+    k2s = sel2(cuts_x, cuts_y, bc2(0.0f), k2s);
+    dips = sel2(cuts_x, cuts_y, bc2(0.0f), dips);
+    const f2 dNX = fast_ndiff2(vXx, vXy, vX2x, vX2y);
+    f2 k2part, fermion;
+    if (SYM) {  // the factor 1/2 of the symmetrisation is folded into cpt
+        k2part = fma2(k2, dip, mul2(k2s, dips));
+        fermion = mul2(mul2(kf, dNX), dN);
+    } else {
+        k2part = mul2(k2, dip);
+        fermion = mul2(mul2(kf, SY), dNX);
+    }
+    f2 alpha;
+    if (COUPLING == 2) {
+        alpha = bc2(ph.fixed_as);
+    } else if (COUPLING == 4) {
+        alpha = bc2(P.alpha_r);
+    } else {
+        const f2 lmin = make_float2(fminf(fminf(Lmin.x, P.lr), (0.5f * LN2) * fminf(L2X.x, L2X2.x)),
+                                    fminf(fminf(Lmin.y, P.lr), (0.5f * LN2) * fminf(L2X.y, L2X2.y)));
+        if (COUPLING == 3) {
+            alpha = make_float2(alpha_of_log(lmin.x, ph), alpha_of_log(lmin.y, ph));
+        } else {
+            const f2 right = fma2(bc2(-10.0f), lmin, bc2(5.0f * ph.log_sc));
+            const f2 m = make_float2(fmaxf(ph.left, right.x), fmaxf(ph.left, right.y));
+            const f2 e = make_float2(ex2_approx(-fabsf(ph.left - right.x) * L2E),
+                                     ex2_approx(-fabsf(ph.left - right.y) * L2E));
+            const f2 lae = fma2(bc2(LN2), lg22(add2(bc2(1.0f), e)), m);
+            alpha = rcp2(mul2(bc2(ph.b0c), lae));
+            if (COUPLING == 1) alpha = make_float2(fminf(alpha.x, ph.alpha_cap), fminf(alpha.y, ph.alpha_cap));
+        }
+    }
+    const f2 scale = mul2(mul2(alpha, alpha), cpt);
+    k2w = mul2(k2part, scale);
+    kfw = mul2(make_float2(-fermion.x, -fermion.y), scale);
+    const f2 tot = add2(k2w, kfw);
+    const bool ok_x = valid_x && fabsf(tot.x) < INFINITY;
+    const bool ok_y = valid_y && fabsf(tot.y) < INFINITY;
+    k2w = sel2(ok_x, ok_y, k2w, bc2(0.0f));
+    kfw = sel2(ok_x, ok_y, kfw, bc2(0.0f));
+}
+
+// Compensated sums of pairs (Kahan per component, packed).
+struct Kahan2 {
+    f2 sum, comp;
+    __device__ __forceinline__ void reset() { sum = bc2(0.0f); comp = bc2(0.0f); }
+    __device__ __forceinline__ void add(f2 v)
+    {
+        const f2 y = sub2(v, comp);
+        const f2 t = add2(sum, y);
+        comp = sub2(sub2(t, sum), y);
+        sum = t;
+    }
+};
+
 template <typename T, bool SYM, int COUPLING>
 __global__ void __launch_bounds__(1024) k2kf_kernel(Phys<T> ph, K2Box<T> box, SobolDirsArg dirs,
                                                     const double* __restrict__ r_grid, int n,
@@ -398,6 +563,7 @@ __global__ void __launch_bounds__(1024) k2kf_kernel(Phys<T> ph, K2Box<T> box, So
     fs.u_off = (float)(-spline[0] / h64);
     fs.u_max = (float)(n - 1);
     fs.last = n - 2;
+    fs.last_f = (float)(n - 2);
 
     const int n_active = *count;
     const int slot = blockIdx.y * blockDim.x + threadIdx.x;
@@ -426,30 +592,57 @@ __global__ void __launch_bounds__(1024) k2kf_kernel(Phys<T> ph, K2Box<T> box, So
     if (any_parent) {
         for (uint64_t tix = blockIdx.x; tix < tiles; tix += gridDim.x) {
             const uint64_t local = tix * tile + threadIdx.x;
-            k2_prepare<T>(s, ph, box, st, st + 120, offset + local, local < samples, recs[threadIdx.x].v);
-            __syncthreads();
-            if (has_parent) {
-                const uint64_t remaining = samples - tix * tile;
-                const int count_here = (int)(remaining < tile ? remaining : tile);
-                Kahan<T> sk2, skf;
-                sk2.reset();
-                skf.reset();
-                T sq = (T)0;  // variance estimate only: plain sum per tile
-                for (int j = 0; j < count_here; ++j) {
-                    T k2w, kfw;
-                    if constexpr (sizeof(T) == sizeof(float))
-                        k2_point_fast<SYM, COUPLING>(fs, ph, PF, reinterpret_cast<const float4*>(recs[j].v), k2w,
-                                                     kfw);
-                    else
-                        k2_point<T, SYM>(s, ph, P, recs[j].v, k2w, kfw);
-                    sk2.add(k2w);
-                    skf.add(kfw);
-                    const T tot = k2w + kfw;
-                    sq += tot * tot;
+            const uint64_t remaining = samples - tix * tile;
+            const int count_here = (int)(remaining < tile ? remaining : tile);
+            if constexpr (sizeof(T) == sizeof(float)) {
+                // pair layout: the fields of samples 2p and 2p+1 side by side (blockDim.x is even;
+                // a padding sample past `samples` carries zero weight)
+                float rec[kRecLen];
+                k2_prepare<float>(s, ph, box, st, st + 120, offset + local, local < samples, rec);
+                float* dst = reinterpret_cast<float*>(recs) + (size_t)(threadIdx.x >> 1) * (2 * kRecLen) +
+                             (threadIdx.x & 1);
+#pragma unroll
+                for (int f = 0; f < kRecLen; ++f) dst[2 * f] = rec[f];
+                __syncthreads();
+                if (has_parent) {
+                    const float4* pr = reinterpret_cast<const float4*>(recs);
+                    Kahan2 sk2, skf;
+                    sk2.reset();
+                    skf.reset();
+                    f2 sq = bc2(0.0f);  // variance estimate only: plain sum per tile
+                    const int pairs = (count_here + 1) >> 1;
+                    for (int j = 0; j < pairs; ++j) {
+                        f2 k2w, kfw;
+                        k2_pair_fast<SYM, COUPLING>(fs, ph, PF, pr + (kRecLen / 2) * j, k2w, kfw);
+                        sk2.add(k2w);
+                        skf.add(kfw);
+                        const f2 tot = add2(k2w, kfw);
+                        sq = fma2(tot, tot, sq);
+                    }
+                    acc_k2 += ((double)sk2.sum.x - (double)sk2.comp.x) + ((double)sk2.sum.y - (double)sk2.comp.y);
+                    acc_kf += ((double)skf.sum.x - (double)skf.comp.x) + ((double)skf.sum.y - (double)skf.comp.y);
+                    acc_sq += (double)sq.x + (double)sq.y;
                 }
-                acc_k2 += (double)sk2.sum - (double)sk2.comp;
-                acc_kf += (double)skf.sum - (double)skf.comp;
-                acc_sq += (double)sq;
+            } else {
+                k2_prepare<T>(s, ph, box, st, st + 120, offset + local, local < samples, recs[threadIdx.x].v);
+                __syncthreads();
+                if (has_parent) {
+                    Kahan<T> sk2, skf;
+                    sk2.reset();
+                    skf.reset();
+                    T sq = (T)0;  // variance estimate only: plain sum per tile
+                    for (int j = 0; j < count_here; ++j) {
+                        T k2w, kfw;
+                        k2_point<T, SYM>(s, ph, P, recs[j].v, k2w, kfw);
+                        sk2.add(k2w);
+                        skf.add(kfw);
+                        const T tot = k2w + kfw;
+                        sq += tot * tot;
+                    }
+                    acc_k2 += (double)sk2.sum - (double)sk2.comp;
+                    acc_kf += (double)skf.sum - (double)skf.comp;
+                    acc_sq += (double)sq;
+                }
             }
             __syncthreads();
         }

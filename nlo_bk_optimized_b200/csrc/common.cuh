@@ -343,6 +343,39 @@ __device__ __forceinline__ T spline_delta_from_knot(const SplineView<T>& s, int 
     return pv - knot_value;
 }
 
+// Packed FP32x2 arithmetic of sm_100 (FFMA2/FADD2/FMUL2): two FP32 operations per
+// instruction, component x and y.
+using f2 = float2;
+__device__ __forceinline__ f2 bc2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ f2 add2(f2 a, f2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ f2 sub2(f2 a, f2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ f2 mul2(f2 a, f2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) { return __ffma2_rn(a, b, c); }
+
+// M<float>::expm1 and M<float>::log1p for a pair.
+__device__ __forceinline__ f2 expm1_2(f2 x)
+{
+    f2 q = fma2(bc2(0.00019823966831129978f), x, bc2(0.0013997217938334417f));
+    q = fma2(q, x, bc2(0.008333698847676367f));
+    q = fma2(q, x, bc2(0.04166532151841506f));
+    q = fma2(q, x, bc2(0.16666662318239217f));
+    q = fma2(q, x, bc2(0.5000000415133041f));
+    q = fma2(q, x, bc2(1.0000000006631342f));
+    const f2 p = mul2(x, q);
+    return make_float2(fabsf(x.x) < 0.5f ? p.x : __expf(x.x) - 1.0f, fabsf(x.y) < 0.5f ? p.y : __expf(x.y) - 1.0f);
+}
+__device__ __forceinline__ f2 log1p_2(f2 v)
+{
+    const f2 sv = make_float2(__fdividef(v.x, 2.0f + v.x), __fdividef(v.y, 2.0f + v.y));
+    const f2 u = mul2(sv, sv);
+    f2 p = fma2(bc2(0.14080726880347302f), u, bc2(0.13982172352285377f));
+    p = fma2(p, u, bc2(0.20012325666926623f));
+    p = fma2(p, u, bc2(0.33333160203202167f));
+    p = fma2(p, u, bc2(1.000000003861989f));
+    const f2 r = mul2(add2(sv, sv), p);
+    return make_float2(fabsf(v.x) <= 0.5f ? r.x : __logf(1.0f + v.x), fabsf(v.y) <= 0.5f ? r.y : __logf(1.0f + v.y));
+}
+
 // Compensated (Kahan) accumulation.
 template <typename T>
 struct Kahan {

@@ -266,6 +266,113 @@ __device__ __forceinline__ T k1_point(const SplineView<T>& s, const K1Parent<T>&
     return M<T>::finite(result) ? result : (T)0;
 }
 
+// k1_point for two angles of one radial node (x: angle j, y: angle j + 1) in the mixed
+// build without the kinematical constraint: the same arithmetic on the packed FP32x2
+// instructions, with the per-angle transcendental and table operations per component.
+__device__ __forceinline__ f2 k1_pair_point(const SplineView<float>& s, const K1Parent<float>& P,
+                                            const K1Z<float>& Z, const Phys<float>& ph, f2 sh2)
+{
+    const float r = P.r, z = Z.z;
+    const f2 Xsq = fma2(bc2((float)4 * r * z), sh2, bc2((r - z) * (r - z)));
+    const bool ok_x = Xsq.x >= M<float>::tiny_square(), ok_y = Xsq.y >= M<float>::tiny_square();
+    if (!ok_x && !ok_y) return bc2(0.0f);
+    const f2 xr2 = fma2(bc2(4.0f * Z.rho), sh2, bc2((1.0f - Z.rho) * (1.0f - Z.rho)));
+    const f2 dX = mul2(bc2(0.5f), make_float2(__logf(xr2.x), __logf(xr2.y)));
+    const f2 alpha_X = make_float2(alpha_of_log(P.lr_abs + dX.x, ph), alpha_of_log(P.lr_abs + dX.y, ph));
+    // X^2 - Y^2 = r (r - 2 z cos theta), cos theta = 1 - 2 sin^2(theta/2)
+    const f2 XmY = mul2(bc2(r), fma2(bc2(-2.0f * z), fma2(bc2(-2.0f), sh2, bc2(1.0f)), bc2(r)));
+    const f2 aY = bc2(Z.alpha_Y);
+    f2 dalpha;
+    if (ph.fixed) {
+        dalpha = bc2(0.0f);
+    } else if (ph.alpha_cap > 0.0f || ph.thresholds) {
+        dalpha = sub2(aY, alpha_X);
+    } else {
+        // alpha_Y - alpha_X = alpha_X alpha_Y b0 c (lae_X - lae_Y)
+        const f2 delta = mul2(bc2(-5.0f), log1p_2(mul2(XmY, bc2(Z.inv_Ysq))));
+        const f2 v = mul2(bc2(Z.sigma), expm1_2(delta));
+        f2 shift = log1p_2(v);
+        if (v.x <= -0.5f) shift.x = logf(Z.sigma_c + Z.sigma * __expf(delta.x));
+        if (v.y <= -0.5f) shift.y = logf(Z.sigma_c + Z.sigma * __expf(delta.y));
+        dalpha = mul2(mul2(alpha_X, aY), mul2(bc2(ph.b0c), shift));
+    }
+    const f2 inv_XY = make_float2(__fdividef(1.0f, Xsq.x * Z.Ysq), __fdividef(1.0f, Xsq.y * Z.Ysq));
+    const float pref = ph.nc * (float)(1.0 / (2.0 * kPi * kPi));
+    // alpha at min(X, Y, r): reuse alpha_X, alpha_Y or alpha_r
+    const f2 alpha_min = make_float2((dX.x <= Z.dY && dX.x <= 0.0f) ? alpha_X.x : (Z.dY <= 0.0f ? Z.alpha_Y : P.alpha_r),
+                                     (dX.y <= Z.dY && dX.y <= 0.0f) ? alpha_X.y : (Z.dY <= 0.0f ? Z.alpha_Y : P.alpha_r));
+    const f2 r2iXY = mul2(bc2(P.r2), inv_XY);
+    f2 lo, alpha_sc;
+    if (ph.rc_lo == NLO_RC_LO_PARENT) {
+        alpha_sc = bc2(P.alpha_r);
+        lo = mul2(bc2(pref * P.alpha_r), r2iXY);
+    } else if (ph.rc_lo == NLO_RC_LO_SMALLEST) {
+        alpha_sc = alpha_min;
+        lo = mul2(mul2(bc2(pref), alpha_min), r2iXY);
+    } else if (ph.rc_lo == NLO_RC_LO_FAC) {
+        alpha_sc = bc2(P.alpha_r);
+        const f2 q = make_float2(__fdividef(dalpha.x, alpha_X.x * Z.alpha_Y), __fdividef(dalpha.y, alpha_X.y * Z.alpha_Y));
+        const f2 den = sub2(bc2(__fdividef(1.0f, P.alpha_r)), mul2(mul2(XmY, bc2(__fdividef(1.0f, P.r2))), q));
+        lo = mul2(mul2(bc2(pref), r2iXY), make_float2(__fdividef(1.0f, den.x), __fdividef(1.0f, den.y)));
+    } else if (ph.rc_lo == NLO_RC_LO_BEUF) {
+        const f2 log_reff = fma2(mul2(bc2(-0.5f * __fdividef(1.0f, P.r2)), XmY), log1p_2(mul2(XmY, bc2(Z.inv_Ysq))),
+                                 bc2(P.lr_abs));
+        alpha_sc = make_float2(alpha_of_log(log_reff.x, ph), alpha_of_log(log_reff.y, ph));
+        lo = mul2(mul2(bc2(pref), alpha_sc), r2iXY);
+    } else {
+        // Balitsky: r^2/(X^2Y^2) + (aY/aX - 1)/Y^2 + (aX/aY - 1)/X^2
+        alpha_sc = bc2(P.alpha_r);
+        const f2 num = fma2(aY, XmY, mul2(bc2(Z.Ysq), dalpha));
+        const f2 frac = make_float2(__fdividef(num.x, alpha_X.x * Z.alpha_Y), __fdividef(num.y, alpha_X.y * Z.alpha_Y));
+        const f2 bracket = mul2(fma2(dalpha, frac, bc2(P.r2)), inv_XY);
+        lo = mul2(bc2(pref * P.alpha_r), bracket);
+    }
+    lo = make_float2(isfinite(lo.x) ? lo.x : 0.0f, isfinite(lo.y) ? lo.y : 0.0f);
+    // dipole N_X + N_Y - N_r - N_X N_Y = S_r (N_Y + D_X) - D_X D_Y  (or with X and Y exchanged)
+    float NXx, DXx, NXy, DXy;
+    k1_amplitude(s, P, dX.x, NXx, DXx);
+    k1_amplitude(s, P, dX.y, NXy, DXy);
+    const f2 DX = make_float2(DXx, DXy);
+    const f2 base = make_float2(Z.NY <= NXx ? Z.NY + DXx : NXx + Z.DY, Z.NY <= NXy ? Z.NY + DXy : NXy + Z.DY);
+    const f2 dipole = fma2(bc2(P.Sr), base, mul2(bc2(-Z.DY), DX));
+    f2 result;
+    if (!ph.resum) {
+        result = mul2(lo, dipole);
+    } else {
+        // double-log resummation (k1.py:109-119) with the RESUM_RC coupling
+        const f2 alpha_res = ph.resum_rc == NLO_RESUM_RC_PARENT
+                                 ? bc2(P.alpha_r)
+                                 : (ph.resum_rc == NLO_RESUM_RC_FIXED ? bc2(ph.fixed_as) : alpha_min);
+        const f2 xarg = mul2(bc2(4.0f * Z.dY), dX);
+        const f2 abar = mul2(alpha_res, bc2(ph.nc * (float)(1.0 / kPi)));
+        const f2 as2 = mul2(abar, make_float2(fabsf(xarg.x), fabsf(xarg.y)));
+        const f2 as_x = make_float2(M<float>::sqrt(as2.x), M<float>::sqrt(as2.y));
+        f2 dlog = bc2(1.0f);
+        if (as_x.x != 0.0f)
+            dlog.x = __fdividef(xarg.x >= 0.0f ? j1f(2.0f * as_x.x) : cyl_bessel_i1f(2.0f * as_x.x), as_x.x);
+        if (as_x.y != 0.0f)
+            dlog.y = __fdividef(xarg.y >= 0.0f ? j1f(2.0f * as_x.y) : cyl_bessel_i1f(2.0f * as_x.y), as_x.y);
+        if (!(r > 1.01f * ph.minr)) dlog = bc2(1.0f);
+        // single-log resummation (k1.py:121-132)
+        f2 slog = bc2(1.0f), slog_exp = bc2(0.0f);
+        if (ph.slog) {
+            const f2 dminxy = make_float2(fminf(dX.x, Z.dY), fminf(dX.y, Z.dY));
+            const f2 arg = fma2(bc2(-2.0f), dminxy, bc2(ph.log_ksub));
+            slog_exp = mul2(mul2(abar, bc2(-11.0f / 12.0f)), make_float2(fabsf(arg.x), fabsf(arg.y)));
+            slog = make_float2(__expf(slog_exp.x), __expf(slog_exp.y));
+        }
+        const f2 lo_single = mul2(mul2(bc2(pref), alpha_sc), r2iXY);
+        const float fin = ph.nc * (float)(1.0 / (4.0 * kPi)) *
+                          ((float)(67.0 / 9.0 - kPi * kPi / 3.0) - (float)(10.0 / 9.0) * ph.nf_over_nc);
+        const f2 k1fin = mul2(mul2(lo, alpha_sc), bc2(fin));
+        const f2 core = add2(sub2(mul2(mul2(dlog, slog), lo), mul2(lo_single, slog_exp)), k1fin);
+        result = mul2(core, dipole);
+        if (!isfinite(dlog.x)) result.x = 0.0f;
+        if (!isfinite(dlog.y)) result.y = 0.0f;
+    }
+    return make_float2(ok_x && isfinite(result.x) ? result.x : 0.0f, ok_y && isfinite(result.y) ? result.y : 0.0f);
+}
+
 template <typename T>
 __device__ __forceinline__ K1Parent<T> k1_parent(const SplineView<T>& s, const Phys<T>& ph, double r, int knot)
 {
@@ -382,12 +489,26 @@ __global__ void __cluster_dims__(1, kK1Split, 1) __launch_bounds__(kK1Threads)
     }
     __syncthreads();
 
-    // phase 2: the flattened (node, angle) evaluations, an equal share per thread
+    // phase 2: the flattened (node, angle) evaluations, an equal share per thread; the
+    // mixed build without the constraint takes two angles of a node per step on the
+    // packed FP32x2 instructions
     double total = 0.0;
-    for (int e = threadIdx.x; e < k_count * 24; e += blockDim.x) {
-        const int L = e / 24, j = e - 24 * (e / 24);
-        const double w = zw[L];
-        if (w != 0.0) total += (double)(k1_point<TF, KC>(sf, Pf, zt[L], phf, sh2f[j], history, r_grid) * awf[j]) * w;
+    if constexpr (sizeof(TF) == sizeof(float) && !KC) {
+        for (int e = threadIdx.x; e < k_count * 12; e += blockDim.x) {
+            const int L = e / 12, j = 2 * (e - 12 * L);
+            const double w = zw[L];
+            if (w != 0.0) {
+                const f2 v = k1_pair_point(sf, Pf, zt[L], phf, make_float2(sh2f[j], sh2f[j + 1]));
+                total += ((double)(v.x * awf[j]) + (double)(v.y * awf[j + 1])) * w;
+            }
+        }
+    } else {
+        for (int e = threadIdx.x; e < k_count * 24; e += blockDim.x) {
+            const int L = e / 24, j = e - 24 * (e / 24);
+            const double w = zw[L];
+            if (w != 0.0)
+                total += (double)(k1_point<TF, KC>(sf, Pf, zt[L], phf, sh2f[j], history, r_grid) * awf[j]) * w;
+        }
     }
     // phase 3: FP64 evaluations of the panel nodes this CTA owns
     for (int e = threadIdx.x; e < 16 * 24; e += blockDim.x) {

@@ -42,24 +42,12 @@ struct K2Box {
     T cpt_scale;  // volume * Nc^2 / (8 pi^4)
 };
 
-// atanh(t)/t - 1 = t^2 g(t^2), g(x) = sum_{k>=0} x^k/(2k+3), for t^2 < 1/4.
-// FP32: degree-6 polynomial fitted to g on [0, 1/4] in relative error (least
-// squares at Chebyshev nodes); 8e-8 relative in FP32 Horner, i.e. FP32 rounding.
+// atanh(t)/t - 1 = t^2 g(t^2), g(x) = sum_{k>=0} x^k/(2k+3), for t^2 < 1/4: the series in
+// FP64; the FP32 pair path (k2_pair_fast) evaluates g by a degree-6 polynomial fitted on
+// [0, 1/4] in relative error (least squares at Chebyshev nodes; 8e-8 relative in FP32
+// Horner, i.e. FP32 rounding).
 template <typename T>
 __device__ __forceinline__ T atanh_ratio_m1(T t2);
-
-template <>
-__device__ __forceinline__ float atanh_ratio_m1<float>(float t2)
-{
-    float s = 0.15609439065092748f;
-    s = fmaf(s, t2, 0.04106302733766397f);
-    s = fmaf(s, t2, 0.09747851219255123f);
-    s = fmaf(s, t2, 0.11051354325642386f);
-    s = fmaf(s, t2, 0.1428825580061165f);
-    s = fmaf(s, t2, 0.19999959971627077f);
-    s = fmaf(s, t2, 0.33333333435159396f);
-    return s * t2;
-}
 
 template <>
 __device__ __forceinline__ double atanh_ratio_m1<double>(double t2)
@@ -211,20 +199,7 @@ __device__ __forceinline__ float rcp_approx(float x)
     return y;
 }
 
-// 2^x - 1 for x <= 0: degree-5 polynomial in x times x on [-1/2, 0] (fitted to
-// (2^x - 1)/x in relative error; 1.2e-7 in FP32), 2^x - 1 directly below.
-__device__ __forceinline__ float exp2m1_nonpositive(float x)
-{
-    float q = 0.0001327910803141678f;
-    q = fmaf(q, x, 0.001321632968973654f);
-    q = fmaf(q, x, 0.009615099576281485f);
-    q = fmaf(q, x, 0.05550375169709732f);
-    q = fmaf(q, x, 0.24022649146109623f);
-    q = fmaf(q, x, 0.6931471804499034f);
-    const float poly = q * x;
-    const float direct = ex2_approx(x) - 1.0f;
-    return x > -0.5f ? poly : direct;
-}
+
 
 struct FastSpline {
     const float4* coef;  // [n-1] pre-scaled (see above)
@@ -263,19 +238,8 @@ __device__ __forceinline__ P2S fast_amplitude_at(const FastSpline& s, float u)
     return {p2, ex2_approx(p2)};
 }
 
-// log2(X^2) -> (log2 S, S) with the edge encoding
-__device__ __forceinline__ P2S fast_amplitude(const FastSpline& s, float l2sq)
-{
-    return fast_amplitude_at(s, fmaf(l2sq, s.u_scale, s.u_off));
-}
 
-// N_A - N_B from log2 S values
-__device__ __forceinline__ float fast_ndiff(const P2S& A, const P2S& B)
-{
-    const float d = B.p2 - A.p2;
-    const float e = exp2m1_nonpositive(-fabsf(d));
-    return d <= 0.0f ? A.S * e : -B.S * e;
-}
+
 
 struct K2ParentF {
     float r, r2, lr, two_r, four_r;
@@ -284,104 +248,12 @@ struct K2ParentF {
 
 // COUPLING: 0 smooth freeze, 1 smooth freeze capped at alpha_cap, 2 fixed, 3 any coupling
 // of alpha_of_log (flavour thresholds), 4 the parent's coupling (RC_NLO = PARENT_NLO).
-template <bool SYM, int COUPLING>
-__device__ __forceinline__ void k2_point_fast(const FastSpline& s, const Phys<float>& ph, const K2ParentF& P,
-                                              const float4* __restrict__ rec4, float& k2w, float& kfw)
-{
-    constexpr float LN2 = 0.69314718055994531f;
-    constexpr float L2E = 1.4426950408889634f;
-    const float4 q0 = rec4[0], q1 = rec4[1], q2 = rec4[2], q3 = rec4[3], q4 = rec4[4];
-    // record layout (enum Rec): z z2 s1 s2 | P1 P2 U1 V1 | U2 V2 q D1 | D2 dN SY Lmin | Cpt Dl zsq z2sq
-    const float z = q0.x, z2 = q0.y, s1 = q0.z, s2 = q0.w;
-    const float P1 = q1.x, P2 = q1.y, U1 = q1.z, V1 = q1.w;
-    const float U2 = q2.x, V2 = q2.y, q = q2.z, D1 = q2.w;
-    const float D2 = q3.x, dN = q3.y, SY = q3.z, Lmin = q3.w;
-    const float cpt = q4.x, Dl = q4.y, zsq = q4.z, z2sq = q4.w;
-    const float r = P.r;
-    const float rz = r - z, rz2 = r - z2;
-    const float Xsq = fmaf(P.four_r * z, s1, rz * rz);
-    const float X2sq = fmaf(P.four_r * z2, s2, rz2 * rz2);
-    const bool valid = Xsq >= 1e-38f && X2sq >= 1e-38f;
-    const float L2X = lg2_approx(Xsq), L2X2 = lg2_approx(X2sq);
-    const P2S vX = fast_amplitude(s, L2X), vX2 = fast_amplitude(s, L2X2);
-    // kernels
-    const float a = Xsq * z2sq, b = X2sq * zsq;
-    const float rs = rcp_approx(a + b);
-    const float d = r * fmaf(r, P1, -P2);
-    const float t = d * rs;
-    const float t2 = t * t;
-    float g = 0.15609439065092748f;
-    g = fmaf(g, t2, 0.04106302733766397f);
-    g = fmaf(g, t2, 0.09747851219255123f);
-    g = fmaf(g, t2, 0.11051354325642386f);
-    g = fmaf(g, t2, 0.1428825580061165f);
-    g = fmaf(g, t2, 0.19999959971627077f);
-    g = fmaf(g, t2, 0.33333333435159396f);
-    const float hm1_series = g * t2;
-    const float Ld = fmaf(LN2, L2X - L2X2, Dl);  // log(a/b)
-    const float hm1_log = fmaf(Ld, 0.5f * rcp_approx(t), -1.0f);
-    const float hm1 = t2 < 0.25f ? hm1_series : hm1_log;
-    const float rs2 = rs + rs;
-    const float L = fmaf(hm1, rs2, rs2);
-    const float r2Lq = P.r2 * L * q;
-    const float fq2 = (hm1 + hm1) * (q * q);
-    const float C0 = fmaf(-4.0f, r2Lq, fq2);
-    const float B1 = fmaf(r, U1, V1), B2 = fmaf(r, U2, V2);
-    const float w = r2Lq * P.two_r;
-    float k2 = fmaf(w * B1, rcp_approx(Xsq * z2), C0);
-    float k2s = fmaf(w * B2, rcp_approx(X2sq * z), C0);
-    const float kf = (r2Lq - fq2) * ph.nf_over_nc;
-    float dip = vX.S * D1, dips = vX2.S * D2;
-    const bool cut = fabsf(k2) > 1e10f && fabsf(dip) < 1e-10f;
-    const bool cut_s = fabsf(k2s) > 1e10f && fabsf(dips) < 1e-10f;
-    k2 = cut ? 0.0f : k2;
-    dip = cut ? 0.0f : dip;
-    k2s = cut_s ? 0.0f : k2s;
-    dips = cut_s ? 0.0f : dips;
-    const float dNX = fast_ndiff(vX, vX2);
-    float k2part, fermion;
-    if (SYM) {  // the factor 1/2 of the symmetrisation is folded into cpt
-        k2part = fmaf(k2, dip, k2s * dips);
-        fermion = kf * dNX * dN;
-    } else {
-        k2part = k2 * dip;
-        fermion = kf * SY * dNX;
-    }
-    float alpha;
-    if (COUPLING == 2) {
-        alpha = ph.fixed_as;
-    } else if (COUPLING == 4) {
-        alpha = P.alpha_r;
-    } else if (COUPLING == 3) {
-        alpha = alpha_of_log(fminf(fminf(Lmin, P.lr), (0.5f * LN2) * fminf(L2X, L2X2)), ph);
-    } else {
-        const float lmin = fminf(fminf(Lmin, P.lr), (0.5f * LN2) * fminf(L2X, L2X2));
-        const float right = fmaf(-10.0f, lmin, 5.0f * ph.log_sc);
-        const float m = fmaxf(ph.left, right);
-        const float e = ex2_approx(-fabsf(ph.left - right) * L2E);
-        const float lae = fmaf(LN2, lg2_approx(1.0f + e), m);
-        alpha = rcp_approx(ph.b0c * lae);
-        if (COUPLING == 1) alpha = fminf(alpha, ph.alpha_cap);
-    }
-    const float scale = alpha * alpha * cpt;
-    k2w = k2part * scale;
-    kfw = -fermion * scale;
-    const bool ok = valid && fabsf(k2w + kfw) < INFINITY;
-    k2w = ok ? k2w : 0.0f;
-    kfw = ok ? kfw : 0.0f;
-}
 
 // ---------------------------------------------------------------------------
 // Two samples per call on the packed FP32x2 pipe of sm_100 (FFMA2/FADD2/FMUL2): the
 // per-evaluation arithmetic of k2_point_fast, component x for sample 2p and y for 2p+1
 // of a pair record (every field of the two samples side by side), so each packed
 // instruction does the work of two.  MUFU operations, compares and selects stay scalar.
-using f2 = float2;
-__device__ __forceinline__ f2 bc2(float a) { return make_float2(a, a); }
-__device__ __forceinline__ f2 add2(f2 a, f2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ f2 sub2(f2 a, f2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
-__device__ __forceinline__ f2 mul2(f2 a, f2 b) { return __fmul2_rn(a, b); }
-__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) { return __ffma2_rn(a, b, c); }
 __device__ __forceinline__ f2 rcp2(f2 a) { return make_float2(rcp_approx(a.x), rcp_approx(a.y)); }
 __device__ __forceinline__ f2 lg22(f2 a) { return make_float2(lg2_approx(a.x), lg2_approx(a.y)); }
 __device__ __forceinline__ f2 sel2(bool cx, bool cy, f2 a, f2 b) { return make_float2(cx ? a.x : b.x, cy ? a.y : b.y); }

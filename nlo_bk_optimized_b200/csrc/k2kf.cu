@@ -10,9 +10,10 @@
 // of samples (one per thread) in shared memory, and every lane then owns one
 // active parent and sweeps the whole tile, reading the sample records as
 // shared-memory broadcasts.  Per (sample, parent) only X, X', their two spline
-// values, the kernels and the coupling remain.  Lane sums are compensated FP32
-// (Kahan) per tile, folded into FP64 per lane; per-CTA partials go to the caller's
-// workspace and a second kernel adds them in a fixed order (deterministic).
+// values, the kernels and the coupling remain.  In the mixed build lane sums are FP32
+// over 32 samples, folded into FP64 per lane (the FP64 build: compensated sums per
+// tile); per-CTA partials go to the caller's workspace and a second kernel adds them in
+// a fixed order (deterministic).
 
 #include <cuda_runtime.h>
 
@@ -383,18 +384,8 @@ __device__ __forceinline__ void k2_pair_fast(const FastSpline& s, const Phys<flo
     kfw = sel2(ok_x, ok_y, kfw, bc2(0.0f));
 }
 
-// Compensated sums of pairs (Kahan per component, packed).
-struct Kahan2 {
-    f2 sum, comp;
-    __device__ __forceinline__ void reset() { sum = bc2(0.0f); comp = bc2(0.0f); }
-    __device__ __forceinline__ void add(f2 v)
-    {
-        const f2 y = sub2(v, comp);
-        const f2 t = add2(sum, y);
-        comp = sub2(sub2(t, sum), y);
-        sum = t;
-    }
-};
+constexpr int kFoldPairs = 16;
+
 
 template <typename T, bool SYM, int COUPLING>
 __global__ void __launch_bounds__(1024) k2kf_kernel(Phys<T> ph, K2Box<T> box, SobolDirsArg dirs,
@@ -483,21 +474,24 @@ __global__ void __launch_bounds__(1024) k2kf_kernel(Phys<T> ph, K2Box<T> box, So
                 __syncthreads();
                 if (has_parent) {
                     const float4* pr = reinterpret_cast<const float4*>(recs);
-                    Kahan2 sk2, skf;
-                    sk2.reset();
-                    skf.reset();
                     f2 sq = bc2(0.0f);  // variance estimate only: plain sum per tile
                     const int pairs = (count_here + 1) >> 1;
-                    for (int j = 0; j < pairs; ++j) {
-                        f2 k2w, kfw;
-                        k2_pair_fast<SYM, COUPLING>(fs, ph, PF, pr + (kRecLen / 2) * j, k2w, kfw);
-                        sk2.add(k2w);
-                        skf.add(kfw);
-                        const f2 tot = add2(k2w, kfw);
-                        sq = fma2(tot, tot, sq);
+                    // FP32x2 partial sums of 16 pairs (32 samples), folded into FP64: the
+                    // rounding of a 32-term FP32 sum instead of compensated summation
+                    for (int j0 = 0; j0 < pairs; j0 += kFoldPairs) {
+                        const int jn = j0 + kFoldPairs < pairs ? j0 + kFoldPairs : pairs;
+                        f2 pk2 = bc2(0.0f), pkf = bc2(0.0f);
+                        for (int j = j0; j < jn; ++j) {
+                            f2 k2w, kfw;
+                            k2_pair_fast<SYM, COUPLING>(fs, ph, PF, pr + (kRecLen / 2) * j, k2w, kfw);
+                            pk2 = add2(pk2, k2w);
+                            pkf = add2(pkf, kfw);
+                            const f2 tot = add2(k2w, kfw);
+                            sq = fma2(tot, tot, sq);
+                        }
+                        acc_k2 += (double)pk2.x + (double)pk2.y;
+                        acc_kf += (double)pkf.x + (double)pkf.y;
                     }
-                    acc_k2 += ((double)sk2.sum.x - (double)sk2.comp.x) + ((double)sk2.sum.y - (double)sk2.comp.y);
-                    acc_kf += ((double)skf.sum.x - (double)skf.comp.x) + ((double)skf.sum.y - (double)skf.comp.y);
                     acc_sq += (double)sq.x + (double)sq.y;
                 }
             } else {

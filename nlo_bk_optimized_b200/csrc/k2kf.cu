@@ -215,30 +215,6 @@ struct P2S {
     float p2, S;
 };
 
-// floor(uc) for 0 <= uc < 2^23, clamped to `last`, without the XU conversions: adding
-// 2^23 rounded down leaves floor(uc) in the low mantissa bits.
-__device__ __forceinline__ float floor_clamped(float uc, float last)
-{
-    return fminf(__fadd_rd(uc, 8388608.0f) - 8388608.0f, last);
-}
-__device__ __forceinline__ int small_float_to_int(float integral)
-{
-    return __float_as_int(integral + 8388608.0f) - 0x4B000000;
-}
-
-// spline position u = (log X - x0)/h -> (log2 S, S) with the edge encoding
-__device__ __forceinline__ P2S fast_amplitude_at(const FastSpline& s, float u)
-{
-    const float uc = fminf(fmaxf(u, 0.0f), s.u_max);
-    const float fl = floor_clamped(uc, s.last_f);
-    const float t = uc - fl;
-    const float4 c = s.coef[small_float_to_int(fl)];
-    float p2 = fmaf(t, fmaf(t, fmaf(t, c.w, c.z), c.y), c.x);
-    p2 = u < 0.0f ? 0.0f : p2;
-    p2 = u > s.u_max ? -150.0f : p2;
-    return {p2, ex2_approx(p2)};
-}
-
 
 
 
@@ -249,6 +225,28 @@ struct K2ParentF {
 
 // COUPLING: 0 smooth freeze, 1 smooth freeze capped at alpha_cap, 2 fixed, 3 any coupling
 // of alpha_of_log (flavour thresholds), 4 the parent's coupling (RC_NLO = PARENT_NLO).
+
+// Spline position u = (log X - x0)/h -> (log2 S, S) with the edge encoding, for a pair of
+// positions.  floor(uc) (0 <= uc < 2^23, clamped to `last`) comes without the XU
+// conversions: adding 2^23 rounded down leaves it in the low mantissa bits.  The clamp,
+// floor, fraction and index arithmetic run on the packed instructions, the table lookup
+// and the cubic per component.
+__device__ __forceinline__ void fast_amplitude_pair(const FastSpline& s, f2 u, P2S& ax, P2S& ay)
+{
+    const f2 uc = make_float2(fminf(fmaxf(u.x, 0.0f), s.u_max), fminf(fmaxf(u.y, 0.0f), s.u_max));
+    const f2 shifted = __fadd2_rd(uc, bc2(8388608.0f));  // 2^23 + floor(uc)
+    const f2 fl = make_float2(fminf(shifted.x - 8388608.0f, s.last_f), fminf(shifted.y - 8388608.0f, s.last_f));
+    const f2 t = sub2(uc, fl);
+    const f2 fi = add2(fl, bc2(8388608.0f));
+    const float4 cx = s.coef[__float_as_int(fi.x) - 0x4B000000];
+    const float4 cy = s.coef[__float_as_int(fi.y) - 0x4B000000];
+    float px = fmaf(t.x, fmaf(t.x, fmaf(t.x, cx.w, cx.z), cx.y), cx.x);
+    float py = fmaf(t.y, fmaf(t.y, fmaf(t.y, cy.w, cy.z), cy.y), cy.x);
+    px = u.x < 0.0f ? 0.0f : (u.x > s.u_max ? -150.0f : px);
+    py = u.y < 0.0f ? 0.0f : (u.y > s.u_max ? -150.0f : py);
+    ax = {px, ex2_approx(px)};
+    ay = {py, ex2_approx(py)};
+}
 
 // ---------------------------------------------------------------------------
 // Two samples per call on the packed FP32x2 pipe of sm_100 (FFMA2/FADD2/FMUL2): the
@@ -278,7 +276,7 @@ __device__ __forceinline__ f2 fast_ndiff2(const P2S& Ax, const P2S& Ay, const P2
 
 template <bool SYM, int COUPLING>
 __device__ __forceinline__ void k2_pair_fast(const FastSpline& s, const Phys<float>& ph, const K2ParentF& P,
-                                             const float4* __restrict__ rec4, f2& k2w, f2& kfw)
+                                             const float4* __restrict__ rec4, f2& k2w, f2& kfw, f2& total)
 {
     constexpr float LN2 = 0.69314718055994531f;
     constexpr float L2E = 1.4426950408889634f;
@@ -303,8 +301,9 @@ __device__ __forceinline__ void k2_pair_fast(const FastSpline& s, const Phys<flo
     const bool valid_y = Xsq.y >= 1e-38f && X2sq.y >= 1e-38f;
     const f2 L2X = lg22(Xsq), L2X2 = lg22(X2sq);
     const f2 uX = fma2(L2X, bc2(s.u_scale), bc2(s.u_off)), uX2 = fma2(L2X2, bc2(s.u_scale), bc2(s.u_off));
-    const P2S vXx = fast_amplitude_at(s, uX.x), vXy = fast_amplitude_at(s, uX.y);
-    const P2S vX2x = fast_amplitude_at(s, uX2.x), vX2y = fast_amplitude_at(s, uX2.y);
+    P2S vXx, vXy, vX2x, vX2y;
+    fast_amplitude_pair(s, uX, vXx, vXy);
+    fast_amplitude_pair(s, uX2, vX2x, vX2y);
     // kernels
     const f2 a = mul2(Xsq, z2sq), b = mul2(X2sq, zsq);
     const f2 rs = rcp2(add2(a, b));
@@ -382,6 +381,7 @@ __device__ __forceinline__ void k2_pair_fast(const FastSpline& s, const Phys<flo
     const bool ok_y = valid_y && fabsf(tot.y) < INFINITY;
     k2w = sel2(ok_x, ok_y, k2w, bc2(0.0f));
     kfw = sel2(ok_x, ok_y, kfw, bc2(0.0f));
+    total = sel2(ok_x, ok_y, tot, bc2(0.0f));
 }
 
 constexpr int kFoldPairs = 16;
@@ -482,11 +482,10 @@ __global__ void __launch_bounds__(1024) k2kf_kernel(Phys<T> ph, K2Box<T> box, So
                         const int jn = j0 + kFoldPairs < pairs ? j0 + kFoldPairs : pairs;
                         f2 pk2 = bc2(0.0f), pkf = bc2(0.0f);
                         for (int j = j0; j < jn; ++j) {
-                            f2 k2w, kfw;
-                            k2_pair_fast<SYM, COUPLING>(fs, ph, PF, pr + (kRecLen / 2) * j, k2w, kfw);
+                            f2 k2w, kfw, tot;
+                            k2_pair_fast<SYM, COUPLING>(fs, ph, PF, pr + (kRecLen / 2) * j, k2w, kfw, tot);
                             pk2 = add2(pk2, k2w);
                             pkf = add2(pkf, kfw);
-                            const f2 tot = add2(k2w, kfw);
                             sq = fma2(tot, tot, sq);
                         }
                         acc_k2 += (double)pk2.x + (double)pk2.y;

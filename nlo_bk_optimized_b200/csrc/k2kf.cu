@@ -260,6 +260,11 @@ __device__ __forceinline__ f2 sel2(bool cx, bool cy, f2 a, f2 b) { return make_f
 // N_A - N_B from log2 S values, for a pair
 __device__ __forceinline__ f2 fast_ndiff2(const P2S& Ax, const P2S& Ay, const P2S& Bx, const P2S& By)
 {
+    // N_A - N_B = S_B - S_A.  Near each other (|pB - pA| < 1/2 in log2 units) it is
+    // S_A (2^(pB-pA) - 1) or -S_B (2^(pA-pB) - 1) with 2^x - 1 = x q(x), q a degree-5
+    // polynomial fitted to (2^x - 1)/x on [-1/2, 0] (1.2e-7 relative in FP32); farther
+    // apart the plain difference S_B - S_A has no cancellation (the ratio is at least
+    // sqrt(2)), and both S are at hand.
     const f2 d = make_float2(Bx.p2 - Ax.p2, By.p2 - Ay.p2);
     const f2 x = make_float2(-fabsf(d.x), -fabsf(d.y));
     f2 q = fma2(bc2(0.0001327910803141678f), x, bc2(0.001321632968973654f));
@@ -267,11 +272,10 @@ __device__ __forceinline__ f2 fast_ndiff2(const P2S& Ax, const P2S& Ay, const P2
     q = fma2(q, x, bc2(0.05550375169709732f));
     q = fma2(q, x, bc2(0.24022649146109623f));
     q = fma2(q, x, bc2(0.6931471804499034f));
-    const f2 poly = mul2(q, x);
-    const f2 e = make_float2(x.x > -0.5f ? poly.x : ex2_approx(x.x) - 1.0f,
-                             x.y > -0.5f ? poly.y : ex2_approx(x.y) - 1.0f);
     const f2 S = make_float2(d.x <= 0.0f ? Ax.S : -Bx.S, d.y <= 0.0f ? Ay.S : -By.S);
-    return mul2(S, e);
+    const f2 near = mul2(S, mul2(q, x));
+    const f2 far = make_float2(Bx.S - Ax.S, By.S - Ay.S);
+    return make_float2(x.x > -0.5f ? near.x : far.x, x.y > -0.5f ? near.y : far.y);
 }
 
 template <bool SYM, int COUPLING>

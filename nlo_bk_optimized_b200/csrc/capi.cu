@@ -136,10 +136,35 @@ RhsBuffers carve(void* ws, int points)
     return b;
 }
 
+// A side stream for K1: K1 and K2+Kf read the same spline and active list and write
+// different buffers, so K1 runs beside K2+Kf and its last, partly filled wave of CTAs
+// overlaps the start of K2+Kf instead of idling most SMs.  One per evolve/rhs call.
+struct SideStream {
+    cudaStream_t aux = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+    bool ok = false;
+    SideStream()
+    {
+        ok = cudaStreamCreateWithFlags(&aux, cudaStreamNonBlocking) == cudaSuccess &&
+             cudaEventCreateWithFlags(&fork, cudaEventDisableTiming) == cudaSuccess &&
+             cudaEventCreateWithFlags(&join, cudaEventDisableTiming) == cudaSuccess;
+        if (!ok) cudaGetLastError();  // fall back to one stream
+    }
+    ~SideStream()
+    {
+        if (join) cudaEventDestroy(join);
+        if (fork) cudaEventDestroy(fork);
+        if (aux) cudaStreamDestroy(aux);
+    }
+    SideStream(const SideStream&) = delete;
+    SideStream& operator=(const SideStream&) = delete;
+};
+
 int run_rhs(const nlo_bk_params& p, const double* r, const double* N, int points, const SobolDirsArg& dirs,
             uint64_t samples, const nlo_bk_box& box, double* dndy, double* k1_out, double* k2kf_out,
             const RhsBuffers& b, bool factor_ready, cudaStream_t stream, int shard = 0, int shards = 1,
-            const double* hist_y = nullptr, const double* hist_N = nullptr, int rows = 0)
+            const double* hist_y = nullptr, const double* hist_N = nullptr, int rows = 0,
+            const SideStream* side = nullptr)
 {
     cudaError_t e;
     K1History history;
@@ -156,14 +181,23 @@ int run_rhs(const nlo_bk_params& p, const double* r, const double* N, int points
         return cuda_fail(e, "splines");
     if ((e = launch_active(N, points, shard, shards, b.active, b.count, stream)) != cudaSuccess)
         return cuda_fail(e, "active");
-    if ((e = launch_k1(p, r, points, b.spline, b.active, b.count, b.k1, stream, history)) != cudaSuccess)
+    const bool beside = side && side->ok;
+    cudaStream_t k1_stream = stream;
+    if (beside) {
+        if ((e = cudaEventRecord(side->fork, stream)) != cudaSuccess) return cuda_fail(e, "fork");
+        if ((e = cudaStreamWaitEvent(side->aux, side->fork, 0)) != cudaSuccess) return cuda_fail(e, "fork");
+        k1_stream = side->aux;
+    }
+    if ((e = launch_k1(p, r, points, b.spline, b.active, b.count, b.k1, k1_stream, history)) != cudaSuccess)
         return cuda_fail(e, "k1");
+    if (beside && (e = cudaEventRecord(side->join, side->aux)) != cudaSuccess) return cuda_fail(e, "join");
     // orders without NLO kernels (Order.has_nlo_kernels, bk/config.py:44-50) take no K2 + Kf:
     // zero samples clear the sums and launch nothing
     const uint64_t nlo_samples = order_has_nlo(p.order) ? samples : 0;
     if ((e = launch_k2kf(p, r, points, b.spline, b.active, b.count, dirs, 0, nlo_samples, box, b.k2kf, b.partial,
                          b.k2kf_blocks, stream)) != cudaSuccess)
         return cuda_fail(e, "k2kf");
+    if (beside && (e = cudaStreamWaitEvent(stream, side->join, 0)) != cudaSuccess) return cuda_fail(e, "join");
     if ((e = launch_assemble(b.k1, b.k2kf, points, nlo_samples ? 1.0 / (double)nlo_samples : 0.0, dndy, k2kf_out,
                              stream)) != cudaSuccess)
         return cuda_fail(e, "assemble");
@@ -331,8 +365,9 @@ int nlo_bk_rhs(const nlo_bk_params* params, const double* r, const double* N, in
     if (!workspace || workspace_bytes < nlo_bk_rhs_workspace_bytes(points))
         return fail(NLO_ERR_WORKSPACE, "workspace too small for nlo_bk_rhs");
     const RhsBuffers b = carve(workspace, points);
+    const SideStream side;
     return run_rhs(*params, r, N, points, to_arg(dirs), (uint64_t)samples, *box, dndy, k1, k2kf, b, false,
-                   (cudaStream_t)stream);
+                   (cudaStream_t)stream, 0, 1, nullptr, nullptr, 0, &side);
 }
 
 int nlo_bk_rhs_shard(const nlo_bk_params* params, const double* r, const double* N, int32_t points, int32_t shard,
@@ -352,8 +387,9 @@ int nlo_bk_rhs_shard(const nlo_bk_params* params, const double* r, const double*
     if (!workspace || workspace_bytes < nlo_bk_rhs_workspace_bytes(points))
         return fail(NLO_ERR_WORKSPACE, "workspace too small for nlo_bk_rhs_shard");
     const RhsBuffers b = carve(workspace, points);
+    const SideStream side;
     return run_rhs(*params, r, N, points, to_arg(dirs), (uint64_t)samples, *box, dndy, nullptr, nullptr, b, false,
-                   (cudaStream_t)stream, shard, shards);
+                   (cudaStream_t)stream, shard, shards, nullptr, nullptr, 0, &side);
 }
 
 int nlo_bk_stage(const double* N, const double* const* k, const double* coef, int32_t nk, int32_t points,
@@ -384,8 +420,9 @@ int nlo_bk_rhs_history(const nlo_bk_params* params, const double* r, int32_t poi
         return fail(NLO_ERR_WORKSPACE, "workspace too small for nlo_bk_rhs_history");
     const RhsBuffers b = carve(workspace, points);
     const double* N = hist_N + (size_t)(rows - 1) * points;
+    const SideStream side;
     return run_rhs(*params, r, N, points, to_arg(dirs), (uint64_t)samples, *box, dndy, k1, k2kf, b, false,
-                   (cudaStream_t)stream, 0, 1, hist_y, hist_N, rows);
+                   (cudaStream_t)stream, 0, 1, hist_y, hist_N, rows, &side);
 }
 
 // Rows first+1..first+steps of `table` from row `first` (the loop of _bk_steps,
@@ -420,6 +457,7 @@ static int evolve_rows(const nlo_bk_params* params, const double* r, int32_t poi
     cudaError_t e = cudaMemsetAsync(status, 0, sizeof(uint32_t), s);
     if (e != cudaSuccess) return cuda_fail(e, "status reset");
     const int clamp = params->force_positive ? 1 : 0;
+    const SideStream side;
     for (int it = first; it < first + steps; ++it) {
         const double* N = table + (size_t)it * points;
         double* next = table + (size_t)(it + 1) * points;
@@ -428,7 +466,7 @@ static int evolve_rows(const nlo_bk_params* params, const double* r, int32_t poi
         bool factor_ready = it > first;
         auto f = [&](const double* in, double* out) {
             const int code = run_rhs(*params, r, in, points, dirs_arg, (uint64_t)samples, *box, out, nullptr,
-                                     nullptr, b, factor_ready, s, 0, 1, y, table, it + 1);
+                                     nullptr, b, factor_ready, s, 0, 1, y, table, it + 1, &side);
             factor_ready = true;
             return code;
         };

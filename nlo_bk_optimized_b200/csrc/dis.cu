@@ -51,6 +51,8 @@ __global__ void table_prepare_kernel(const double* __restrict__ r, const double*
         hdr[kHdrLogR0] = ::log(r[0]);
         hdr[kHdrInvDlogR] = (nr - 1) / (::log(r[nr - 1]) - ::log(r[0]));
         hdr[kHdrInterp] = interp;
+        hdr[kHdrY0] = y[0] + y0;
+        hdr[kHdrInvDY] = ny > 1 ? (ny - 1) / ((y[ny - 1] + y0) - (y[0] + y0)) : 0.0;
     }
     // window weights: second derivatives of the natural spline through the 7/9 window
     // points as linear maps of the window values (one Thomas solve per unit vector)
@@ -99,6 +101,38 @@ __global__ void table_prepare_kernel(const double* __restrict__ r, const double*
         }
     }
     (void)v;
+}
+
+// Per-row coefficients of the local splines: for table row k and r interval i, the
+// window spline through row k's values (second derivatives from the window weights),
+// in the power form a + b dx + c dx^2 + d dx^3 on [r_i, r_{i+1}).
+__global__ void table_local_kernel(double* table, int nr, int ny)
+{
+    const TableView v = table_view(table, nr, ny);
+    double* local = table + (v.local - table);
+    const int64_t total = (int64_t)ny * (nr - 1);
+    for (int64_t item = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; item < total;
+         item += (int64_t)gridDim.x * blockDim.x) {
+        const int k = (int)(item / (nr - 1));
+        const int i = (int)(item - (int64_t)k * (nr - 1));
+        const double* w = v.window + (size_t)i * kWindowStride;
+        const int start = (int)w[0];
+        const int points = (int)w[1];
+        const int j = i - start;
+        const double* vals = v.N + (size_t)k * nr + start;
+        double mj = 0.0, mj1 = 0.0;
+        for (int q = 0; q < points; ++q) {
+            mj = fma(w[2 + q], vals[q], mj);
+            mj1 = fma(w[2 + kWindowMax + q], vals[q], mj1);
+        }
+        const double vj = vals[j], vj1 = vals[j + 1];
+        const double h = v.r[i + 1] - v.r[i];
+        double* out = local + (size_t)item * 4;
+        out[0] = vj;
+        out[1] = (vj1 - vj) / h - h * (2.0 * mj + mj1) / 6.0;
+        out[2] = mj / 2.0;
+        out[3] = (mj1 - mj) / (6.0 * h);
+    }
 }
 
 // initialize_interpolation (dipole/amplitude.py:105-133) and _find_maxr_interpolate
@@ -591,6 +625,12 @@ cudaError_t dis_launch_table_prepare(const double* r, const double* y, const dou
     int blocks = (nr * ny + 255) / 256;
     blocks = blocks > 1024 ? 1024 : (blocks < 1 ? 1 : blocks);
     dis::table_prepare_kernel<<<blocks, 256, 0, stream>>>(r, y, N, nr, ny, y0, interp, table);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    int64_t items = (int64_t)ny * (nr - 1);
+    int64_t local_blocks = (items + 255) / 256;
+    local_blocks = local_blocks > 2048 ? 2048 : (local_blocks < 1 ? 1 : local_blocks);
+    dis::table_local_kernel<<<(unsigned)local_blocks, 256, 0, stream>>>(table, nr, ny);
     return cudaGetLastError();
 }
 

@@ -76,6 +76,23 @@ __device__ __forceinline__ T amplitude(const DisArgs<T>& a, double r, double Y)
     return gbw_amplitude(a.gbw, (T)r, (T)Y);
 }
 
+// The three dipoles of a qg sample at one rapidity: a table looks its rows up once.
+template <typename T>
+__device__ __forceinline__ void amplitudes3(const DisArgs<T>& a, double r01, double r02, double r21, double Y, T& N01,
+                                            T& N02, T& N21)
+{
+    if (a.table) {
+        const TableRow row = table_row(a.tab, Y);
+        N01 = (T)table_amplitude_at(a.tab, row, r01);
+        N02 = (T)table_amplitude_at(a.tab, row, r02);
+        N21 = (T)table_amplitude_at(a.tab, row, r21);
+    } else {
+        N01 = gbw_amplitude(a.gbw, (T)r01, (T)Y);
+        N02 = gbw_amplitude(a.gbw, (T)r02, (T)Y);
+        N21 = gbw_amplitude(a.gbw, (T)r21, (T)Y);
+    }
+}
+
 template <typename T>
 __device__ __forceinline__ double dipole_min_r(const DisArgs<T>& a)
 {
@@ -865,9 +882,11 @@ __device__ T qg_term(const DisArgs<T>& a, const double* x, const InnerRule& rule
     const double jac = (1.0 - z2min) * (1.0 - z1 - z2min) * x01 * x02 * a.maxr * a.maxr * 2.0 * kPi;
     const double Y = ::log(a.W2 * z2 / kQ0sqr);
     if (!(Y >= 0.0)) return (T)0;
-    const T S01 = (T)1 - amplitude(a, x01, Y);
-    const T S02 = (T)1 - amplitude(a, x02, Y);
-    const T S12 = (T)1 - amplitude(a, x21, Y);
+    T N01, N02, N21;
+    amplitudes3(a, x01, x02, x21, Y, N01, N02, N21);
+    const T S01 = (T)1 - N01;
+    const T S02 = (T)1 - N02;
+    const T S12 = (T)1 - N21;
     const T N012 = a.finite_nc ? (T)1 - (T)(kNc / (2.0 * kCF)) * (S02 * S12 - S01 / (T)(kNc * kNc))
                                : (T)1 - S02 * S12;
     const double ra = a.parent_coupling ? x01 : fmin(x01, fmin(x02, x21));
@@ -923,9 +942,11 @@ __device__ void qg_triple(const DisArgs<T>& a, const double* x, const InnerRule&
     const double jac = (1.0 - z2min) * (1.0 - z1 - z2min) * x01 * x02 * a.maxr * a.maxr * 2.0 * kPi;
     const double Y = ::log(a.W2 * z2 / kQ0sqr);
     if (!(Y >= 0.0)) return;
-    const T S01 = (T)1 - amplitude(a, x01, Y);
-    const T S02 = (T)1 - amplitude(a, x02, Y);
-    const T S12 = (T)1 - amplitude(a, x21, Y);
+    T N01, N02, N21;
+    amplitudes3(a, x01, x02, x21, Y, N01, N02, N21);
+    const T S01 = (T)1 - N01;
+    const T S02 = (T)1 - N02;
+    const T S12 = (T)1 - N21;
     const T N012 = a.finite_nc ? (T)1 - (T)(kNc / (2.0 * kCF)) * (S02 * S12 - S01 / (T)(kNc * kNc))
                                : (T)1 - S02 * S12;
     const double ra = a.parent_coupling ? x01 : fmin(x01, fmin(x02, x21));

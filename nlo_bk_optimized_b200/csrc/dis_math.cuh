@@ -113,6 +113,13 @@ __device__ __forceinline__ float ex2_approx_f(float x)
     return y;
 }
 
+__device__ __forceinline__ float lg2_approx_f(float x)
+{
+    float y;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 __device__ __forceinline__ float rcp_approx_f(float x)
 {
     float y;
@@ -132,6 +139,10 @@ __device__ __forceinline__ float exp_neg_f(float x)
     return ex2_approx_f(-hi) * fmaf(-lo, 0.69314718055994531f, 1.0f);
 }
 
+// FP32 K0 and K1: the series in t = x^2/4 up to x = 2, e^-x/sqrt(x) times a polynomial
+// in 2/x above.  log(x/2) comes from the hardware log2 (absolute error near 1e-7), which
+// near x = 2, where log(x/2) -> 0, bounds the relative error of K0 by about 3e-6; the
+// FP32 build's integrals are held to 1e-4 of the FP64 ones.
 __device__ __forceinline__ K01<float> bessel_k01(float x)
 {
     using namespace nlo_special;
@@ -139,7 +150,7 @@ __device__ __forceinline__ K01<float> bessel_k01(float x)
     const float rx = rcp_approx_f(x);
     if (x <= 2.0f) {
         const float t = 0.25f * x * x;
-        const float L = logf(0.5f * x);
+        const float L = 0.69314718055994531f * lg2_approx_f(0.5f * x);
         out.k0 = fmaf(-L, horner(kI0SeriesF, t), horner(kQ0SeriesF, t));
         out.k1 = rx + 0.5f * x * fmaf(L, horner(kI1SeriesF, t), -0.5f * horner(kQ1SeriesF, t));
     } else {

@@ -766,7 +766,7 @@ __device__ __forceinline__ K01<float> bessel_k01_rcp(float x, float& rx)
     rx = rcp_approx_f(x);
     if (x <= 2.0f) {
         const float t = 0.25f * x * x;
-        const float L = logf(0.5f * x);
+        const float L = 0.69314718055994531f * lg2_approx_f(0.5f * x);
         out.k0 = fmaf(-L, horner(kI0SeriesF, t), horner(kQ0SeriesF, t));
         out.k1 = rx + 0.5f * x * fmaf(L, horner(kI1SeriesF, t), -0.5f * horner(kQ1SeriesF, t));
     } else {

@@ -277,6 +277,14 @@ def run_ours(args) -> None:
     # end to end through the public API with host buffers: host IC -> device -> evolve -> host table
     e2e_config = config
     e2e_maxy = steps * STEP
+    # one untimed call of the same API (one step) first, as the device leg has its warm-up
+    # steps: the first call of a process pays one-time module loading and host setup
+    if world == 1:
+        solve_bk(MV(qs0sqr=QS0SQR), STEP, e2e_config, device=device, dtype=torch.float32, seed=0).N.cpu()
+    else:
+        from nlo_bk_optimized_b200.bk.sharded import solve_bk_sharded
+
+        solve_bk_sharded(MV(qs0sqr=QS0SQR), STEP, e2e_config, device=device, dtype=torch.float32, seed=0).N.cpu()
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()

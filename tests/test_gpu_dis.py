@@ -135,6 +135,67 @@ def test_amplitudes(dtype):
     assert rel_err(init, GOLDEN["amp_init"]) < 1e-12
 
 
+@pytest.mark.parametrize("interpolation", ["spline_linear", "linear_linear"])
+def test_table_irregular_grids(interpolation):
+    """Tables whose r knots sit up to 0.9 % off the logarithmic grid (BKDipole accepts 1 %)
+    and whose rows are unevenly spaced in Y: the device finds the r interval and the two
+    rows from a uniform-grid guess, corrected against the knots or replaced by a search;
+    amplitudes on and between the knots, below and above the r range and on the rows
+    equal the oracle's (dipole/amplitude.py:135-252)."""
+    from nlo_bk_optimized_b200.dipole import AmplitudeInterpolation, BKDipole, DipoleTable
+
+    rng = np.random.default_rng(11)
+    r = np.geomspace(1e-6, 50.0, 80) * (1.0 + 0.009 * rng.uniform(-1.0, 1.0, 80))
+    r[0], r[1] = 1e-6, 1e-6 * (50.0 / 1e-6) ** (1 / 79)  # the check measures from the first ratio
+    y = np.array([0.0, 0.05, 0.1, 0.9, 1.0, 3.5, 3.6, 7.0, 12.0])
+    N = 1.0 - np.exp(-np.outer(0.3 * np.exp(0.3 * y), r * r) / 4.0)
+    rr = np.exp(rng.uniform(math.log(5e-7), math.log(60.0), 3000))
+    YY = rng.uniform(0.0, 12.0, 3000)
+    rr[: r.size] = r
+    YY[: y.size] = y
+    YY[y.size : 2 * y.size] = y[::-1]
+    mode = AmplitudeInterpolation.LINEAR_LINEAR if interpolation == "linear_linear" else None
+    kwargs = {"interpolation": mode} if mode is not None else {}
+    tab = BKDipole(DipoleTable(dev(r), dev(y), dev(N), 1.0), **kwargs)
+    got = tab.dipole_amplitude(dev(rr), dev(YY)).cpu().numpy()
+    ref = od.TableDipole(r, y, N, 1.0, interpolation=interpolation)(rr, YY)
+    assert rel_err(got, ref) < 1e-12
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_table_clustered_r_grid_c_abi(lib, mode):
+    """The C ABI takes any increasing r grid (BKDipole, like the reference, insists on a
+    logarithmic one): on knots clustered in three bands the log-grid guess misses the
+    interval by up to 20 and the lookup falls back to its search; amplitudes still equal
+    the oracle's table (dipole/amplitude.py:135-252)."""
+    import ctypes
+
+    from nlo_bk_optimized_b200 import _native
+
+    r = np.concatenate([np.geomspace(1e-6, 1e-3, 12), np.geomspace(1.1e-3, 2.0, 60), np.geomspace(2.3, 50.0, 8)])
+    y = np.array([0.0, 0.05, 0.1, 0.9, 1.0, 3.5, 3.6, 7.0, 12.0])
+    N = 1.0 - np.exp(-np.outer(0.3 * np.exp(0.3 * y), r * r) / 4.0)
+    rng = np.random.default_rng(5)
+    rr = np.exp(rng.uniform(math.log(5e-7), math.log(60.0), 3000))
+    YY = rng.uniform(0.0, 12.0, 3000)
+    rr[: r.size] = r
+    table = torch.empty(int(lib.nlo_dis_table_doubles(r.size, y.size)), dtype=torch.float64, device="cuda")
+    stream = _native.stream_handle(torch.device("cuda", torch.cuda.current_device()))
+    r_dev, y_dev, N_dev = dev(r), dev(y), dev(N)  # held until the prepare kernel has read them
+    _native.check(lib.nlo_dis_table_prepare_interpolated(r_dev.data_ptr(), y_dev.data_ptr(), N_dev.data_ptr(),
+                                                         r.size, y.size, 1.0, mode, table.data_ptr(), stream))
+    d = _native.Dipole()
+    d.kind = _native.DIPOLE_TABLE
+    d.table = table.data_ptr()
+    d.nr, d.ny = r.size, y.size
+    rd, Yd = dev(rr), dev(YY)
+    out = torch.empty_like(rd)
+    _native.check(lib.nlo_dis_dipole_amplitude(ctypes.byref(d), rd.data_ptr(), Yd.data_ptr(), rd.numel(),
+                                                _native.PRECISION_FP64, out.data_ptr(), stream))
+    ref = od.TableDipole(r, y, N, 1.0, interpolation="linear_linear" if mode else "spline_linear")(rr, YY)
+    assert rel_err(out.cpu().numpy(), ref) < 1e-12
+
+
 def bilinear_obj():
     from nlo_bk_optimized_b200.dipole import AmplitudeInterpolation, BKDipole, DipoleTable
 

@@ -402,9 +402,11 @@ struct K1Consts {
 
 // TF: arithmetic of the regular intervals (float in the mixed build); KC: the
 // kinematical constraint (a separate instantiation keeps the history code out of the
-// production kernel's registers).
+// production kernel's registers).  Without the constraint the kernel is bounded to four
+// CTAs per SM (64 registers): its dependent integrand chain is latency-bound, and the
+// extra warps gain more than the few values spilled to the stack cost.
 template <typename TF, bool KC>
-__global__ void __cluster_dims__(1, kK1Split, 1) __launch_bounds__(kK1Threads)
+__global__ void __cluster_dims__(1, kK1Split, 1) __launch_bounds__(kK1Threads, KC ? 1 : 4)
     k1_kernel(Phys<TF> phf, Phys<double> phd, K1Consts consts, K1History history,
                                                         const double* __restrict__ r_grid, int n,
                                                         const double* __restrict__ spline,

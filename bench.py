@@ -51,10 +51,14 @@ RPOINTS = 399
 MINR, MAXR = 1e-7, 1e2
 SAMPLES = 1 << 20
 QS0SQR = 0.2
-# Hand count of FP32 operations in k2_point<float, true> (csrc/k2kf.cu) per
-# (sample, parent) evaluation: FMA = 2, every other arithmetic op or MUFU
-# transcendental = 1, compares/selects excluded.
-FLOPS_PER_EVAL = 181
+# Hand count of the FP32 operations of one (sample, parent) evaluation in
+# k2_pair_fast<true, 0> (csrc/k2kf.cu), per component of the packed pair: FMA = 2,
+# every other arithmetic op or MUFU transcendental = 1, compares, selects and min/max
+# excluded.  11 of them are MUFU operations (2 lg2 and 2 ex2 for the amplitudes at X and
+# X2, 4 rcp in the kernels, ex2 + lg2 + rcp in the coupling).
+FLOPS_PER_EVAL = 136
+MUFU_PER_EVAL = 11
+MUFU_PER_SM_PER_CLOCK = 16
 # Launches of our kernels per RK4 step: 4 right-hand sides x (spline refit, active
 # list, K1, K2+Kf, K2+Kf finalize, assemble) + 4 stage combinations.
 LAUNCHES_PER_STEP = 4 * 6 + 4
@@ -324,9 +328,16 @@ def run_ours(args) -> None:
         "unit": "TFLOP/s",
         "frac": round(achieved / peak, 4),
         "traffic": None,
-        "kernel": "k2kf_kernel<float,true> (csrc/k2kf.cu)",
+        "kernel": "k2kf_kernel<float,true,0> (csrc/k2kf.cu)",
         "peak_source": "nominal FP32 (148 SM x 128 lanes x 2 x 1965 MHz); MEASURED_PEAKS.json has only HBM and bf16",
         "flops_per_eval": FLOPS_PER_EVAL,
+        "mufu": {
+            "ops_per_eval": MUFU_PER_EVAL,
+            "achieved_per_s": round(evals * MUFU_PER_EVAL / (k2_ms * 1e-3), 1),
+            "peak_per_s": SM_COUNT * MUFU_PER_SM_PER_CLOCK * sm_mhz * 1e6,
+            "frac": round(evals * MUFU_PER_EVAL / (k2_ms * 1e-3) / (SM_COUNT * MUFU_PER_SM_PER_CLOCK * sm_mhz * 1e6), 4),
+            "peak_source": "nominal 16 MUFU operations per SM per clock at 1965 MHz",
+        },
         "evals_per_launch": evals,
         "launch_ms": round(k2_ms, 4),
         "evals_per_s": round(evals / (k2_ms * 1e-3), 1),

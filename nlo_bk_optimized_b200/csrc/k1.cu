@@ -402,8 +402,9 @@ struct K1Consts {
 
 // TF: arithmetic of the regular intervals (float in the mixed build); KC: the
 // kinematical constraint (a separate instantiation keeps the history code out of the
-// production kernel's registers).  Without the constraint the kernel is bounded to four
-// CTAs per SM (64 registers): its dependent integrand chain is latency-bound, and the
+// production kernel's registers).  Without the constraint four CTAs share an SM: 64
+// registers a thread and about 51 KB of shared memory a CTA (the FP64 coefficients
+// stay in global memory).  The dependent integrand chain is latency-bound, and the
 // extra warps gain more than the few values spilled to the stack cost.
 template <typename TF, bool KC>
 __global__ void __cluster_dims__(1, kK1Split, 1) __launch_bounds__(kK1Threads, KC ? 1 : 4)
@@ -432,7 +433,6 @@ __global__ void __cluster_dims__(1, kK1Split, 1) __launch_bounds__(kK1Threads, K
         return p;
     };
     double* x64 = reinterpret_cast<double*>(carve(sizeof(double) * n));
-    double* c64 = reinterpret_cast<double*>(carve(sizeof(double) * 4 * (n - 1)));
     TF* xf = reinterpret_cast<TF*>(carve(sizeof(TF) * n));
     TF* cf = reinterpret_cast<TF*>(carve(sizeof(TF) * 4 * (n - 1)));
     K1Z<TF>* zt = reinterpret_cast<K1Z<TF>*>(carve(sizeof(K1Z<TF>) * per_split));
@@ -447,10 +447,7 @@ __global__ void __cluster_dims__(1, kK1Split, 1) __launch_bounds__(kK1Threads, K
         x64[i] = spline[i] - x_knot;
         xf[i] = (TF)(spline[i] - x_knot);
     }
-    for (int i = threadIdx.x; i < 4 * (n - 1); i += blockDim.x) {
-        c64[i] = src_coef[i];
-        cf[i] = (TF)src_coef[i];
-    }
+    for (int i = threadIdx.x; i < 4 * (n - 1); i += blockDim.x) cf[i] = (TF)src_coef[i];
     if (threadIdx.x < 24) {
         sh2f[threadIdx.x] = (TF)consts.sh2[threadIdx.x];
         awf[threadIdx.x] = (TF)consts.aw[threadIdx.x];
@@ -458,7 +455,9 @@ __global__ void __cluster_dims__(1, kK1Split, 1) __launch_bounds__(kK1Threads, K
     if (threadIdx.x < 16) zdw[threadIdx.x] = 0.0;
     __syncthreads();
     SplineView<double> sd;
-    sd.x = x64; sd.coef = c64; sd.n = n; sd.x0 = x64[0];
+    // the FP64 panel nodes read the coefficients from global memory (L1/L2): keeping them
+    // out of shared memory lets four CTAs share an SM
+    sd.x = x64; sd.coef = src_coef; sd.n = n; sd.x0 = x64[0];
     sd.inv_h = (double)(n - 1) / (x64[n - 1] - x64[0]);
     SplineView<TF> sf;
     sf.x = xf; sf.coef = cf; sf.n = n; sf.x0 = xf[0];
@@ -609,7 +608,7 @@ cudaError_t launch_k1(const nlo_bk_params& p, const double* r, int points, const
     const size_t per_split = (size_t)((points - 1 + kK1Split - 1) / kK1Split) * 8;
     auto smem_for = [&](size_t tf) {
         auto a16 = [](size_t v) { return (v + 15) & ~(size_t)15; };
-        return a16(8 * (size_t)points) + a16(8 * 4 * (size_t)(points - 1)) + a16(tf * (size_t)points) +
+        return a16(8 * (size_t)points) + a16(tf * (size_t)points) +
                a16(tf * 4 * (size_t)(points - 1)) + a16((tf == 4 ? sizeof(K1Z<float>) : sizeof(K1Z<double>)) * per_split) +
                a16(8 * per_split) + a16(sizeof(K1Z<double>) * 16) + a16(8 * 16);
     };

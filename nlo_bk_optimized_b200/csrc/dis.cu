@@ -289,8 +289,18 @@ __global__ void gauss_legendre_kernel(const DisArgs<T>* __restrict__ args, Inner
 
 // partial layout per (job, block): [total, total2, hist[D][bins]] doubles and
 // count[D][bins] int32 in a parallel array
+// CTAs per SM the register bound aims at: the FP32 LO and dipole terms are latency-bound
+// and run faster at four (64 registers); the qqbar-g terms keep three (80 registers),
+// where the nested ones issue an instruction nearly every cycle and I1 gains nothing
+// from a fourth CTA but spills.
 template <typename T, int TERM>
-__global__ void __launch_bounds__(kVegasThreads, 3) vegas_iteration_kernel(
+constexpr int vegas_min_blocks()
+{
+    return sizeof(T) == 4 && TERM <= kTermDip2 ? 4 : 3;
+}
+
+template <typename T, int TERM>
+__global__ void __launch_bounds__(kVegasThreads, (vegas_min_blocks<T, TERM>())) vegas_iteration_kernel(
     const DisArgs<T>* __restrict__ args, const SobolDirsArg* __restrict__ dirs, InnerRule rule,
     double* __restrict__ state, int state_stride, int bins, uint64_t offset, uint64_t samples, int blocks_per_job,
     double* __restrict__ partial, int32_t* __restrict__ counts)

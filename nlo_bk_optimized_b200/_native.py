@@ -276,10 +276,6 @@ def require_cuda(tensor: torch.Tensor, name: str) -> None:
         raise ValueError(f"{name} must be contiguous")
 
 
-def ptr(tensor: torch.Tensor | None) -> int | None:
-    return None if tensor is None else tensor.data_ptr()
-
-
 def stream_handle(device: torch.device) -> int:
     return torch.cuda.current_stream(device).cuda_stream
 

@@ -203,17 +203,6 @@ __device__ __forceinline__ T alpha_of_log(T log_d, const Phys<T>& ph)
     return a;
 }
 
-// logaddexp(c, t + delta) - logaddexp(c, t) without cancellation.
-template <typename T>
-__device__ __forceinline__ T lae_difference(T c, T t, T delta)
-{
-    const T sigma = M<T>::rcp((T)1 + M<T>::exp_fast(c - t));
-    const T v = sigma * M<T>::expm1(delta);
-    if (v > (T)-0.5) return M<T>::log1p(v);
-    const T sigma_c = M<T>::rcp((T)1 + M<T>::exp_fast(t - c));
-    return M<T>::log_acc(sigma_c + sigma * M<T>::exp_fast(delta));
-}
-
 // ---------------------------------------------------------------------------
 // Log-log spline in shared memory: knots x[n] (log r), coefficients (a,b,c,d) per interval.
 // The r grid is logarithmically uniform, so the interval is found in O(1) from

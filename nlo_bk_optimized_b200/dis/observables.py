@@ -561,13 +561,6 @@ def _integrand(term: int, x: torch.Tensor, kin: _native.DisKinematics, dipole: D
     return out.to(x.dtype)
 
 
-def integrand_photon_target_LO_unit(x: torch.Tensor, Q2: float, xbj: float, polarization: Polarization,
-                                    dipole: Dipole, config: DISConfig) -> torch.Tensor:
-    """The LO integrand on the unit square with its 2 pi r maxr Jacobian
-    (dis/observables.py:352-359)."""
-    return _integrand(TERMS["LO"], x, kinematics(float(Q2), float(xbj), polarization, config), dipole, config)
-
-
 def integrand_dip_massive(x: torch.Tensor, Q2: torch.Tensor, xbj: torch.Tensor, polarization: Polarization,
                           quark: Quark, contribution: str, dipole: Dipole, config: DISConfig) -> torch.Tensor:
     order = _DIP_CONTRIBUTIONS[polarization].index(contribution) if contribution in _DIP_CONTRIBUTIONS[

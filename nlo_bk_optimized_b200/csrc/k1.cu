@@ -467,25 +467,32 @@ __global__ void __cluster_dims__(1, kK1Split, 1) __launch_bounds__(kK1Threads, K
     const K1Parent<double> Pd = k1_parent<double>(sd, phd, r, knot);
 
     // phase 1: per-node data of this CTA's range; the two intervals adjacent to the
-    // parent knot (z -> x) go to the FP64 table
+    // parent knot (z -> x) are left to the FP64 table, which every CTA of the cluster
+    // prepares (16 nodes) so that the FP64 evaluations can be shared among them
     for (int L = threadIdx.x; L < k_count; L += blockDim.x) {
         const int k = k_begin + L;
         const int iv = k >> 3, m = k & 7;
+        if (iv == knot - 1 || iv == knot) {
+            zw[L] = 0.0;
+            continue;
+        }
         // node positions from the absolute knots (the reference rule), then relative to log r
         const double xa = spline[iv], xb = spline[iv + 1];
         const double hw = 0.5 * (xb - xa);
         const double lz = 0.5 * (xa + xb) + hw * consts.rule.x8[m];
-        const double dlz = lz - x_knot;
         const double rw = hw * consts.rule.w8[m];
-        if (iv == knot - 1 || iv == knot) {
-            const int idx = (iv - (knot - 1)) * 8 + m;
-            zd[idx] = k1_prepare_z<double>(sd, Pd, phd, dlz, lz);
-            zdw[idx] = 2.0 * zd[idx].z * zd[idx].z * rw;
-            zw[L] = 0.0;
-        } else {
-            zt[L] = k1_prepare_z<TF>(sf, Pf, phf, dlz, lz);
-            const double z = (double)zt[L].z;
-            zw[L] = 2.0 * z * z * rw;
+        zt[L] = k1_prepare_z<TF>(sf, Pf, phf, lz - x_knot, lz);
+        const double z = (double)zt[L].z;
+        zw[L] = 2.0 * z * z * rw;
+    }
+    if (threadIdx.x < 16) {
+        const int iv = knot - 1 + (int)(threadIdx.x >> 3), m = threadIdx.x & 7;
+        if (iv >= 0 && iv < n - 1) {
+            const double xa = spline[iv], xb = spline[iv + 1];
+            const double hw = 0.5 * (xb - xa);
+            const double lz = 0.5 * (xa + xb) + hw * consts.rule.x8[m];
+            zd[threadIdx.x] = k1_prepare_z<double>(sd, Pd, phd, lz - x_knot, lz);
+            zdw[threadIdx.x] = 2.0 * zd[threadIdx.x].z * zd[threadIdx.x].z * (hw * consts.rule.w8[m]);
         }
     }
     __syncthreads();
@@ -511,8 +518,8 @@ __global__ void __cluster_dims__(1, kK1Split, 1) __launch_bounds__(kK1Threads, K
                 total += (double)(k1_point<TF, KC>(sf, Pf, zt[L], phf, sh2f[j], history, r_grid) * awf[j]) * w;
         }
     }
-    // phase 3: FP64 evaluations of the panel nodes this CTA owns
-    for (int e = threadIdx.x; e < 16 * 24; e += blockDim.x) {
+    // phase 3: the FP64 evaluations of the panel nodes, every kK1Split-th one per CTA
+    for (int e = split + kK1Split * threadIdx.x; e < 16 * 24; e += kK1Split * blockDim.x) {
         const int idx = e / 24, j = e - 24 * (e / 24);
         const double w = zdw[idx];
         if (w != 0.0)

@@ -63,25 +63,35 @@ __global__ void __launch_bounds__(256) splines_kernel(const double* __restrict__
         }
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < m; i += blockDim.x) {
-        inv_den[i] = factor[i];
-        up[i] = i < m - 1 ? factor[n + i] : 0.0;
+    // The forward sweep s_i = (b_i - h_i s_{i-1}) / d_i as s_i = c_i + a_i s_{i-1} with
+    // c_i = b_i / d_i and a_i = -h_i / d_i formed in parallel, so the sequential chain is
+    // one FMA a step whose operands load ahead of it; the back substitution likewise
+    // with the negated upper diagonal.
+    for (int item = threadIdx.x; item < 2 * m; item += blockDim.x) {
+        const int row = item / m, i = item - row * m;
+        rhs[row * n + i] *= factor[i];
+        if (row == 0) {
+            inv_den[i] = i > 0 ? -(x[i + 1] - x[i]) * factor[i] : 0.0;
+            up[i] = i < m - 1 ? -factor[n + i] : 0.0;
+        }
     }
     __syncthreads();
-    // forward and back substitution; warp 0 solves row 0, warp 1 row 1
+    // warp 0 solves row 0, warp 1 row 1
     if ((threadIdx.x & 31) == 0 && threadIdx.x < 64 && m >= 1) {
         const int row = threadIdx.x >> 5;
-        const double* b = rhs + row * n;
+        const double* c = rhs + row * n;
         double* s = sol + row * n;
-        double prev = b[0] * inv_den[0];
+        double prev = c[0];
         s[0] = prev;
+#pragma unroll 8
         for (int i = 1; i < m; ++i) {
-            prev = fma(-(x[i + 1] - x[i]), prev, b[i]) * inv_den[i];
+            prev = fma(inv_den[i], prev, c[i]);
             s[i] = prev;
         }
-        double next = s[m - 1];
+        double next = prev;
+#pragma unroll 8
         for (int i = m - 2; i >= 0; --i) {
-            next = fma(-up[i], next, s[i]);
+            next = fma(up[i], next, s[i]);
             s[i] = next;
         }
     }

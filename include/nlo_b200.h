@@ -287,7 +287,8 @@ typedef struct nlo_dipole {
 size_t nlo_dis_table_doubles(int32_t nr, int32_t ny);
 
 /* Prepare a BK table for the device amplitude (BKDipole.__init__, dipole/amplitude.py:48-83):
- * r: device double[nr] (logarithmic, increasing, nr >= 9), y: device double[ny] (increasing),
+ * r: device double[nr] (increasing, nr >= 9; BKDipole requires the reference's logarithmic
+ * spacing, the device lookup itself takes any increasing grid), y: device double[ny] (increasing),
  * N: device double[ny*nr] (row y), x0: DipoleTable.x0; table: device double[nlo_dis_table_doubles].
  * The rapidities are stored as y + max(0, ln(1/x0)) like BKDipole.Y. */
 int nlo_dis_table_prepare(const double* r, const double* y, const double* N, int32_t nr, int32_t ny, double x0,

@@ -18,7 +18,9 @@ ranks with one NCCL all-reduce of dN/dY per RK stage; the total work is fixed (s
 scaling) and the value is the slowest rank's device time.
 
 The line also carries a "dis" object: NLO DIS sigma_r throughput on a BK table evolved by
-the same workload (see measure_dis); --workload dis prints that measurement alone.
+the same workload (see measure_dis); --workload dis prints that measurement alone.  And a
+"fixed_sobol" object: the reference's own fixed-Sobol qqbar-g benchmark setting timed
+against its published C++ time (see measure_fixed; --workload fixed alone).
 
 --impl reference times the reference algorithm on the host cores (the oracle's
 C restatement, all threads) on a bounded sample of every step and reports the
@@ -382,6 +384,7 @@ def run_ours(args) -> None:
     if not args.no_dis and world == 1:
         # the second half of the metric: NLO DIS sigma_r points/s on an evolved table
         line["dis"] = measure_dis(args.dis_points, args.dis_single, args.dis_check)
+        line["fixed_sobol"] = measure_fixed()
     print(json.dumps(line))
 
 
@@ -618,6 +621,82 @@ def measure_dis(points: int = 0, single: int = 4, check: int = 4) -> dict:
     return line
 
 
+# The reference's published C++ timings (20 CPU workers) of its six-term fixed-Sobol
+# qqbar-g benchmark, benchmarks/dis_fixed_sobol_all_qg.py:69-76, in seconds.
+FIXED_CPP_SECONDS = {"L_I1": 0.248004322, "L_I2": 0.315235827, "L_I3": 0.427307533,
+                     "T_I1": 0.341898261, "T_I2": 0.932526175, "T_I3": 1.359838948}
+
+
+def measure_fixed(reps: int = 20) -> dict:
+    """The reference's fixed-Sobol qqbar-g benchmark setting (GBW Qs0^2 = 1, lambda = 0.3,
+    gamma = 1, x0 = 1; charm m = 1.4; Q^2 = 9, x_Bj = 1e-3; maxr = 5, nf = 1; seed 3100):
+    I1, I2 and I3 of both polarisations, one device call per polarisation (grid training on
+    3 x 65,536 points, then 7 replicates of 32,768: 851,968 evaluations of the combined
+    integrand), mixed precision.  Device time by CUDA events over `reps` repetitions, and
+    end to end with the replicate estimates read back to the host."""
+    import numpy as np
+    import torch
+
+    from nlo_bk_optimized_b200 import _native
+    from nlo_bk_optimized_b200.dipole import GBW
+    from nlo_bk_optimized_b200.dis import DISConfig, Polarization, Quark, QuarkType
+    from nlo_bk_optimized_b200.dis.fixed_sobol import fixed_sobol_device
+
+    device = torch.device("cuda", torch.cuda.current_device())
+    config = DISConfig(quarks=(Quark(QuarkType.C, 1.4),), maxr=5.0, nf_alphas=1, epsrel=0.001)
+    dipole = GBW(Qs0sqr=1.0, lambda_=0.3, gamma=1.0, x0=1.0)
+    pols = (("L", Polarization.L), ("T", Polarization.T))
+
+    def run():
+        return [fixed_sobol_device(9.0, 1e-3, pol, config.quarks[0], dipole, config, seed=3100, device=device,
+                                   precision=_native.PRECISION_MIXED)[1] for _, pol in pols]
+
+    for _ in range(3):
+        run()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream(device)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(reps):
+        run()
+    end.record(stream)
+    torch.cuda.synchronize()
+    device_s = start.elapsed_time(end) / 1000.0 / reps
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        estimates = [e.cpu().numpy() for e in run()]
+    e2e_s = (time.perf_counter() - t0) / reps
+    terms = {}
+    for (tag, _), est in zip(pols, estimates):
+        for k in range(3):
+            column = est[:, k]
+            terms[f"{tag}_I{k + 1}"] = [float(column.mean()), float(column.std(ddof=1) / np.sqrt(column.size))]
+    cpp = sum(FIXED_CPP_SECONDS.values())
+    return {
+        "metric": "six-term fixed-Sobol DIS qqbar-g evaluation (both polarisations, I1+I2+I3)",
+        "value": round(device_s, 6),
+        "unit": "s",
+        "higher_is_better": False,
+        "vs_baseline": round(device_s / cpp, 7),
+        "baseline": {"value": round(cpp, 6), "unit": "s",
+                     "source": "reference C++ on 20 CPU workers, benchmarks/dis_fixed_sobol_all_qg.py:69-76; "
+                               "the reference's own GPU path is quoted at 186-189x faster (RTX 3090)"},
+        "speedup_vs_cpp": round(cpp / device_s, 1),
+        "e2e": {"value": round(e2e_s, 6), "unit": "s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 2 * 7 * 3 * 8},
+        "dtype": "f32+f64",
+        "data": "synthetic: the reference benchmark's GBW charm setting",
+        "config": {"workload": "GBW(1, 0.3, 1, 1), charm m=1.4, Q^2=9, x=1e-3, maxr=5, nf=1, seed 3100; "
+                               "3 x 2^16 training + 7 x 2^15 replicate Sobol points per polarisation",
+                   "reps": reps},
+        "terms": terms,
+    }
+
+
+def run_fixed(args) -> None:
+    print(json.dumps(measure_fixed()))
+
+
 def run_dis(args) -> None:
     print(json.dumps(measure_dis(args.dis_points, args.dis_single, args.dis_check)))
 
@@ -775,9 +854,10 @@ def main() -> None:
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--kernel-case", action="store_true",
                         help="run only the small K2+Kf/K1 case used for ncu captures")
-    parser.add_argument("--workload", choices=["bk", "dis", "batch", "serve"], default="bk",
-                        help="bk: the NLO BK evolution (default); dis: NLO DIS sigma_r throughput; "
-                             "batch: many parameter sets at once; serve: the request loop under Poisson arrivals")
+    parser.add_argument("--workload", choices=["bk", "dis", "fixed", "batch", "serve"], default="bk",
+                        help="bk: the NLO BK evolution (default); dis: NLO DIS sigma_r throughput; fixed: the "
+                             "reference's fixed-Sobol qqbar-g benchmark; batch: many parameter sets at once; "
+                             "serve: the request loop under Poisson arrivals")
     parser.add_argument("--batch-sets", type=int, default=256)
     parser.add_argument("--batch-maxy", type=float, default=8.0)
     parser.add_argument("--serve-rate", type=float, default=200.0)
@@ -793,6 +873,9 @@ def main() -> None:
         return
     if args.workload == "serve":
         run_serve(args)
+        return
+    if args.workload == "fixed":
+        run_fixed(args)
         return
     if args.workload == "dis":
         if args.kernel_case:

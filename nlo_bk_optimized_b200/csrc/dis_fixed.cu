@@ -96,28 +96,44 @@ __global__ void __launch_bounds__(kFixedThreads, 3) fixed_triple_kernel(
     for (int k = threadIdx.x; k < kFixedDims * 30; k += blockDim.x) sst[k / 30][k % 30] = sd.state[k / 30][k % 30];
     if (threadIdx.x < kFixedDims) ssh[threadIdx.x] = sd.shift[threadIdx.x];
     __syncthreads();
+    // Two lanes per sample: the even lane evaluates the first endpoint, the odd lane the
+    // second, and the even lane forms the sample's weight from its partner's values by the
+    // same expression as one lane would.  The loop runs over whole warps (the stride is a
+    // multiple of 32) so that every lane reaches the exchange.
     double acc[3] = {0.0, 0.0, 0.0};
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        float u[kFixedDims];
-#pragma unroll
-        for (int d = 0; d < kFixedDims; ++d) u[d] = sobol_unit<float>(sobol_bits(sst[d], ssh[d], i), i);
-        double first[kFixedDims], second[kFixedDims], fw, sw;
+    const uint64_t lanes = 2 * n;
+    const uint64_t span = (lanes + 31) & ~(uint64_t)31;
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < span; t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t i = t >> 1;
+        const bool odd = (t & 1) != 0;
+        const bool valid = t < lanes;
+        double fw = 0.0, sw = 0.0;
         int bin[kFixedDims];
-        endpoint_map(edges, g, u, first, second, fw, sw, bin);
-        T v1[3], v2[3];
-        qg_triple(a, first, rule, v1);
-        qg_triple(a, second, rule, v2);
-        double w[3];
+        T v[3] = {(T)0, (T)0, (T)0};
+        if (valid) {
+            float u[kFixedDims];
 #pragma unroll
-        for (int k = 0; k < 3; ++k) w[k] = (double)v1[k] * fw + (double)v2[k] * sw;
-        if constexpr (TRAIN) {
+            for (int d = 0; d < kFixedDims; ++d) u[d] = sobol_unit<float>(sobol_bits(sst[d], ssh[d], i), i);
+            double first[kFixedDims], second[kFixedDims];
+            endpoint_map(edges, g, u, first, second, fw, sw, bin);
+            qg_triple(a, odd ? second : first, rule, v);
+        }
+        T v2[3];
 #pragma unroll
-            for (int k = 0; k < 3; ++k) wout[i * 3 + k] = w[k];
+        for (int k = 0; k < 3; ++k) v2[k] = __shfl_xor_sync(0xffffffffu, v[k], 1);
+        if (valid && !odd) {
+            double w[3];
 #pragma unroll
-            for (int d = 0; d < kFixedDims; ++d) bout[i * kFixedDims + d] = (uint8_t)bin[d];
-        } else {
+            for (int k = 0; k < 3; ++k) w[k] = (double)v[k] * fw + (double)v2[k] * sw;
+            if constexpr (TRAIN) {
 #pragma unroll
-            for (int k = 0; k < 3; ++k) acc[k] += w[k];
+                for (int k = 0; k < 3; ++k) wout[i * 3 + k] = w[k];
+#pragma unroll
+                for (int d = 0; d < kFixedDims; ++d) bout[i * kFixedDims + d] = (uint8_t)bin[d];
+            } else {
+#pragma unroll
+                for (int k = 0; k < 3; ++k) acc[k] += w[k];
+            }
         }
     }
     if constexpr (!TRAIN) {
@@ -261,6 +277,8 @@ struct FixedCarve {
 constexpr size_t kAl = 256;
 size_t al(size_t v) { return (v + kAl - 1) & ~(kAl - 1); }
 
+// CTAs of a launch over n samples: two lanes a sample (fixed_triple_kernel), up to four
+// waves of three CTAs per SM.  The workspace carve and the launches both size by it.
 int fixed_blocks(uint64_t n)
 {
     static int sms = [] {
@@ -268,7 +286,7 @@ int fixed_blocks(uint64_t n)
         if (cudaGetDevice(&device) == cudaSuccess) cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device);
         return v > 0 ? v : 148;
     }();
-    const uint64_t by_n = (n + dis::kFixedThreads - 1) / dis::kFixedThreads;
+    const uint64_t by_n = (2 * n + dis::kFixedThreads - 1) / dis::kFixedThreads;
     const uint64_t cap = (uint64_t)4 * 3 * sms;
     const uint64_t b = by_n < cap ? by_n : cap;
     return (int)(b < 1 ? 1 : b);

@@ -413,23 +413,42 @@ __global__ void __launch_bounds__(kVegasThreads, (vegas_min_blocks<T, TERM>())) 
 
 // Sum the per-CTA partials of every job in a fixed order: grid (key chunks, jobs), one
 // thread per key (the |w| histogram bins, then total and total^2), looping over the CTAs.
-__global__ void vegas_reduce_kernel(const double* __restrict__ partial, int keys, int blocks_per_job,
-                                    double* __restrict__ reduced)
+// Per job: sum the per-CTA partials [blocks][keys] over the CTAs.  Each thread takes one
+// key and every kReduceSlices-th CTA row (four chains), and the slices of a key are added
+// in slice order through shared memory, so the order is fixed; a warp reads 32 consecutive
+// keys of a row.
+constexpr int kReduceKeys = 32;
+constexpr int kReduceSlices = 8;
+
+__global__ void __launch_bounds__(kReduceKeys * kReduceSlices)
+    vegas_reduce_kernel(const double* __restrict__ partial, int keys, int blocks_per_job, double* __restrict__ reduced)
 {
+    __shared__ double sums[kReduceSlices][kReduceKeys];
     const int job = blockIdx.y;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;  // 0..keys-1 over [total, total2, hist...]
-    if (k >= keys) return;
-    const double* p = partial + (size_t)job * blocks_per_job * keys + k;
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-    int b = 0;
-    for (; b + 4 <= blocks_per_job; b += 4) {
-        a0 += p[(size_t)(b + 0) * keys];
-        a1 += p[(size_t)(b + 1) * keys];
-        a2 += p[(size_t)(b + 2) * keys];
-        a3 += p[(size_t)(b + 3) * keys];
+    const int kl = threadIdx.x % kReduceKeys, slice = threadIdx.x / kReduceKeys;
+    const int k = blockIdx.x * kReduceKeys + kl;  // 0..keys-1 over [total, total2, hist...]
+    double total = 0.0;
+    if (k < keys) {
+        const double* p = partial + (size_t)job * blocks_per_job * keys + k;
+        constexpr int S = kReduceSlices;
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+        int b = slice;
+        for (; b + 3 * S < blocks_per_job; b += 4 * S) {
+            a0 += p[(size_t)b * keys];
+            a1 += p[(size_t)(b + S) * keys];
+            a2 += p[(size_t)(b + 2 * S) * keys];
+            a3 += p[(size_t)(b + 3 * S) * keys];
+        }
+        for (; b < blocks_per_job; b += S) a0 += p[(size_t)b * keys];
+        total = (a0 + a1) + (a2 + a3);
     }
-    for (; b < blocks_per_job; ++b) a0 += p[(size_t)b * keys];
-    reduced[(size_t)job * keys + k] = (a0 + a1) + (a2 + a3);
+    sums[slice][kl] = total;
+    __syncthreads();
+    if (slice == 0 && k < keys) {
+        double v = sums[0][kl];
+        for (int q = 1; q < kReduceSlices; ++q) v += sums[q][kl];
+        reduced[(size_t)job * keys + k] = v;
+    }
 }
 
 // One CTA per job: adapt the grid (numerics/integration.py:804-866) from the reduced
@@ -577,8 +596,9 @@ cudaError_t launch_vegas_round_t(const VegasLaunch& L, cudaStream_t stream)
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const int keys = 2 + D * L.bins;
-    dim3 rgrid((keys + 127) / 128, L.jobs);
-    vegas_reduce_kernel<<<rgrid, 128, 0, stream>>>(L.partial, keys, L.blocks_per_job, L.reduced);
+    dim3 rgrid((keys + kReduceKeys - 1) / kReduceKeys, L.jobs);
+    vegas_reduce_kernel<<<rgrid, kReduceKeys * kReduceSlices, 0, stream>>>(L.partial, keys, L.blocks_per_job,
+                                                                           L.reduced);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const size_t fsmem = sizeof(double) * (D * L.bins + 2 * D * (L.bins + 1));
@@ -694,8 +714,9 @@ cudaError_t dis_launch_reduce_finalize(int D, int bins, int jobs, int blocks_per
                                        cudaStream_t stream)
 {
     const int keys = 2 + D * bins;
-    dim3 rgrid((keys + 127) / 128, jobs);
-    dis::vegas_reduce_kernel<<<rgrid, 128, 0, stream>>>(partial, keys, blocks_per_job, reduced);
+    dim3 rgrid((keys + dis::kReduceKeys - 1) / dis::kReduceKeys, jobs);
+    dis::vegas_reduce_kernel<<<rgrid, dis::kReduceKeys * dis::kReduceSlices, 0, stream>>>(partial, keys,
+                                                                                       blocks_per_job, reduced);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const size_t fsmem = sizeof(double) * (D * bins + 2 * D * (bins + 1));

@@ -82,7 +82,7 @@ __device__ __forceinline__ void endpoint_map(const double* __restrict__ edges, c
 // TRAIN = false: per-CTA sums of the weighted values (fixed order).
 template <typename T, bool TRAIN>
 __global__ void __launch_bounds__(kFixedThreads, 3) fixed_triple_kernel(
-    const DisArgs<T> args, const InnerRule rule, const SobolDirsArg* __restrict__ dirs, int dir_index, uint64_t n,
+    const DisArgs<T> args, const InnerRule rule, const SobolDirsArg* __restrict__ dirs, int dir_base, uint64_t n,
     const double* __restrict__ edges, FixedGeom g, double* __restrict__ wout, uint8_t* __restrict__ bout,
     double* __restrict__ partial)
 {
@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(kFixedThreads, 3) fixed_triple_kernel(
     __shared__ uint32_t ssh[kFixedDims];
     __shared__ double red[3][kFixedThreads / 32];
     if (threadIdx.x == 0) a = args;
-    const SobolDirsArg& sd = dirs[dir_index];
+    const SobolDirsArg& sd = dirs[dir_base + blockIdx.y];  // replicates: one per grid row
     for (int k = threadIdx.x; k < kFixedDims * 30; k += blockDim.x) sst[k / 30][k % 30] = sd.state[k / 30][k % 30];
     if (threadIdx.x < kFixedDims) ssh[threadIdx.x] = sd.shift[threadIdx.x];
     __syncthreads();
@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(kFixedThreads, 3) fixed_triple_kernel(
         if (threadIdx.x < 3) {
             double v = 0.0;
             for (int w = 0; w < kFixedThreads / 32; ++w) v += red[threadIdx.x][w];
-            partial[blockIdx.x * 3 + threadIdx.x] = v;
+            partial[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * 3 + threadIdx.x] = v;
         }
     }
 }
@@ -236,13 +236,15 @@ __global__ void fixed_score_hist_kernel(const double* __restrict__ w, const uint
 }
 
 // estimates[j][k] = (sum over CTAs of partial[b][k]) / n, fixed order
+// One CTA per replicate: its CTA sums in CTA order.
 __global__ void fixed_estimate_kernel(const double* __restrict__ partial, int blocks, uint64_t n,
                                       double* __restrict__ estimate)
 {
     if (threadIdx.x >= 3) return;
+    const double* p = partial + (size_t)blockIdx.x * blocks * 3;
     double v = 0.0;
-    for (int b = 0; b < blocks; ++b) v += partial[b * 3 + threadIdx.x];
-    estimate[threadIdx.x] = v / (double)n;
+    for (int b = 0; b < blocks; ++b) v += p[b * 3 + threadIdx.x];
+    estimate[3 * blockIdx.x + threadIdx.x] = v / (double)n;
 }
 
 __global__ void fixed_grid_init_kernel(double* state, int D, int bins)
@@ -303,7 +305,11 @@ FixedCarve fixed_carve(const nlo_fixed_sobol_options& o)
     c.w = al(c.dirs + sizeof(SobolDirsArg) * (size_t)rounds);
     c.b = al(c.w + sizeof(double) * 3 * (size_t)o.training_samples);
     c.partial = al(c.b + (size_t)dis::kFixedDims * o.training_samples);
-    c.abs_partial = al(c.partial + sizeof(double) * (size_t)blocks * (2 + dis::kFixedDims * (size_t)o.bins));
+    // per-CTA partials: the training histograms, or all replicates' sums at once
+    const size_t train_partial = (size_t)blocks * (2 + dis::kFixedDims * (size_t)o.bins);
+    const size_t replicate_partial = (size_t)o.replicates * fixed_blocks((uint64_t)o.samples_per_replicate) * 3;
+    c.abs_partial = al(c.partial + sizeof(double) * (train_partial > replicate_partial ? train_partial
+                                                                                       : replicate_partial));
     c.reduced = al(c.abs_partial + sizeof(double) * 3 * (size_t)blocks);
     c.counts = al(c.reduced + sizeof(double) * (2 + dis::kFixedDims * (size_t)o.bins));
     c.total = al(c.counts + sizeof(int32_t) * dis::kFixedDims * (size_t)o.bins);
@@ -348,13 +354,12 @@ int run_fixed(const dis::DisArgs<T>& args, const dis::InnerRule& rule, const nlo
     }
     const uint64_t nr = (uint64_t)o.samples_per_replicate;
     const int rb = fixed_blocks(nr);
-    for (int j = 0; j < o.replicates; ++j) {
-        fixed_triple_kernel<T, false><<<rb, kFixedThreads, 0, s>>>(args, rule, dirs, o.training_rounds + j, nr,
-                                                                   grid_state, g, nullptr, nullptr, partial);
-        fixed_estimate_kernel<<<1, 32, 0, s>>>(partial, rb, nr, estimates + 3 * j);
-        e = cudaGetLastError();
-        if (e != cudaSuccess) return fcuda(e, "fixed-Sobol replicate launch");
-    }
+    // the replicates are independent (own Sobol seeds, the frozen grid): one launch
+    fixed_triple_kernel<T, false><<<dim3(rb, o.replicates), kFixedThreads, 0, s>>>(
+        args, rule, dirs, o.training_rounds, nr, grid_state, g, nullptr, nullptr, partial);
+    fixed_estimate_kernel<<<o.replicates, 32, 0, s>>>(partial, rb, nr, estimates);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fcuda(e, "fixed-Sobol replicate launch");
     return NLO_OK;
 }
 

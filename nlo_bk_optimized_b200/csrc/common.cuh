@@ -2,7 +2,8 @@
 //
 // Every kernel is templated on the arithmetic type T:
 //   T = float  : the mixed build -- integrands in FP32 on the FMA/MUFU pipes,
-//                compensated FP32 partial sums folded into FP64;
+//                FP32 partial sums of 32 samples folded into FP64 (K2+Kf), FP64
+//                sums (K1);
 //   T = double : the all-FP64 build used to check parity at 1e-10.
 // The formulas are the reference's (torch_nlo_clean/src/nlo_torch: bk_kernels/k1.py,
 // k2.py, kf.py, bk/derivatives.py, coupling.py) rewritten in algebraically identical

@@ -780,24 +780,29 @@ __device__ __forceinline__ K01<float> bessel_k01_rcp(float x, float& rx)
 
 __device__ __forceinline__ GSet<float> g_moments_f32(const Trip<float>& t, const InnerRule& rule)
 {
-    GSet<float> m;
-    float M2[2], sM2[2], lm2[2], x3[2], wx2[2], om[2];
+    // The side constants of the moments (8 omega, 4 omega, 4, 2) are applied after the
+    // loop, and sqrt(y) cancels between sqrt(A/B) = z sqrt(y)/B and the 1/sqrt(y) of the
+    // G functions:
+    //   G11 = 2 sum w/y K0(z1)             G21 = 4 sum w/B z1 K1(z1)
+    //   G12 = 4 omega sum w/(y B) D12      G22 = 8 omega sum w/B E
+    // with D12 = z1 K1(z1) - z0 K1(z0) (or the Euler-Maclaurin d1) and
+    // E = (A1 F(z1) - M2 F(z0))/y, F(z) = K0 + 2 K1/z (or d2/B).
+    float acc22[2], acc12[2], acc21[2], acc11[2];
+    float M2[2], sM2[2], lm2[2], x3[2], wx2[2];
 #pragma unroll
     for (int s = 0; s < 2; ++s) {
-        m.g22[s] = m.g12[s] = m.g21[s] = m.g11[s] = 0.0f;
+        acc22[s] = acc12[s] = acc21[s] = acc11[s] = 0.0f;
         M2[s] = t.Qb2[s] + t.m2;
         sM2[s] = sqrtf(M2[s]);
         lm2[s] = t.lam[s] * t.m2;
         x3[s] = t.x3sq[s];
         wx2[s] = t.omega[s] * t.x2sq[s];
-        om[s] = t.omega[s];
     }
     for (int i = 0; i < rule.n; ++i) {
         const float y = (float)rule.y[i];
         const float w = (float)rule.w[i];
         const float iy = rcp_approx_f(y);
-        const float sqy = sqrtf(y);
-        const float isqy = sqy * iy;  // 1/sqrt(y)
+        const float wiy = w * iy;
 #pragma unroll
         for (int s = 0; s < 2; ++s) {
             const float B = fmaf(y, x3[s], wx2[s]);
@@ -810,34 +815,40 @@ __device__ __forceinline__ GSet<float> g_moments_f32(const Trip<float>& t, const
             float r1, r0;
             const K01<float> kl = bessel_k01_rcp(z1, r1);
             const K01<float> k0 = bessel_k01_rcp(z0, r0);
-            const float sl = z1 * sqy * iB, s0 = z0 * sqy * iB;  // sqrt(A/B)
             const float h = q * delta * rcp_approx_f(sAl + sM2[s]);
-            float g22b, g12b;
+            const float z1k1 = z1 * kl.k1;
+            float d12, e22;
             if (h < 0.3f && h < 0.1f * z0) {
                 // Euler-Maclaurin integral of dF/dz over [z0, z1] (see f_differences_em)
                 const float h2 = h * h;
                 const float e2 = h2 * (1.0f / 12.0f), e4 = h2 * h2 * (1.0f / 720.0f);
                 const float d1 = 0.5f * h * (-z0 * k0.k0 - z1 * kl.k0) -
-                                 e2 * ((z1 * kl.k1 - kl.k0) - (z0 * k0.k1 - k0.k0)) +
-                                 e4 * ((z1 * kl.k1 - 2.0f * kl.k0 - kl.k1 * r1) - (z0 * k0.k1 - 2.0f * k0.k0 - k0.k1 * r0));
-                const float d2 = 0.5f * h * (-z0 * z0 * k0.k1 - z1 * z1 * kl.k1) -
-                                 e2 * ((z1 * z1 * kl.k0 - z1 * kl.k1) - (z0 * z0 * k0.k0 - z0 * k0.k1)) +
-                                 e4 * (((3.0f + z1 * z1) * kl.k0 - 4.0f * z1 * kl.k1) -
+                                 e2 * ((z1k1 - kl.k0) - (z0 * k0.k1 - k0.k0)) +
+                                 e4 * ((z1k1 - 2.0f * kl.k0 - kl.k1 * r1) - (z0 * k0.k1 - 2.0f * k0.k0 - k0.k1 * r0));
+                const float d2 = 0.5f * h * (-z0 * z0 * k0.k1 - z1 * z1k1) -
+                                 e2 * ((z1 * z1 * kl.k0 - z1k1) - (z0 * z0 * k0.k0 - z0 * k0.k1)) +
+                                 e4 * (((3.0f + z1 * z1) * kl.k0 - 4.0f * z1k1) -
                                        ((3.0f + z0 * z0) * k0.k0 - 4.0f * z0 * k0.k1));
-                g12b = 4.0f * om[s] * iy * iB * d1;
-                g22b = 8.0f * om[s] * iB * iB * d2;
+                d12 = d1;
+                e22 = iB * d2;
             } else {
-                const float rl = Al * iB, rz = M2[s] * iB;
-                g22b = 8.0f * iy * om[s] * (rl * (kl.k0 + 2.0f * kl.k1 * r1) - rz * (k0.k0 + 2.0f * k0.k1 * r0));
-                g12b = 4.0f * iy * isqy * om[s] * (sl * kl.k1 - s0 * k0.k1);
+                d12 = z1k1 - z0 * k0.k1;
+                e22 = iy * (Al * fmaf(2.0f * kl.k1, r1, kl.k0) - M2[s] * fmaf(2.0f * k0.k1, r0, k0.k0));
             }
-            const float g21 = 4.0f * isqy * sl * kl.k1;
-            const float g11 = 2.0f * iy * kl.k0;
-            m.g22[s] = fmaf(w, g22b, m.g22[s]);
-            m.g12[s] = fmaf(w, g12b, m.g12[s]);
-            m.g21[s] = fmaf(w, g21, m.g21[s]);
-            m.g11[s] = fmaf(w, g11, m.g11[s]);
+            const float wiB = w * iB;
+            acc22[s] = fmaf(wiB, e22, acc22[s]);
+            acc12[s] = fmaf(wiy * iB, d12, acc12[s]);
+            acc21[s] = fmaf(wiB, z1k1, acc21[s]);
+            acc11[s] = fmaf(wiy, kl.k0, acc11[s]);
         }
+    }
+    GSet<float> m;
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+        m.g22[s] = 8.0f * t.omega[s] * acc22[s];
+        m.g12[s] = 4.0f * t.omega[s] * acc12[s];
+        m.g21[s] = 4.0f * acc21[s];
+        m.g11[s] = 2.0f * acc11[s];
     }
     return m;
 }

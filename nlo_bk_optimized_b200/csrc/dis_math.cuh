@@ -69,6 +69,22 @@ __device__ __forceinline__ T horner(const T (&c)[N], T t)
     return acc;
 }
 
+// Horner in v of the polynomial with coefficients c_k a^k b.  With a (a power of two) and
+// b constants at the call site the scaled coefficients fold into the instructions, so a
+// change of variable or an overall factor costs nothing at run time.
+template <int N>
+__device__ __forceinline__ float horner_scaled(const float (&c)[N], float a, float b, float v)
+{
+    float p[N];
+    p[0] = b;
+#pragma unroll
+    for (int k = 1; k < N; ++k) p[k] = p[k - 1] * a;
+    float acc = c[N - 1] * p[N - 1];
+#pragma unroll
+    for (int i = N - 2; i >= 0; --i) acc = fmaf(acc, v, c[i] * p[i]);
+    return acc;
+}
+
 template <int N>
 __device__ __forceinline__ double clenshaw(const double (&c)[N], double y)
 {
@@ -139,28 +155,34 @@ __device__ __forceinline__ float exp_neg_f(float x)
     return ex2_approx_f(-hi) * fmaf(-lo, 0.69314718055994531f, 1.0f);
 }
 
-// FP32 K0 and K1: the series in t = x^2/4 up to x = 2, e^-x/sqrt(x) times a polynomial
-// in 2/x above.  log(x/2) comes from the hardware log2 (absolute error near 1e-7), which
-// near x = 2, where log(x/2) -> 0, bounds the relative error of K0 by about 3e-6; the
-// FP32 build's integrals are held to 1e-4 of the FP64 ones.
-__device__ __forceinline__ K01<float> bessel_k01(float x)
+// K0 and K1 from x and 1/x, FP32: the series in t = x^2/4 up to x = 2 (variable x^2, ln 2
+// and the factors of K1 folded into the coefficients), e^-x/sqrt(x) times a polynomial in
+// s = 2/x above (variable 1/x).  log(x/2) comes from the hardware log2 (absolute error
+// near 1e-7), which near x = 2, where log(x/2) -> 0, bounds the relative error of K0 by
+// about 3e-6; the FP32 build's integrals are held to 1e-4 of the FP64 ones.
+__device__ __forceinline__ K01<float> bessel_k01_from_rcp(float x, float rx)
 {
     using namespace nlo_special;
+    constexpr float kLn2 = 0.69314718055994531f;
     K01<float> out;
-    const float rx = rcp_approx_f(x);
     if (x <= 2.0f) {
-        const float t = 0.25f * x * x;
-        const float L = 0.69314718055994531f * lg2_approx_f(0.5f * x);
-        out.k0 = fmaf(-L, horner(kI0SeriesF, t), horner(kQ0SeriesF, t));
-        out.k1 = rx + 0.5f * x * fmaf(L, horner(kI1SeriesF, t), -0.5f * horner(kQ1SeriesF, t));
+        // K0 = -ln(x/2) I0(t) + Q0(t), K1 = 1/x + (x/2) (ln(x/2) I1(t) - Q1(t)/2), t = x^2/4,
+        // with ln(x/2) = ln 2 (log2 x - 1)
+        const float x2 = x * x;
+        const float lg = lg2_approx_f(x) - 1.0f;
+        out.k0 = fmaf(-lg, horner_scaled(kI0SeriesF, 0.25f, kLn2, x2), horner_scaled(kQ0SeriesF, 0.25f, 1.0f, x2));
+        out.k1 = fmaf(x, fmaf(lg, horner_scaled(kI1SeriesF, 0.25f, 0.5f * kLn2, x2),
+                              horner_scaled(kQ1SeriesF, 0.25f, -0.25f, x2)),
+                      rx);
     } else {
-        const float s = 2.0f * rx;
         const float e = exp_neg_f(x) * rsqrtf(x);
-        out.k0 = e * horner(kK0PolyF, s);
-        out.k1 = e * horner(kK1PolyF, s);
+        out.k0 = e * horner_scaled(kK0PolyF, 2.0f, 1.0f, rx);
+        out.k1 = e * horner_scaled(kK1PolyF, 2.0f, 1.0f, rx);
     }
     return out;
 }
+
+__device__ __forceinline__ K01<float> bessel_k01(float x) { return bessel_k01_from_rcp(x, rcp_approx_f(x)); }
 
 template <typename T>
 __device__ __forceinline__ T bessel_k0(T x)

@@ -754,28 +754,15 @@ __device__ T l_i3(const Trip<T>& t, const GSet<T>& G1, const GSet<T>& G2)
                      - (T)2 * c * a * G1.g11[0] * G2.g11[1]));
 }
 
-// FP32 form of the moment loop.  Per node y the reciprocal 1/y and sqrt(y) are shared by
-// the two sides; per side the quantities that do not depend on y (M2 = Qbar^2 + m^2, its
-// square root, lambda m^2, x3^2, omega x2^2) are formed once.  With q = sqrt(B/y):
-//   z0 = sqrt(M2) q,  z1 = sqrt(A1) q,  sqrt(A/B) = z sqrt(y)/B,  z1 - z0 = q delta/(sqrt(A1)+sqrt(M2)),
+// FP32 form of the moment loop.  Per node y the reciprocal 1/y is shared by the two sides;
+// per side the quantities that do not depend on y (M2 = Qbar^2 + m^2, its square root,
+// lambda m^2, x3^2, omega x2^2) are formed once.  With q = sqrt(B/y):
+//   z0 = sqrt(M2) q,  z1 = sqrt(A1) q,  z1 - z0 = q delta/(sqrt(A1)+sqrt(M2)),
 // so each (node, side) needs two square roots and two reciprocals besides the Bessel pairs.
 __device__ __forceinline__ K01<float> bessel_k01_rcp(float x, float& rx)
 {
-    using namespace nlo_special;
-    K01<float> out;
     rx = rcp_approx_f(x);
-    if (x <= 2.0f) {
-        const float t = 0.25f * x * x;
-        const float L = 0.69314718055994531f * lg2_approx_f(0.5f * x);
-        out.k0 = fmaf(-L, horner(kI0SeriesF, t), horner(kQ0SeriesF, t));
-        out.k1 = rx + 0.5f * x * fmaf(L, horner(kI1SeriesF, t), -0.5f * horner(kQ1SeriesF, t));
-    } else {
-        const float e = exp_neg_f(x) * rsqrtf(x);
-        const float s = 2.0f * rx;
-        out.k0 = e * horner(kK0PolyF, s);
-        out.k1 = e * horner(kK1PolyF, s);
-    }
-    return out;
+    return bessel_k01_from_rcp(x, rx);
 }
 
 __device__ __forceinline__ GSet<float> g_moments_f32(const Trip<float>& t, const InnerRule& rule)

@@ -4,7 +4,6 @@ dis/lo.py:12-51), evaluated by the device LO kernel."""
 from __future__ import annotations
 
 import math
-from dataclasses import replace
 
 import torch
 

@@ -25,7 +25,6 @@ import torch
 from nlo_bk_optimized_b200 import _native
 from nlo_bk_optimized_b200.dipole.amplitude import GBW, BKDipole
 from nlo_bk_optimized_b200.dis.config import (
-    CF,
     NC,
     AlphaEM,
     DISConfig,

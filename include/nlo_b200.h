@@ -159,8 +159,11 @@ int nlo_bk_k2kf(const nlo_bk_params* params, const double* r, int32_t points, co
  * workspace argument and nothing is allocated; the per-CTA partial sums live in a
  * fixed device array of 296 x 512 x 3 doubles (3.6 MB) that every GPU loading the
  * library holds until the process exits.  points must be <= 512 (larger grids are
- * rejected with NLO_ERR_INVALID).  The first call on a device looks up the
+ * rejected with NLO_ERR_INVALID), and the parameters and direction numbers are
+ * checked as nlo_bk_k2kf checks them.  The first call on a device looks up the
  * array's address with that device current; make it before any stream capture.
+ * The address is cached for the device's context: do not use the library across a
+ * cudaDeviceReset.
  * All calls share the array: calls that overlap on the GPU race and must be
  * serialised by the caller.  This entry point has no counterpart in the reference. */
 int nlo_bk_k2kf_static(const nlo_bk_params* params, const double* r, int32_t points, const double* spline,

@@ -12,6 +12,7 @@ from __future__ import annotations
 from dataclasses import dataclass
 from pathlib import Path
 
+import numpy as np
 import torch
 
 from nlo_bk_optimized_b200.numerics.interpolation import NaturalCubicSpline
@@ -45,10 +46,27 @@ class MV:
         return torch.where(exponent < 1e-5, exponent, 1 - torch.exp(-exponent))
 
 
+def _read_table(path: Path) -> tuple[torch.Tensor, torch.Tensor]:
+    """The (r, N) columns of a whitespace-separated text table in float64.  ``#`` starts a
+    comment; blank lines are skipped; further columns are ignored."""
+    try:
+        data = np.loadtxt(path, comments="#", usecols=(0, 1), ndmin=2, dtype=np.float64)
+    except ValueError as error:
+        raise ValueError(f"{path}: every data line needs numeric r and N columns ({error})") from None
+    r, N = torch.from_numpy(data[:, 0].copy()), torch.from_numpy(data[:, 1].copy())
+    if r.numel() < 10:
+        raise ValueError(f"{path}: {r.numel()} rows; a tabulated initial condition needs at least 10")
+    if not (bool(torch.isfinite(r).all()) and bool(torch.isfinite(N).all())):
+        raise ValueError(f"{path}: r and N must be finite")
+    if not bool((r.diff() > 0).all()):
+        raise ValueError(f"{path}: r must increase strictly from row to row")
+    return r, N
+
+
 class ICDataFile:
-    """Natural-cubic initial condition from a two-column ``r N`` file
-    (initial_conditions.py:38-91): comments '#' and blank lines skipped, at least
-    ten rows, N = 0 below the first r and 1 above the last."""
+    """Tabulated initial condition (the reference's ICDataFile, bk/initial_conditions.py:38-91):
+    a natural cubic spline through the rows of a two-column ``r N`` text file, with N = 0
+    below its first r and N = 1 above its last."""
 
     def __init__(
         self,
@@ -60,31 +78,9 @@ class ICDataFile:
     ) -> None:
         self.path = Path(path)
         self.x0 = x0
-        r_values: list[float] = []
-        N_values: list[float] = []
-        for line_number, line in enumerate(self.path.read_text(encoding="utf-8").splitlines(), start=1):
-            stripped = line.strip()
-            if not stripped or stripped.startswith("#"):
-                continue
-            columns = stripped.split()
-            if len(columns) < 2:
-                raise ValueError(f"{self.path}:{line_number} requires two columns: r N")
-            try:
-                r_values.append(float(columns[0]))
-                N_values.append(float(columns[1]))
-            except ValueError as error:
-                raise ValueError(f"{self.path}:{line_number} contains a non-numeric r or N") from error
-        if len(N_values) < 10:
-            raise ValueError(f"{self.path} contains {len(N_values)} points; at least 10 are required")
-        r64 = torch.tensor(r_values, dtype=torch.float64)
-        N64 = torch.tensor(N_values, dtype=torch.float64)
-        if not bool(torch.isfinite(r64).all()) or not bool(torch.isfinite(N64).all()):
-            raise ValueError("x and y must contain only finite values")
-        if not bool((r64[1:] > r64[:-1]).all()):
-            raise ValueError("x must be strictly increasing")
-        self._r64, self._N64 = r64, N64  # the file's values, the device fit's input
-        self.r = r64.to(dtype=dtype, device=device)
-        self.N = N64.to(dtype=dtype, device=device)
+        self._r64, self._N64 = _read_table(self.path)  # the file's values, the device fit's input
+        self.r = self._r64.to(dtype=dtype, device=device)
+        self.N = self._N64.to(dtype=dtype, device=device)
         self._host_spline: NaturalCubicSpline | None = None
         self._device_splines: dict[int, torch.Tensor] = {}
 

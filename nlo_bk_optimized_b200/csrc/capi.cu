@@ -63,42 +63,6 @@ void gauss_legendre(int n, double* x, double* w)
     }
 }
 
-bool check_params(const nlo_bk_params* p, std::string& why)
-{
-    if (!p) { why = "params is NULL"; return false; }
-    if (!(p->nc > 0)) { why = "NC must be positive"; return false; }
-    if (!(p->nf == 0.0 || p->nf == 3.0 || p->nf == 5.0)) { why = "NF must be 0, 3 or 5"; return false; }
-    if (p->order < NLO_ORDER_NLO_RESUM_DLOG_SLOG || p->order > NLO_ORDER_LO) { why = "unknown order"; return false; }
-    if (p->rc_lo < NLO_RC_LO_BALITSKY || p->rc_lo > NLO_RC_LO_BEUF) { why = "unknown RC_LO"; return false; }
-    if (p->resum_rc < NLO_RESUM_RC_SMALLEST || p->resum_rc > NLO_RESUM_RC_FIXED) { why = "unknown RESUM_RC"; return false; }
-    if (p->rc_nlo != NLO_RC_NLO_SMALLEST && p->rc_nlo != NLO_RC_NLO_PARENT) { why = "unknown RC_NLO"; return false; }
-    if (!(p->lambda_qcd > 0) || !(p->c2 > 0) || !(p->ksub > 0)) { why = "LambdaQCD, C2 and KSUB must be positive"; return false; }
-    if (p->precision != NLO_PRECISION_MIXED && p->precision != NLO_PRECISION_FP64) { why = "unknown precision"; return false; }
-    return true;
-}
-
-bool check_dirs(const nlo_sobol_dirs* d, int need, std::string& why)
-{
-    if (!d) { why = "dirs is NULL"; return false; }
-    if (d->dims < need || d->dims > 8) { why = "Sobol dimension count out of range"; return false; }
-    for (int j = 0; j < d->dims; ++j) {
-        if (d->shift[j] >= (1u << 30)) { why = "Sobol shift exceeds 30 bits"; return false; }
-        for (int k = 0; k < 30; ++k)
-            if (d->state[j][k] >= (1u << 30)) { why = "Sobol direction number exceeds 30 bits"; return false; }
-    }
-    return true;
-}
-
-SobolDirsArg to_arg(const nlo_sobol_dirs* d)
-{
-    SobolDirsArg a;
-    std::memset(&a, 0, sizeof(a));
-    a.dims = d->dims;
-    std::memcpy(a.state, d->state, sizeof(a.state));
-    std::memcpy(a.shift, d->shift, sizeof(a.shift));
-    return a;
-}
-
 size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
 
 // Workspace layout of one right-hand-side evaluation.
@@ -210,6 +174,42 @@ int run_rhs(const nlo_bk_params& p, const double* r, const double* N, int points
 }
 
 }  // namespace
+
+bool check_params(const nlo_bk_params* p, std::string& why)
+{
+    if (!p) { why = "params is NULL"; return false; }
+    if (!(p->nc > 0)) { why = "NC must be positive"; return false; }
+    if (!(p->nf == 0.0 || p->nf == 3.0 || p->nf == 5.0)) { why = "NF must be 0, 3 or 5"; return false; }
+    if (p->order < NLO_ORDER_NLO_RESUM_DLOG_SLOG || p->order > NLO_ORDER_LO) { why = "unknown order"; return false; }
+    if (p->rc_lo < NLO_RC_LO_BALITSKY || p->rc_lo > NLO_RC_LO_BEUF) { why = "unknown RC_LO"; return false; }
+    if (p->resum_rc < NLO_RESUM_RC_SMALLEST || p->resum_rc > NLO_RESUM_RC_FIXED) { why = "unknown RESUM_RC"; return false; }
+    if (p->rc_nlo != NLO_RC_NLO_SMALLEST && p->rc_nlo != NLO_RC_NLO_PARENT) { why = "unknown RC_NLO"; return false; }
+    if (!(p->lambda_qcd > 0) || !(p->c2 > 0) || !(p->ksub > 0)) { why = "LambdaQCD, C2 and KSUB must be positive"; return false; }
+    if (p->precision != NLO_PRECISION_MIXED && p->precision != NLO_PRECISION_FP64) { why = "unknown precision"; return false; }
+    return true;
+}
+
+bool check_dirs(const nlo_sobol_dirs* d, int need, std::string& why)
+{
+    if (!d) { why = "dirs is NULL"; return false; }
+    if (d->dims < need || d->dims > 8) { why = "Sobol dimension count out of range"; return false; }
+    for (int j = 0; j < d->dims; ++j) {
+        if (d->shift[j] >= (1u << 30)) { why = "Sobol shift exceeds 30 bits"; return false; }
+        for (int k = 0; k < 30; ++k)
+            if (d->state[j][k] >= (1u << 30)) { why = "Sobol direction number exceeds 30 bits"; return false; }
+    }
+    return true;
+}
+
+SobolDirsArg to_arg(const nlo_sobol_dirs* d)
+{
+    SobolDirsArg a;
+    std::memset(&a, 0, sizeof(a));
+    a.dims = d->dims;
+    std::memcpy(a.state, d->state, sizeof(a.state));
+    std::memcpy(a.shift, d->shift, sizeof(a.shift));
+    return a;
+}
 
 const K1Rule& k1_rule()
 {

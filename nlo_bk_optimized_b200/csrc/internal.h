@@ -5,6 +5,8 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include <string>
+
 #include "../../include/nlo_b200.h"
 
 namespace nlo {
@@ -23,6 +25,12 @@ struct K1Rule {
 };
 
 const K1Rule& k1_rule();
+
+// Host checks shared by every entry point that takes BK parameters or Sobol directions:
+// false with the reason in `why` when an argument is out of range.
+bool check_params(const nlo_bk_params* p, std::string& why);
+bool check_dirs(const nlo_sobol_dirs* d, int need, std::string& why);
+SobolDirsArg to_arg(const nlo_sobol_dirs* d);
 
 // Buffers of one right-hand-side evaluation carved from the caller's workspace.
 struct RhsBuffers {

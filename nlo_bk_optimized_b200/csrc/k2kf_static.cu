@@ -17,6 +17,9 @@
 //  * the first call on a device looks up the array's device address with that
 //    device current (cudaGetSymbolAddress) and caches it; make that first call
 //    before any stream capture;
+//  * the cached address belongs to the device's context of that first call: after
+//    cudaDeviceReset (or anything else that destroys and recreates the primary
+//    context) it is stale, so the library must not be used across a device reset;
 //  * every call uses the same array, which keeps the last call's contents; each
 //    launch writes all the partials it later reads, so nothing needs clearing,
 //    but calls that overlap on the GPU (other streams or threads, same device)
@@ -24,8 +27,8 @@
 
 #include <cuda_runtime.h>
 
-#include <cstring>
 #include <mutex>
+#include <string>
 
 #include "common.cuh"
 #include "internal.h"
@@ -74,22 +77,13 @@ extern "C" int nlo_bk_k2kf_static(const nlo_bk_params* params, const double* r, 
                                   const nlo_sobol_dirs* dirs, int64_t offset, int64_t samples,
                                   const nlo_bk_box* box, double* out, void* stream)
 {
-    if (!params || !dirs || !box || !r || !spline || !active || !count || !out)
+    if (!r || !spline || !active || !count || !out || !box)
         return set_last_error(NLO_ERR_INVALID, "nlo_bk_k2kf_static: NULL argument");
-    if (!(params->nc > 0) || !(params->nf == 0.0 || params->nf == 3.0 || params->nf == 5.0) ||
-        !(params->lambda_qcd > 0) || !(params->c2 > 0) || !(params->ksub > 0) ||
-        (params->rc_nlo != NLO_RC_NLO_SMALLEST && params->rc_nlo != NLO_RC_NLO_PARENT) ||
-        (params->precision != NLO_PRECISION_MIXED && params->precision != NLO_PRECISION_FP64))
-        return set_last_error(NLO_ERR_INVALID, "nlo_bk_k2kf_static: unsupported physics parameters");
-    if (dirs->dims < 4 || dirs->dims > 8)
-        return set_last_error(NLO_ERR_INVALID, "nlo_bk_k2kf_static: Sobol dimension count out of range");
-    for (int j = 0; j < dirs->dims; ++j) {
-        if (dirs->shift[j] >= (1u << 30))
-            return set_last_error(NLO_ERR_INVALID, "nlo_bk_k2kf_static: Sobol shift exceeds 30 bits");
-        for (int k = 0; k < 30; ++k)
-            if (dirs->state[j][k] >= (1u << 30))
-                return set_last_error(NLO_ERR_INVALID, "nlo_bk_k2kf_static: Sobol direction number exceeds 30 bits");
-    }
+    // the same parameter and direction-number checks as nlo_bk_k2kf, so both K2+Kf entry
+    // points accept and reject the same inputs
+    std::string why;
+    if (!check_params(params, why)) return set_last_error(NLO_ERR_INVALID, ("nlo_bk_k2kf_static: " + why).c_str());
+    if (!check_dirs(dirs, 4, why)) return set_last_error(NLO_ERR_INVALID, ("nlo_bk_k2kf_static: " + why).c_str());
     if (points < 3 || points > kStaticMaxPoints)
         return set_last_error(NLO_ERR_INVALID,
                               "nlo_bk_k2kf_static: points must be 3..512 (the fixed scratch array's limit); "
@@ -99,12 +93,7 @@ extern "C" int nlo_bk_k2kf_static(const nlo_bk_params* params, const double* r, 
     double* scratch = nullptr;
     const int rc = scratch_on_current_device(&scratch);
     if (rc != NLO_OK) return rc;
-    SobolDirsArg arg;
-    std::memset(&arg, 0, sizeof(arg));
-    arg.dims = dirs->dims;
-    std::memcpy(arg.state, dirs->state, sizeof(arg.state));
-    std::memcpy(arg.shift, dirs->shift, sizeof(arg.shift));
-    const cudaError_t e = launch_k2kf(*params, r, points, spline, active, count, arg, (uint64_t)offset,
+    const cudaError_t e = launch_k2kf(*params, r, points, spline, active, count, to_arg(dirs), (uint64_t)offset,
                                       (uint64_t)samples, *box, out, scratch, kStaticBlocks, (cudaStream_t)stream);
     if (e != cudaSuccess) return set_last_error(NLO_ERR_CUDA, cudaGetErrorString(e));
     return NLO_OK;

@@ -1,5 +1,21 @@
-"""Dipole table and the legacy four-header BK text format
-(mirrors torch_nlo_clean/src/nlo_torch/dipole/table.py:12-144)."""
+"""BK amplitude tables and the legacy text format the C++ solver writes.
+
+``DipoleTable`` keeps the interface of the reference's table type
+(torch_nlo_clean/src/nlo_torch/dipole/table.py:12-45): amplitudes ``N[len(y), len(r)]``
+on a positive, increasing r grid at increasing rapidities, with the ``x0`` the table
+starts from.  ``load_bk_table`` / ``save_bk_table`` read and write the text format of
+the C++ ``nlobk`` solver (the shipped ``xb_001_mc50w.dat``; the reference's reader and
+writer are dipole/table.py:48-144).
+
+The format, as this module implements it:
+
+* lines are stripped; blank lines and comments (``#`` not followed by ``##``) are ignored;
+* a *directive* is a line ``###<number>``;
+* the first four directives describe the grid: the smallest r, the ratio of consecutive
+  r, the number of r points and x0, so r_i = minr * ratio**i;
+* every further directive opens a block at rapidity ``<number>``, followed by exactly one
+  amplitude per r point, one per line.
+"""
 
 from __future__ import annotations
 
@@ -7,7 +23,35 @@ import math
 from dataclasses import dataclass
 from pathlib import Path
 
+import numpy as np
 import torch
+
+
+def _problems(table: "DipoleTable"):
+    """Yield (exception type, message) for the first rule the table breaks; the rules are
+    checked in order and the later ones assume the earlier hold."""
+    r, y, N = table.r, table.y, table.N
+    rules = (
+        (lambda: r.ndim == 1 and y.ndim == 1 and N.ndim == 2, ValueError,
+         "expected one-dimensional r and y and a two-dimensional N"),
+        (lambda: r.numel() >= 2 and y.numel() >= 1, ValueError, "a table needs at least 2 r points and 1 rapidity"),
+        (lambda: tuple(N.shape) == (y.numel(), r.numel()), ValueError,
+         f"N has shape {tuple(N.shape)}; expected (len(y), len(r)) = ({y.numel()}, {r.numel()})"),
+        (lambda: r.device == y.device == N.device, ValueError, "r, y and N live on different devices"),
+        (lambda: r.dtype == y.dtype == N.dtype, ValueError, "r, y and N have different dtypes"),
+        (lambda: r.is_floating_point(), TypeError, "r, y and N must be floating point"),
+        (lambda: bool(torch.isfinite(r).all()), ValueError, "r has a non-finite value"),
+        (lambda: bool(torch.isfinite(y).all()), ValueError, "y has a non-finite value"),
+        (lambda: bool(torch.isfinite(N).all()), ValueError, "N has a non-finite value"),
+        (lambda: bool((r > 0).all()) and bool((r.diff() > 0).all()), ValueError,
+         "r must be positive and strictly increasing"),
+        (lambda: y.numel() == 1 or bool((y.diff() > 0).all()), ValueError, "y must be strictly increasing"),
+        (lambda: math.isfinite(table.x0) and table.x0 > 0, ValueError, "x0 must be a positive finite number"),
+    )
+    for holds, kind, message in rules:
+        if not holds():
+            yield kind, message
+            return
 
 
 @dataclass(frozen=True, slots=True)
@@ -20,30 +64,19 @@ class DipoleTable:
     x0: float
 
     def __post_init__(self) -> None:
-        if self.r.ndim != 1 or self.y.ndim != 1 or self.N.ndim != 2:
-            raise ValueError("r and y must be one-dimensional and N must be two-dimensional")
-        if self.r.numel() < 2 or self.y.numel() < 1:
-            raise ValueError("a dipole table requires at least two r points and one y point")
-        if self.N.shape != (self.y.numel(), self.r.numel()):
-            raise ValueError("N must have shape (len(y), len(r))")
-        if self.r.device != self.y.device or self.r.device != self.N.device:
-            raise ValueError("r, y, and N must be on the same device")
-        if self.r.dtype != self.y.dtype or self.r.dtype != self.N.dtype:
-            raise ValueError("r, y, and N must have the same dtype")
-        if not self.r.is_floating_point():
-            raise TypeError("r, y, and N must be floating-point tensors")
-        if not bool(torch.isfinite(self.r).all()):
-            raise ValueError("r must contain only finite values")
-        if not bool(torch.isfinite(self.y).all()):
-            raise ValueError("y must contain only finite values")
-        if not bool(torch.isfinite(self.N).all()):
-            raise ValueError("N must contain only finite values")
-        if not bool((self.r > 0).all()) or not bool((self.r[1:] > self.r[:-1]).all()):
-            raise ValueError("r must be positive and strictly increasing")
-        if self.y.numel() > 1 and not bool((self.y[1:] > self.y[:-1]).all()):
-            raise ValueError("y must be strictly increasing")
-        if not math.isfinite(self.x0) or self.x0 <= 0:
-            raise ValueError("x0 must be positive and finite")
+        for kind, message in _problems(self):
+            raise kind(f"invalid dipole table: {message}")
+
+
+def _directive(line: str) -> str | None:
+    return line[3:].strip() if line.startswith("###") else None
+
+
+def _number(text: str, what: str, source: Path) -> float:
+    try:
+        return float(text)
+    except ValueError:
+        raise ValueError(f"{source}: {what} {text!r} is not a number") from None
 
 
 def load_bk_table(
@@ -52,108 +85,93 @@ def load_bk_table(
     dtype: torch.dtype = torch.float64,
     device: torch.device | str | None = None,
 ) -> DipoleTable:
-    """Read the four-header format: ###minr, ###r multiplier, ###points, ###x0,
-    then per rapidity '###y' followed by one amplitude per line (table.py:48-118)."""
+    """Read a table in the C++ solver's text format (see the module docstring)."""
 
-    filename = Path(path)
-    lines = filename.read_text(encoding="utf-8").splitlines()
-    headers: list[str] = []
-    data_start = 0
-    for number, line in enumerate(lines):
-        stripped = line.strip()
-        if stripped.startswith("###"):
-            headers.append(stripped[3:].strip())
-            if len(headers) == 4:
-                data_start = number + 1
-                break
-    if len(headers) != 4:
-        raise ValueError(f"{filename} does not contain four BK configuration headers")
+    source = Path(path)
+    directives: list[tuple[int, str]] = []  # (position in `values`, text)
+    values: list[str] = []
+    for raw in source.read_text(encoding="utf-8").splitlines():
+        line = raw.strip()
+        if not line:
+            continue
+        text = _directive(line)
+        if text is not None:
+            directives.append((len(values), text))
+        elif not line.startswith("#"):
+            values.append(line)
+    if len(directives) < 4:
+        raise ValueError(f"{source}: expected four grid directives (minr, ratio, points, x0)")
+    grid, blocks = directives[:4], directives[4:]
+    if grid[-1][0] != 0 or (blocks and blocks[0][0] != 0) or (not blocks and values):
+        raise ValueError(f"{source}: amplitude values before the first rapidity directive")
+    minr = _number(grid[0][1], "minr", source)
+    ratio = _number(grid[1][1], "r ratio", source)
+    count = _number(grid[2][1], "number of r points", source)
+    x0 = _number(grid[3][1], "x0", source)
+    if not (minr > 0 and ratio > 1 and count >= 2 and count == int(count) and x0 > 0):
+        raise ValueError(f"{source}: grid directives out of range (minr {minr}, ratio {ratio}, points {count}, "
+                         f"x0 {x0})")
+    points = int(count)
+    if not blocks:
+        raise ValueError(f"{source}: no rapidity blocks")
+    # each block's values run from its directive to the next one
+    bounds = [start for start, _ in blocks] + [len(values)]
+    for k, (start, stop) in enumerate(zip(bounds[:-1], bounds[1:])):
+        if stop - start != points:
+            raise ValueError(f"{source}: rapidity block {k} holds {stop - start} amplitudes, expected {points}")
+    ys = [_number(text, "rapidity", source) for _, text in blocks]
     try:
-        minr = float(headers[0])
-        multiplier = float(headers[1])
-        points = int(headers[2])
-        x0 = float(headers[3])
-    except ValueError as error:
-        raise ValueError(f"{filename} has an invalid BK configuration header") from error
-    if minr <= 0 or multiplier <= 1 or points < 2 or x0 <= 0:
-        raise ValueError(f"{filename} has invalid BK grid metadata")
-
-    ys: list[float] = []
-    rows: list[list[float]] = []
-    row: list[float] | None = None
-    for line in lines[data_start:]:
-        stripped = line.strip()
-        if not stripped or (stripped.startswith("#") and not stripped.startswith("###")):
-            continue
-        if stripped.startswith("###"):
-            if row is not None:
-                _append_row(filename, rows, row, points)
-            try:
-                ys.append(float(stripped[3:].strip()))
-            except ValueError as error:
-                raise ValueError(f"{filename} has an invalid rapidity header") from error
-            row = []
-            continue
-        if row is None:
-            raise ValueError(f"{filename} contains amplitude data before a rapidity header")
-        try:
-            row.append(float(stripped))
-        except ValueError as error:
-            raise ValueError(f"{filename} contains an invalid amplitude value") from error
-    if row is not None:
-        _append_row(filename, rows, row, points)
-    if not rows or len(rows) != len(ys):
-        raise ValueError(f"{filename} contains no complete rapidity blocks")
-    r = minr * torch.pow(
-        torch.tensor(multiplier, dtype=dtype, device=device),
-        torch.arange(points, dtype=dtype, device=device),
-    )
+        amplitudes = np.asarray(values, dtype=np.float64).reshape(len(blocks), points)
+    except ValueError:
+        bad = next(v for v in values if not _is_float(v))
+        raise ValueError(f"{source}: amplitude {bad!r} is not a number") from None
+    exponent = torch.arange(points, dtype=dtype, device=device)
+    r = minr * torch.pow(torch.tensor(ratio, dtype=dtype, device=device), exponent)
     return DipoleTable(
         r=r,
         y=torch.tensor(ys, dtype=dtype, device=device),
-        N=torch.tensor(rows, dtype=dtype, device=device),
+        N=torch.as_tensor(amplitudes, device=device).to(dtype),
         x0=x0,
     )
 
 
+def _is_float(text: str) -> bool:
+    try:
+        float(text)
+        return True
+    except ValueError:
+        return False
+
+
 def save_bk_table(path: str | Path, table: DipoleTable) -> None:
-    """Write the four-header format with 15-digit mantissas (table.py:121-144).
+    """Write ``table`` in the C++ solver's text format, 15-digit mantissas.
 
-    A float32 grid here is the float64 grid rounded once (solve_bk forms it in float64),
-    so r[1]/r[0] carries a rounding error that the 100th power turns into ~1e-5: the
-    multiplier of a float32 grid is taken from its end points in float64 instead, which
-    both passes the uniformity check and writes a header that reproduces the grid."""
+    The format stores the grid as (minr, ratio), so the grid must be logarithmically
+    uniform.  A float64 grid is written with ratio r[1]/r[0] and checked to 2e-12.  A
+    float32 grid is the float64 grid rounded once (solve_bk forms it in float64): its
+    r[1]/r[0] is off by about 1e-7, which the 100th power turns into 1e-5, so its ratio is
+    taken from the end points in float64 instead and checked to 5e-6; the header then
+    reproduces the grid to float32 rounding."""
 
-    r = table.r.detach().cpu()
-    y = table.y.detach().cpu()
-    N = table.N.detach().cpu()
-    if r.dtype == torch.float32:
-        r = r.double()
-        multiplier = (r[-1] / r[0]) ** (1.0 / (r.numel() - 1))
+    r = table.r.detach().to("cpu", torch.float64)
+    if table.r.dtype == torch.float32:
+        ratio = float((r[-1] / r[0]) ** (1.0 / (r.numel() - 1)))
         tolerance = 5e-6
     else:
-        multiplier = r[1] / r[0]
+        ratio = float(r[1] / r[0])
         tolerance = 2e-12
-    expected = r[0] * torch.pow(multiplier, torch.arange(r.numel(), dtype=r.dtype))
-    if not bool(torch.allclose(r, expected, rtol=tolerance, atol=0)):
-        raise ValueError("the legacy BK format requires a logarithmically uniform r grid")
-    output = [
-        "# nlo_bk_optimized_b200 BK dipole table",
-        f"###{r[0].item():.15e}",
-        f"###{multiplier.item():.15e}",
-        f"###{r.numel()}",
-        f"###{table.x0:.15e}",
-    ]
-    for index in range(y.numel()):
-        output.append(f"###{y[index].item():.15e}")
-        output.extend(f"{value:.15e}" for value in N[index].tolist())
-    Path(path).write_text("\n".join(output) + "\n", encoding="utf-8")
-
-
-def _append_row(filename: Path, rows: list[list[float]], row: list[float], points: int) -> None:
-    if len(row) != points:
-        raise ValueError(f"{filename} has {len(row)} amplitudes in a block; expected {points}")
-    rows.append(row)
+    rebuilt = float(r[0]) * ratio ** np.arange(r.numel(), dtype=np.float64)
+    if not np.allclose(r.numpy(), rebuilt, rtol=tolerance, atol=0.0):
+        raise ValueError("the legacy BK format stores (minr, ratio): the r grid must be logarithmically uniform")
+    y = table.y.detach().to("cpu", torch.float64).numpy()
+    N = table.N.detach().to("cpu", torch.float64).numpy()
+    header = ["# nlo_bk_optimized_b200 BK dipole table",
+              *(f"###{v:.15e}" for v in (float(r[0]), ratio)), f"###{r.numel()}", f"###{table.x0:.15e}"]
+    body = []
+    for rapidity, row in zip(y, N):
+        body.append(f"###{rapidity:.15e}")
+        body.extend(f"{v:.15e}" for v in row)
+    Path(path).write_text("\n".join(header + body) + "\n", encoding="utf-8")
 
 
 __all__ = ["DipoleTable", "load_bk_table", "save_bk_table"]

@@ -1,8 +1,11 @@
 """Generate ``dis_reference.npz`` from the reference implementation's DIS path.
 
-Run in a container that has the reference checkout (read-only) at ``/root/reference``:
+Run with the root of a reference checkout (read-only is enough) in the environment
+variable ``NLO_REFERENCE_ROOT`` (or as the first argument)::
 
-    PYTHONPATH=/root/reference/torch_nlo_clean/src python tests/golden/make_golden_dis.py
+    NLO_REFERENCE_ROOT=<checkout> python tests/golden/make_golden_dis.py [<checkout>]
+
+The script puts ``<checkout>/torch_nlo_clean/src`` on the import path itself.
 
 It imports the reference package ``nlo_torch`` and records, in float64 on the CPU,
 what its own functions return for seeded inputs:
@@ -31,10 +34,17 @@ Unit-cube points come from numpy's default_rng(20260301); each case is listed in
 from __future__ import annotations
 
 import math
+import os
+import sys
 from pathlib import Path
 
 import numpy as np
 import torch
+
+_ROOT = next((a for a in reversed(sys.argv[1:]) if Path(a).is_dir()), os.environ.get("NLO_REFERENCE_ROOT"))
+if not _ROOT:
+    raise SystemExit("set NLO_REFERENCE_ROOT (or pass the checkout) to the reference checkout's root")
+sys.path.insert(0, str(Path(_ROOT) / "torch_nlo_clean" / "src"))
 
 from nlo_torch.coupling import dis_alpha_s_freeze, dis_alpha_s_smooth
 from nlo_torch.dipole.amplitude import GBW, BKDipole

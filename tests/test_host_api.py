@@ -82,6 +82,29 @@ def test_table_round_trip_and_legacy_format(tmp_path):
     assert float(golden["x0"][0]) == pytest.approx(0.01)
 
 
+def test_legacy_table_reader_rejects_malformed_files(tmp_path):
+    grid = "###1e-5\n###1.5\n###3\n###0.01\n"
+    cases = {
+        "short_block": grid + "###0\n0.1\n0.2\n",
+        "long_block": grid + "###0\n0.1\n0.2\n0.3\n0.4\n",
+        "values_first": grid + "0.5\n###0\n0.1\n0.2\n0.3\n",
+        "no_blocks": grid,
+        "bad_value": grid + "###0\n0.1\nx\n0.3\n",
+        "bad_grid": "###1e-5\n###0.5\n###3\n###0.01\n###0\n0.1\n0.2\n0.3\n",
+        "three_directives": "###1e-5\n###1.5\n###3\n",
+    }
+    for name, text in cases.items():
+        path = tmp_path / f"{name}.dat"
+        path.write_text(text)
+        with pytest.raises(ValueError):
+            load_bk_table(path)
+    good = tmp_path / "good.dat"
+    good.write_text("# comment\n" + grid + "\n###0\n0.1\n0.2\n0.3\n## another comment\n###0.4\n0.2\n0.3\n0.4\n")
+    table = load_bk_table(good)
+    assert table.N.shape == (2, 3) and table.y.tolist() == [0.0, 0.4]
+    torch.testing.assert_close(table.r, torch.tensor([1e-5, 1.5e-5, 2.25e-5], dtype=torch.float64))
+
+
 def test_table_validation():
     r = torch.logspace(-3, 1, 8, dtype=torch.float64)
     with pytest.raises(ValueError):

@@ -49,12 +49,17 @@ def test_static_entry_point_matches_workspace_entry_point(precision):
     assert lib.nlo_bk_k2kf(params, r.data_ptr(), n, spline.data_ptr(), idx.data_ptr(), count.data_ptr(), dirs, 0,
                            samples, box, reference.data_ptr(), ws.data_ptr(), ws.numel(), stream) == 0
 
-    for _ in range(2):
-        out = torch.full((n, 3), float("nan"), dtype=torch.float64, device="cuda")
+    outs = [torch.full((n, 3), float("nan"), dtype=torch.float64, device="cuda") for _ in range(2)]
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]  # driver-level free bytes, not the caching allocator's
+    for out in outs:
         code = lib.nlo_bk_k2kf_static(params, r.data_ptr(), n, spline.data_ptr(), idx.data_ptr(), count.data_ptr(),
                                       dirs, 0, samples, box, out.data_ptr(), ctypes.c_void_p(stream))
         assert code == 0, lib.nlo_last_error().decode()
         torch.cuda.synchronize()
+    # the property the entry point exists for: nothing was allocated on the device
+    assert torch.cuda.mem_get_info()[0] == free_before
+    for out in outs:
         torch.testing.assert_close(out, reference, rtol=1e-12, atol=0.0)
 
 
@@ -67,3 +72,15 @@ def test_static_entry_point_rejects_grids_beyond_its_limit():
                                   1024, box, out.data_ptr(), None)
     assert code == 1
     assert b"512" in lib.nlo_last_error()
+
+
+def test_static_entry_point_rejects_what_the_workspace_entry_point_rejects():
+    lib = _native.load()
+    config, r, spline, idx, count, box = _inputs(99)
+    out = torch.empty((r.numel(), 3), dtype=torch.float64, device="cuda")
+    for field, value in (("order", 9), ("rc_lo", -1), ("resum_rc", 7)):
+        params = params_of(config, _native.PRECISION_MIXED)
+        setattr(params, field, value)
+        code = lib.nlo_bk_k2kf_static(params, r.data_ptr(), r.numel(), spline.data_ptr(), idx.data_ptr(),
+                                      count.data_ptr(), _native.sobol_dirs(4, 0), 0, 1024, box, out.data_ptr(), None)
+        assert code == 1, field

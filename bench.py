@@ -7,15 +7,17 @@ coupling, RK4 in rapidity with step 0.1 up to Y = 10, 2^20 scrambled Sobol point
 per parent per stage for K2+Kf, the fixed 8 x 24 rule per r interval for K1;
 FP32 integrands with FP64 sums, spline refit and RK update.
 
-A bench "step" is one RK4 step (four right-hand sides).  With the default
---steps 100 the timed region is exactly the evolution from Y = 0 to Y = 10;
-``value`` is seconds to Y = 10 (scaled by 100/K when K != 100).
+A bench "step" is one whole evolution from Y = 0 to Y = 10 (100 RK4 steps, 400
+right-hand sides, one nlo_bk_evolve call); ``value`` is the mean device time of the K
+timed evolutions, in seconds to Y = 10 -- measured, not scaled.  Outside the timed region
+the same evolution runs once in the all-FP64 device build on the same Sobol points, and
+``max_rel_err_vs_fp64`` is the largest relative difference of the timed build's rows.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-With --gpus N > 1 (one process per GPU under torchrun) the parents are sharded over the
-ranks with one NCCL all-reduce of dN/dY per RK stage; the total work is fixed (strong
-scaling) and the value is the slowest rank's device time.
+With --gpus N > 1 (one process per GPU under torchrun) K2+Kf is sharded over the ranks
+by Sobol index range and K1 by parent, with one NCCL all-reduce of dN/dY per RK stage;
+the total work is fixed (strong scaling) and the value is the slowest rank's device time.
 
 The line also carries a "dis" object: NLO DIS sigma_r throughput on a BK table evolved by
 the same workload (see measure_dis); --workload dis prints that measurement alone.  And a
@@ -23,8 +25,9 @@ the same workload (see measure_dis); --workload dis prints that measurement alon
 against its published C++ time (see measure_fixed; --workload fixed alone).
 
 --impl reference times the reference algorithm on the host cores (the oracle's
-C restatement, all threads) on a bounded sample of every step and reports the
-same metric extrapolated to the full workload.
+C restatement, all threads): each of its steps is one complete right-hand side of the
+workload at a rapidity spread over 0..10 (amplitudes from the oracle's own evolution),
+and the value is the mean stage time times the 400 stages.
 """
 
 from __future__ import annotations
@@ -33,7 +36,6 @@ import argparse
 import json
 import math
 import os
-import re
 import statistics
 import subprocess
 import sys
@@ -52,22 +54,29 @@ RPOINTS = 399
 MINR, MAXR = 1e-7, 1e2
 SAMPLES = 1 << 20
 QS0SQR = 0.2
-# Hand count of the FP32 operations of one (sample, parent) evaluation in
-# k2_pair_fast<true, 0> (csrc/k2kf.cu), per component of the packed pair: FMA = 2,
-# every other arithmetic op or MUFU transcendental = 1, compares, selects and min/max
-# excluded.  11 of them are MUFU operations (2 lg2 and 2 ex2 for the amplitudes at X and
-# X2, 4 rcp in the kernels, ex2 + lg2 + rcp in the coupling).
-FLOPS_PER_EVAL = 136
-MUFU_PER_EVAL = 11
+RK_STEPS = 100  # RK4 steps of one whole evolution (Y = 0 -> 10)
+SAMPLES_LOG2 = 20
+# Op census of one K2+Kf evaluation, from oracle/census.py (an op-counting run of the
+# oracle's FP64 restatement of _nlo_integrand x Jacobian on the workload's points at the
+# final state): per (sample, parent) pair, and per sample for the parent-independent part.
+# Arithmetic = add, sub, mul, div, sqrt; transcendental = exp, log, sin, cos, expm1, log1p.
+CENSUS_EVAL_FLOPS = 135
+CENSUS_EVAL_TRANSCENDENTALS = 13
+CENSUS_SAMPLE_FLOPS = 41
+CENSUS_SAMPLE_TRANSCENDENTALS = 20
 MUFU_PER_SM_PER_CLOCK = 16
+# DRAM bytes of one K2+Kf launch (dram__bytes_read.sum + dram__bytes_write.sum) from the
+# ncu capture of the kernel case (bench.py --kernel-case: 400 parents x 2^18 points): the
+# spline is staged into shared memory once per CTA and each CTA writes 3 doubles per
+# parent, so the bytes do not grow with the number of samples.
+K2KF_DRAM_BYTES_PER_LAUNCH = 52992
 # Launches of our kernels per RK4 step: 4 right-hand sides x (spline refit, active
 # list, K1, K2+Kf, K2+Kf finalize, assemble) + 4 stage combinations.
-LAUNCHES_PER_STEP = 4 * 6 + 4
+LAUNCHES_PER_RK4_STEP = 4 * 6 + 4
 SM_COUNT = 148
 FP32_LANES_PER_SM = 128
-# CPU baseline sample (about 10 s of host work): K2+Kf points per parent and K1 parents
-CPU_K2_LOG2 = 21
-CPU_K1_PARENTS = 128
+# CPU baseline sample: complete right-hand sides spread over the evolution
+CPU_STAGES = 3
 
 
 def workload_config():
@@ -192,49 +201,36 @@ def run_ours(args) -> None:
     status = torch.zeros(1, dtype=torch.int32, device=device)
     stream = torch.cuda.current_stream(device)
     steps, warmup = args.steps, args.warmup
-    table = torch.empty((max(steps, warmup) + 1, points), dtype=torch.float64, device=device)
+    table = torch.empty((RK_STEPS + 1, points), dtype=torch.float64, device=device)
+    N0 = N0_host.to(device)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)
 
     if world == 1:
-        def rk4_step(row: int) -> None:
-            _native.check(lib.nlo_bk_evolve(params, r.data_ptr(), points, 1, STEP, _native.STEPPERS["rk4"], dirs,
-                                            SAMPLES, box, table[row].data_ptr(), status.data_ptr(), ws.data_ptr(),
-                                            ws.numel(), stream.cuda_stream))
+        def evolution(precision_params) -> None:
+            """One bench step: the whole evolution Y = 0 -> 10 (100 RK4 steps) in one call."""
+            table[0].copy_(N0)
+            _native.check(lib.nlo_bk_evolve(precision_params, r.data_ptr(), points, RK_STEPS, STEP,
+                                            _native.STEPPERS["rk4"], dirs, SAMPLES, box, table.data_ptr(),
+                                            status.data_ptr(), ws.data_ptr(), ws.numel(), stream.cuda_stream))
     else:
-        # parents sharded over the ranks (i % world == rank), one NCCL all-reduce of the
-        # R-point derivative per stage (nlo_bk_optimized_b200/bk/sharded.py)
-        import ctypes
+        # K2+Kf sharded over the ranks by Sobol index range, K1 by parent; one NCCL
+        # all-reduce of the R-point derivative per stage (nlo_bk_optimized_b200/bk/sharded.py)
+        from nlo_bk_optimized_b200.bk.sharded import ShardedRhs, shard_steps
 
-        from nlo_bk_optimized_b200.bk.sharded import shard_steps
+        def evolution(precision_params) -> None:
+            sharded = ShardedRhs(precision_params, r, dirs, SAMPLES, box, rank, world, ws, status, stream)
+            table[0].copy_(N0)
+            rows = shard_steps(table[0], RK_STEPS, STEP, "rk4", sharded.rhs,
+                               lambda k: dist.all_reduce(k, op=dist.ReduceOp.SUM), sharded.stage, True)
+            for i, row in enumerate(rows[1:], start=1):
+                table[i].copy_(row)
 
-        def shard_rhs(N):
-            out = torch.empty_like(N)
-            _native.check(lib.nlo_bk_rhs_shard(params, r.data_ptr(), N.data_ptr(), points, rank, world, dirs,
-                                               SAMPLES, box, out.data_ptr(), ws.data_ptr(), ws.numel(),
-                                               stream.cuda_stream))
-            return out
-
-        def shard_stage(N, ks, coefs, clamp):
-            out = torch.empty_like(N)
-            kp = (ctypes.c_void_p * len(ks))(*[k.data_ptr() for k in ks])
-            cf = (ctypes.c_double * len(coefs))(*coefs)
-            _native.check(lib.nlo_bk_stage(N.data_ptr(), kp, cf, len(ks), points, int(clamp), out.data_ptr(),
-                                           status.data_ptr() if clamp else None, stream.cuda_stream))
-            return out
-
-        def rk4_step(row: int) -> None:
-            rows = shard_steps(table[row], 1, STEP, "rk4", shard_rhs,
-                               lambda k: dist.all_reduce(k, op=dist.ReduceOp.SUM), shard_stage, True)
-            table[row + 1].copy_(rows[1])
-
-    # warm-up: W steps from the initial condition (discarded)
-    table[0].copy_(N0_host.to(device))
-    for i in range(warmup):
-        rk4_step(i)
+    # warm-up: W whole evolutions (discarded)
+    for _ in range(warmup):
+        evolution(params)
     torch.cuda.synchronize()
 
-    # timed region: K steps from the initial condition
-    table[0].copy_(N0_host.to(device))
+    # timed region: K whole evolutions, the L2 flushed before each
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
     if world > 1:
@@ -245,17 +241,29 @@ def run_ours(args) -> None:
         for i in range(steps):
             flush.zero_()
             starts[i].record(stream)
-            rk4_step(i)
+            evolution(params)
             ends[i].record(stream)
         torch.cuda.synchronize()
     wall = time.perf_counter() - wall0
     if world > 1:
         dist.barrier()
-    device_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     if int(status.item()) != 0:
         raise FloatingPointError("non-finite amplitude in the benchmark evolution")
     clocks = sampler.summary()
-    final_N = table[steps].clone()
+    mixed_rows = table.clone()
+
+    # accuracy of the timed (mixed) build: the same evolution on the same Sobol points in
+    # the all-FP64 device build, outside the timed region
+    params64 = params_of(config, _native.PRECISION_FP64)
+    t64 = time.perf_counter()
+    evolution(params64)
+    torch.cuda.synchronize()
+    fp64_s = time.perf_counter() - t64
+    if int(status.item()) != 0:
+        raise FloatingPointError("non-finite amplitude in the FP64 evolution")
+    accuracy = mixed_vs_fp64(mixed_rows, table, r)
+    final_N = mixed_rows[RK_STEPS].clone()
 
     # dominant kernel (K2+Kf) timed alone with events on its stream, at the final state
     idx = torch.empty(points, dtype=torch.int32, device=device)
@@ -279,78 +287,36 @@ def run_ours(args) -> None:
     k2_ms = sum(k_start[i].elapsed_time(k_end[i]) for i in range(1, reps + 1)) / reps
     n_active = int(count.item())
 
-    # end to end through the public API with host buffers: host IC -> device -> evolve -> host table
-    e2e_config = config
-    e2e_maxy = steps * STEP
-    # one untimed call of the same API (one step) first, as the device leg has its warm-up
-    # steps: the first call of a process pays one-time module loading and host setup
+    # end to end through the public API with host buffers, whole evolutions: the host
+    # initial condition goes in, the full table comes back to the host
     if world == 1:
-        solve_bk(MV(qs0sqr=QS0SQR), STEP, e2e_config, device=device, dtype=torch.float32, seed=0).N.cpu()
+        def solve():
+            return solve_bk(MV(qs0sqr=QS0SQR), MAXY, config, device=device, dtype=torch.float32, seed=0)
     else:
         from nlo_bk_optimized_b200.bk.sharded import solve_bk_sharded
 
-        solve_bk_sharded(MV(qs0sqr=QS0SQR), STEP, e2e_config, device=device, dtype=torch.float32, seed=0).N.cpu()
+        def solve():
+            return solve_bk_sharded(MV(qs0sqr=QS0SQR), MAXY, config, device=device, dtype=torch.float32, seed=0)
+    solve().N.cpu()  # one untimed call: the first call of a process pays one-time module loading
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
+    e2e_reps = max(1, min(steps, args.e2e_steps))
     t0 = time.perf_counter()
-    if world == 1:
-        result = solve_bk(MV(qs0sqr=QS0SQR), e2e_maxy, e2e_config, device=device, dtype=torch.float32, seed=0)
-    else:
-        from nlo_bk_optimized_b200.bk.sharded import solve_bk_sharded
+    for _ in range(e2e_reps):
+        host_table = solve().N.cpu()
+    e2e_s = (time.perf_counter() - t0) / e2e_reps
+    h2d = 2 * points * 8  # the r grid and the initial row (float64)
+    d2h = host_table.numel() * host_table.element_size() + 4  # the table and the status word
 
-        result = solve_bk_sharded(MV(qs0sqr=QS0SQR), e2e_maxy, e2e_config, device=device, dtype=torch.float32,
-                                  seed=0)
-    host_table = result.N.cpu()
-    e2e_s = time.perf_counter() - t0
-    h2d = 2 * points * 8
-    d2h = host_table.numel() * host_table.element_size() + 4
-
-    step_ms = device_ms / steps
-    seconds = step_ms * (MAXY / STEP) / 1000.0
-    e2e_seconds = e2e_s * (MAXY / e2e_maxy)
+    seconds = sum(step_ms) / steps / 1000.0
     if world > 1:
-        t = torch.tensor([seconds, e2e_seconds], dtype=torch.float64, device=device)
+        t = torch.tensor([seconds, e2e_s], dtype=torch.float64, device=device)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        seconds, e2e_seconds = float(t[0]), float(t[1])
+        seconds, e2e_s = float(t[0]), float(t[1])
         dist.destroy_process_group()
     if rank != 0:
         return
-
-    # roofline of the dominant kernel: algorithmic FP32 flops per launch / launch time
-    evals = n_active * SAMPLES
-    achieved = evals * FLOPS_PER_EVAL / (k2_ms * 1e-3) / 1e12
-    sm_mhz = 1965.0
-    peak = SM_COUNT * FP32_LANES_PER_SM * 2 * sm_mhz * 1e6 / 1e12
-    roofline = {
-        "bound": "fp32",
-        "achieved": round(achieved, 3),
-        "peak": round(peak, 2),
-        "unit": "TFLOP/s",
-        "frac": round(achieved / peak, 4),
-        "traffic": None,
-        "kernel": "k2kf_kernel<float,true,0> (csrc/k2kf.cu)",
-        "peak_source": "nominal FP32 (148 SM x 128 lanes x 2 x 1965 MHz); MEASURED_PEAKS.json has only HBM and bf16",
-        "flops_per_eval": FLOPS_PER_EVAL,
-        "mufu": {
-            "ops_per_eval": MUFU_PER_EVAL,
-            "achieved_per_s": round(evals * MUFU_PER_EVAL / (k2_ms * 1e-3), 1),
-            "peak_per_s": SM_COUNT * MUFU_PER_SM_PER_CLOCK * sm_mhz * 1e6,
-            "frac": round(evals * MUFU_PER_EVAL / (k2_ms * 1e-3) / (SM_COUNT * MUFU_PER_SM_PER_CLOCK * sm_mhz * 1e6), 4),
-            "peak_source": "nominal 16 MUFU operations per SM per clock at 1965 MHz",
-        },
-        "evals_per_launch": evals,
-        "launch_ms": round(k2_ms, 4),
-        "evals_per_s": round(evals / (k2_ms * 1e-3), 1),
-    }
-    # DRAM bytes per K2+Kf launch from the committed ncu summary (constant in the
-    # number of Sobol points: the spline is staged into shared memory once per CTA)
-    summary = ROOT / "profiles" / "k2kf_k1_400r_kernel_case.md"
-    if summary.exists():
-        match = re.search(r"dram_bytes_per_launch_k2kf = (\d+)", summary.read_text())
-        if match:
-            roofline["traffic"] = int(match.group(1))
-            roofline["traffic_source"] = "profiles/k2kf_k1_400r_kernel_case.md"
 
     line = {
         "metric": METRIC,
@@ -359,27 +325,32 @@ def run_ours(args) -> None:
         "n_gpus": world,
         "steps": steps,
         "warmup": warmup,
-        "ms_per_step": round(step_ms, 4),
+        "ms_per_step": round(seconds * 1000.0, 3),
+        "step": "one whole evolution Y = 0 -> 10 (100 RK4 steps, 400 right-hand sides)",
+        "step_ms_min_max": [round(min(step_ms), 3), round(max(step_ms), 3)],
         "higher_is_better": False,
         "scaling": "strong",
         "vs_baseline": None,
         "dtype": "f32+f64",
         "data": "synthetic (MV initial condition)",
-        "config": workload_description({"parallelism": (f"r parents sharded over {world} GPUs, one NCCL "
-                                                         "all-reduce of dN/dY per stage") if world > 1
-                                        else "single GPU",
+        "config": workload_description({"parallelism": (f"K2+Kf Sobol range and K1 parents sharded over {world} "
+                                                         "GPUs, one NCCL all-reduce of dN/dY per stage")
+                                        if world > 1 else "single GPU",
                                         "active_parents_final": n_active}),
-        "e2e": {"value": round(e2e_seconds, 4), "unit": UNIT, "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h,
+        "max_rel_err_vs_fp64": accuracy["max_rel_err"],
+        "accuracy": dict(accuracy, fp64_evolution_s=round(fp64_s, 3),
+                         reference="the all-FP64 device build of the same evolution on the same Sobol points"),
+        "e2e": {"value": round(e2e_s, 4), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "steps": e2e_reps,
                 "api": ("nlo_bk_optimized_b200.solve_bk" if world == 1 else
                         "nlo_bk_optimized_b200.bk.sharded.solve_bk_sharded") + " + table.N.cpu()"},
-        "gpu_launches": LAUNCHES_PER_STEP * steps,
-        "roofline": roofline,
+        "gpu_launches": LAUNCHES_PER_RK4_STEP * RK_STEPS * steps,
+        "roofline": k2kf_roofline(n_active, k2_ms),
         "clocks": clocks,
         "wall_s_timed_region": round(wall, 3),
     }
     if not args.no_cpu_baseline and world == 1:
-        line["cpu_baseline"] = cpu_baseline(final_N.cpu().numpy(), r_host.numpy())
+        line["cpu_baseline"] = cpu_baseline()
     if not args.no_dis and world == 1:
         # the second half of the metric: NLO DIS sigma_r points/s on an evolved table
         line["dis"] = measure_dis(args.dis_points, args.dis_single, args.dis_check)
@@ -387,100 +358,175 @@ def run_ours(args) -> None:
     print(json.dumps(line))
 
 
-# ---------------------------------------------------------------------------
-def _oracle_rates(N, r, k2_samples: int, k1_parents: int) -> dict:
-    """Time the oracle (C restatement, all host threads) on a bounded sample."""
+def mixed_vs_fp64(mixed, fp64, r) -> dict:
+    """Relative difference of the mixed build's rows from the FP64 build's, over every row
+    after the initial one and every parent with N > 0 in the FP64 rows."""
+    import torch
 
+    m, f = mixed[1:].double(), fp64[1:].double()
+    keep = f > 0
+    rel = torch.where(keep, (m - f).abs() / f.abs().clamp_min(1e-300), torch.zeros_like(f))
+    per_row = rel.max(dim=1).values
+    per_parent = rel.max(dim=0).values
+    worst = int(torch.argmax(per_parent))
+    return {"max_rel_err": float(per_row.max()), "final_row_max_rel_err": float(per_row[-1]),
+            "max_abs_err": float((m - f).abs().max()), "worst_parent_r": float(r[worst]),
+            "rows_compared": int(f.shape[0]), "parents_compared": int(keep.any(dim=0).sum())}
+
+
+def k2kf_roofline(n_active: int, k2_ms: float) -> dict:
+    """Roofline of the dominant kernel from the op census of the FP64 restatement: per
+    launch, every (sample, active parent) pair costs CENSUS_EVAL_FLOPS arithmetic operations
+    and CENSUS_EVAL_TRANSCENDENTALS transcendental calls, and every sample costs
+    CENSUS_SAMPLE_* once (the parent-independent part)."""
+    evals = n_active * SAMPLES
+    flops = evals * CENSUS_EVAL_FLOPS + SAMPLES * CENSUS_SAMPLE_FLOPS
+    trans = evals * CENSUS_EVAL_TRANSCENDENTALS + SAMPLES * CENSUS_SAMPLE_TRANSCENDENTALS
+    seconds = k2_ms * 1e-3
+    sm_mhz = 1965.0
+    peak = SM_COUNT * FP32_LANES_PER_SM * 2 * sm_mhz * 1e6 / 1e12
+    mufu_peak = SM_COUNT * MUFU_PER_SM_PER_CLOCK * sm_mhz * 1e6
+    achieved = flops / seconds / 1e12
+    return {
+        "bound": "fp32",
+        "achieved": round(achieved, 3),
+        "peak": round(peak, 2),
+        "unit": "TFLOP/s",
+        "frac": round(achieved / peak, 4),
+        "traffic": K2KF_DRAM_BYTES_PER_LAUNCH,
+        "kernel": "k2kf_kernel<float,true,0> (csrc/k2kf.cu)",
+        "peak_source": "nominal FP32 (148 SM x 128 lanes x 2 x 1965 MHz); MEASURED_PEAKS.json has only HBM and bf16",
+        "census": {"source": "oracle/census.py: op-counting run of the oracle's FP64 K2+Kf restatement",
+                   "flops_per_eval": CENSUS_EVAL_FLOPS, "transcendentals_per_eval": CENSUS_EVAL_TRANSCENDENTALS,
+                   "flops_per_sample": CENSUS_SAMPLE_FLOPS,
+                   "transcendentals_per_sample": CENSUS_SAMPLE_TRANSCENDENTALS},
+        "transcendental": {"achieved_per_s": round(trans / seconds, 1), "peak_per_s": mufu_peak,
+                           "frac": round(trans / seconds / mufu_peak, 4),
+                           "peak_source": "nominal 16 MUFU operations per SM per clock at 1965 MHz"},
+        "evals_per_launch": evals,
+        "launch_ms": round(k2_ms, 4),
+        "evals_per_s": round(evals / seconds, 1),
+        "traffic_source": "ncu capture of one K2+Kf launch (400 parents x 2^18 points); the spline is staged "
+                          "once per CTA, so DRAM bytes do not grow with the sample count",
+    }
+
+
+# ---------------------------------------------------------------------------
+def _rows_at(ys):
+    """The oracle-evolved amplitude (oracle/evolution_rows_400r.npz) at rapidities ys,
+    linear between the stored rows."""
     import numpy as np
 
+    with np.load(ROOT / "oracle" / "evolution_rows_400r.npz") as data:
+        r, y, N = data["r"], data["y"], data["N"]
+    out = []
+    for v in ys:
+        k = int(min(max(np.searchsorted(y, v) - 1, 0), y.size - 2))
+        t = (v - y[k]) / (y[k + 1] - y[k])
+        out.append((1 - t) * N[k] + t * N[k + 1])
+    return r, out
+
+
+def _stage_seconds(N, r, points) -> tuple[float, int]:
+    """Wall time of one complete right-hand side of the oracle (C, OpenMP, all host threads):
+    the splines, K1 on every active parent, K2+Kf on every active parent x the given points."""
     import oracle
 
-    config = workload_config()
-    phys = oracle.physics(config)
-    active = np.nonzero((np.arange(r.size) > 0) & (N <= 0.99999))[0]
-    nspl = oracle.loglog_spline(r, N, 0)
-    sspl = oracle.loglog_spline(r, N, 1)
+    phys = oracle.physics(workload_config())
+    t0 = time.perf_counter()
+    d = oracle.derivative(N, r, phys, points, True)
+    return time.perf_counter() - t0, int((d.dNdy != 0).sum())
+
+
+def _sobol_points():
+    import oracle
+
     state, shift = oracle.sobol_state(4, 0)
-    points = oracle.sobol(state, shift, 0, k2_samples, as_f32=True)
-    lower, width = oracle.nlo_box(r)
-    t0 = time.perf_counter()
-    oracle.k2kf_sums(r[active], points, lower, width, True, sspl, phys)
-    t_k2 = time.perf_counter() - t0
-    pick = active[:: max(1, active.size // k1_parents)][:k1_parents]
-    t0 = time.perf_counter()
-    oracle.k1_fixed(r[pick], nspl, phys)
-    t_k1 = time.perf_counter() - t0
-    k2_rate = active.size * k2_samples / t_k2
-    k1_per_parent = t_k1 / pick.size
-    stage = active.size * SAMPLES / k2_rate + active.size * k1_per_parent
-    return {"k2kf_evals_per_s": k2_rate, "k1_s_per_parent": k1_per_parent, "stage_s": stage,
-            "active": int(active.size), "k1_parents": int(pick.size), "elapsed": t_k2 + t_k1}
+    return oracle.sobol(state, shift, 0, SAMPLES, as_f32=True)
 
 
-def cpu_baseline(N, r) -> dict:
+def _cpu_model() -> str:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_baseline() -> dict:
+    """The oracle timed on a bounded sample of the workload: CPU_STAGES complete stages
+    (2^20 points) spread over Y = 0..10, their mean times the 400 stages of the evolution."""
     import oracle
 
-    rates = _oracle_rates(N, r, k2_samples=1 << CPU_K2_LOG2, k1_parents=CPU_K1_PARENTS)
-    stages = 4 * MAXY / STEP
+    ys = [MAXY * (k + 0.5) / CPU_STAGES for k in range(CPU_STAGES)]
+    r, rows = _rows_at(ys)
+    points = _sobol_points()
+    times = [_stage_seconds(N, r, points)[0] for N in rows]
+    mean = sum(times) / len(times)
     return {
-        "value": round(rates["stage_s"] * stages, 1),
+        "value": round(mean * RK_STEPS * 4, 1),
         "unit": UNIT,
         "cores": oracle.num_threads(),
+        "cpu_model": _cpu_model(),
         "kind": "port",
-        "sample": (f"oracle (C, OpenMP) K2+Kf on {rates['active']} parents x 2^{CPU_K2_LOG2} Sobol points and K1 on "
-                   f"{rates['k1_parents']} parents at the final state; extrapolated to 400 stages x 2^20 points "
-                   f"({rates['elapsed']:.1f} s measured)"),
-        "k2kf_evals_per_s": round(rates["k2kf_evals_per_s"], 1),
+        "sample": (f"oracle (C, OpenMP): {CPU_STAGES} complete right-hand sides (every active parent, 2^20 Sobol "
+                   f"points, K1 fixed rule) at Y = {', '.join(f'{v:.2f}' for v in ys)}, mean x 400 stages "
+                   f"({sum(times):.1f} s measured)"),
+        "measured_s": round(sum(times), 2),
+        "extrapolation_factor": round(RK_STEPS * 4 / CPU_STAGES, 2),
     }
 
 
 def run_reference(args) -> None:
+    """The reference algorithm on the host cores (the oracle's C restatement, all threads):
+    each step is one complete right-hand side of the workload (splines, K1 on every active
+    parent, K2+Kf on every active parent x 2^20 Sobol points), step i at rapidity
+    Y_i = 10 (i + 1/2)/K on the oracle's own evolution rows; value = the mean stage time
+    x the 400 stages of the evolution (only the stage count is extrapolated)."""
     world, rank, local = dist_setup()
     if rank != 0:
         return
-    import numpy as np
-
     import oracle
 
-    config = workload_config()
-    r = oracle.r_grid(MINR, MAXR, RPOINTS)
-    N = oracle.mv_amplitude(r, QS0SQR)
-    k2_samples = 1 << 11
-
-    def step_sampled(N):
-        """One RK4 step's cost on a bounded sample: for each of the 4 stages, K2+Kf on all
-        active parents x 2^11 points and K1 on 32 parents, timed and extrapolated to the
-        full stage (2^20 points, every active parent)."""
-
-        return sum(_oracle_rates(N, r, k2_samples, 32)["stage_s"] for _ in range(4))
-
-    for _ in range(args.warmup):
-        step_sampled(N)
-    total = 0.0
+    steps, warmup = args.steps, args.warmup
+    ys = [MAXY * (k + 0.5) / steps for k in range(steps)]
+    r, rows = _rows_at(ys)
+    points = _sobol_points()
+    for k in range(warmup):
+        _stage_seconds(rows[k % len(rows)], r, points)
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        total += step_sampled(N)
+    times, active = [], []
+    for N in rows:
+        seconds, n_active = _stage_seconds(N, r, points)
+        times.append(seconds)
+        active.append(n_active)
     elapsed = time.perf_counter() - t0
-    step_s = total / args.steps
-    seconds = step_s * MAXY / STEP
+    stage_s = sum(times) / steps
+    seconds = stage_s * RK_STEPS * 4
+    sample = (f"{steps} complete right-hand sides (every active parent, 2^20 Sobol points, K1 fixed rule) at "
+              f"Y = {ys[0]:.2f}..{ys[-1]:.2f}; mean stage x 400 stages; {elapsed:.1f} s measured")
     line = {
         "metric": METRIC,
         "impl": "reference",
         "value": round(seconds, 2),
         "unit": UNIT,
         "n_gpus": world,
-        "steps": args.steps,
-        "warmup": args.warmup,
-        "ms_per_step": round(step_s * 1000, 2),
+        "steps": steps,
+        "warmup": warmup,
+        "ms_per_step": round(stage_s * 1000, 2),
+        "step": "one complete right-hand side (a quarter RK4 step) of the evolution",
         "higher_is_better": False,
         "scaling": "strong",
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (MV initial condition)",
-        "config": workload_description({"parallelism": "host cores"}),
-        "cpu_baseline": {"value": round(seconds, 2), "unit": UNIT, "cores": oracle.num_threads(), "kind": "port",
-                         "sample": "per stage: K2+Kf on all active parents x 2^11 Sobol points and K1 on 32 parents "
-                                   f"(oracle, C/OpenMP), extrapolated to the full stage; {elapsed:.1f} s measured"},
+        "config": workload_description({"parallelism": "host cores", "active_parents": active}),
+        "measured_s": round(elapsed, 2),
+        "extrapolation_factor": round(RK_STEPS * 4 / steps, 2),
+        "cpu_baseline": {"value": round(seconds, 2), "unit": UNIT, "cores": oracle.num_threads(),
+                         "cpu_model": _cpu_model(), "kind": "port", "sample": sample},
         "e2e": {"value": round(seconds, 2), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -847,10 +893,11 @@ def run_serve(args) -> None:
 def main() -> None:
     parser = argparse.ArgumentParser()
     parser.add_argument("--gpus", type=int, default=1)
-    parser.add_argument("--steps", type=int, default=100)
+    parser.add_argument("--steps", type=int, default=5)
     parser.add_argument("--warmup", type=int, default=3)
     parser.add_argument("--impl", choices=["ours", "reference"], default="ours")
     parser.add_argument("--no-cpu-baseline", action="store_true")
+    parser.add_argument("--e2e-steps", type=int, default=5, help="whole evolutions timed through solve_bk")
     parser.add_argument("--kernel-case", action="store_true",
                         help="run only the small K2+Kf/K1 case used for ncu captures")
     parser.add_argument("--workload", choices=["bk", "dis", "fixed", "batch", "serve"], default="bk",

@@ -190,9 +190,13 @@ int nlo_bk_rhs(const nlo_bk_params* params, const double* r, const double* N, in
                const nlo_sobol_dirs* dirs, int64_t samples, const nlo_bk_box* box, double* dndy, double* k1,
                double* k2kf, void* workspace, size_t workspace_bytes, void* stream);
 
-/* The right-hand side of nlo_bk_rhs restricted to the parents i with i % shards == shard
- * (the others get 0), for evolutions sharded over several GPUs: the ranks sum their dndy rows
- * with one all-reduce per stage (no counterpart in the reference, which runs on one GPU). */
+/* One shard's part of the right-hand side of nlo_bk_rhs, for evolutions sharded over several
+ * GPUs: K1 of the active parents i with i % shards == shard, plus K2+Kf of every active parent
+ * summed over this shard's Sobol indices [shard*samples/shards, (shard+1)*samples/shards) and
+ * divided by the total `samples`.  The shards' dndy rows add up to nlo_bk_rhs's (to FP64
+ * summation order), so the ranks sum them with one all-reduce per stage; every lane of the
+ * K2+Kf kernel stays busy on every rank (no counterpart in the reference, which runs on one
+ * GPU). */
 int nlo_bk_rhs_shard(const nlo_bk_params* params, const double* r, const double* N, int32_t points, int32_t shard,
                      int32_t shards, const nlo_sobol_dirs* dirs, int64_t samples, const nlo_bk_box* box, double* dndy,
                      void* workspace, size_t workspace_bytes, void* stream);
@@ -236,6 +240,57 @@ int nlo_bk_evolve_history(const nlo_bk_params* params, const double* r, int32_t 
                           int32_t first, int32_t steps, double step, int32_t stepper, const nlo_sobol_dirs* dirs,
                           int64_t samples, const nlo_bk_box* box, double* table, uint32_t* status, void* workspace,
                           size_t workspace_bytes, void* stream);
+
+/* ------------------------------------------------------------------ K2+Kf by Vegas
+ * The reference's default integrator of the NLO part (BKConfig.INTMETHOD_NLO = VEGAS;
+ * rapidity_derivative_nlo, bk/derivatives.py:389-421, driving vegas(),
+ * numerics/integration.py:120-589): one Vegas integral per active parent over the box of
+ * nlo_bk_box, on scrambled Sobol points of `dirs` (indices 0, 1, ... across the rounds of one
+ * right-hand side, the warm-up first).  Each parent's grid lives in the caller's `state` and,
+ * with reuse_grid, carries over to the next right-hand side with a shortened warm-up (the
+ * per-parent vegas_states of bk/evolution.py:85-100, 354-424).  Defaults in brackets are
+ * the reference's. */
+typedef struct nlo_bk_vegas_options {
+    int64_t samples_per_iteration; /* [MCINTPOINTS] >= 2 */
+    int64_t warmup_samples;        /* [max(2, MCINTPOINTS / 5)] 0 or >= 2: an adaptation-only round first */
+    int32_t max_iterations;        /* [4] */
+    int32_t min_iterations;        /* [2] 1 <= min <= max */
+    int32_t bins;                  /* [32] bins per dimension, 2..256 */
+    int32_t reuse_grid;            /* [1] VEGAS_REUSE_GRID: keep each parent's grid for the next right-hand side */
+    double reuse_warmup_fraction;  /* [0.25] VEGAS_REUSE_WARMUP_FRACTION: warm-up of a kept grid =
+                                      max(2, warmup_samples x fraction), none when either is 0 */
+    double epsrel;                 /* [0.2] converged after min_iterations once error <= max(epsabs, epsrel |value|) */
+    double epsabs;                 /* [0] */
+} nlo_bk_vegas_options;
+
+/* Per-parent Vegas state in doubles for a grid of `points` parents: per parent the grid
+ * edges [4][bins+1] and 16 scalars.  A zero-filled state holds no grid yet (each parent then
+ * starts from the uniform grid with the full warm-up). */
+size_t nlo_bk_vegas_state_doubles(int32_t points, int32_t bins);
+
+/* Workspace bytes of nlo_bk_rhs_vegas / nlo_bk_evolve_vegas (at least nlo_bk_rhs_workspace_bytes). */
+size_t nlo_bk_vegas_workspace_bytes(int32_t points, const nlo_bk_vegas_options* options);
+
+/* The right-hand side of nlo_bk_rhs_history with K2+Kf by Vegas for the active parents
+ * i with i % shards == shard (shard = 0, shards = 1: all of them; K1 takes the same parents,
+ * so the shards' rows add up to the whole right-hand side).  hist_y may be NULL without the
+ * kinematical constraint; hist_N's last row is the amplitude.  state: device
+ * double[nlo_bk_vegas_state_doubles(points, bins)], read and updated.  k2kf (optional)
+ * receives the Vegas value of each parent (the combined estimate of its iterations). */
+int nlo_bk_rhs_vegas(const nlo_bk_params* params, const double* r, int32_t points, const double* hist_y,
+                     const double* hist_N, int32_t rows, int32_t shard, int32_t shards,
+                     const nlo_bk_vegas_options* options, const nlo_sobol_dirs* dirs, const nlo_bk_box* box,
+                     double* state, double* dndy, double* k1, double* k2kf, void* workspace, size_t workspace_bytes,
+                     void* stream);
+
+/* nlo_bk_evolve_history with K2+Kf by Vegas (the reference's production evolution: the
+ * parents' grids carried through every right-hand side of the evolution when
+ * options->reuse_grid is set).  y may be NULL without the kinematical constraint. */
+int nlo_bk_evolve_vegas(const nlo_bk_params* params, const double* r, int32_t points, const double* y,
+                        int32_t first, int32_t steps, double step, int32_t stepper,
+                        const nlo_bk_vegas_options* options, const nlo_sobol_dirs* dirs, const nlo_bk_box* box,
+                        double* state, double* table, uint32_t* status, void* workspace, size_t workspace_bytes,
+                        void* stream);
 
 /* ======================================================================== NLO DIS
  * The NLO DIS cross-section integrands (dis/observables.py, dis/lo.py, dis/transverse.py,

@@ -1,12 +1,16 @@
 """BK evolution sharded over the GPUs of one node (one process per GPU).
 
-The right-hand side is independent across parent sizes r: rank k computes dN/dY for the
-parents i with i % world == k (``nlo_bk_rhs_shard``; interleaving balances the saturated,
-inactive parents) and the ranks sum their rows with one all-reduce of R doubles per
-stage (3.2 KB at R = 400, over NCCL).  Every rank then holds the full derivative, forms
-the stage with ``nlo_bk_stage`` and refits the full spline itself, so the ranks carry
-identical amplitude rows.  The stage sequence is that of ``nlo_bk_evolve`` (Euler,
-Kutta RK3 of bk/evolution.py:190-236, classical RK4).
+Rank k of W computes its share of the right-hand side (``nlo_bk_rhs_shard``): K1 of the
+parents i with i % W == k (interleaving balances the saturated, inactive parents), and
+K2+Kf of every active parent over the k-th W-th of the Sobol indices, divided by the total
+sample count.  The ranks sum their rows with one all-reduce of R doubles per stage (3.2 KB
+at R = 400, over NCCL), which gives every rank the whole derivative: K1 exactly, K2+Kf up
+to the order of the FP64 sums.  Splitting K2+Kf by sample range rather than by parent
+keeps every lane of its kernel busy on every rank, and each rank stages only its own
+share of the (parent-independent) sample records.  Every rank then forms the stage with
+``nlo_bk_stage`` and refits the full spline itself, so the ranks carry identical rows.  The
+stage sequence is that of ``nlo_bk_evolve`` (Euler, Kutta RK3 of bk/evolution.py:190-236,
+classical RK4).
 
 ``shard_steps`` is the device-independent driver: it takes the rank's partial
 right-hand side, the all-reduce and the stage combination as functions, which lets the
@@ -63,6 +67,36 @@ def shard_steps(N0: torch.Tensor, steps: int, step: float, stepper: str, rhs: Rh
     return rows
 
 
+class ShardedRhs:
+    """A rank's share of the right-hand side (``nlo_bk_rhs_shard``) and the stage
+    combination (``nlo_bk_stage``) on its device, as the functions ``shard_steps`` takes."""
+
+    def __init__(self, params, r: torch.Tensor, dirs, samples: int, box, rank: int, world: int,
+                 workspace: torch.Tensor, status: torch.Tensor, stream) -> None:
+        self.lib = _native.load()
+        self.params, self.r, self.dirs, self.samples, self.box = params, r, dirs, int(samples), box
+        self.rank, self.world = rank, world
+        self.workspace, self.status = workspace, status
+        self.stream = stream if isinstance(stream, int) or stream is None else stream.cuda_stream
+
+    def rhs(self, N: torch.Tensor) -> torch.Tensor:
+        out = torch.empty_like(N)
+        _native.check(self.lib.nlo_bk_rhs_shard(self.params, self.r.data_ptr(), N.data_ptr(), self.r.numel(),
+                                                self.rank, self.world, self.dirs, self.samples, self.box,
+                                                out.data_ptr(), self.workspace.data_ptr(), self.workspace.numel(),
+                                                self.stream))
+        return out
+
+    def stage(self, N: torch.Tensor, ks: list, coefs: list, clamp: bool) -> torch.Tensor:
+        out = torch.empty_like(N)
+        kp = (ctypes.c_void_p * len(ks))(*[k.data_ptr() for k in ks])
+        cf = (ctypes.c_double * len(coefs))(*coefs)
+        # like nlo_bk_evolve, only the completed step is clamped and checked
+        _native.check(self.lib.nlo_bk_stage(N.data_ptr(), kp, cf, len(ks), self.r.numel(), int(clamp),
+                                            out.data_ptr(), self.status.data_ptr() if clamp else None, self.stream))
+        return out
+
+
 def solve_bk_sharded(initial_condition, maxy: float, config: BKConfig = BKConfig(), *,
                      device: torch.device | str | None = None, dtype: torch.dtype = torch.float32, seed: int = 0,
                      group: "torch.distributed.ProcessGroup | None" = None) -> DipoleTable:
@@ -84,7 +118,6 @@ def solve_bk_sharded(initial_condition, maxy: float, config: BKConfig = BKConfig
     device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
     if device.type != "cuda":
         raise ValueError("the sharded evolution runs on CUDA devices only")
-    lib = _native.load()
     params = params_of(config, precision_of(config, dtype))
     r_host = _r_grid(config, device="cpu", dtype=torch.float64)
     N0 = initial_row(initial_condition, r_host, device).contiguous()
@@ -100,28 +133,15 @@ def solve_bk_sharded(initial_condition, maxy: float, config: BKConfig = BKConfig
     steps = len(ys)
     clamp = bool(config.FORCE_POSITIVE_N)
 
-    def rhs(N: torch.Tensor) -> torch.Tensor:
-        out = torch.empty_like(N)
-        _native.check(lib.nlo_bk_rhs_shard(params, r.data_ptr(), N.data_ptr(), points, rank, world, dirs,
-                                           int(config.MCINTPOINTS), box, out.data_ptr(), ws.data_ptr(), ws.numel(),
-                                           stream))
-        return out
+    sharded = ShardedRhs(params, r, dirs, int(config.MCINTPOINTS), box, rank, world, ws, status, stream)
 
     def all_reduce(k: torch.Tensor) -> None:
         if world > 1:
             dist.all_reduce(k, op=dist.ReduceOp.SUM, group=group)
 
-    def stage(N: torch.Tensor, ks: list, coefs: list, clamp_: bool) -> torch.Tensor:
-        out = torch.empty_like(N)
-        kp = (ctypes.c_void_p * len(ks))(*[k.data_ptr() for k in ks])
-        cf = (ctypes.c_double * len(coefs))(*coefs)
-        # like nlo_bk_evolve, only the completed step is clamped and checked
-        _native.check(lib.nlo_bk_stage(N.data_ptr(), kp, cf, len(ks), points, int(clamp_), out.data_ptr(),
-                                       status.data_ptr() if clamp_ else None, stream))
-        return out
-
     with torch.cuda.device(device):
-        rows = shard_steps(N0, steps, config.DE_SOLVER_STEP, config.stepper, rhs, all_reduce, stage, clamp)
+        rows = shard_steps(N0, steps, config.DE_SOLVER_STEP, config.stepper, sharded.rhs, all_reduce,
+                           sharded.stage, clamp)
         if int(status.item()) != 0:
             raise FloatingPointError("non-finite BK amplitude during the rapidity evolution")
     y = torch.tensor([0.0, *ys], dtype=dtype, device=device)
@@ -129,4 +149,4 @@ def solve_bk_sharded(initial_condition, maxy: float, config: BKConfig = BKConfig
     return DipoleTable(r=r.to(dtype), y=y, N=N.to(dtype), x0=initial_condition.x0)
 
 
-__all__ = ["shard_steps", "solve_bk_sharded"]
+__all__ = ["ShardedRhs", "shard_steps", "solve_bk_sharded"]

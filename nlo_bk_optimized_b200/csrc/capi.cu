@@ -66,10 +66,10 @@ void gauss_legendre(int n, double* x, double* w)
 size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
 
 // Workspace layout of one right-hand-side evaluation.
-size_t rhs_bytes(int points, size_t* offsets /*[8] or NULL*/)
+size_t rhs_bytes(int points, size_t* offsets /*[10] or NULL*/)
 {
     size_t o = 0;
-    size_t off[8];
+    size_t off[10];
     off[0] = o; o = align_up(o + sizeof(double) * spline_doubles(points));
     off[1] = o; o = align_up(o + sizeof(int32_t) * (size_t)points);
     off[2] = o; o = align_up(o + sizeof(int32_t) * 4);
@@ -78,13 +78,15 @@ size_t rhs_bytes(int points, size_t* offsets /*[8] or NULL*/)
     off[5] = o; o = align_up(o + sizeof(double) * 3 * (size_t)points * (size_t)k2kf_max_blocks());
     off[6] = o; o = align_up(o + sizeof(double) * 2 * (size_t)points);
     off[7] = o; o = align_up(o + sizeof(double) * kc_weights_doubles(points));
+    off[8] = o; o = align_up(o + sizeof(int32_t) * (size_t)points);
+    off[9] = o; o = align_up(o + sizeof(int32_t) * 4);
     if (offsets) std::memcpy(offsets, off, sizeof(off));
     return o;
 }
 
 RhsBuffers carve(void* ws, int points)
 {
-    size_t off[8];
+    size_t off[10];
     rhs_bytes(points, off);
     char* base = static_cast<char*>(ws);
     RhsBuffers b;
@@ -96,6 +98,8 @@ RhsBuffers carve(void* ws, int points)
     b.partial = reinterpret_cast<double*>(base + off[5]);
     b.factor = reinterpret_cast<double*>(base + off[6]);
     b.kc = reinterpret_cast<double*>(base + off[7]);
+    b.k1_active = reinterpret_cast<int32_t*>(base + off[8]);
+    b.k1_count = reinterpret_cast<int32_t*>(base + off[9]);
     b.k2kf_blocks = k2kf_max_blocks();
     return b;
 }
@@ -128,7 +132,7 @@ int run_rhs(const nlo_bk_params& p, const double* r, const double* N, int points
             uint64_t samples, const nlo_bk_box& box, double* dndy, double* k1_out, double* k2kf_out,
             const RhsBuffers& b, bool factor_ready, cudaStream_t stream, int shard = 0, int shards = 1,
             const double* hist_y = nullptr, const double* hist_N = nullptr, int rows = 0,
-            const SideStream* side = nullptr)
+            const SideStream* side = nullptr, const BkVegasCall* vegas = nullptr)
 {
     cudaError_t e;
     K1History history;
@@ -143,8 +147,20 @@ int run_rhs(const nlo_bk_params& p, const double* r, const double* N, int points
     if ((e = launch_splines(r, N, points, p.force_positive, b.factor, factor_ready ? 0 : 1, b.spline, stream)) !=
         cudaSuccess)
         return cuda_fail(e, "splines");
-    if ((e = launch_active(N, points, shard, shards, b.active, b.count, stream)) != cudaSuccess)
+    // Sobol QMC: K2+Kf takes every active parent (a shard owns a range of Sobol indices), K1
+    // the active parents i with i % shards == shard.  Vegas: both take the shard's parents.
+    const bool split_samples = vegas == nullptr;
+    if ((e = launch_active(N, points, split_samples ? 0 : shard, split_samples ? 1 : shards, b.active, b.count,
+                           stream)) != cudaSuccess)
         return cuda_fail(e, "active");
+    const int32_t* k1_active = b.active;
+    const int32_t* k1_count = b.count;
+    if (shards > 1 && split_samples) {
+        if ((e = launch_active(N, points, shard, shards, b.k1_active, b.k1_count, stream)) != cudaSuccess)
+            return cuda_fail(e, "active");
+        k1_active = b.k1_active;
+        k1_count = b.k1_count;
+    }
     const bool beside = side && side->ok;
     cudaStream_t k1_stream = stream;
     if (beside) {
@@ -152,18 +168,34 @@ int run_rhs(const nlo_bk_params& p, const double* r, const double* N, int points
         if ((e = cudaStreamWaitEvent(side->aux, side->fork, 0)) != cudaSuccess) return cuda_fail(e, "fork");
         k1_stream = side->aux;
     }
-    if ((e = launch_k1(p, r, points, b.spline, b.active, b.count, b.k1, k1_stream, history)) != cudaSuccess)
+    if ((e = launch_k1(p, r, points, b.spline, k1_active, k1_count, b.k1, k1_stream, history)) != cudaSuccess)
         return cuda_fail(e, "k1");
     if (beside && (e = cudaEventRecord(side->join, side->aux)) != cudaSuccess) return cuda_fail(e, "join");
     // orders without NLO kernels (Order.has_nlo_kernels, bk/config.py:44-50) take no K2 + Kf:
     // zero samples clear the sums and launch nothing
-    const uint64_t nlo_samples = order_has_nlo(p.order) ? samples : 0;
-    if ((e = launch_k2kf(p, r, points, b.spline, b.active, b.count, dirs, 0, nlo_samples, box, b.k2kf, b.partial,
-                         b.k2kf_blocks, stream)) != cudaSuccess)
-        return cuda_fail(e, "k2kf");
+    double k2kf_factor = 0.0;
+    if (vegas) {
+        if (order_has_nlo(p.order)) {
+            if ((e = launch_k2kf_vegas(p, r, N, points, b.spline, shard, shards, dirs, box, *vegas, b.k2kf, stream)) !=
+                cudaSuccess)
+                return cuda_fail(e, "k2kf vegas");
+            k2kf_factor = 1.0;  // the Vegas values are integrals already
+        } else if ((e = cudaMemsetAsync(b.k2kf, 0, sizeof(double) * 3 * (size_t)points, stream)) != cudaSuccess) {
+            return cuda_fail(e, "k2kf clear");
+        }
+    } else {
+        const uint64_t nlo_samples = order_has_nlo(p.order) ? samples : 0;
+        // this shard's Sobol indices [first, last) of the nlo_samples points; the sums are
+        // divided by nlo_samples, so the shards' right-hand sides add up to the whole one
+        const uint64_t first = nlo_samples * (uint64_t)shard / (uint64_t)shards;
+        const uint64_t last = nlo_samples * (uint64_t)(shard + 1) / (uint64_t)shards;
+        if ((e = launch_k2kf(p, r, points, b.spline, b.active, b.count, dirs, first, last - first, box, b.k2kf,
+                             b.partial, b.k2kf_blocks, stream)) != cudaSuccess)
+            return cuda_fail(e, "k2kf");
+        k2kf_factor = nlo_samples ? 1.0 / (double)nlo_samples : 0.0;
+    }
     if (beside && (e = cudaStreamWaitEvent(stream, side->join, 0)) != cudaSuccess) return cuda_fail(e, "join");
-    if ((e = launch_assemble(b.k1, b.k2kf, points, nlo_samples ? 1.0 / (double)nlo_samples : 0.0, dndy, k2kf_out,
-                             stream)) != cudaSuccess)
+    if ((e = launch_assemble(b.k1, b.k2kf, points, k2kf_factor, dndy, k2kf_out, stream)) != cudaSuccess)
         return cuda_fail(e, "assemble");
     if (k1_out) {
         if ((e = cudaMemcpyAsync(k1_out, b.k1, sizeof(double) * points, cudaMemcpyDeviceToDevice, stream)) !=
@@ -431,7 +463,7 @@ int nlo_bk_rhs_history(const nlo_bk_params* params, const double* r, int32_t poi
 static int evolve_rows(const nlo_bk_params* params, const double* r, int32_t points, const double* y, int32_t first,
                 int32_t steps, double step, int32_t stepper, const nlo_sobol_dirs* dirs, int64_t samples,
                 const nlo_bk_box* box, double* table, uint32_t* status, void* workspace, size_t workspace_bytes,
-                void* stream)
+                void* stream, const BkVegasCall* vegas = nullptr)
 {
     std::string why;
     if (!check_params(params, why)) return fail(NLO_ERR_INVALID, why);
@@ -466,7 +498,7 @@ static int evolve_rows(const nlo_bk_params* params, const double* r, int32_t poi
         bool factor_ready = it > first;
         auto f = [&](const double* in, double* out) {
             const int code = run_rhs(*params, r, in, points, dirs_arg, (uint64_t)samples, *box, out, nullptr,
-                                     nullptr, b, factor_ready, s, 0, 1, y, table, it + 1, &side);
+                                     nullptr, b, factor_ready, s, 0, 1, y, table, it + 1, &side, vegas);
             factor_ready = true;
             return code;
         };
@@ -517,6 +549,91 @@ int nlo_bk_evolve(const nlo_bk_params* params, const double* r, int32_t points, 
                                      "nlo_bk_evolve_history");
     return evolve_rows(params, r, points, nullptr, 0, steps, step, stepper, dirs, samples, box, table, status,
                        workspace, workspace_bytes, stream);
+}
+
+size_t nlo_bk_vegas_state_doubles(int32_t points, int32_t bins)
+{
+    if (points < 1 || bins < 2 || bins > 256) return 0;
+    return (size_t)points * bk_vegas_state_doubles(bins);
+}
+
+static bool check_vegas(const nlo_bk_vegas_options* o, std::string& why)
+{
+    if (!o) { why = "Vegas options are NULL"; return false; }
+    if (o->samples_per_iteration < 2) { why = "Vegas requires at least two samples per iteration"; return false; }
+    if (o->warmup_samples == 1 || o->warmup_samples < 0) { why = "warmup_samples must be zero or at least two"; return false; }
+    if (o->max_iterations < 1) { why = "Vegas requires at least one iteration"; return false; }
+    if (o->min_iterations < 1 || o->min_iterations > o->max_iterations) {
+        why = "min_iterations must lie between one and max_iterations";
+        return false;
+    }
+    if (o->bins < 2 || o->bins > 256) { why = "bins must be 2..256"; return false; }
+    if (!(o->reuse_warmup_fraction >= 0.0 && o->reuse_warmup_fraction <= 1.0)) {
+        why = "reuse_warmup_fraction must lie between zero and one";
+        return false;
+    }
+    if (!(o->epsrel >= 0.0) || !(o->epsabs >= 0.0)) { why = "epsrel and epsabs must be non-negative"; return false; }
+    if (o->warmup_samples + (int64_t)o->max_iterations * o->samples_per_iteration > (int64_t(1) << 30)) {
+        why = "the Vegas rounds of one right-hand side exceed 2^30 Sobol points";
+        return false;
+    }
+    return true;
+}
+
+size_t nlo_bk_vegas_workspace_bytes(int32_t points, const nlo_bk_vegas_options* options)
+{
+    std::string why;
+    if (points < 3 || !check_vegas(options, why)) return 0;
+    return nlo_bk_rhs_workspace_bytes(points) + align_up(bk_vegas_scratch_bytes(points, options->bins));
+}
+
+// The Vegas buffers at the end of the workspace (after the right-hand side and stage rows).
+static BkVegasCall vegas_call(void* workspace, int points, const nlo_bk_vegas_options* options, double* state)
+{
+    char* scratch = static_cast<char*>(workspace) + nlo_bk_rhs_workspace_bytes(points);
+    return bk_vegas_carve(scratch, points, *options, state);
+}
+
+int nlo_bk_rhs_vegas(const nlo_bk_params* params, const double* r, int32_t points, const double* hist_y,
+                     const double* hist_N, int32_t rows, int32_t shard, int32_t shards,
+                     const nlo_bk_vegas_options* options, const nlo_sobol_dirs* dirs, const nlo_bk_box* box,
+                     double* state, double* dndy, double* k1, double* k2kf, void* workspace, size_t workspace_bytes,
+                     void* stream)
+{
+    std::string why;
+    if (!check_params(params, why)) return fail(NLO_ERR_INVALID, why);
+    if (!check_dirs(dirs, 4, why)) return fail(NLO_ERR_INVALID, why);
+    if (!check_vegas(options, why)) return fail(NLO_ERR_INVALID, why);
+    if (points < 3 || points > 4096) return fail(NLO_ERR_INVALID, "points must be 3..4096");
+    if (rows < 1) return fail(NLO_ERR_INVALID, "the history needs at least one row");
+    if (shards < 1 || shard < 0 || shard >= shards) return fail(NLO_ERR_INVALID, "shard must lie in [0, shards)");
+    if (params->kinematical_constraint && !hist_y)
+        return fail(NLO_ERR_INVALID, "the kinematical constraint needs the history rapidities");
+    if (!r || !hist_N || !dndy || !box || !state) return fail(NLO_ERR_INVALID, "NULL buffer");
+    if (!workspace || workspace_bytes < nlo_bk_vegas_workspace_bytes(points, options))
+        return fail(NLO_ERR_WORKSPACE, "workspace too small for nlo_bk_rhs_vegas");
+    const RhsBuffers b = carve(workspace, points);
+    const BkVegasCall call = vegas_call(workspace, points, options, state);
+    const double* N = hist_N + (size_t)(rows - 1) * points;
+    const SideStream side;
+    return run_rhs(*params, r, N, points, to_arg(dirs), (uint64_t)options->samples_per_iteration, *box, dndy, k1, k2kf,
+                   b, false, (cudaStream_t)stream, shard, shards, hist_y, hist_N, rows, &side, &call);
+}
+
+int nlo_bk_evolve_vegas(const nlo_bk_params* params, const double* r, int32_t points, const double* y, int32_t first,
+                        int32_t steps, double step, int32_t stepper, const nlo_bk_vegas_options* options,
+                        const nlo_sobol_dirs* dirs, const nlo_bk_box* box, double* state, double* table,
+                        uint32_t* status, void* workspace, size_t workspace_bytes, void* stream)
+{
+    std::string why;
+    if (!check_vegas(options, why)) return fail(NLO_ERR_INVALID, why);
+    if (!state) return fail(NLO_ERR_INVALID, "NULL buffer");
+    if (points < 3 || points > 4096) return fail(NLO_ERR_INVALID, "points must be 3..4096");
+    if (!workspace || workspace_bytes < nlo_bk_vegas_workspace_bytes(points, options))
+        return fail(NLO_ERR_WORKSPACE, "workspace too small for nlo_bk_evolve_vegas");
+    const BkVegasCall call = vegas_call(workspace, points, options, state);
+    return evolve_rows(params, r, points, y, first, steps, step, stepper, dirs, options->samples_per_iteration, box,
+                       table, status, workspace, workspace_bytes, stream, &call);
 }
 
 int nlo_bk_evolve_history(const nlo_bk_params* params, const double* r, int32_t points, const double* y,

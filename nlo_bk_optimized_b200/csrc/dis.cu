@@ -15,6 +15,7 @@
 #include "dis_internal.h"
 #include "dis_terms.cuh"
 #include "sobol.cuh"
+#include "vegas_common.cuh"
 
 namespace nlo {
 namespace dis {
@@ -469,71 +470,12 @@ __global__ void vegas_finalize_kernel(double* __restrict__ state, int state_stri
     if (sc[kStConverged] != 0.0) return;
     const int keys = 2 + D * bins;
     const double* red = reduced + (size_t)job * keys;
-    const double* hist = red + 2;
-    // smoothed importance (+ eps), per dimension
-    for (int k = threadIdx.x; k < D * bins; k += blockDim.x) {
-        const int d = k / bins, b = k % bins;
-        auto imp = [&](int q) {
-            const int n = c[d * bins + q];
-            return hist[d * bins + q] / (double)(n > 1 ? n : 1);
-        };
-        double v;
-        if (b == 0)
-            v = (imp(0) + imp(1)) / 2.0;
-        else if (b == bins - 1)
-            v = (imp(bins - 2) + imp(bins - 1)) / 2.0;
-        else
-            v = (imp(b - 1) + imp(b) + imp(b + 1)) / 3.0;
-        smooth[k] = v + 2.220446049250313e-16;
-    }
+    vegas::rebin(st, red + 2, c, D, bins, smooth, cum, ne);
     __syncthreads();
-    if (threadIdx.x < D) {
-        const int d = threadIdx.x;
-        double* cd = cum + d * (bins + 1);
-        cd[0] = 0.0;
-        for (int b = 0; b < bins; ++b) cd[b + 1] = cd[b] + smooth[d * bins + b];
-        const double* e = st + d * (bins + 1);
-        double* out = ne + d * (bins + 1);
-        const double total = cd[bins];
-        const double step = total / bins;
-        int idx = 0;
-        for (int k = 0; k <= bins; ++k) {
-            // torch.linspace(0, total, bins + 1); the targets increase, so the
-            // searchsorted(right) - 1 index only moves forward
-            const double target = k < (bins + 1) / 2 ? step * k : total - step * (bins - k);
-            while (idx < bins && cd[idx + 1] <= target) ++idx;
-            const int i = idx > bins - 1 ? bins - 1 : idx;
-            const double frac = (target - cd[i]) / smooth[d * bins + i];
-            out[k] = e[i] + frac * (e[i + 1] - e[i]);
-        }
-        out[0] = 0.0;
-        out[bins] = 1.0;
-    }
-    __syncthreads();
-    for (int k = threadIdx.x; k < D * (bins + 1); k += blockDim.x) st[k] = ne[k];
     for (int k = threadIdx.x; k < D * bins; k += blockDim.x) c[k] = 0;
     if (threadIdx.x == 0) {
         sc[kStEvals] += (double)samples;
-        if (!warmup) {
-            const double s = red[0], s2 = red[1];
-            const double n = (double)samples;
-            const double est = s / n;
-            double var = (s2 - s * s / n);
-            var = var > 0.0 ? var : 0.0;
-            var = var / (n - 1.0) / n;
-            var = var > 2.2250738585072014e-308 ? var : 2.2250738585072014e-308;
-            sc[kStSumWeightedEst] += est / var;
-            sc[kStSumWeights] += 1.0 / var;
-            sc[kStIterations] += 1.0;
-            sc[kStLastEstimate] = est;
-            sc[kStLastVariance] = var;
-            const double value = sc[kStSumWeightedEst] / sc[kStSumWeights];
-            const double error = ::sqrt(1.0 / sc[kStSumWeights]);
-            sc[kStValue] = value;
-            sc[kStError] = error;
-            const double tol = epsabs > epsrel * ::fabs(value) ? epsabs : epsrel * ::fabs(value);
-            if (sc[kStIterations] >= (double)min_iterations && error <= tol) sc[kStConverged] = 1.0;
-        }
+        if (!warmup) vegas::combine(sc, red[0], red[1], (double)samples, min_iterations, epsrel, epsabs);
     }
 }
 
@@ -724,6 +666,15 @@ cudaError_t dis_launch_reduce_finalize(int D, int bins, int jobs, int blocks_per
     if (e != cudaSuccess) return e;
     dis::vegas_finalize_kernel<<<jobs, 128, fsmem, stream>>>(state, state_stride, D, bins, samples, reduced, counts,
                                                                warmup, min_iterations, epsrel, epsabs);
+    return cudaGetLastError();
+}
+
+cudaError_t vegas_launch_reduce(const double* partial, int keys, int blocks_per_job, int jobs, double* reduced,
+                                cudaStream_t stream)
+{
+    dim3 rgrid((keys + dis::kReduceKeys - 1) / dis::kReduceKeys, jobs);
+    dis::vegas_reduce_kernel<<<rgrid, dis::kReduceKeys * dis::kReduceSlices, 0, stream>>>(partial, keys,
+                                                                                       blocks_per_job, reduced);
     return cudaGetLastError();
 }
 

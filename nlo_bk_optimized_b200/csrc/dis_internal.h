@@ -8,6 +8,7 @@
 #include <string>
 
 #include "internal.h"
+#include "vegas_common.cuh"
 
 namespace nlo {
 namespace dis {
@@ -24,19 +25,19 @@ struct GLRules {
     double x_coarse[32], w_coarse[32];
 };
 
-// Per-integral Vegas state: edges[D][bins+1] followed by these scalar slots.
-enum StateSlot {
-    kStSumWeightedEst = 0,  // sum of estimate / variance over reported iterations
-    kStSumWeights = 1,      // sum of 1 / variance
-    kStValue = 2,
-    kStError = 3,
-    kStEvals = 4,
-    kStIterations = 5,
-    kStConverged = 6,
-    kStLastEstimate = 7,
-    kStLastVariance = 8,
-    kStSlots = 16,
-};
+// Per-integral Vegas state: edges[D][bins+1] followed by the scalar slots of
+// vegas_common.cuh (kSt*).
+using vegas::StateSlot;
+using vegas::kStSumWeightedEst;
+using vegas::kStSumWeights;
+using vegas::kStValue;
+using vegas::kStError;
+using vegas::kStEvals;
+using vegas::kStIterations;
+using vegas::kStConverged;
+using vegas::kStLastEstimate;
+using vegas::kStLastVariance;
+using vegas::kStSlots;
 
 struct VegasLaunch {
     const void* args;            // device DisArgs<T>[jobs]

@@ -42,6 +42,8 @@ struct RhsBuffers {
     double* partial;  // [k2kf_blocks][points][3]
     double* factor;   // [2][points] spline factorisation (grid only)
     double* kc;       // kc_weights_doubles(points): kinematical-constraint window weights
+    int32_t* k1_active;  // [points] K1's parents of a shard (sharded right-hand sides)
+    int32_t* k1_count;   // [1]
     int k2kf_blocks;
 };
 
@@ -83,6 +85,29 @@ cudaError_t launch_k2kf(const nlo_bk_params& p, const double* r, int points, con
                         const int32_t* active, const int32_t* count, const SobolDirsArg& dirs, uint64_t offset,
                         uint64_t samples, const nlo_bk_box& box, double* out, double* partial, int max_blocks,
                         cudaStream_t stream);
+// K2+Kf by Vegas (k2kf_vegas.cu): the per-call buffers, carved from the caller's workspace.
+struct BkVegasCall {
+    nlo_bk_vegas_options options;
+    double* state = nullptr;   // [points][stride], persistent grids
+    int stride = 0;
+    int blocks_per_job = 1;
+    double* partial = nullptr;  // [points][blocks][4 + 4 bins]
+    double* reduced = nullptr;  // [points][4 + 4 bins]
+    int32_t* counts = nullptr;  // [points][4 bins]
+};
+size_t bk_vegas_state_doubles(int bins);
+int bk_vegas_blocks_per_job(int points);
+size_t bk_vegas_scratch_bytes(int points, int bins);
+BkVegasCall bk_vegas_carve(void* scratch, int points, const nlo_bk_vegas_options& options, double* state);
+// Vegas K2+Kf of the active parents i % shards == shard of N into out[points][3] = [value, 0,
+// error^2] (zeros elsewhere).
+cudaError_t launch_k2kf_vegas(const nlo_bk_params& p, const double* r, const double* N, int points,
+                              const double* spline, int shard, int shards, const SobolDirsArg& dirs,
+                              const nlo_bk_box& box, const BkVegasCall& call, double* out, cudaStream_t stream);
+// Fixed-order sum of per-CTA partial rows [jobs][blocks][keys] over the CTAs (dis.cu).
+cudaError_t vegas_launch_reduce(const double* partial, int keys, int blocks_per_job, int jobs, double* reduced,
+                                cudaStream_t stream);
+
 cudaError_t launch_assemble(const double* k1, const double* k2kf, int points, double inv_samples, double* dndy,
                             double* k2kf_total, cudaStream_t stream);
 cudaError_t launch_axpy_stage(const double* N, const double* const* k, const double* coef, int nk, int points,

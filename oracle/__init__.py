@@ -13,6 +13,8 @@ the reference's evolution driver:
 * ``derivative``   -- dN/dY assembly, bk/evolution.py:329-351 and 354-488
                       (K1 by the fixed rule of custom_kernels/bk/k1/kernel.cu:2040-2092,
                       K2+Kf by quasi-Monte Carlo on fixed Sobol points)
+* ``derivative_shard`` -- one shard's part of it (K1 by parent, K2+Kf by point range),
+                      for the multi-rank evolution (no counterpart in the reference)
 * ``evolve``       -- stepping loop bk/evolution.py:85-159 with the Euler
                       (:110-122), Kutta RK3 (:190-236) or classical RK4 stepper
 * ``r_grid``       -- bk/evolution.py:584-592
@@ -390,6 +392,31 @@ def derivative(N: np.ndarray, r: np.ndarray, phys: Physics, points: np.ndarray, 
     dNdy = K1 + K2 + Kf
     dNdy = np.where(np.isfinite(dNdy), dNdy, 0.0)
     return Derivative(dNdy, K1, K2, Kf, sq)
+
+
+def derivative_shard(N: np.ndarray, r: np.ndarray, phys: Physics, points: np.ndarray, map_f32: bool, shard: int,
+                     shards: int, force_positive: bool = True) -> np.ndarray:
+    """One shard's part of ``derivative``: K1 of the active parents i with i % shards == shard,
+    plus K2+Kf of every active parent summed over the shard's points
+    [shard n / shards, (shard + 1) n / shards) and divided by the total n; the shards' parts
+    add up to ``derivative(...).dNdy``."""
+
+    nspl = loglog_spline(r, N, 0, force_positive)
+    sspl = loglog_spline(r, N, 1, force_positive)
+    active = np.nonzero((np.arange(r.size) > 0) & (N <= 0.99999))[0]
+    out = np.zeros_like(N)
+    if active.size:
+        mine = active[active % shards == shard]
+        if mine.size:
+            out[mine] += k1_fixed(r[mine], nspl, phys)
+        if has_nlo_kernels(phys):
+            n = points.shape[0]
+            lo, hi = n * shard // shards, n * (shard + 1) // shards
+            if hi > lo:
+                lower, width = nlo_box(r)
+                sums = k2kf_sums(r[active], points[lo:hi], lower, width, map_f32, sspl, phys)
+                out[active] += (sums[:, 0] + sums[:, 1]) / n
+    return np.where(np.isfinite(out), out, 0.0)
 
 
 def evolve(N0: np.ndarray, r: np.ndarray, phys: Physics, points: np.ndarray, map_f32: bool, step: float,

@@ -1,5 +1,5 @@
 """The bench's own arm on a B200: the JSON line carries the contract's keys with
-consistent values (a short run: 2 timed RK4 steps, no CPU baseline, no DIS), and the
+consistent values (a short run: 2 timed whole evolutions, no CPU baseline, no DIS), and the
 fixed-Sobol workload line agrees with the reference's C++ values it is compared with."""
 
 from __future__ import annotations
@@ -26,21 +26,28 @@ def _line(*args: str) -> dict:
 
 
 def test_bench_line_contract():
-    d = _line("--steps", "2", "--warmup", "3", "--no-cpu-baseline", "--no-dis")
+    d = _line("--steps", "2", "--warmup", "3", "--e2e-steps", "1", "--no-cpu-baseline", "--no-dis")
     for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
-                "vs_baseline", "dtype", "data", "config", "e2e", "gpu_launches", "roofline", "clocks"):
+                "vs_baseline", "dtype", "data", "config", "e2e", "gpu_launches", "roofline", "clocks",
+                "max_rel_err_vs_fp64", "accuracy"):
         assert key in d, key
     assert d["n_gpus"] == 1 and d["steps"] == 2 and d["warmup"] == 3
-    # value is seconds to Y = 10 scaled from the timed steps (h = 0.1: 100 steps)
-    assert d["value"] == pytest.approx(d["ms_per_step"] * 100 / 1000, rel=1e-3)
-    assert d["gpu_launches"] == 28 * 2
+    # a step is one whole evolution to Y = 10: value is its mean device time, not a scaled one
+    assert d["value"] == pytest.approx(d["ms_per_step"] / 1000, rel=1e-3)
+    lo, hi = d["step_ms_min_max"]
+    assert lo <= d["ms_per_step"] <= hi
+    assert d["gpu_launches"] == 28 * 100 * 2
+    # the headline precision bound, against the all-FP64 device build on the same points
+    assert 0 < d["max_rel_err_vs_fp64"] <= 1e-4
+    assert d["accuracy"]["rows_compared"] == 100
     e2e = d["e2e"]
     assert e2e["value"] > 0 and e2e["h2d_bytes_per_step"] > 0 and e2e["d2h_bytes_per_step"] > 0
     roof = d["roofline"]
     assert roof["bound"] == "fp32" and roof["unit"] == "TFLOP/s"
     assert 0 < roof["frac"] < 1.5 and roof["frac"] == pytest.approx(roof["achieved"] / roof["peak"], rel=1e-2)
-    assert 0 < roof["mufu"]["frac"] < 1.5
-    assert roof["traffic"] is None or roof["traffic"] > 0
+    assert 0 < roof["transcendental"]["frac"] < 1.5
+    assert roof["census"]["flops_per_eval"] > 0
+    assert roof["traffic"] > 0
 
 
 def test_fixed_sobol_workload_line():

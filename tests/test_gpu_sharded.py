@@ -11,16 +11,18 @@ import torch
 pytestmark = pytest.mark.gpu
 
 
-def test_shard_rhs_sum_to_full_rhs():
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_shard_rhs_sum_to_full_rhs(precision):
     from nlo_bk_optimized_b200 import MV, BKConfig, _native
     from nlo_bk_optimized_b200.bk.evolution import _r_grid, nlo_box, params_of, rhs, workspace
 
-    config = BKConfig(RPOINTS=99, MINR=1e-6, MAXR=1e2, MCINTPOINTS=1 << 12, PRECISION="fp64")
+    config = BKConfig(RPOINTS=99, MINR=1e-6, MAXR=1e2, MCINTPOINTS=1 << 12, PRECISION=precision)
     r = _r_grid(config, device="cuda", dtype=torch.float64)
     N = MV(qs0sqr=0.2).dipole_amplitude(r.cpu()).to("cuda", torch.float64)
     full, _, _ = rhs(N, r, config, seed=0)
     lib = _native.load()
-    params = params_of(config, _native.PRECISION_FP64)
+    code = _native.PRECISION_FP64 if precision == "fp64" else _native.PRECISION_MIXED
+    params = params_of(config, code)
     lower, width = nlo_box(float(r[0]), float(r[-1]))
     ws = workspace(r.device, r.numel())
     for shards in (2, 3):
@@ -31,11 +33,12 @@ def test_shard_rhs_sum_to_full_rhs():
                                                _native.sobol_dirs(4, 0), config.MCINTPOINTS,
                                                _native.box(lower, width), out.data_ptr(), ws.data_ptr(), ws.numel(),
                                                _native.stream_handle(r.device)))
-            mask = (torch.arange(r.numel(), device="cuda") % shards) != shard
-            assert torch.all(out[mask] == 0)
             total += out
-        rel = ((total - full).abs() / full.abs().clamp_min(1e-300)).max()
-        assert float(rel) < 1e-12
+        # K1 is split exactly; K2+Kf's sums over the shards' point ranges are added in another
+        # order (the mixed build's FP32 partial sums also group the samples differently)
+        scale = full.abs() + 1e-9 * full.abs().max()
+        rel = ((total - full).abs() / scale).max()
+        assert float(rel) < (1e-12 if precision == "fp64" else 1e-6)
 
 
 def test_single_rank_sharded_driver_matches_solve_bk():

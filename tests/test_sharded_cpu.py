@@ -1,7 +1,8 @@
 """The multi-rank BK evolution driver (nlo_bk_optimized_b200/bk/sharded.py) over gloo on
-CPU, world size 2: each rank supplies the oracle right-hand side of its own parents
-(i % 2 == rank) and the driver's all-reduce and stage sequence must reproduce the
-single-process oracle evolution."""
+CPU, world size 2: each rank supplies the oracle's shard right-hand side (K1 of its own
+parents i % 2 == rank, K2+Kf of every active parent over its half of the Sobol points),
+and the driver's all-reduce and stage sequence must reproduce the single-process oracle
+evolution."""
 
 from __future__ import annotations
 
@@ -46,9 +47,7 @@ def _worker(rank, world, port, stepper, results):
         r, N0, phys, pts = problem()
 
         def rhs(N):
-            full = oracle.derivative(N.numpy(), r, phys, pts, True).dNdy
-            mine = np.where(np.arange(r.size) % world == rank, full, 0.0)
-            return torch.from_numpy(mine.copy())
+            return torch.from_numpy(oracle.derivative_shard(N.numpy(), r, phys, pts, True, rank, world))
 
         rows = shard_steps(torch.from_numpy(N0.copy()), STEPS, STEP, stepper, rhs,
                            lambda k: dist.all_reduce(k, op=dist.ReduceOp.SUM), stage_torch, True)
@@ -82,3 +81,11 @@ def test_two_rank_evolution_matches_single_process(stepper):
         assert got.shape == ref.shape
         assert np.max(np.abs(got - ref)) < 1e-12
     assert np.array_equal(results[0], results[1])
+
+
+def test_shard_parts_add_up_to_the_whole_derivative():
+    r, N0, phys, pts = problem()
+    whole = oracle.derivative(N0, r, phys, pts, True).dNdy
+    for shards in (2, 3, 5):
+        total = sum(oracle.derivative_shard(N0, r, phys, pts, True, k, shards) for k in range(shards))
+        assert np.max(np.abs(total - whole) / np.maximum(np.abs(whole), 1e-300)) < 1e-12

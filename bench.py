@@ -81,9 +81,10 @@ CPU_STAGES = 3
 
 def workload_config():
     from nlo_bk_optimized_b200 import BKConfig
+    from nlo_bk_optimized_b200.bk.config import IntegrationMethod
 
     return BKConfig(RPOINTS=RPOINTS, MINR=MINR, MAXR=MAXR, MCINTPOINTS=SAMPLES, DE_SOLVER_STEP=STEP,
-                    STEPPER="rk4", PRECISION="mixed")
+                    STEPPER="rk4", PRECISION="mixed", INTMETHOD_NLO=IntegrationMethod.SOBOL)
 
 
 def workload_description(extra: dict | None = None) -> dict:
@@ -766,9 +767,10 @@ def _sets(n: int, seed: int = 0):
 
 def _small_bk_config(samples: int = 1 << 16):
     from nlo_bk_optimized_b200 import BKConfig
+    from nlo_bk_optimized_b200.bk.config import IntegrationMethod
 
     return BKConfig(RPOINTS=199, MINR=1e-6, MAXR=1e2, MCINTPOINTS=samples, DE_SOLVER_STEP=0.2, STEPPER="rk4",
-                    PRECISION="mixed", ALPHA_S_CAP=0.7)
+                    PRECISION="mixed", ALPHA_S_CAP=0.7, INTMETHOD_NLO=IntegrationMethod.SOBOL)
 
 
 def run_batch(args) -> None:

@@ -114,6 +114,22 @@ class VegasOptions(ctypes.Structure):
     ]
 
 
+class BKVegasOptions(ctypes.Structure):
+    """nlo_bk_vegas_options: Vegas of the K2+Kf integral (IntegrationMethod.VEGAS)."""
+
+    _fields_ = [
+        ("samples_per_iteration", ctypes.c_int64),
+        ("warmup_samples", ctypes.c_int64),
+        ("max_iterations", ctypes.c_int32),
+        ("min_iterations", ctypes.c_int32),
+        ("bins", ctypes.c_int32),
+        ("reuse_grid", ctypes.c_int32),
+        ("reuse_warmup_fraction", ctypes.c_double),
+        ("epsrel", ctypes.c_double),
+        ("epsabs", ctypes.c_double),
+    ]
+
+
 class FixedSobolOptions(ctypes.Structure):
     _fields_ = [
         ("training_samples", ctypes.c_int64),
@@ -149,6 +165,10 @@ EXPORTED = (
     "nlo_ic_evaluate",
     "nlo_bk_rhs_shard",
     "nlo_bk_stage",
+    "nlo_bk_vegas_state_doubles",
+    "nlo_bk_vegas_workspace_bytes",
+    "nlo_bk_rhs_vegas",
+    "nlo_bk_evolve_vegas",
     "nlo_dis_table_doubles",
     "nlo_dis_table_prepare",
     "nlo_dis_table_prepare_interpolated",
@@ -214,6 +234,16 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.nlo_bk_rhs_shard.argtypes = [P(BKParams), vp, vp, i32, i32, i32, P(SobolDirs), i64, P(Box), vp, vp, sz, vp]
     lib.nlo_bk_stage.restype = ctypes.c_int
     lib.nlo_bk_stage.argtypes = [vp, P(vp), P(d), i32, i32, i32, vp, vp, vp]
+    lib.nlo_bk_vegas_state_doubles.restype = sz
+    lib.nlo_bk_vegas_state_doubles.argtypes = [i32, i32]
+    lib.nlo_bk_vegas_workspace_bytes.restype = sz
+    lib.nlo_bk_vegas_workspace_bytes.argtypes = [i32, P(BKVegasOptions)]
+    lib.nlo_bk_rhs_vegas.restype = ctypes.c_int
+    lib.nlo_bk_rhs_vegas.argtypes = [P(BKParams), vp, i32, vp, vp, i32, i32, i32, P(BKVegasOptions), P(SobolDirs),
+                                     P(Box), vp, vp, vp, vp, vp, sz, vp]
+    lib.nlo_bk_evolve_vegas.restype = ctypes.c_int
+    lib.nlo_bk_evolve_vegas.argtypes = [P(BKParams), vp, i32, vp, i32, i32, d, i32, P(BKVegasOptions), P(SobolDirs),
+                                        P(Box), vp, vp, vp, vp, sz, vp]
     lib.nlo_dis_table_doubles.restype = sz
     lib.nlo_dis_table_doubles.argtypes = [i32, i32]
     lib.nlo_dis_table_prepare.restype = ctypes.c_int

@@ -18,7 +18,7 @@ from concurrent.futures import ThreadPoolExecutor
 import torch
 
 from nlo_bk_optimized_b200 import _native
-from nlo_bk_optimized_b200.bk.config import BKConfig
+from nlo_bk_optimized_b200.bk.config import BKConfig, require_sobol
 from nlo_bk_optimized_b200.dipole.table import DipoleTable
 
 STREAM_CHOICES = (1, 2, 4, 8, 16)
@@ -45,6 +45,7 @@ def evolve_batch(N0: torch.Tensor, r: torch.Tensor, steps: int, config: BKConfig
     """Rows [B, steps+1, R] (float64, on the device of r) for initial rows N0 [B, R]."""
     from nlo_bk_optimized_b200.bk.evolution import nlo_box, params_of, precision_of
 
+    require_sobol(config, "the batched evolution")
     device = r.device
     B, points = N0.shape
     if len(samples) != B:

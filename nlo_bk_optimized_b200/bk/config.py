@@ -3,12 +3,18 @@
 Field names, enum names, defaults and validation follow the reference ``BKConfig``
 so that user code constructs it unchanged.  Additions for the B200 path:
 
-* ``IntegrationMethod.SOBOL`` -- quasi-Monte Carlo K2+Kf on the first
-  ``MCINTPOINTS`` points of ``SobolEngine(4, scramble=True, seed)`` for every
-  parent and stage (the default here; the reference's VEGAS/MISER/MULTIPLE
-  choices are accepted by the dataclass but are not implemented on the device).
-* ``STEPPER`` -- "rk4" (default), "rk3" (the reference's Kutta RK3,
-  bk/evolution.py:190-236) or "euler"; ``EULER_METHOD=True`` selects "euler".
+* ``IntegrationMethod.VEGAS`` (the default, as in the reference) integrates K2+Kf per
+  parent by Vegas on the device with the reference's settings (32 bins, warm-up
+  max(2, MCINTPOINTS/5), 2..4 iterations of MCINTPOINTS, epsrel 0.2) and, with
+  ``VEGAS_REUSE_GRID``, each parent's grid carried through the evolution with a warm-up
+  shortened by ``VEGAS_REUSE_WARMUP_FRACTION``.  ``IntegrationMethod.SOBOL`` (new) is
+  quasi-Monte Carlo on the first ``MCINTPOINTS`` points of ``SobolEngine(4,
+  scramble=True, seed)`` for every parent and stage: the fast B200 path, which the
+  headline benchmark uses.  MISER and MULTIPLE are accepted by the dataclass and rejected
+  by the device path.
+* ``STEPPER`` -- "rk3" (the default: the reference's Kutta RK3 of its CUDA production
+  path, bk/evolution.py:190-236), "rk4" (classical) or "euler"; ``EULER_METHOD=True``
+  selects "euler".
 * ``PRECISION`` -- "mixed" (FP32 integrands, FP64 sums/splines/RK update) or
   "fp64"; ``None`` picks "mixed" for float32 tables and "fp64" otherwise.
 * ``ALPHA_S_CAP`` -- if positive, alpha_s = min(alpha_s, ALPHA_S_CAP)
@@ -75,7 +81,7 @@ class BKOrder(Enum):
         return self in {BKOrder.LO_RESUM_DLOG_SLOG, BKOrder.NLO_RESUM_DLOG_SLOG}
 
 
-STEPPERS = ("rk4", "rk3", "euler")
+STEPPERS = ("rk3", "rk4", "euler")
 PRECISIONS = ("mixed", "fp64")
 
 
@@ -99,7 +105,7 @@ class BKConfig:
     RC_LO: RunningCouplingLO = RunningCouplingLO.BALITSKY_LO
     RC_NLO: RunningCouplingNLO = RunningCouplingNLO.SMALLEST_NLO
     RESUM_RC: ResummationCoupling = ResummationCoupling.RESUM_RC_SMALLEST
-    INTMETHOD_NLO: IntegrationMethod = IntegrationMethod.SOBOL
+    INTMETHOD_NLO: IntegrationMethod = IntegrationMethod.VEGAS
     FORCE_POSITIVE_N: bool = True
     SYMMETRIZE_Z_Z2_INTEGRATION: bool = True
     DNDY: bool = False
@@ -113,7 +119,7 @@ class BKConfig:
     K1_FIXED_REFINE: bool = False
     VEGAS_REUSE_GRID: bool = True
     VEGAS_REUSE_WARMUP_FRACTION: float = 0.25
-    STEPPER: str = "rk4"
+    STEPPER: str = "rk3"
     PRECISION: str | None = None
     ALPHA_S_CAP: float = 0.0
 
@@ -157,12 +163,21 @@ def device_supported(config: BKConfig) -> str | None:
     """Return why a configuration is outside the device kernels, or None.
 
     Every Order, RC_LO, RC_NLO, RESUM_RC and NF of BKConfig, and the kinematical
-    constraint, run on the device; the K2+Kf integral is always the fixed Sobol QMC
-    estimate."""
+    constraint, run on the device; K2+Kf integrates by VEGAS or SOBOL."""
 
-    if config.Order.has_nlo_kernels and config.INTMETHOD_NLO is not IntegrationMethod.SOBOL:
-        return "the device K2+Kf integrates with IntegrationMethod.SOBOL"
+    if config.Order.has_nlo_kernels and config.INTMETHOD_NLO not in (IntegrationMethod.VEGAS,
+                                                                     IntegrationMethod.SOBOL):
+        return (f"the device K2+Kf integrates with IntegrationMethod.VEGAS or SOBOL, not "
+                f"{config.INTMETHOD_NLO.name}")
     return None
+
+
+def require_sobol(config: BKConfig, what: str) -> None:
+    """The batched and served evolutions take a Monte Carlo budget per parameter set or
+    request as a Sobol point count, so they integrate K2+Kf by IntegrationMethod.SOBOL."""
+    if config.Order.has_nlo_kernels and config.INTMETHOD_NLO is not IntegrationMethod.SOBOL:
+        raise ValueError(f"{what} integrates K2+Kf with IntegrationMethod.SOBOL (its budgets are Sobol point "
+                         f"counts); got {config.INTMETHOD_NLO.name}")
 
 
 ORDER_CODES = {
@@ -208,4 +223,5 @@ __all__ = [
     "RunningCouplingNLO",
     "device_supported",
     "fixed_coupling",
+    "require_sobol",
 ]

@@ -1,11 +1,14 @@
 """BK rapidity evolution on the B200 (mirrors torch_nlo_clean/src/nlo_torch/bk/evolution.py).
 
 ``solve_bk`` / ``compute_dndy`` keep the reference signatures.  The whole
-evolution runs on one CUDA stream through ``nlo_bk_evolve`` of libnlo_b200.so:
-per stage a FP64 spline refit, K1 (fixed 8 x 24 rule), K2+Kf (scrambled Sobol
-QMC) and the FP64 RK combination -- no host synchronisation between stages.
-The host reads back once, at the end, to check the non-finite flag
-(bk/evolution.py:152-153 raises FloatingPointError).
+evolution runs on one CUDA stream through ``nlo_bk_evolve`` (K2+Kf by scrambled Sobol
+QMC) or ``nlo_bk_evolve_vegas`` (K2+Kf by Vegas per parent, the reference's default) of
+libnlo_b200.so: per stage a FP64 spline refit, K1 (fixed 8 x 24 rule), K2+Kf and the FP64
+RK combination -- no host synchronisation between stages.  The host reads back once, at
+the end, to check the non-finite flag (bk/evolution.py:152-153 raises
+FloatingPointError).  The Vegas grids of one evolution (one per parent) live in a device
+buffer that the whole evolution shares, like the reference's per-parent vegas_states of
+one _bk_steps run (bk/evolution.py:85-100).
 """
 
 from __future__ import annotations
@@ -23,6 +26,7 @@ from nlo_bk_optimized_b200.bk.config import (
     RC_NLO_CODES,
     RESUM_RC_CODES,
     BKConfig,
+    IntegrationMethod,
     device_supported,
     fixed_coupling,
 )
@@ -84,16 +88,47 @@ def params_of(config: BKConfig, precision: int) -> _native.BKParams:
     return p
 
 
+VEGAS_BINS = 32
+
+
+def vegas_options_of(config: BKConfig) -> _native.BKVegasOptions | None:
+    """The Vegas settings of rapidity_derivative_nlo (bk/derivatives.py:389-421) for
+    IntegrationMethod.VEGAS: MCINTPOINTS per iteration, a warm-up of max(2, MCINTPOINTS/5),
+    2..4 iterations, 32 bins, epsrel 0.2, and the grid reuse of BKConfig; None otherwise."""
+    if config.INTMETHOD_NLO is not IntegrationMethod.VEGAS:
+        return None
+    o = _native.BKVegasOptions()
+    o.samples_per_iteration = int(config.MCINTPOINTS)
+    o.warmup_samples = max(2, int(config.MCINTPOINTS) // 5)
+    o.max_iterations = 4
+    o.min_iterations = 2
+    o.bins = VEGAS_BINS
+    o.reuse_grid = int(bool(config.VEGAS_REUSE_GRID))
+    o.reuse_warmup_fraction = float(config.VEGAS_REUSE_WARMUP_FRACTION)
+    o.epsrel = 0.2
+    o.epsabs = 0.0
+    return o
+
+
+def vegas_state(device: torch.device, points: int) -> torch.Tensor:
+    """A zero-filled per-parent Vegas state (no grids yet) for one evolution."""
+    lib = _native.load()
+    return torch.zeros(int(lib.nlo_bk_vegas_state_doubles(points, VEGAS_BINS)), dtype=torch.float64, device=device)
+
+
 _workspaces: dict[tuple[int, int], torch.Tensor] = {}
 
 
-def workspace(device: torch.device, points: int) -> torch.Tensor:
-    """Device scratch for the right-hand side (cached per device and grid size)."""
+def workspace(device: torch.device, points: int, vegas: _native.BKVegasOptions | None = None) -> torch.Tensor:
+    """Device scratch for the right-hand side (cached per device and grid size), large
+    enough for the Vegas buffers when ``vegas`` options are given."""
 
     lib = _native.load()
     index = device.index if device.index is not None else torch.cuda.current_device()
     key = (index, points)
     need = int(lib.nlo_bk_rhs_workspace_bytes(points))
+    if vegas is not None:
+        need = max(need, int(lib.nlo_bk_vegas_workspace_bytes(points, vegas)))
     buffer = _workspaces.get(key)
     if buffer is None or buffer.numel() < need:
         buffer = torch.empty(need, dtype=torch.uint8, device=torch.device("cuda", index))
@@ -142,12 +177,15 @@ def rhs(
     seed: int | None = None,
     precision: int | None = None,
     history: tuple[torch.Tensor, torch.Tensor] | None = None,
+    vegas_grids: torch.Tensor | None = None,
 ) -> tuple[torch.Tensor, torch.Tensor, torch.Tensor]:
     """dN/dY, K1 and K2+Kf (each [R] float64) for one amplitude row (bk/evolution.py:329-488).
 
     ``history`` = (y [rows], N [rows, R]) is the amplitude history the kinematical
     constraint reads (its last row the current amplitude; _derivative_components'
-    rapidity, history_y, history_N)."""
+    rapidity, history_y, history_N).  With IntegrationMethod.VEGAS, ``vegas_grids`` (from
+    ``vegas_state``) carries the parents' grids from call to call; without it every call
+    starts from uniform grids, as the reference does without vegas_states."""
 
     device = _cuda_device(r.device)
     r64 = r.to(device=device, dtype=torch.float64).contiguous()
@@ -161,8 +199,29 @@ def rhs(
     dndy = torch.empty_like(N64)
     k1 = torch.empty_like(N64)
     k2kf = torch.empty_like(N64)
-    ws = workspace(device, points)
+    opts = vegas_options_of(config)
+    ws = workspace(device, points, opts)
     lib = _native.load()
+    if opts is not None:
+        if config.KINEMATICAL_CONSTRAINT:
+            if history is None:
+                raise ValueError("kinematical evolution requires rapidity and amplitude history")
+            hist_y = history[0].to(device=device, dtype=torch.float64).contiguous()
+            hist_N = history[1].to(device=device, dtype=torch.float64).contiguous()
+            if hist_N.ndim != 2 or hist_N.shape[1] != points or hist_y.numel() != hist_N.shape[0]:
+                raise ValueError("history must be (y [rows], N [rows, points])")
+        else:
+            hist_y, hist_N = None, N64.unsqueeze(0)
+        grids = vegas_grids if vegas_grids is not None else vegas_state(device, points)
+        with torch.cuda.device(device):
+            _native.check(
+                lib.nlo_bk_rhs_vegas(
+                    params, r64.data_ptr(), points, None if hist_y is None else hist_y.data_ptr(), hist_N.data_ptr(),
+                    hist_N.shape[0], 0, 1, opts, dirs, box, grids.data_ptr(), dndy.data_ptr(), k1.data_ptr(),
+                    k2kf.data_ptr(), ws.data_ptr(), ws.numel(), _native.stream_handle(device),
+                )
+            )
+        return dndy, k1, k2kf
     if config.KINEMATICAL_CONSTRAINT:
         if history is None:
             raise ValueError("kinematical evolution requires rapidity and amplitude history")
@@ -200,10 +259,12 @@ def _evolve_rows(
     *,
     history_N: torch.Tensor | None = None,
     y_all: list[float] | None = None,
+    vegas_grids: torch.Tensor | None = None,
 ) -> torch.Tensor:
     """Rows [steps+1, R] from N0.  With the kinematical constraint the evolution reads
     the history: ``history_N`` the rows before N0 (may be empty) and ``y_all`` the
-    rapidities of history, N0 and every new row."""
+    rapidities of history, N0 and every new row.  ``vegas_grids`` (IntegrationMethod.VEGAS)
+    holds the parents' grids; a fresh buffer is used when it is None."""
     device = r64.device
     points = r64.numel()
     status = torch.zeros(1, dtype=torch.int32, device=device)
@@ -211,8 +272,33 @@ def _evolve_rows(
     lower, width = nlo_box(float(r64[0]), float(r64[-1]))
     dirs = _native.sobol_dirs(4, 0 if seed is None else seed)
     box = _native.box(lower, width)
-    ws = workspace(device, points)
+    opts = vegas_options_of(config)
+    ws = workspace(device, points, opts)
     lib = _native.load()
+    if opts is not None:
+        kc = bool(config.KINEMATICAL_CONSTRAINT)
+        before = 0 if (history_N is None or not kc) else history_N.shape[0]
+        table = torch.empty((before + steps + 1, points), dtype=torch.float64, device=device)
+        if before:
+            table[:before] = history_N.to(device=device, dtype=torch.float64)
+        table[before] = N0
+        if kc:
+            if y_all is None or len(y_all) != before + steps + 1:
+                raise ValueError("kinematical evolution requires the rapidities of every row")
+            y = torch.tensor(y_all, dtype=torch.float64, device=device)
+        grids = vegas_grids if vegas_grids is not None else vegas_state(device, points)
+        with torch.cuda.device(device):
+            _native.check(
+                lib.nlo_bk_evolve_vegas(
+                    params, r64.data_ptr(), points, y.data_ptr() if kc else None, before, steps,
+                    float(config.DE_SOLVER_STEP), _native.STEPPERS[config.stepper], opts, dirs, box,
+                    grids.data_ptr(), table.data_ptr(), status.data_ptr(), ws.data_ptr(), ws.numel(),
+                    _native.stream_handle(device),
+                )
+            )
+        if int(status.item()) != 0:
+            raise FloatingPointError("non-finite BK amplitude during the rapidity evolution")
+        return table[before:]
     if config.KINEMATICAL_CONSTRAINT:
         before = 0 if history_N is None else history_N.shape[0]
         if y_all is None or len(y_all) != before + steps + 1:
@@ -283,9 +369,11 @@ def evolve_table(
     config: BKConfig = BKConfig(),
     *,
     seed: int | None = None,
+    vegas_grids: torch.Tensor | None = None,
 ) -> DipoleTable:
     """Continue an existing table (e.g. one read by load_bk_table) from its last row:
-    the resume path of bk/evolution.py:85-96."""
+    the resume path of bk/evolution.py:85-96.  With IntegrationMethod.VEGAS the parents'
+    grids start uniform unless ``vegas_grids`` (``vegas_state``) carries earlier ones."""
 
     device = _cuda_device(table.r.device)
     r64 = table.r.to(torch.float64)
@@ -294,7 +382,7 @@ def evolve_table(
     history = table.N[:-1] if config.KINEMATICAL_CONSTRAINT else None
     rows = _evolve_rows(table.N[-1].to(torch.float64), r64, len(ys), config, seed,
                         precision_of(config, table.r.dtype), history_N=history,
-                        y_all=[float(v) for v in table.y.double().tolist()] + list(ys))
+                        y_all=[float(v) for v in table.y.double().tolist()] + list(ys), vegas_grids=vegas_grids)
     y = torch.cat((table.y, torch.tensor(ys, dtype=table.y.dtype, device=device)))
     N = torch.cat((table.N, rows[1:].to(table.N.dtype)), dim=0)
     return DipoleTable(r=table.r, y=y, N=N, x0=table.x0)
@@ -302,11 +390,14 @@ def evolve_table(
 
 def bk_steps(table: DipoleTable, maxy: float, config: BKConfig = BKConfig(), *,
              seed: int | None = None) -> Iterator[DipoleTable]:
-    """Yield the growing table after every step (the generator of bk/evolution.py:85-159)."""
+    """Yield the growing table after every step (the generator of bk/evolution.py:85-159);
+    the Vegas grids of the parents carry over from step to step as in the reference."""
 
     current = table
+    grids = vegas_state(_cuda_device(table.r.device), table.r.numel()) \
+        if config.INTMETHOD_NLO is IntegrationMethod.VEGAS else None
     for y in _steps_to(float(table.y[-1].item()), maxy, config.DE_SOLVER_STEP):
-        current = evolve_table(current, y, config, seed=seed)
+        current = evolve_table(current, y, config, seed=seed, vegas_grids=grids)
         yield current
 
 
@@ -337,4 +428,5 @@ def compute_dndy(
                       N=N[keep].to(dtype))
 
 
-__all__ = ["DNDYResult", "bk_steps", "compute_dndy", "evolve_table", "nlo_box", "rhs", "solve_bk"]
+__all__ = ["DNDYResult", "bk_steps", "compute_dndy", "evolve_table", "nlo_box", "rhs", "solve_bk",
+           "vegas_options_of", "vegas_state"]

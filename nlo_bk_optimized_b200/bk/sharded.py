@@ -68,19 +68,33 @@ def shard_steps(N0: torch.Tensor, steps: int, step: float, stepper: str, rhs: Rh
 
 
 class ShardedRhs:
-    """A rank's share of the right-hand side (``nlo_bk_rhs_shard``) and the stage
-    combination (``nlo_bk_stage``) on its device, as the functions ``shard_steps`` takes."""
+    """A rank's share of the right-hand side (``nlo_bk_rhs_shard``, or with Vegas options
+    ``nlo_bk_rhs_vegas``) and the stage combination (``nlo_bk_stage``) on its device, as the
+    functions ``shard_steps`` takes.  A Vegas integral needs all of one parent's samples for
+    its grid, so with Vegas the rank takes K1 and K2+Kf of its own parents (i % W == k) and
+    keeps their grids from stage to stage."""
 
     def __init__(self, params, r: torch.Tensor, dirs, samples: int, box, rank: int, world: int,
-                 workspace: torch.Tensor, status: torch.Tensor, stream) -> None:
+                 workspace: torch.Tensor, status: torch.Tensor, stream, vegas=None) -> None:
         self.lib = _native.load()
         self.params, self.r, self.dirs, self.samples, self.box = params, r, dirs, int(samples), box
         self.rank, self.world = rank, world
         self.workspace, self.status = workspace, status
         self.stream = stream if isinstance(stream, int) or stream is None else stream.cuda_stream
+        self.vegas = vegas
+        if vegas is not None:
+            from nlo_bk_optimized_b200.bk.evolution import vegas_state
+
+            self.grids = vegas_state(r.device, r.numel())
 
     def rhs(self, N: torch.Tensor) -> torch.Tensor:
         out = torch.empty_like(N)
+        if self.vegas is not None:
+            _native.check(self.lib.nlo_bk_rhs_vegas(self.params, self.r.data_ptr(), self.r.numel(), None,
+                                                    N.data_ptr(), 1, self.rank, self.world, self.vegas, self.dirs,
+                                                    self.box, self.grids.data_ptr(), out.data_ptr(), None, None,
+                                                    self.workspace.data_ptr(), self.workspace.numel(), self.stream))
+            return out
         _native.check(self.lib.nlo_bk_rhs_shard(self.params, self.r.data_ptr(), N.data_ptr(), self.r.numel(),
                                                 self.rank, self.world, self.dirs, self.samples, self.box,
                                                 out.data_ptr(), self.workspace.data_ptr(), self.workspace.numel(),
@@ -110,6 +124,7 @@ def solve_bk_sharded(initial_condition, maxy: float, config: BKConfig = BKConfig
         nlo_box,
         params_of,
         precision_of,
+        vegas_options_of,
         workspace,
     )
 
@@ -126,14 +141,17 @@ def solve_bk_sharded(initial_condition, maxy: float, config: BKConfig = BKConfig
     lower, width = nlo_box(float(r_host[0]), float(r_host[-1]))
     box = _native.box(lower, width)
     dirs = _native.sobol_dirs(4, seed)
-    ws = workspace(device, points)
+    ws = workspace(device, points, vegas_options_of(config))
     status = torch.zeros(1, dtype=torch.int32, device=device)
     stream = _native.stream_handle(device)
     ys = _steps_to(0.0, maxy, config.DE_SOLVER_STEP)
     steps = len(ys)
     clamp = bool(config.FORCE_POSITIVE_N)
 
-    sharded = ShardedRhs(params, r, dirs, int(config.MCINTPOINTS), box, rank, world, ws, status, stream)
+    if config.KINEMATICAL_CONSTRAINT:
+        raise ValueError("the sharded evolution has no kinematical constraint (it reads no amplitude history)")
+    sharded = ShardedRhs(params, r, dirs, int(config.MCINTPOINTS), box, rank, world, ws, status, stream,
+                         vegas=vegas_options_of(config))
 
     def all_reduce(k: torch.Tensor) -> None:
         if world > 1:

@@ -9,9 +9,10 @@ Differences, all forced by the device path:
 
 * ``--device`` defaults to ``cuda`` (the reference defaults to ``mps``); a non-CUDA
   device is an argument error.
-* ``--integration`` adds ``sobol``, the device's K2+Kf method, and makes it the default;
-  the reference's ``vegas``/``miser``/``multiple`` are accepted and rejected like every
-  other switch the device kernels do not implement, as an argument error naming it.
+* ``--integration`` adds ``sobol``, the fast quasi-Monte Carlo K2+Kf of the device; the
+  default stays the reference's ``vegas``; ``miser``/``multiple`` are accepted and
+  rejected like every other switch the device kernels do not implement, as an argument
+  error naming it.
 """
 
 from __future__ import annotations
@@ -78,7 +79,7 @@ def _parser() -> argparse.ArgumentParser:
     parser.add_argument("--rc-lo", choices=tuple(_RC_LO), default="balitsky")
     parser.add_argument("--rc-nlo", choices=tuple(_RC_NLO), default="smallest")
     parser.add_argument("--resum-rc", choices=tuple(_RESUM_RC), default="smallest")
-    parser.add_argument("--integration", choices=tuple(_INTEGRATION), default="sobol")
+    parser.add_argument("--integration", choices=tuple(_INTEGRATION), default="vegas")
     parser.add_argument("--nf", type=int, choices=(0, 3, 5), default=3)
     parser.add_argument("--C2", type=float, default=1.0)
     parser.add_argument("--fixed-alpha-s", type=float, default=0.2)

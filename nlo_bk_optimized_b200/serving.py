@@ -27,7 +27,7 @@ from dataclasses import dataclass, field
 import torch
 
 from nlo_bk_optimized_b200 import _native
-from nlo_bk_optimized_b200.bk.config import BKConfig
+from nlo_bk_optimized_b200.bk.config import BKConfig, require_sobol
 from nlo_bk_optimized_b200.bk.initial_conditions import MV
 from nlo_bk_optimized_b200.dipole.amplitude import BKDipole
 from nlo_bk_optimized_b200.dipole.table import DipoleTable
@@ -109,6 +109,7 @@ class Server:
     def __init__(self, bk_config: BKConfig, dis_config: DISConfig, *, device: torch.device | str = "cuda",
                  slots: int = 8, cache_tables: int = 64, reserve_bytes: int = 1 << 30,
                  sqrt_s: float | None = 318.0):
+        require_sobol(bk_config, "the request loop")
         self.bk_config = bk_config
         self.dis_config = dis_config
         self.device = torch.device(device)

@@ -15,6 +15,9 @@ the reference's evolution driver:
                       K2+Kf by quasi-Monte Carlo on fixed Sobol points)
 * ``derivative_shard`` -- one shard's part of it (K1 by parent, K2+Kf by point range),
                       for the multi-rank evolution (no counterpart in the reference)
+* ``vegas_k2kf`` / ``derivative_vegas`` -- K2+Kf by Vegas per parent with grid reuse
+                      (bk/derivatives.py:389-421, numerics/integration.py:120-589,
+                      bk/evolution.py:354-424)
 * ``evolve``       -- stepping loop bk/evolution.py:85-159 with the Euler
                       (:110-122), Kutta RK3 (:190-236) or classical RK4 stepper
 * ``r_grid``       -- bk/evolution.py:584-592
@@ -105,6 +108,7 @@ def lib() -> ctypes.CDLL:
         handle.or_nlo_kernels.argtypes = [D, D, D, D, D, D, D, DP]
         handle.or_k2kf_integrand.argtypes = [D, DP, P(_Spline), P(Physics), DP]
         handle.or_k2kf_sums.argtypes = [DP, I, DP, ctypes.c_long, DP, DP, I, P(_Spline), P(Physics), DP]
+        handle.or_k2kf_values.argtypes = [D, DP, ctypes.c_long, P(_Spline), P(Physics), DP, DP]
         handle.or_sobol.argtypes = [
             P(ctypes.c_int64), P(ctypes.c_int64), I, ctypes.c_long, ctypes.c_long, I, DP
         ]
@@ -417,6 +421,134 @@ def derivative_shard(N: np.ndarray, r: np.ndarray, phys: Physics, points: np.nda
                 sums = k2kf_sums(r[active], points[lo:hi], lower, width, map_f32, sspl, phys)
                 out[active] += (sums[:, 0] + sums[:, 1]) / n
     return np.where(np.isfinite(out), out, 0.0)
+
+
+def k2kf_values(r: float, x: np.ndarray, sspline: Spline, phys: Physics) -> tuple[np.ndarray, np.ndarray]:
+    """_nlo_integrand x Jacobian (K2 part, Kf part) at box points x [n, 4]."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    n = x.shape[0]
+    k2, kf = np.empty(n), np.empty(n)
+    lib().or_k2kf_values(r, _dp(x), n, ctypes.byref(sspline.struct()), ctypes.byref(phys), _dp(k2), _dp(kf))
+    return k2, kf
+
+
+@dataclass
+class VegasGrid:
+    """One parent's Vegas state between right-hand sides (the reference's VegasState)."""
+
+    edges: np.ndarray | None = None
+    last_components: np.ndarray | None = None
+    last_error: float | None = None
+
+
+@dataclass
+class VegasResult:
+    value: float
+    error: float
+    n_eval: int
+    iterations: int
+    converged: bool
+    components: np.ndarray  # combined K2, Kf estimates
+    edges: np.ndarray
+
+
+def vegas_k2kf(r: float, sspline: Spline, phys: Physics, box: tuple[np.ndarray, np.ndarray], seed: int, *,
+               samples: int, warmup: int, max_iterations: int = 4, min_iterations: int = 2, bins: int = 32,
+               epsrel: float = 0.2, epsabs: float = 0.0, state: VegasGrid | None = None,
+               reuse_warmup_fraction: float = 0.0, f32_points: bool = False) -> VegasResult:
+    """vegas() of numerics/integration.py:120-589 for the K2+Kf integrand of one parent
+    (rapidity_derivative_nlo, bk/derivatives.py:389-421) on the Sobol points of `seed`,
+    indices 0, 1, ... across the rounds: coordinate u gives the bin floor(u bins) and the
+    fraction u bins - bin.  A `state` holding edges starts from them with the warm-up
+    max(2, warmup x reuse_warmup_fraction) (none when either is 0); the final edges and the
+    combined K2/Kf components are written back.  f32_points rounds the box points to float32
+    before the integrand (the positions the mixed device build evaluates at)."""
+    from oracle import dis as odis
+
+    lower, width = box
+    volume = float(np.prod(width))
+    reused = state is not None and state.edges is not None
+    edges = state.edges.copy() if reused else np.tile(np.linspace(0, 1, bins + 1), (4, 1))
+    if reused:
+        warm = max(2, int(warmup * reuse_warmup_fraction)) if warmup > 0 and reuse_warmup_fraction > 0 else 0
+    else:
+        warm = warmup
+    sobol_state_, sobol_shift = sobol_state(4, seed)
+    offset = 0
+    estimates, variances, comps = [], [], []
+    n_eval, value, error, converged = 0, 0.0, 0.0, False
+    rounds = max_iterations + int(warm > 0)
+    for k in range(rounds):
+        is_warm = warm > 0 and k == 0
+        n = warm if is_warm else samples
+        u = sobol(sobol_state_, sobol_shift, offset, n, as_f32=False)
+        offset += n
+        scaled = u * bins
+        bi = np.minimum(np.floor(scaled).astype(np.int64), bins - 1)
+        fr = scaled - bi
+        unit, inv = odis.vegas_map(edges, bi, fr)
+        x = lower + width * unit
+        if f32_points:
+            x = x.astype(np.float32).astype(np.float64)
+        k2, kf = k2kf_values(r, x, sspline, phys)
+        w_k2, w_kf = k2 * volume * inv, kf * volume * inv
+        w = (k2 + kf) * volume * inv
+        hist = np.zeros((4, bins))
+        count = np.zeros((4, bins))
+        for d in range(4):
+            hist[d] = np.bincount(bi[:, d], weights=np.abs(w), minlength=bins)
+            count[d] = np.bincount(bi[:, d], minlength=bins)
+        n_eval += n
+        edges = odis.adapt_edges(edges, hist, count)
+        if is_warm:
+            continue
+        total, total2 = float(np.sum(w)), float(np.sum(w * w))
+        est = total / n
+        var = max(max(total2 - total * total / n, 0.0) / (n - 1) / n, np.finfo(np.float64).tiny)
+        estimates.append(est)
+        variances.append(var)
+        comps.append(np.array([np.sum(w_k2) / n, np.sum(w_kf) / n]))
+        wts = 1 / np.array(variances)
+        value = float(np.sum(wts * np.array(estimates)) / wts.sum())
+        error = float(math.sqrt(1 / wts.sum()))
+        converged = len(estimates) >= min_iterations and error <= max(epsabs, epsrel * abs(value))
+        if converged:
+            break
+    wts = 1 / np.array(variances)
+    components = (wts[:, None] * np.stack(comps)).sum(axis=0) / wts.sum()
+    if state is not None:
+        state.edges = edges.copy()
+        state.last_components = components
+        state.last_error = error
+    return VegasResult(value, error, n_eval, len(estimates), converged, components, edges)
+
+
+def derivative_vegas(N: np.ndarray, r: np.ndarray, phys: Physics, seed: int, *, samples: int,
+                     grids: dict[int, VegasGrid] | None = None, reuse_warmup_fraction: float = 0.25,
+                     f32_points: bool = False, force_positive: bool = True, **options) -> dict:
+    """dN/dY with K2+Kf by Vegas per active parent (_derivative_components with
+    IntegrationMethod.VEGAS, bk/evolution.py:354-424): `grids` keyed by grid index are the
+    per-parent states carried between calls (None: fresh grids, as without vegas_states)."""
+    nspl = loglog_spline(r, N, 0, force_positive)
+    sspl = loglog_spline(r, N, 1, force_positive)
+    active = np.nonzero((np.arange(r.size) > 0) & (N <= 0.99999))[0]
+    K1 = np.zeros_like(N)
+    K2Kf = np.zeros_like(N)
+    results = {}
+    if active.size:
+        K1[active] = k1_fixed(r[active], nspl, phys)
+        if has_nlo_kernels(phys):
+            box = nlo_box(r)
+            for i in active:
+                state = None if grids is None else grids.setdefault(int(i), VegasGrid())
+                res = vegas_k2kf(float(r[i]), sspl, phys, box, seed, samples=samples,
+                                 warmup=max(2, samples // 5), state=state,
+                                 reuse_warmup_fraction=reuse_warmup_fraction if grids is not None else 0.0,
+                                 f32_points=f32_points, **options)
+                K2Kf[i] = res.value
+                results[int(i)] = res
+    dNdy = K1 + K2Kf
+    return {"dNdy": np.where(np.isfinite(dNdy), dNdy, 0.0), "K1": K1, "K2Kf": K2Kf, "vegas": results}
 
 
 def evolve(N0: np.ndarray, r: np.ndarray, phys: Physics, points: np.ndarray, map_f32: bool, step: float,

@@ -758,6 +758,20 @@ void or_k2kf_integrand(double r, const double* x, const or_spline* sspl, const o
     k2_eval(r, log(r), &pt, sspl, p, &out[0], &out[1]);
 }
 
+/* _nlo_integrand x Jacobian at n box points xs[n][4] = (log z, log z', theta_z, theta_z')
+ * for one parent (the Vegas samples): out_k2[i], out_kf[i]. */
+void or_k2kf_values(double r, const double* xs, long n, const or_spline* sspl, const or_physics* p, double* out_k2,
+                    double* out_kf)
+{
+    const double lr = log(r);
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < n; ++i) {
+        k2_point pt;
+        k2_prepare(xs[4 * i], xs[4 * i + 1], xs[4 * i + 2], xs[4 * i + 3], sspl, &pt);
+        k2_eval(r, lr, &pt, sspl, p, &out_k2[i], &out_kf[i]);
+    }
+}
+
 /*
  * Sums over n box samples for each of nr parents.  pts: [n][4] unit-cube
  * coordinates u (values already rounded to the generator's precision).

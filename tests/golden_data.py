@@ -49,6 +49,8 @@ def variant_config(name: str):
                     value = enum[value]
                     break
         kwargs[field] = value
+    kwargs.setdefault("INTMETHOD_NLO", bkc.IntegrationMethod.SOBOL)  # the oracle's fixed Sobol points
+    kwargs.setdefault("STEPPER", "rk4")
     return bkc.BKConfig(RPOINTS=99, MINR=1e-6, MAXR=1e2, **kwargs)
 
 

@@ -31,7 +31,7 @@ def test_nlobk_defaults_build_a_device_configuration():
     assert config.Order is BKOrder.NLO_RESUM_DLOG_SLOG
     assert config.RC_LO is RunningCouplingLO.BALITSKY_LO and config.RC_NLO is RunningCouplingNLO.SMALLEST_NLO
     assert config.RESUM_RC is ResummationCoupling.RESUM_RC_SMALLEST
-    assert config.INTMETHOD_NLO is IntegrationMethod.SOBOL
+    assert config.INTMETHOD_NLO is IntegrationMethod.VEGAS  # the reference's default
     assert config.FORCE_POSITIVE_N and not config.DNDY and not config.EULER_METHOD
     assert (config.RPOINTS, config.MINR, config.MAXR, config.MCINTPOINTS) == (100, 1e-6, 30.0, 100_000)
     assert device_supported(config) is None
@@ -49,8 +49,8 @@ def test_nlobk_option_mapping():
 
 
 @pytest.mark.parametrize("argv,why", [
-    (["--integration", "vegas"], "SOBOL"),
-    (["--integration", "miser"], "SOBOL"),
+    (["--integration", "miser"], "MISER"),
+    (["--integration", "multiple"], "MULTIPLE"),
 ])
 def test_nlobk_switches_outside_the_device_kernels(argv, why):
     config = nlobk.config_from_args(nlobk._parser().parse_args(argv))
@@ -61,9 +61,9 @@ def test_nlobk_switches_outside_the_device_kernels(argv, why):
     ["--order", "lo"], ["--order", "nlo"], ["--order", "lo_resum_dlog"], ["--order", "nlo_resum_dlog"],
     ["--rc-lo", "parent"], ["--rc-lo", "smallest"], ["--rc-lo", "fac"], ["--rc-lo", "beuf"],
     ["--resum-rc", "fixed"], ["--resum-rc", "parent"], ["--rc-nlo", "parent"], ["--nf", "5"], ["--nf", "0"],
-    ["--kinematical-constraint", "--euler"],
+    ["--kinematical-constraint", "--euler"], ["--integration", "sobol", "--order", "nlo"],
     # orders without NLO kernels never integrate K2 + Kf, so its method does not matter
-    ["--order", "lo", "--integration", "vegas"],
+    ["--order", "lo", "--integration", "miser"],
 ])
 def test_nlobk_variants_run_on_the_device(argv):
     from nlo_bk_optimized_b200.bk.evolution import params_of

@@ -1,16 +1,16 @@
 """Accuracy of the headline configuration: 400 log-spaced r in [1e-7, 1e2], MV Qs0^2 = 0.2,
-RK4 h = 0.1 from Y = 0 to Y = 10, on the same scrambled Sobol points in both builds.
+RK4 h = 0.1 from Y = 0 to Y = 10, 2^20 scrambled Sobol points per parent per stage, the
+same points in both builds.
 
 * The mixed build (FP32 integrands, FP32 partial sums of 32 samples folded into FP64, FP64
   spline refit and RK update) stays within 1e-4 relative of the all-FP64 device build over
-  every row and every parent with N > 0 -- the precision bound of the headline metric.
+  every row and every parent with N > 0 -- the precision bound of the headline metric.  The
+  difference falls as 1/samples (3e-4 at 2^15, 1e-5 at 2^20): it comes from the few
+  samples within FP32 rounding of the integrable X -> 0 singularities, whose FP32 point
+  positions move them, so the bound is checked at the headline budget itself.
 * The FP64 build's right-hand side at the evolved final state equals the oracle's on the
-  same points to 1e-10.
-
-The sample budget is 2^15 points per parent per stage (the benchmark's 2^20 would take
-minutes in the FP64 build); the error of the mixed build comes from the FP32 integrand per
-sample, not from the number of samples, and the benchmark line reports the same
-comparison at 2^20."""
+  same points to 1e-10 (2^16 points, so that the CPU oracle takes seconds).
+"""
 
 from __future__ import annotations
 
@@ -22,16 +22,19 @@ import torch
 
 import oracle
 from nlo_bk_optimized_b200 import MV, BKConfig, solve_bk
+from nlo_bk_optimized_b200.bk.config import IntegrationMethod
 from nlo_bk_optimized_b200.bk.evolution import rhs
 
 pytestmark = pytest.mark.gpu
 
-SAMPLES = 1 << 15
+SAMPLES = 1 << 20
+ORACLE_SAMPLES = 1 << 16
 
 
 @pytest.fixture(scope="module")
 def evolutions():
-    config = BKConfig(RPOINTS=399, MINR=1e-7, MAXR=1e2, MCINTPOINTS=SAMPLES, DE_SOLVER_STEP=0.1, STEPPER="rk4")
+    config = BKConfig(RPOINTS=399, MINR=1e-7, MAXR=1e2, MCINTPOINTS=SAMPLES, DE_SOLVER_STEP=0.1, STEPPER="rk4",
+                      INTMETHOD_NLO=IntegrationMethod.SOBOL)
     ic = MV(qs0sqr=0.2)
     mixed = solve_bk(ic, 10.0, replace(config, PRECISION="mixed"), device="cuda", dtype=torch.float64, seed=0)
     fp64 = solve_bk(ic, 10.0, replace(config, PRECISION="fp64"), device="cuda", dtype=torch.float64, seed=0)
@@ -55,10 +58,10 @@ def test_final_state_rhs_matches_oracle(evolutions):
     config, _, fp64 = evolutions
     r = fp64.r.double()
     N = fp64.N[-1].double()
-    dndy, k1, k2kf = rhs(N, r, replace(config, PRECISION="fp64"), seed=0)
+    dndy, k1, k2kf = rhs(N, r, replace(config, PRECISION="fp64", MCINTPOINTS=ORACLE_SAMPLES), seed=0)
     rn, Nn = r.cpu().numpy(), N.cpu().numpy()
     state, shift = oracle.sobol_state(4, 0)
-    points = oracle.sobol(state, shift, 0, SAMPLES, as_f32=False)
+    points = oracle.sobol(state, shift, 0, ORACLE_SAMPLES, as_f32=False)
     ref = oracle.derivative(Nn, rn, oracle.physics(config), points, False)
     got = dndy.cpu().numpy()
     active = ref.dNdy != 0

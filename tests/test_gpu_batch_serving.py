@@ -6,9 +6,11 @@ from __future__ import annotations
 import pytest
 import torch
 
+from nlo_bk_optimized_b200.bk.config import IntegrationMethod
+
 pytestmark = pytest.mark.gpu
 
-BK = dict(RPOINTS=63, MINR=1e-6, MAXR=1e2, DE_SOLVER_STEP=0.2, STEPPER="rk4")
+BK = dict(RPOINTS=63, MINR=1e-6, MAXR=1e2, DE_SOLVER_STEP=0.2, STEPPER="rk4", INTMETHOD_NLO=IntegrationMethod.SOBOL)
 
 
 def test_batch_equals_individual_solves():

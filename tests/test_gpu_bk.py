@@ -17,6 +17,7 @@ import torch
 import oracle
 from nlo_bk_optimized_b200 import MV, BKConfig, compute_dndy, kernels, solve_bk
 from nlo_bk_optimized_b200 import _native
+from nlo_bk_optimized_b200.bk.config import IntegrationMethod
 from nlo_bk_optimized_b200.bk.evolution import _r_grid, evolve_table, rhs
 
 pytestmark = pytest.mark.gpu
@@ -32,6 +33,9 @@ def _rel_err(gpu: np.ndarray, ref: np.ndarray, floor: float = 1e-3) -> float:
 
 
 def _setup(rpoints=99, minr=1e-6, maxr=1e2, qs=0.2, **kw):
+    # the oracle integrates K2+Kf on fixed Sobol points and steps with RK4 unless told otherwise
+    kw.setdefault("INTMETHOD_NLO", IntegrationMethod.SOBOL)
+    kw.setdefault("STEPPER", "rk4")
     config = BKConfig(RPOINTS=rpoints, MINR=minr, MAXR=maxr, **kw)
     r = _r_grid(config, device=DEVICE, dtype=torch.float64)
     N = MV(qs0sqr=qs).dipole_amplitude(r)

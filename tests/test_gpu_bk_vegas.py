@@ -1,0 +1,170 @@
+"""K2+Kf by Vegas on the device (IntegrationMethod.VEGAS, the reference's default:
+rapidity_derivative_nlo, bk/derivatives.py:389-421, with per-parent grids carried between
+right-hand sides, bk/evolution.py:85-100 and 354-424) against the oracle's Vegas on the same
+Sobol points: values, errors, evaluation counts and grids."""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import replace
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from nlo_bk_optimized_b200 import MV, BKConfig, _native, solve_bk
+from nlo_bk_optimized_b200.bk.config import IntegrationMethod
+from nlo_bk_optimized_b200.bk.evolution import (
+    VEGAS_BINS,
+    _r_grid,
+    nlo_box,
+    params_of,
+    rhs,
+    vegas_options_of,
+    vegas_state,
+    workspace,
+)
+
+pytestmark = pytest.mark.gpu
+
+STRIDE = 4 * (VEGAS_BINS + 1) + 16
+VALUE, ERROR, EVALS, ITERATIONS, CONVERGED = 2, 3, 4, 5, 6
+
+
+def _config(**kw):
+    kw.setdefault("PRECISION", "fp64")
+    return BKConfig(RPOINTS=31, MINR=1e-6, MAXR=1e2, MCINTPOINTS=2048, DE_SOLVER_STEP=0.2, **kw)
+
+
+def _state_rows(grids: torch.Tensor) -> np.ndarray:
+    return grids.cpu().numpy().reshape(-1, STRIDE)
+
+
+def _scale(values: np.ndarray) -> np.ndarray:
+    return np.maximum(np.abs(values), 1e-3 * np.max(np.abs(values)))
+
+
+def test_vegas_rhs_matches_oracle_with_grid_reuse():
+    config = _config()
+    assert config.INTMETHOD_NLO is IntegrationMethod.VEGAS
+    r = _r_grid(config, device="cuda", dtype=torch.float64)
+    N = MV(qs0sqr=0.2).dipole_amplitude(r)
+    grids = vegas_state(r.device, r.numel())
+    rn, Nn = r.cpu().numpy(), N.cpu().numpy()
+    phys = oracle.physics(config)
+    ref_grids: dict = {}
+    for call in range(2):  # the second call starts from the first call's grids
+        dndy, k1, k2kf = rhs(N, r, config, seed=0, vegas_grids=grids)
+        ref = oracle.derivative_vegas(Nn, rn, phys, 0, samples=config.MCINTPOINTS, grids=ref_grids)
+        got = k2kf.cpu().numpy()
+        active = sorted(ref["vegas"])
+        assert len(active) > 20
+        err = np.abs(got[active] - ref["K2Kf"][active]) / _scale(ref["K2Kf"][active])
+        assert err.max() <= 1e-10, f"call {call}: K2+Kf {err.max():.3e}"
+        d = dndy.cpu().numpy()
+        assert np.max(np.abs(d[active] - ref["dNdy"][active]) / _scale(ref["dNdy"][active])) <= 1e-10
+        rows = _state_rows(grids)
+        for i in active:
+            res = ref["vegas"][i]
+            edges = rows[i, : 4 * (VEGAS_BINS + 1)].reshape(4, VEGAS_BINS + 1)
+            np.testing.assert_allclose(edges, res.edges, rtol=0, atol=1e-12)
+            slots = rows[i, 4 * (VEGAS_BINS + 1):]
+            assert slots[EVALS] == res.n_eval and slots[ITERATIONS] == res.iterations
+            assert bool(slots[CONVERGED]) == res.converged
+            assert abs(slots[ERROR] - res.error) <= 1e-8 * res.error
+        # the reference's counts: a fresh grid takes the warm-up max(2, S/5) = 409, a kept one 102
+        warm = 409 if call == 0 else 102
+        assert all(ref["vegas"][i].n_eval == warm + ref["vegas"][i].iterations * 2048 for i in active)
+
+
+def test_vegas_evolution_matches_oracle():
+    """Kutta RK3 (the reference's production stepper) to Y = 0.4 with the grids carried through
+    all six right-hand sides, FP64 build against the oracle."""
+    config = _config(STEPPER="rk3")
+    table = solve_bk(MV(qs0sqr=0.2), 0.4, config, device="cuda", dtype=torch.float64, seed=0)
+    r = _r_grid(config, device="cpu", dtype=torch.float64).numpy()
+    N = MV(qs0sqr=0.2).dipole_amplitude(torch.tensor(r)).numpy()
+    phys = oracle.physics(config)
+    grids: dict = {}
+
+    def f(state):
+        return oracle.derivative_vegas(state, r, phys, 0, samples=config.MCINTPOINTS, grids=grids)["dNdy"]
+
+    rows = [N]
+    h = 0.2
+    for _ in range(2):
+        k1 = f(N)
+        k2 = f(N + 0.5 * h * k1)
+        k3 = f(N + h * (-k1 + 2.0 * k2))
+        N = np.clip(N + h * (k1 + 4.0 * k2 + k3) / 6.0, 0.0, 1.0)
+        rows.append(N)
+    got = table.N.cpu().numpy()
+    ref = np.stack(rows)
+    assert got.shape == ref.shape
+    assert np.max(np.abs(got - ref) / np.maximum(np.abs(ref), 1e-300)) <= 1e-10
+
+
+def _direct(config, N, r, options, grids):
+    lib = _native.load()
+    precision = _native.PRECISION_FP64 if config.PRECISION == "fp64" else _native.PRECISION_MIXED
+    params = params_of(config, precision)
+    lower, width = nlo_box(float(r[0]), float(r[-1]))
+    ws = workspace(r.device, r.numel(), options)
+    dndy, k1, k2kf = (torch.empty_like(N) for _ in range(3))
+    hist = N.unsqueeze(0).contiguous()
+    _native.check(lib.nlo_bk_rhs_vegas(params, r.data_ptr(), r.numel(), None, hist.data_ptr(), 1, 0, 1,
+                                       ctypes.byref(options), _native.sobol_dirs(4, 0), _native.box(lower, width),
+                                       grids.data_ptr(), dndy.data_ptr(), k1.data_ptr(), k2kf.data_ptr(),
+                                       ws.data_ptr(), ws.numel(), _native.stream_handle(r.device)))
+    return k2kf
+
+
+def test_mixed_build_on_identical_points():
+    """One iteration on the uniform grid (no warm-up): the mixed build evaluates the FP32
+    integrand at the float32-rounded box points; the oracle evaluates in FP64 at the same
+    points.  The estimates agree to FP32 accuracy."""
+    config = _config(PRECISION="mixed")
+    r = _r_grid(config, device="cuda", dtype=torch.float64)
+    N = MV(qs0sqr=0.2).dipole_amplitude(r)
+    options = vegas_options_of(config)
+    options.warmup_samples, options.max_iterations, options.min_iterations, options.epsrel = 0, 1, 1, 0.0
+    options.samples_per_iteration = 4096
+    got = _direct(config, N, r, options, vegas_state(r.device, r.numel())).cpu().numpy()
+    rn, Nn = r.cpu().numpy(), N.cpu().numpy()
+    active = np.nonzero((np.arange(rn.size) > 0) & (Nn <= 0.99999))[0]
+    sp = oracle.loglog_spline(rn, Nn, 1)
+    box = oracle.nlo_box(rn)
+    want = np.array([oracle.vegas_k2kf(float(rn[i]), sp, oracle.physics(config), box, 0, samples=4096, warmup=0,
+                                       max_iterations=1, min_iterations=1, epsrel=0.0, f32_points=True).value
+                     for i in active])
+    err = np.abs(got[active] - want) / _scale(want)
+    assert err.max() <= 1e-4, f"mixed Vegas vs oracle on identical points: {err.max():.3e}"
+
+
+def test_mixed_build_agrees_with_fp64_within_the_vegas_error():
+    config = _config(PRECISION="mixed")
+    r = _r_grid(config, device="cuda", dtype=torch.float64)
+    N = MV(qs0sqr=0.2).dipole_amplitude(r)
+    gm, gf = vegas_state(r.device, r.numel()), vegas_state(r.device, r.numel())
+    _, _, km = rhs(N, r, config, seed=0, vegas_grids=gm)
+    _, _, kf = rhs(N, r, replace(config, PRECISION="fp64"), seed=0, vegas_grids=gf)
+    sm, sf = _state_rows(gm), _state_rows(gf)
+    err_m = sm[:, 4 * (VEGAS_BINS + 1) + ERROR]
+    err_f = sf[:, 4 * (VEGAS_BINS + 1) + ERROR]
+    active = np.nonzero(err_f > 0)[0]
+    assert active.size > 20
+    diff = np.abs(km.cpu().numpy() - kf.cpu().numpy())[active]
+    assert np.all(diff <= 3.0 * np.hypot(err_m[active], err_f[active]))
+
+
+def test_vegas_options_are_checked():
+    config = _config()
+    r = _r_grid(config, device="cuda", dtype=torch.float64)
+    N = MV(qs0sqr=0.2).dipole_amplitude(r)
+    for field, value in (("samples_per_iteration", 1), ("warmup_samples", 1), ("min_iterations", 5),
+                         ("bins", 1), ("reuse_warmup_fraction", 1.5)):
+        options = vegas_options_of(config)
+        setattr(options, field, value)
+        with pytest.raises(RuntimeError):
+            _direct(config, N, r, options, vegas_state(r.device, r.numel()))

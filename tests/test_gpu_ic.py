@@ -13,6 +13,7 @@ import torch
 
 from golden_data import bk_ic, synthetic_ic, write_synthetic_ic
 from nlo_bk_optimized_b200 import BKConfig, _native, solve_bk
+from nlo_bk_optimized_b200.bk.config import IntegrationMethod
 from nlo_bk_optimized_b200.bk.evolution import _r_grid, compute_dndy
 from nlo_bk_optimized_b200.bk.initial_conditions import ICDataFile
 
@@ -52,7 +53,8 @@ def test_device_amplitude_equals_the_reference(ic_file):
 
 def test_evolution_starts_from_the_device_row(ic_file):
     g = bk_ic()
-    config = BKConfig(RPOINTS=399, MINR=1e-7, MAXR=1e2, MCINTPOINTS=256, DE_SOLVER_STEP=0.1)
+    config = BKConfig(RPOINTS=399, MINR=1e-7, MAXR=1e2, MCINTPOINTS=256, DE_SOLVER_STEP=0.1,
+                      INTMETHOD_NLO=IntegrationMethod.SOBOL)
     table = solve_bk(ICDataFile(ic_file, x0=0.01), 0.1, config, device="cuda", dtype=torch.float64, seed=0)
     grid = _r_grid(config, device="cpu", dtype=torch.float64).numpy()
     np.testing.assert_array_equal(grid, g["ic_points"][:400])

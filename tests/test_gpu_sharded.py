@@ -8,6 +8,8 @@ import ctypes
 import pytest
 import torch
 
+from nlo_bk_optimized_b200.bk.config import IntegrationMethod
+
 pytestmark = pytest.mark.gpu
 
 
@@ -16,7 +18,8 @@ def test_shard_rhs_sum_to_full_rhs(precision):
     from nlo_bk_optimized_b200 import MV, BKConfig, _native
     from nlo_bk_optimized_b200.bk.evolution import _r_grid, nlo_box, params_of, rhs, workspace
 
-    config = BKConfig(RPOINTS=99, MINR=1e-6, MAXR=1e2, MCINTPOINTS=1 << 12, PRECISION=precision)
+    config = BKConfig(RPOINTS=99, MINR=1e-6, MAXR=1e2, MCINTPOINTS=1 << 12, PRECISION=precision,
+                      INTMETHOD_NLO=IntegrationMethod.SOBOL)
     r = _r_grid(config, device="cuda", dtype=torch.float64)
     N = MV(qs0sqr=0.2).dipole_amplitude(r.cpu()).to("cuda", torch.float64)
     full, _, _ = rhs(N, r, config, seed=0)
@@ -41,11 +44,13 @@ def test_shard_rhs_sum_to_full_rhs(precision):
         assert float(rel) < (1e-12 if precision == "fp64" else 1e-6)
 
 
-def test_single_rank_sharded_driver_matches_solve_bk():
+@pytest.mark.parametrize("method", ["SOBOL", "VEGAS"])
+def test_single_rank_sharded_driver_matches_solve_bk(method):
     from nlo_bk_optimized_b200 import MV, BKConfig, solve_bk
     from nlo_bk_optimized_b200.bk.sharded import solve_bk_sharded
 
     config = BKConfig(RPOINTS=63, MINR=1e-6, MAXR=1e2, MCINTPOINTS=1 << 11, DE_SOLVER_STEP=0.2, STEPPER="rk4",
+                      INTMETHOD_NLO=IntegrationMethod[method],
                       PRECISION="fp64")
     a = solve_bk(MV(qs0sqr=0.2), 0.4, config, device="cuda", dtype=torch.float64, seed=0)
     b = solve_bk_sharded(MV(qs0sqr=0.2), 0.4, config, device="cuda", dtype=torch.float64, seed=0)

@@ -24,8 +24,10 @@ ROOT = Path(__file__).resolve().parent.parent
 def test_config_defaults_and_validation():
     config = BKConfig()
     assert config.NC == 3.0 and config.NF == 3 and config.RPOINTS == 100
-    assert config.INTMETHOD_NLO is IntegrationMethod.SOBOL
-    assert config.stepper == "rk4"
+    # the reference's production path: Vegas per parent with grid reuse, Kutta RK3
+    assert config.INTMETHOD_NLO is IntegrationMethod.VEGAS
+    assert config.VEGAS_REUSE_GRID and config.VEGAS_REUSE_WARMUP_FRACTION == 0.25
+    assert config.stepper == "rk3"
     assert BKConfig(EULER_METHOD=True).stepper == "euler"
     with pytest.raises(ValueError):
         BKConfig(NF=4)
@@ -38,7 +40,8 @@ def test_config_defaults_and_validation():
     with pytest.raises(ValueError):
         BKConfig(KINEMATICAL_CONSTRAINT=True)
     assert device_supported(config) is None
-    assert "VEGAS" not in (device_supported(BKConfig(INTMETHOD_NLO=IntegrationMethod.VEGAS)) or "VEGAS")
+    assert device_supported(BKConfig(INTMETHOD_NLO=IntegrationMethod.SOBOL)) is None
+    assert "MISER" in device_supported(BKConfig(INTMETHOD_NLO=IntegrationMethod.MISER))
 
 
 def test_r_grid_matches_reference_construction():

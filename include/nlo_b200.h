@@ -292,6 +292,37 @@ int nlo_bk_evolve_vegas(const nlo_bk_params* params, const double* r, int32_t po
                         double* state, double* table, uint32_t* status, void* workspace, size_t workspace_bytes,
                         void* stream);
 
+/* --------------------------------------------------- Vegas for a caller's integrand
+ * The vegas() integrator (numerics/integration.py:120-589) for any integrand the caller
+ * evaluates itself (the reference integrates arbitrary torch functions with it).  The library
+ * does the sampling and the bookkeeping on the device; per round (the warm-up, then each
+ * iteration): nlo_vegas_sample for a batch of Sobol points, the caller's f at the batch's box
+ * points, nlo_vegas_accumulate; after the round's last batch nlo_vegas_end_round re-bins the
+ * grid (:804-866) and, for an iteration, updates the inverse-variance-weighted value, error and
+ * convergence flag (:510-582).  The state holds the grid edges [dims][bins+1] (the unit cube)
+ * and then value, error, n_eval, iterations and converged at NLO_VEGAS_VALUE.. after them. */
+size_t nlo_vegas_state_doubles(int32_t dims, int32_t bins);     /* dims 1..8, bins 2..256 */
+size_t nlo_vegas_workspace_bytes(int32_t dims, int32_t bins);
+/* Clear the sums; a uniform grid unless keep_edges (the edges already in `state`, a kept VegasState). */
+int nlo_vegas_begin(int32_t dims, int32_t bins, int32_t keep_edges, double* state, void* workspace,
+                    size_t workspace_bytes, void* stream);
+/* Points offset..offset+n-1 of the scrambled Sobol sequence `dirs` mapped through the grid:
+ * x[n][dims] = lower + width * grid(u), factor[n] = prod(width) * prod(bins * bin width), bin[n][dims].
+ * lower, width: host double[dims]; x, factor, bin: device. */
+int nlo_vegas_sample(const nlo_sobol_dirs* dirs, int64_t offset, int64_t n, int32_t dims, int32_t bins,
+                     const double* state, const double* lower, const double* width, double* x, double* factor,
+                     int32_t* bin, void* stream);
+/* Add the weights w = f * factor of a batch (f: device double[n], the integrand at the batch's
+ * points) to the round's sums and |w| histograms, in a fixed order. */
+int nlo_vegas_accumulate(const double* f, const double* factor, const int32_t* bin, int64_t n, int32_t dims,
+                         int32_t bins, void* workspace, size_t workspace_bytes, void* stream);
+/* Close a round of `samples` points: re-bin the grid; unless warmup, fold the round's estimate
+ * into the combination and set converged once iterations >= min_iterations and
+ * error <= max(epsabs, epsrel |value|). */
+int nlo_vegas_end_round(int32_t dims, int32_t bins, double* state, int64_t samples, int32_t warmup,
+                        int32_t min_iterations, double epsrel, double epsabs, void* workspace, size_t workspace_bytes,
+                        void* stream);
+
 /* ======================================================================== NLO DIS
  * The NLO DIS cross-section integrands (dis/observables.py, dis/lo.py, dis/transverse.py,
  * dis/longitudinal.py) with the GBW or BK-table dipole, their tensor Gauss-Legendre rule and

@@ -169,6 +169,12 @@ EXPORTED = (
     "nlo_bk_vegas_workspace_bytes",
     "nlo_bk_rhs_vegas",
     "nlo_bk_evolve_vegas",
+    "nlo_vegas_state_doubles",
+    "nlo_vegas_workspace_bytes",
+    "nlo_vegas_begin",
+    "nlo_vegas_sample",
+    "nlo_vegas_accumulate",
+    "nlo_vegas_end_round",
     "nlo_dis_table_doubles",
     "nlo_dis_table_prepare",
     "nlo_dis_table_prepare_interpolated",
@@ -244,6 +250,18 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.nlo_bk_evolve_vegas.restype = ctypes.c_int
     lib.nlo_bk_evolve_vegas.argtypes = [P(BKParams), vp, i32, vp, i32, i32, d, i32, P(BKVegasOptions), P(SobolDirs),
                                         P(Box), vp, vp, vp, vp, sz, vp]
+    lib.nlo_vegas_state_doubles.restype = sz
+    lib.nlo_vegas_state_doubles.argtypes = [i32, i32]
+    lib.nlo_vegas_workspace_bytes.restype = sz
+    lib.nlo_vegas_workspace_bytes.argtypes = [i32, i32]
+    lib.nlo_vegas_begin.restype = ctypes.c_int
+    lib.nlo_vegas_begin.argtypes = [i32, i32, i32, vp, vp, sz, vp]
+    lib.nlo_vegas_sample.restype = ctypes.c_int
+    lib.nlo_vegas_sample.argtypes = [P(SobolDirs), i64, i64, i32, i32, vp, P(d), P(d), vp, vp, vp, vp]
+    lib.nlo_vegas_accumulate.restype = ctypes.c_int
+    lib.nlo_vegas_accumulate.argtypes = [vp, vp, vp, i64, i32, i32, vp, sz, vp]
+    lib.nlo_vegas_end_round.restype = ctypes.c_int
+    lib.nlo_vegas_end_round.argtypes = [i32, i32, vp, i64, i32, i32, d, d, vp, sz, vp]
     lib.nlo_dis_table_doubles.restype = sz
     lib.nlo_dis_table_doubles.argtypes = [i32, i32]
     lib.nlo_dis_table_prepare.restype = ctypes.c_int

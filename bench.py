@@ -352,6 +352,9 @@ def run_ours(args) -> None:
     }
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline()
+    timing = reference_torch_cpu()
+    if timing is not None:
+        line["reference_torch_cpu"] = timing
     if not args.no_dis and world == 1:
         # the second half of the metric: NLO DIS sigma_r points/s on an evolved table
         line["dis"] = measure_dis(args.dis_points, args.dis_single, args.dis_check)
@@ -480,6 +483,17 @@ def cpu_baseline() -> dict:
     }
 
 
+def reference_torch_cpu() -> dict | None:
+    """The reference package's own CPU evolution as shipped (solve_bk(..., device="cpu",
+    dtype=float64) at its defaults to Y = 0.4), timed once in the build container by
+    oracle/reference_cpu_timing.py -- the package does not travel to the GPU machine.  A
+    secondary baseline, reported with where it was measured; not used for any ratio."""
+    path = ROOT / "oracle" / "reference_cpu_timing.json"
+    if not path.exists():
+        return None
+    return json.loads(path.read_text())
+
+
 def run_reference(args) -> None:
     """The reference algorithm on the host cores (the oracle's C restatement, all threads):
     each step is one complete right-hand side of the workload (splines, K1 on every active
@@ -530,6 +544,9 @@ def run_reference(args) -> None:
                          "cpu_model": _cpu_model(), "kind": "port", "sample": sample},
         "e2e": {"value": round(seconds, 2), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    timing = reference_torch_cpu()
+    if timing is not None:
+        line["reference_torch_cpu"] = timing
     print(json.dumps(line))
 
 

@@ -1,0 +1,81 @@
+"""Time the reference's own BK evolution on the CPU, as shipped -- measurement infrastructure.
+
+The reference package (torch_nlo_clean/src/nlo_torch) cannot travel to the GPU machine, so
+its own CPU path is timed here, once, and the result is committed beside this script as
+``reference_cpu_timing.json``; ``bench.py`` reports it as a secondary baseline with this
+provenance.  What runs is the reference's public call
+``solve_bk(MV(qs0sqr=0.2), 0.4, BKConfig(), device="cpu", dtype=torch.float64, seed=0)``:
+its defaults (RPOINTS = 100 on [1e-6, 30], MCINTPOINTS = 1e5, step 0.2), which on the CPU mean
+adaptive Gauss-Kronrod K1, Vegas K2+Kf per parent and the adaptive RK2 stepper
+(bk/evolution.py:33-58, 239-326, 354-488).  Its derivative count and the time per derivative
+are recorded too.
+
+    NLO_REFERENCE_ROOT=<checkout> python -m oracle.reference_cpu_timing [<checkout>]
+"""
+
+from __future__ import annotations
+
+import json
+import os
+import platform
+import sys
+import time
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+OUTPUT = HERE / "reference_cpu_timing.json"
+
+
+def _cpu_model() -> str:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return platform.processor() or "unknown"
+
+
+def main() -> None:
+    root = next((a for a in sys.argv[1:] if Path(a).is_dir()), os.environ.get("NLO_REFERENCE_ROOT"))
+    if not root:
+        raise SystemExit("set NLO_REFERENCE_ROOT (or pass the checkout) to the reference checkout's root")
+    sys.path.insert(0, str(Path(root) / "torch_nlo_clean" / "src"))
+    import torch
+
+    import nlo_torch.bk.evolution as evolution
+    from nlo_torch.bk.config import BKConfig
+    from nlo_torch.bk.initial_conditions import MV
+
+    calls = {"n": 0}
+    original = evolution._evolve_derivative
+
+    def counted(*args, **kwargs):
+        calls["n"] += 1
+        return original(*args, **kwargs)
+
+    evolution._evolve_derivative = counted
+    config = BKConfig()
+    t0 = time.perf_counter()
+    table = evolution.solve_bk(MV(qs0sqr=0.2), 0.4, config, device="cpu", dtype=torch.float64, seed=0)
+    seconds = time.perf_counter() - t0
+    result = {
+        "call": "nlo_torch.solve_bk(MV(qs0sqr=0.2), 0.4, BKConfig(), device='cpu', dtype=torch.float64, seed=0)",
+        "config": {"RPOINTS": config.RPOINTS, "MINR": config.MINR, "MAXR": config.MAXR,
+                   "MCINTPOINTS": config.MCINTPOINTS, "DE_SOLVER_STEP": config.DE_SOLVER_STEP,
+                   "INTMETHOD_NLO": config.INTMETHOD_NLO.name},
+        "seconds_to_y_0_4": round(seconds, 2),
+        "derivatives": calls["n"],
+        "seconds_per_derivative": round(seconds / max(calls["n"], 1), 2),
+        "rows": int(table.N.shape[0]),
+        "threads": torch.get_num_threads(),
+        "cpu_model": _cpu_model(),
+        "torch": torch.__version__,
+        "where": "the build container (the reference package does not travel to the GPU machine)",
+    }
+    OUTPUT.write_text(json.dumps(result, indent=1) + "\n")
+    print(json.dumps(result))
+
+
+if __name__ == "__main__":
+    main()

@@ -359,6 +359,9 @@ def run_ours(args) -> None:
         # the second half of the metric: NLO DIS sigma_r points/s on an evolved table
         line["dis"] = measure_dis(args.dis_points, args.dis_single, args.dis_check)
         line["fixed_sobol"] = measure_fixed()
+    if not args.no_batch and world == 1:
+        line["batch"] = measure_batch(args.line_batch_sets)
+        line["serve"] = measure_serve(args.line_serve_seconds, args.serve_rate, args.serve_slots, args.serve_lanes)
     print(json.dumps(line))
 
 
@@ -660,6 +663,7 @@ def measure_dis(points: int = 0, single: int = 4, check: int = 4) -> dict:
     fp64 = structure_functions(Qg[:check_n], Xg[:check_n], dipole, cfg("fp64"), sqrt_s=DIS_SQRT_S, seed=0, **opts)
     rel = (batch["sigma_r"][:check_n] - fp64["sigma_r"]).abs() / fp64["sigma_r"].abs()
     same = max(abs(singles[i] / float(batch["sigma_r"][i]) - 1) for i in range(single_n)) if single_n else None
+    roofline = dis_nested_roofline(Qg, Xg, dipole, cfg("mixed"))
     line = {
         "metric": "DIS sigma_r points/s (NLO, batched)",
         "value": round(Qg.numel() / batch_s, 3),
@@ -680,8 +684,75 @@ def measure_dis(points: int = 0, single: int = 4, check: int = 4) -> dict:
         "single_vs_batched_max_rel": same,
         "sigma_r_sample": [float(v) for v in batch["sigma_r"][:4]],
         "sigma_r_error_sample": [float(v) for v in batch["sigma_r_error"][:4]],
+        "roofline": roofline,
     }
     return line
+
+
+# Op census of one outer sample of the nested qqbar-g terms, from oracle/census_dis.py (an
+# op-counting run of the DIS oracle's FP64 restatement; the mean of both polarisations):
+# arithmetic = add, sub, mul, div; special = exp, log, sqrt, power, trigonometric, Bessel K0/K1.
+DIS_CENSUS = {"I2N": {"arithmetic": 9866, "special": 3106}, "I3N": {"arithmetic": 9845, "special": 3091}}
+
+
+def dis_nested_roofline(Qg, Xg, dipole, config) -> dict:
+    """The nested I2 and I3 Vegas rounds of the DIS workload (all 512 points, both
+    polarisations: 1,024 integrals, one round of 2^18 samples each), timed alone with CUDA
+    events on their stream, against the census of the oracle restatement."""
+    import torch
+
+    from nlo_bk_optimized_b200 import _native
+    from nlo_bk_optimized_b200.dis import Polarization
+    from nlo_bk_optimized_b200.dis.observables import kinematics
+    from nlo_bk_optimized_b200.numerics.integration import VegasOptions, vegas_terms
+
+    device = torch.device("cuda", 0)
+    kins = [kinematics(float(q), float(x), pol, config, config.quarks[0])
+            for q, x in zip(Qg.tolist(), Xg.tolist()) for pol in (Polarization.T, Polarization.L)]
+    opts = VegasOptions(samples_per_iteration=DIS_SAMPLES, max_iterations=1, min_iterations=1, bins=DIS_BINS,
+                        epsrel=1e-12)
+    native = dipole.native()
+    stream = torch.cuda.current_stream(device)
+    out = {}
+    flops = specials = seconds = 0.0
+    for term in ("I2N", "I3N"):
+        code = _native.DIS_TERMS[term]
+        vegas_terms(code, kins[:2], native, opts, [0, 1], precision=_native.PRECISION_MIXED, device=device)  # warm
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        start.record(stream)
+        vegas_terms(code, kins, native, opts, list(range(len(kins))), precision=_native.PRECISION_MIXED,
+                    device=device)
+        stop.record(stream)
+        torch.cuda.synchronize()
+        t = start.elapsed_time(stop) / 1e3
+        n = len(kins) * DIS_SAMPLES
+        out[term] = {"round_ms": round(t * 1e3, 3), "outer_samples": n}
+        flops += n * DIS_CENSUS[term]["arithmetic"]
+        specials += n * DIS_CENSUS[term]["special"]
+        seconds += t
+    sm_mhz = 1965.0
+    peak = SM_COUNT * FP32_LANES_PER_SM * 2 * sm_mhz * 1e6 / 1e12
+    mufu_peak = SM_COUNT * MUFU_PER_SM_PER_CLOCK * sm_mhz * 1e6
+    achieved = flops / seconds / 1e12
+    return {
+        "bound": "fp32",
+        "achieved": round(achieved, 3),
+        "peak": round(peak, 2),
+        "unit": "TFLOP/s",
+        "frac": round(achieved / peak, 4),
+        "traffic": None,
+        "traffic_source": "not captured at the workload size; the kernel-case capture (one job, 2^16 samples) read "
+                          "72-79 KB per launch: job arguments, grid and dipole table only",
+        "kernel": "vegas_iteration_kernel<float, I2 nested / I3 nested> (csrc/dis.cu)",
+        "peak_source": "nominal FP32 (148 SM x 128 lanes x 2 x 1965 MHz); MEASURED_PEAKS.json has only HBM and bf16",
+        "census": {"source": "oracle/census_dis.py: op-counting run of the DIS oracle's FP64 nested integrands",
+                   **DIS_CENSUS},
+        "transcendental": {"achieved_per_s": round(specials / seconds, 1), "peak_per_s": mufu_peak,
+                           "frac": round(specials / seconds / mufu_peak, 4),
+                           "peak_source": "nominal 16 MUFU operations per SM per clock at 1965 MHz"},
+        "rounds": out,
+    }
 
 
 # The reference's published C++ timings (20 CPU workers) of its six-term fixed-Sobol
@@ -790,88 +861,177 @@ def _small_bk_config(samples: int = 1 << 16):
                     PRECISION="mixed", ALPHA_S_CAP=0.7, INTMETHOD_NLO=IntegrationMethod.SOBOL)
 
 
-def run_batch(args) -> None:
-    """256 parameter sets evolved to Y = 8 (the rapidity 8 points of Q^2 in [1, 50], x in
-    [1e-3, 1e-2] reach is ln(Q^2/(x Q0^2)) <= 10.8; the sets stop at Y = 8 and the DIS points
-    of each set are drawn so that they stay inside its table) in one stream-parallel run,
-    against the same sets solved one after another on one stream (a sample of them)."""
+def _set_points(k: int, count: int = 8) -> list[tuple[float, float]]:
+    """The DIS points of parameter set k: Q^2 log-uniform in [1, 50] GeV^2 and x_Bj log-uniform
+    in [1e-2, 5e-2] (seeded by k), inside the rapidity range of a table evolved to Y = 4 from
+    x0 = 0.01: ln(Q^2 / (x Q0^2)) <= 8.52 < 4 + ln(1/x0)."""
     import torch
 
-    from nlo_bk_optimized_b200 import MV
+    g = torch.Generator().manual_seed(1000 + k)
+    u = torch.rand((count, 2), generator=g, dtype=torch.float64)
+    Q2 = torch.exp(u[:, 0] * math.log(50.0))
+    xs = 1e-2 * torch.exp(u[:, 1] * math.log(5.0))
+    return [(float(q), float(x)) for q, x in zip(Q2, xs)]
+
+
+BATCH_MAXY = 4.0  # the evolution of the batched parameter sets: RK4, h = 0.2, to Y = 4
+
+
+def measure_batch(n_sets: int) -> dict:
+    """The batched solve: n_sets MV parameter sets (Qs0^2 ~ U[0.05, 0.5], gamma ~ U[0.8, 1.3],
+    e_c ~ logU[1, 100], budgets 2^U{16..20} Sobol points per r per stage) evolved on 200 r in
+    [1e-6, 1e2] (RK4 h = 0.2 to Y = 4, alpha_s capped at 0.7), then each set's 8 (Q^2, x_Bj)
+    points (NLO F_T, F_L, F_2, sigma_r at sqrt(s) = 318 GeV, light quarks, Vegas of 4
+    iterations x budget/16 samples) -- all evolutions concurrently on CUDA streams and all
+    points of all sets in one merged DIS run -- against the plain single-solve path
+    (solve_bk of one set, then sigma_r of one point at a time), timed on one set of each
+    budget class and summed over the classes' set counts."""
+    import torch
+
+    from nlo_bk_optimized_b200 import MV, solve_bk
     from nlo_bk_optimized_b200.bk.batch import evolve_batch, tune_streams
     from nlo_bk_optimized_b200.bk.evolution import _r_grid, _steps_to
+    from nlo_bk_optimized_b200.dipole import BKDipole, DipoleTable
+    from nlo_bk_optimized_b200.dis import DISConfig, DISOrder, Quark, QuarkType, sigma_r, structure_functions
+    from nlo_bk_optimized_b200.dis import structure_functions_many
+    from nlo_bk_optimized_b200.serving import dis_options_for
 
     device = torch.device("cuda", 0)
-    torch.cuda.set_device(device)
-    sets = _sets(args.batch_sets)
+    sets = _sets(n_sets)
     config = _small_bk_config()
+    dis = DISConfig(order=DISOrder.NLO, quarks=(Quark(QuarkType.LIGHT, 0.14),))
     r_host = _r_grid(config, device="cpu", dtype=torch.float64)
     N0 = torch.stack([MV(qs0sqr=q, gamma=g, ec=e).dipole_amplitude(r_host).to(torch.float64)
                       for q, g, e, _ in sets]).to(device)
     r = r_host.to(device)
     budgets = [b for *_, b in sets]
-    steps = len(_steps_to(0.0, args.batch_maxy, 0.2))
+    ys = _steps_to(0.0, BATCH_MAXY, 0.2)
+    y = torch.tensor([0.0, *ys], dtype=torch.float64, device=device)
+    points = [_set_points(k) for k in range(n_sets)]
+
+    def batched():
+        tables = evolve_batch(N0, r, len(ys), config, budgets, streams=streams)
+        dipoles = [BKDipole(DipoleTable(r=r, y=y, N=tables[k], x0=0.01)) for k in range(n_sets)]
+        Q2 = [q for pts in points for q, _ in pts]
+        xs = [x for pts in points for _, x in pts]
+        dips = [dipoles[k] for k, pts in enumerate(points) for _ in pts]
+        seeds = [k for k, pts in enumerate(points) for _ in pts]
+        opts = [dis_options_for(budgets[k]) for k, pts in enumerate(points) for _ in pts]
+        out = structure_functions_many(Q2, xs, dips, dis, sqrt_s=DIS_SQRT_S, seeds=seeds, options=opts)
+        return out["sigma_r"].cpu()
+
     streams = tune_streams(N0, r, config, budgets)
-    evolve_batch(N0[:2], r, 1, config, budgets[:2], streams=2)  # warm-up
+    # warm-up of every kernel on the path: a short evolution of two sets and two of their points
+    warm = evolve_batch(N0[:2], r, len(ys), config, [1 << 10] * 2, streams=2)
+    warm_dipoles = [BKDipole(DipoleTable(r=r, y=y, N=warm[k], x0=0.01)) for k in range(2)]
+    structure_functions_many([points[0][0][0], points[1][0][0]], [points[0][0][1], points[1][0][1]], warm_dipoles,
+                             dis, sqrt_s=DIS_SQRT_S, seeds=[0, 1], options=[dis_options_for(1 << 16)] * 2)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    evolve_batch(N0, r, steps, config, budgets, streams=streams)
+    sig_batched = batched()
     torch.cuda.synchronize()
-    batched = time.perf_counter() - t0
-    sample = list(range(0, len(sets), max(1, len(sets) // 16)))[:16]
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for i in sample:
-        evolve_batch(N0[i:i + 1], r, steps, config, budgets[i:i + 1], streams=1)
-    torch.cuda.synchronize()
-    single = (time.perf_counter() - t0) / len(sample)
-    evals = sum(budgets) * 200 * 4 * steps
-    line = {
-        "metric": "batched NLO BK evolutions per second",
-        "value": round(len(sets) / batched, 3),
+    batched_s = time.perf_counter() - t0
+
+    # the plain path on one set of each budget class
+    classes: dict[int, list[int]] = {}
+    for k, b in enumerate(budgets):
+        classes.setdefault(b, []).append(k)
+    per_class_point, per_class_set = {}, {}
+    ic_of = lambda k: MV(qs0sqr=sets[k][0], gamma=sets[k][1], ec=sets[k][2])  # noqa: E731
+    single_vs_batched = 0.0
+    for b, members in sorted(classes.items()):
+        k = members[0]
+        cfg = _small_bk_config(b)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        table = solve_bk(ic_of(k), BATCH_MAXY, cfg, device=device, dtype=torch.float64, seed=0)
+        dipole = BKDipole(table)
+        vals = []
+        for j, (q2, x) in enumerate(points[k]):
+            res = sigma_r(torch.tensor(q2, dtype=torch.float64, device=device),
+                          torch.tensor(x, dtype=torch.float64, device=device), dipole, dis, sqrt_s=DIS_SQRT_S,
+                          seed=k, **dis_options_for(b))
+            vals.append(float(res.value))
+        torch.cuda.synchronize()
+        per_class_point[b] = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        sf = structure_functions(torch.tensor([q for q, _ in points[k]], dtype=torch.float64),
+                                 torch.tensor([x for _, x in points[k]], dtype=torch.float64),
+                                 BKDipole(solve_bk(ic_of(k), BATCH_MAXY, cfg, device=device, dtype=torch.float64,
+                                                   seed=0)), dis, sqrt_s=DIS_SQRT_S, seed=k, **dis_options_for(b))
+        sf["sigma_r"].cpu()
+        per_class_set[b] = time.perf_counter() - t0
+        base = sum(len(p) for p in points[:k])
+        for j, v in enumerate(vals):
+            single_vs_batched = max(single_vs_batched, abs(v / float(sig_batched[base + j]) - 1))
+    plain_points = sum(per_class_point[b] * len(m) for b, m in classes.items())
+    plain_sets = sum(per_class_set[b] * len(m) for b, m in classes.items())
+    n_points = sum(len(p) for p in points)
+    return {
+        "metric": "batched NLO BK + DIS: parameter sets evolved and evaluated per second",
+        "value": round(n_sets / batched_s, 3),
         "unit": "parameter sets/s",
         "n_gpus": 1,
         "higher_is_better": True,
         "dtype": "f32+f64",
-        "data": "synthetic: MV parameter sets from torch.Generator().manual_seed(0)",
-        "config": {"workload": f"{len(sets)} MV sets, 200 r in [1e-6,1e2], RK4 h=0.2 to Y={args.batch_maxy}, "
-                               "budgets 2^U{16..20} per r per stage, alpha_s cap 0.7",
-                   "streams_chosen": streams, "k2kf_evaluations": evals},
-        "batched_s": round(batched, 4),
-        "single_set_s_mean": round(single, 5),
-        "speedup_vs_one_at_a_time": round(single * len(sets) / batched, 3),
+        "data": "synthetic: MV parameter sets from torch.Generator().manual_seed(0), seeded DIS points",
+        "config": {"workload": f"{n_sets} MV sets, 200 r in [1e-6,1e2], RK4 h=0.2 to Y={BATCH_MAXY}, alpha_s cap 0.7, "
+                               "budgets 2^U{16..20} per r per stage; 8 (Q^2,x) points per set, NLO sigma_r, "
+                               "Vegas 4 it x budget/16", "sets": n_sets, "points": n_points, "streams": streams},
+        "batched_s": round(batched_s, 3),
+        "dis_points_per_s": round(n_points / batched_s, 2),
+        "plain_single_point_s": round(plain_points, 2),
+        "plain_single_point_per_set_s": {str(b): round(t, 4) for b, t in sorted(per_class_point.items())},
+        "speedup_vs_plain_single_point": round(plain_points / batched_s, 3),
+        "plain_per_set_s": round(plain_sets, 2),
+        "speedup_vs_plain_per_set": round(plain_sets / batched_s, 3),
+        "plain_timing": "one set of each budget class timed, times its class's set count",
+        "single_vs_batched_max_rel": single_vs_batched,
     }
-    print(json.dumps(line))
 
 
-def run_serve(args) -> None:
-    """Poisson arrivals: each request is one parameter set, 1-64 (Q^2, x) points of the
-    32 x 16 DIS grid restricted to x >= 1e-3 (table range), and its Monte Carlo budget; p50/p99
-    latency and points/s of the server against the same requests run one at a time."""
+def run_batch(args) -> None:
+    print(json.dumps(measure_batch(args.batch_sets)))
+
+
+def _requests_for(seconds: float, rate: float, seed: int = 0):
     import random
 
-    import torch
+    from nlo_bk_optimized_b200.serving import Request
 
-    from nlo_bk_optimized_b200.dis import DISConfig, DISOrder, Quark, QuarkType
-    from nlo_bk_optimized_b200.serving import Request, Server, run_alone
-
-    device = torch.device("cuda", 0)
-    torch.cuda.set_device(device)
-    rng = random.Random(0)
+    rng = random.Random(seed)
     sets = _sets(4096, seed=1)
     Q2s = [1.0 * (50.0 ** (k / 31)) for k in range(32)]
     xs = [1e-3 * (10.0 ** (k / 15)) for k in range(16)]
     grid = [(q, x) for q in Q2s for x in xs]
     t, requests = 0.0, []
-    while t < args.serve_seconds:
-        t += rng.expovariate(args.serve_rate)
-        q, g, e, budget = sets[len(requests) % len(sets)]
+    while t < seconds:
+        t += rng.expovariate(rate)
+        q, g, e, _ = sets[len(requests) % len(sets)]
+        budget = int(round(2 ** rng.uniform(16, 20)))  # log-uniform in [2^16, 2^20]
         pts = tuple(rng.sample(grid, rng.randint(1, 64)))
         requests.append((t, Request(q, g, e, pts, budget, seed=len(requests))))
+    return requests
+
+
+def measure_serve(seconds: float, rate: float, slots: int, lanes: int, sample: int = 8) -> dict:
+    """Poisson arrivals at `rate`/s for `seconds`: each request is one parameter set (drawn as
+    in the batched workload), 1-64 points of the 32 x 16 DIS grid restricted to x >= 1e-3 and
+    an MC budget log-uniform in [2^16, 2^20].  p50/p99 latency and points/s of the server
+    (continuous batching) against the same requests run one at a time through the plain
+    single-solve path (a sample of them)."""
+    import torch
+
+    from nlo_bk_optimized_b200.dis import DISConfig, DISOrder, Quark, QuarkType
+    from nlo_bk_optimized_b200.serving import Server, run_alone
+
+    device = torch.device("cuda", 0)
+    torch.cuda.set_device(device)
+    requests = _requests_for(seconds, rate)
     bk = _small_bk_config()
-    dis = DISConfig(order=DISOrder.NLO, quarks=(Quark(QuarkType.LIGHT, 0.14),), vegas_bins=32)
+    dis = DISConfig(order=DISOrder.NLO, quarks=(Quark(QuarkType.LIGHT, 0.14),))
     run_alone(requests[0][1], bk, dis)  # warm-up
-    server = Server(bk, dis, slots=args.serve_slots)
+    server = Server(bk, dis, slots=slots, lanes=lanes)
     t0 = time.perf_counter()
     futures = []
     for at, req in requests:
@@ -883,13 +1043,14 @@ def run_serve(args) -> None:
         f.result()
     server.close()
     served = server.stats.summary()
-    sample = requests[: min(8, len(requests))]
+    pick = requests[:: max(1, len(requests) // sample)][:sample]
     t1 = time.perf_counter()
-    for _, req in sample:
+    for _, req in pick:
         run_alone(req, bk, dis)
-    alone = (time.perf_counter() - t1) / len(sample)
-    alone_pts = sum(len(r.points) for _, r in sample) / len(sample)
-    line = {
+    alone = (time.perf_counter() - t1) / len(pick)
+    alone_pts = sum(len(r.points) for _, r in pick) / len(pick)
+    sequential_pps = alone_pts / alone
+    return {
         "metric": "served NLO BK + DIS requests: p50/p99 latency and points/s",
         "value": round(served["points_per_s"], 3),
         "unit": "points/s",
@@ -897,16 +1058,22 @@ def run_serve(args) -> None:
         "higher_is_better": True,
         "dtype": "f32+f64",
         "data": "synthetic Poisson arrivals, seeded",
-        "config": {"workload": f"Poisson {args.serve_rate}/s for {args.serve_seconds} s, 1-64 points per request, "
-                               "budgets 2^U{16..20}", "slots": args.serve_slots, "requests": len(requests)},
+        "config": {"workload": f"Poisson {rate}/s for {seconds} s, 1-64 points per request, budgets logU[2^16, 2^20]",
+                   "slots": slots, "lanes": lanes, "requests": len(requests)},
         "p50_s": served["p50_s"],
         "p99_s": served["p99_s"],
         "requests_per_s": served["requests_per_s"],
-        "sequential_points_per_s": round(alone_pts / alone, 3),
+        "dis_batches": len(server.batches),
+        "mean_requests_per_dis_batch": round(sum(server.batches) / max(1, len(server.batches)), 2),
+        "sequential_points_per_s": round(sequential_pps, 3),
         "sequential_request_s_mean": round(alone, 4),
-        "speedup_vs_sequential": round(served["points_per_s"] / (alone_pts / alone), 3),
+        "sequential_sample": len(pick),
+        "speedup_vs_sequential": round(served["points_per_s"] / sequential_pps, 3),
     }
-    print(json.dumps(line))
+
+
+def run_serve(args) -> None:
+    print(json.dumps(measure_serve(args.serve_seconds, args.serve_rate, args.serve_slots, args.serve_lanes)))
 
 
 def main() -> None:
@@ -927,7 +1094,11 @@ def main() -> None:
     parser.add_argument("--batch-maxy", type=float, default=8.0)
     parser.add_argument("--serve-rate", type=float, default=200.0)
     parser.add_argument("--serve-seconds", type=float, default=1.0)
-    parser.add_argument("--serve-slots", type=int, default=8)
+    parser.add_argument("--serve-slots", type=int, default=64)
+    parser.add_argument("--serve-lanes", type=int, default=8)
+    parser.add_argument("--no-batch", action="store_true", help="skip the batched and served objects of the line")
+    parser.add_argument("--line-batch-sets", type=int, default=32, help="parameter sets of the line's batch object")
+    parser.add_argument("--line-serve-seconds", type=float, default=0.5, help="arrival window of the line's serve object")
     parser.add_argument("--no-dis", action="store_true", help="skip the DIS sigma_r measurement")
     parser.add_argument("--dis-points", type=int, default=0, help="DIS: first N of the 512 points (0 = all)")
     parser.add_argument("--dis-single", type=int, default=4, help="DIS: points timed through single sigma_r calls")

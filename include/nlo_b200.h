@@ -418,6 +418,12 @@ int nlo_dis_gauss_legendre(const nlo_dis_kinematics* kin, int32_t jobs, int32_t 
                            int32_t points, int32_t precision, double* out, void* workspace, size_t workspace_bytes,
                            void* stream);
 size_t nlo_dis_gauss_legendre_workspace_bytes(int32_t jobs);
+/* nlo_dis_gauss_legendre with a dipole per job (dipoles: host array [jobs]), so that one launch
+ * serves kinematic points of different BK tables -- the requests of a batch or of the
+ * serving loop (no counterpart in the reference, which evaluates one dipole at a time). */
+int nlo_dis_gauss_legendre_dipoles(const nlo_dis_kinematics* kin, int32_t jobs, int32_t term,
+                                   const nlo_dipole* dipoles, int32_t points, int32_t precision, double* out,
+                                   void* workspace, size_t workspace_bytes, void* stream);
 
 /* Vegas options (numerics/integration.py:120-138). */
 typedef struct nlo_vegas_options {
@@ -450,6 +456,14 @@ size_t nlo_dis_vegas_workspace_bytes(int32_t jobs, int32_t term, const nlo_vegas
 int nlo_dis_vegas(const nlo_dis_kinematics* kin, int32_t jobs, int32_t term, const nlo_dipole* dipole,
                   const nlo_vegas_options* options, const nlo_sobol_dirs* dirs, double* state, void* workspace,
                   size_t workspace_bytes, void* stream);
+
+/* nlo_dis_vegas with a dipole per job (dipoles: host array [jobs]): the integrals of many
+ * parameter sets or requests, each with its own BK table, in one sequence of launches (no
+ * counterpart in the reference, which evaluates one dipole at a time).  Workspace and state
+ * sizes are those of nlo_dis_vegas. */
+int nlo_dis_vegas_dipoles(const nlo_dis_kinematics* kin, int32_t jobs, int32_t term, const nlo_dipole* dipoles,
+                          const nlo_vegas_options* options, const nlo_sobol_dirs* dirs, double* state,
+                          void* workspace, size_t workspace_bytes, void* stream);
 
 /* Fixed-Sobol options (dis/fixed_sobol.py:30-37 defaults in brackets). */
 typedef struct nlo_fixed_sobol_options {

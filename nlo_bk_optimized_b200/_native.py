@@ -183,9 +183,11 @@ EXPORTED = (
     "nlo_dis_integrand",
     "nlo_dis_gauss_legendre_workspace_bytes",
     "nlo_dis_gauss_legendre",
+    "nlo_dis_gauss_legendre_dipoles",
     "nlo_dis_vegas_state_doubles",
     "nlo_dis_vegas_workspace_bytes",
     "nlo_dis_vegas",
+    "nlo_dis_vegas_dipoles",
     "nlo_dis_fixed_sobol_grid_doubles",
     "nlo_dis_fixed_sobol_workspace_bytes",
     "nlo_dis_fixed_sobol",
@@ -278,6 +280,11 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.nlo_dis_gauss_legendre_workspace_bytes.argtypes = [i32]
     lib.nlo_dis_gauss_legendre.restype = ctypes.c_int
     lib.nlo_dis_gauss_legendre.argtypes = [P(DisKinematics), i32, i32, P(Dipole), i32, i32, vp, vp, sz, vp]
+    lib.nlo_dis_gauss_legendre_dipoles.restype = ctypes.c_int
+    lib.nlo_dis_gauss_legendre_dipoles.argtypes = [P(DisKinematics), i32, i32, P(Dipole), i32, i32, vp, vp, sz, vp]
+    lib.nlo_dis_vegas_dipoles.restype = ctypes.c_int
+    lib.nlo_dis_vegas_dipoles.argtypes = [P(DisKinematics), i32, i32, P(Dipole), P(VegasOptions), P(SobolDirs), vp,
+                                          vp, sz, vp]
     lib.nlo_dis_vegas_state_doubles.restype = sz
     lib.nlo_dis_vegas_state_doubles.argtypes = [i32, i32]
     lib.nlo_dis_vegas_workspace_bytes.restype = sz

@@ -127,17 +127,19 @@ constexpr size_t kAlign = 256;
 size_t align_up(size_t v) { return (v + kAlign - 1) & ~(kAlign - 1); }
 size_t args_bytes(int jobs) { return align_up((size_t)jobs * std::max(sizeof(DisArgs<double>), sizeof(DisArgs<float>))); }
 
-int upload_args(const nlo_dis_kinematics* kin, int jobs, const nlo_dipole& d, int precision, void* dst,
-                cudaStream_t stream)
+// Argument blocks of `jobs` jobs; job j takes the dipole dipoles[j * dipole_stride]
+// (stride 0: one dipole for every job).
+int upload_args(const nlo_dis_kinematics* kin, int jobs, const nlo_dipole* dipoles, int dipole_stride, int precision,
+                void* dst, cudaStream_t stream)
 {
     cudaError_t e;
     if (precision == NLO_PRECISION_FP64) {
         std::vector<DisArgs<double>> h(jobs);
-        for (int j = 0; j < jobs; ++j) h[j] = make_args<double>(kin[j], d);
+        for (int j = 0; j < jobs; ++j) h[j] = make_args<double>(kin[j], dipoles[(size_t)j * dipole_stride]);
         e = cudaMemcpyAsync(dst, h.data(), sizeof(DisArgs<double>) * jobs, cudaMemcpyHostToDevice, stream);
     } else {
         std::vector<DisArgs<float>> h(jobs);
-        for (int j = 0; j < jobs; ++j) h[j] = make_args<float>(kin[j], d);
+        for (int j = 0; j < jobs; ++j) h[j] = make_args<float>(kin[j], dipoles[(size_t)j * dipole_stride]);
         e = cudaMemcpyAsync(dst, h.data(), sizeof(DisArgs<float>) * jobs, cudaMemcpyHostToDevice, stream);
     }
     return e == cudaSuccess ? NLO_OK : dcuda(e, "DIS argument upload");
@@ -292,19 +294,20 @@ int nlo_dis_dipole_amplitude(const nlo_dipole* dipole, const double* r, const do
 
 size_t nlo_dis_gauss_legendre_workspace_bytes(int32_t jobs) { return jobs < 1 ? 0 : args_bytes(jobs); }
 
-int nlo_dis_gauss_legendre(const nlo_dis_kinematics* kin, int32_t jobs, int32_t term, const nlo_dipole* dipole,
-                           int32_t points, int32_t precision, double* out, void* workspace, size_t workspace_bytes,
-                           void* stream)
+static int gauss_legendre_jobs(const nlo_dis_kinematics* kin, int32_t jobs, int32_t term, const nlo_dipole* dipoles,
+                               int dipole_stride, int32_t points, int32_t precision, double* out, void* workspace,
+                               size_t workspace_bytes, void* stream)
 {
     std::string why;
-    if (!kin || !out) return dfail(NLO_ERR_INVALID, "nlo_dis_gauss_legendre: NULL argument");
+    if (!kin || !out || !dipoles) return dfail(NLO_ERR_INVALID, "nlo_dis_gauss_legendre: NULL argument");
     if (jobs < 1) return dfail(NLO_ERR_INVALID, "jobs must be positive");
     if (term != dis::kTermLO && term != dis::kTermDip0) return dfail(NLO_ERR_INVALID, "the tensor rule serves the 2D terms");
     if (points < 4 || points > 64) return dfail(NLO_ERR_INVALID, "points must lie in 4..64");
     if (precision != NLO_PRECISION_MIXED && precision != NLO_PRECISION_FP64) return dfail(NLO_ERR_INVALID, "unknown precision");
-    if (!check_dipole(dipole, why)) return dfail(NLO_ERR_INVALID, why);
-    for (int j = 0; j < jobs; ++j)
+    for (int j = 0; j < jobs; ++j) {
+        if (!check_dipole(&dipoles[(size_t)j * dipole_stride], why)) return dfail(NLO_ERR_INVALID, why);
         if (!check_kin(kin[j], term, why)) return dfail(NLO_ERR_INVALID, why);
+    }
     if (!workspace || workspace_bytes < args_bytes(jobs)) return dfail(NLO_ERR_WORKSPACE, "workspace missing or too small");
     dis::GLRules gl;
     std::memset(&gl, 0, sizeof(gl));
@@ -324,10 +327,24 @@ int nlo_dis_gauss_legendre(const nlo_dis_kinematics* kin, int32_t jobs, int32_t 
     InnerRule rule;
     make_rule(term, 48, rule, why);
     const cudaStream_t s = static_cast<cudaStream_t>(stream);
-    int rc = upload_args(kin, jobs, *dipole, precision, workspace, s);
+    int rc = upload_args(kin, jobs, dipoles, dipole_stride, precision, workspace, s);
     if (rc != NLO_OK) return rc;
     cudaError_t e = dis_launch_gl(precision, term, workspace, jobs, rule, gl, out, s);
     return e == cudaSuccess ? NLO_OK : dcuda(e, "DIS Gauss-Legendre launch");
+}
+
+int nlo_dis_gauss_legendre(const nlo_dis_kinematics* kin, int32_t jobs, int32_t term, const nlo_dipole* dipole,
+                           int32_t points, int32_t precision, double* out, void* workspace, size_t workspace_bytes,
+                           void* stream)
+{
+    return gauss_legendre_jobs(kin, jobs, term, dipole, 0, points, precision, out, workspace, workspace_bytes, stream);
+}
+
+int nlo_dis_gauss_legendre_dipoles(const nlo_dis_kinematics* kin, int32_t jobs, int32_t term,
+                                   const nlo_dipole* dipoles, int32_t points, int32_t precision, double* out,
+                                   void* workspace, size_t workspace_bytes, void* stream)
+{
+    return gauss_legendre_jobs(kin, jobs, term, dipoles, 1, points, precision, out, workspace, workspace_bytes, stream);
 }
 
 size_t nlo_dis_vegas_state_doubles(int32_t term, int32_t bins)
@@ -343,17 +360,18 @@ size_t nlo_dis_vegas_workspace_bytes(int32_t jobs, int32_t term, const nlo_vegas
     return vegas_carve(jobs, term, *options).total;
 }
 
-int nlo_dis_vegas(const nlo_dis_kinematics* kin, int32_t jobs, int32_t term, const nlo_dipole* dipole,
-                  const nlo_vegas_options* options, const nlo_sobol_dirs* dirs, double* state, void* workspace,
-                  size_t workspace_bytes, void* stream)
+static int vegas_jobs(const nlo_dis_kinematics* kin, int32_t jobs, int32_t term, const nlo_dipole* dipoles,
+                      int dipole_stride, const nlo_vegas_options* options, const nlo_sobol_dirs* dirs, double* state,
+                      void* workspace, size_t workspace_bytes, void* stream)
 {
     std::string why;
-    if (!kin || !dirs || !state) return dfail(NLO_ERR_INVALID, "nlo_dis_vegas: NULL argument");
+    if (!kin || !dirs || !state || !dipoles) return dfail(NLO_ERR_INVALID, "nlo_dis_vegas: NULL argument");
     if (jobs < 1) return dfail(NLO_ERR_INVALID, "jobs must be positive");
     if (term < 0 || term >= dis::kTermCount) return dfail(NLO_ERR_INVALID, "unknown DIS term");
-    if (!check_options(options, term, why) || !check_dipole(dipole, why)) return dfail(NLO_ERR_INVALID, why);
+    if (!check_options(options, term, why)) return dfail(NLO_ERR_INVALID, why);
     const int D = dis::term_dims(term);
     for (int j = 0; j < jobs; ++j) {
+        if (!check_dipole(&dipoles[(size_t)j * dipole_stride], why)) return dfail(NLO_ERR_INVALID, why);
         if (!check_kin(kin[j], term, why)) return dfail(NLO_ERR_INVALID, why);
         if (dirs[j].dims < D || dirs[j].dims > 8) return dfail(NLO_ERR_INVALID, "Sobol dimension count does not match the term");
     }
@@ -363,7 +381,7 @@ int nlo_dis_vegas(const nlo_dis_kinematics* kin, int32_t jobs, int32_t term, con
     if (!workspace || workspace_bytes < c.total) return dfail(NLO_ERR_WORKSPACE, "workspace missing or too small");
     unsigned char* ws = static_cast<unsigned char*>(workspace);
     const cudaStream_t s = static_cast<cudaStream_t>(stream);
-    int rc = upload_args(kin, jobs, *dipole, options->precision, ws + c.args, s);
+    int rc = upload_args(kin, jobs, dipoles, dipole_stride, options->precision, ws + c.args, s);
     if (rc != NLO_OK) return rc;
     static_assert(sizeof(SobolDirsArg) == sizeof(nlo_sobol_dirs), "Sobol direction layouts differ");
     cudaError_t e = cudaMemcpyAsync(ws + c.dirs, dirs, sizeof(nlo_sobol_dirs) * (size_t)jobs, cudaMemcpyHostToDevice, s);
@@ -399,6 +417,20 @@ int nlo_dis_vegas(const nlo_dis_kinematics* kin, int32_t jobs, int32_t term, con
         offset += L.samples;
     }
     return NLO_OK;
+}
+
+int nlo_dis_vegas(const nlo_dis_kinematics* kin, int32_t jobs, int32_t term, const nlo_dipole* dipole,
+                  const nlo_vegas_options* options, const nlo_sobol_dirs* dirs, double* state, void* workspace,
+                  size_t workspace_bytes, void* stream)
+{
+    return vegas_jobs(kin, jobs, term, dipole, 0, options, dirs, state, workspace, workspace_bytes, stream);
+}
+
+int nlo_dis_vegas_dipoles(const nlo_dis_kinematics* kin, int32_t jobs, int32_t term, const nlo_dipole* dipoles,
+                          const nlo_vegas_options* options, const nlo_sobol_dirs* dirs, double* state,
+                          void* workspace, size_t workspace_bytes, void* stream)
+{
+    return vegas_jobs(kin, jobs, term, dipoles, 1, options, dirs, state, workspace, workspace_bytes, stream);
 }
 
 size_t nlo_dis_fixed_sobol_grid_doubles(int32_t bins)

@@ -58,12 +58,13 @@ __device__ __forceinline__ float rcp_approx(float x)
 
 
 struct FastSpline {
-    const float4* coef;  // [n-1] pre-scaled (see above)
-    float u_scale;       // (ln 2 / 2) / h : u from log2(X^2)
-    float u_off;         // -x0 / h
-    float u_max;         // n - 1
-    int last;            // n - 2
-    float last_f;        // n - 2
+    // [n + 1] pre-scaled rows (see above): row 0 is (0, 0, 0, 0), the value below r_min
+    // (log2 S = 0, S = 1); rows 1..n-1 are the intervals; row n is (-150, 0, 0, 0), above
+    // r_max (S = 0)
+    const float4* coef;
+    float u_scale;  // (ln 2 / 2) / h : u from log2(X^2)
+    float u_off;    // -x0 / h
+    float u_top;    // n - 1
 };
 
 struct P2S {
@@ -81,24 +82,21 @@ struct K2ParentF {
 // COUPLING: 0 smooth freeze, 1 smooth freeze capped at alpha_cap, 2 fixed, 3 any coupling
 // of alpha_of_log (flavour thresholds), 4 the parent's coupling (RC_NLO = PARENT_NLO).
 
-// Spline position u = (log X - x0)/h -> (log2 S, S) with the edge encoding, for a pair of
-// positions.  floor(uc) (0 <= uc < 2^23, clamped to `last`) comes without the XU
-// conversions: adding 2^23 rounded down leaves it in the low mantissa bits.  The clamp,
-// floor, fraction and index arithmetic run on the packed instructions, the table lookup
-// and the cubic per component.
+// Spline position u = (log X - x0)/h -> (log2 S, S) for a pair of positions.  u is clamped
+// to [-1, n-1]; the row floor(u) + 1 of the table with its two edge rows serves every case
+// (below the grid, inside, above), so there is no edge select.  floor(u) + 1 comes without
+// the XU conversions: u + (2^23 + 1) rounded down holds it in the low mantissa bits.  The
+// clamp, floor and fraction run on the packed instructions, the table lookup and the cubic
+// per component.
 __device__ __forceinline__ void fast_amplitude_pair(const FastSpline& s, f2 u, P2S& ax, P2S& ay)
 {
-    const f2 uc = make_float2(fminf(fmaxf(u.x, 0.0f), s.u_max), fminf(fmaxf(u.y, 0.0f), s.u_max));
-    const f2 shifted = __fadd2_rd(uc, bc2(8388608.0f));  // 2^23 + floor(uc)
-    const f2 fl = make_float2(fminf(shifted.x - 8388608.0f, s.last_f), fminf(shifted.y - 8388608.0f, s.last_f));
-    const f2 t = sub2(uc, fl);
-    const f2 fi = add2(fl, bc2(8388608.0f));
-    const float4 cx = s.coef[__float_as_int(fi.x) - 0x4B000000];
-    const float4 cy = s.coef[__float_as_int(fi.y) - 0x4B000000];
-    float px = fmaf(t.x, fmaf(t.x, fmaf(t.x, cx.w, cx.z), cx.y), cx.x);
-    float py = fmaf(t.y, fmaf(t.y, fmaf(t.y, cy.w, cy.z), cy.y), cy.x);
-    px = u.x < 0.0f ? 0.0f : (u.x > s.u_max ? -150.0f : px);
-    py = u.y < 0.0f ? 0.0f : (u.y > s.u_max ? -150.0f : py);
+    const f2 uc = make_float2(fminf(fmaxf(u.x, -1.0f), s.u_top), fminf(fmaxf(u.y, -1.0f), s.u_top));
+    const f2 shifted = __fadd2_rd(uc, bc2(8388609.0f));  // 2^23 + 1 + floor(uc)
+    const f2 t = sub2(uc, sub2(shifted, bc2(8388609.0f)));
+    const float4 cx = s.coef[__float_as_int(shifted.x) - 0x4B000000];
+    const float4 cy = s.coef[__float_as_int(shifted.y) - 0x4B000000];
+    const float px = fmaf(t.x, fmaf(t.x, fmaf(t.x, cx.w, cx.z), cx.y), cx.x);
+    const float py = fmaf(t.y, fmaf(t.y, fmaf(t.y, cy.w, cy.z), cy.y), cy.x);
     ax = {px, ex2_approx(px)};
     ay = {py, ex2_approx(py)};
 }
@@ -186,25 +184,23 @@ __device__ __forceinline__ void k2_pair_fast(const FastSpline& s, const Phys<flo
     const f2 C0 = fma2(bc2(-4.0f), r2Lq, fq2);
     const f2 B1 = fma2(r, U1, V1), B2 = fma2(r, U2, V2);
     const f2 w = mul2(r2Lq, bc2(P.two_r));
-    f2 k2 = fma2(mul2(w, B1), rcp2(mul2(Xsq, z2)), C0);
-    f2 k2s = fma2(mul2(w, B2), rcp2(mul2(X2sq, z)), C0);
+    const f2 k2 = fma2(mul2(w, B1), rcp2(mul2(Xsq, z2)), C0);
+    const f2 k2s = fma2(mul2(w, B2), rcp2(mul2(X2sq, z)), C0);
     const f2 kf = mul2(sub2(r2Lq, fq2), bc2(ph.nf_over_nc));
-    f2 dip = mul2(make_float2(vXx.S, vXy.S), D1), dips = mul2(make_float2(vX2x.S, vX2y.S), D2);
+    const f2 dip = mul2(make_float2(vXx.S, vXy.S), D1), dips = mul2(make_float2(vX2x.S, vX2y.S), D2);
+    // the cut |K2| > 1e10 with |dipole| < 1e-10 sets both factors to zero: zero their product
     const bool cut_x = fabsf(k2.x) > 1e10f && fabsf(dip.x) < 1e-10f;
     const bool cut_y = fabsf(k2.y) > 1e10f && fabsf(dip.y) < 1e-10f;
-    const bool cuts_x = fabsf(k2s.x) > 1e10f && fabsf(dips.x) < 1e-10f;
-    const bool cuts_y = fabsf(k2s.y) > 1e10f && fabsf(dips.y) < 1e-10f;
-    k2 = sel2(cut_x, cut_y, bc2(0.0f), k2);
-    dip = sel2(cut_x, cut_y, bc2(0.0f), dip);
-    k2s = sel2(cuts_x, cuts_y, bc2(0.0f), k2s);
-    dips = sel2(cuts_x, cuts_y, bc2(0.0f), dips);
+    const f2 prod = sel2(cut_x, cut_y, bc2(0.0f), mul2(k2, dip));
     const f2 dNX = fast_ndiff2(vXx, vXy, vX2x, vX2y);
     f2 k2part, fermion;
     if (SYM) {  // the factor 1/2 of the symmetrisation is folded into cpt
-        k2part = fma2(k2, dip, mul2(k2s, dips));
+        const bool cuts_x = fabsf(k2s.x) > 1e10f && fabsf(dips.x) < 1e-10f;
+        const bool cuts_y = fabsf(k2s.y) > 1e10f && fabsf(dips.y) < 1e-10f;
+        k2part = add2(prod, sel2(cuts_x, cuts_y, bc2(0.0f), mul2(k2s, dips)));
         fermion = mul2(mul2(kf, dNX), dN);
     } else {
-        k2part = mul2(k2, dip);
+        k2part = prod;
         fermion = mul2(mul2(kf, SY), dNX);
     }
     f2 alpha;
@@ -247,7 +243,7 @@ constexpr int kFoldPairs = 16;
 
 
 template <typename T, bool SYM, int COUPLING>
-__global__ void __launch_bounds__(1024) k2kf_kernel(Phys<T> ph, K2Box<T> box, SobolDirsArg dirs,
+__global__ void __launch_bounds__(448, (sizeof(T) == 4 ? 2 : 1)) k2kf_kernel(Phys<T> ph, K2Box<T> box, SobolDirsArg dirs,
                                                     const double* __restrict__ r_grid, int n,
                                                     const double* __restrict__ spline,
                                                     const int32_t* __restrict__ active,
@@ -257,8 +253,8 @@ __global__ void __launch_bounds__(1024) k2kf_kernel(Phys<T> ph, K2Box<T> box, So
     extern __shared__ __align__(16) unsigned char k2_smem[];
     K2Rec<T>* recs = reinterpret_cast<K2Rec<T>*>(k2_smem);  // [blockDim.x], 16-byte aligned rows
     T* cs = reinterpret_cast<T*>(recs + blockDim.x);          // [n-1][4] natural units, 16-byte aligned
-    float4* cs2 = reinterpret_cast<float4*>(cs + 4 * (n - 1)); // [n-1] pre-scaled (FP32 path)
-    T* xs = reinterpret_cast<T*>(cs2 + (sizeof(T) == sizeof(float) ? n - 1 : 0));
+    float4* cs2 = reinterpret_cast<float4*>(cs + 4 * (n - 1)); // [n+1] pre-scaled with edge rows (FP32 path)
+    T* xs = reinterpret_cast<T*>(cs2 + (sizeof(T) == sizeof(float) ? n + 1 : 0));
     uint32_t* st = reinterpret_cast<uint32_t*>(xs + n);         // [4][30] + shift[4]
     const double* src_coef = spline + n + 4 * (size_t)(n - 1);     // log S block
     const double h64 = (spline[n - 1] - spline[0]) / (double)(n - 1);
@@ -268,8 +264,12 @@ __global__ void __launch_bounds__(1024) k2kf_kernel(Phys<T> ph, K2Box<T> box, So
         const double l2e = 1.4426950408889634;
         for (int i = threadIdx.x; i < n - 1; i += blockDim.x) {
             const double* c = src_coef + 4 * (size_t)i;
-            cs2[i] = make_float4((float)(c[0] * l2e), (float)(c[1] * h64 * l2e), (float)(c[2] * h64 * h64 * l2e),
-                                 (float)(c[3] * h64 * h64 * h64 * l2e));
+            cs2[i + 1] = make_float4((float)(c[0] * l2e), (float)(c[1] * h64 * l2e),
+                                     (float)(c[2] * h64 * h64 * l2e), (float)(c[3] * h64 * h64 * h64 * l2e));
+        }
+        if (threadIdx.x == 0) {
+            cs2[0] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            cs2[n] = make_float4(-150.0f, 0.0f, 0.0f, 0.0f);
         }
     }
     for (int i = threadIdx.x; i < 120; i += blockDim.x) st[i] = dirs.state[i / 30][i % 30];
@@ -288,9 +288,7 @@ __global__ void __launch_bounds__(1024) k2kf_kernel(Phys<T> ph, K2Box<T> box, So
     fs.coef = cs2;
     fs.u_scale = (float)(0.5 * 0.69314718055994531 / h64);
     fs.u_off = (float)(-spline[0] / h64);
-    fs.u_max = (float)(n - 1);
-    fs.last = n - 2;
-    fs.last_f = (float)(n - 2);
+    fs.u_top = (float)(n - 1);
 
     const int n_active = *count;
     const int slot = blockIdx.y * blockDim.x + threadIdx.x;
@@ -421,7 +419,7 @@ cudaError_t launch_typed(const nlo_bk_params& p, const double* r, int points, co
                          int parent_tiles, int* used_blocks, cudaStream_t stream)
 {
     const size_t smem = sizeof(K2Rec<T>) * threads + sizeof(T) * (size_t)(points + 4 * (points - 1)) +
-                        (sizeof(T) == sizeof(float) ? sizeof(float4) * (size_t)(points - 1) : 0) +
+                        (sizeof(T) == sizeof(float) ? sizeof(float4) * (size_t)(points + 1) : 0) +
                         sizeof(uint32_t) * 124;
     cudaError_t e = raise_dynamic_smem((const void*)k2kf_kernel<T, SYM, COUPLING>, smem);
     if (e != cudaSuccess) return e;
@@ -469,7 +467,9 @@ cudaError_t launch_k2kf(const nlo_bk_params& p, const double* r, int points, con
 {
     cudaError_t e = cudaMemsetAsync(out, 0, sizeof(double) * 3 * (size_t)points, stream);
     if (e != cudaSuccess || samples == 0) return e;
-    const int cap = 1024;
+    // at most 448 lanes (parents) per CTA: the FP32 kernel's bounds (448 threads, two CTAs per
+    // SM) give it 72 registers without spills; larger grids take several parent tiles
+    const int cap = 448;
     int threads = ((points < cap ? points : cap) + 31) / 32 * 32;
     if (threads < 64) threads = 64;
     const int parent_tiles = (points + threads - 1) / threads;

@@ -138,6 +138,7 @@ class _Job:
     points: int = 24
     lo_Y: float | None = None            # LO jobs on a BK table: rapidity to initialise at
     fixed: tuple | None = None           # fixed-Sobol qqbar-g job: (polarisation, quark)
+    dipole: Dipole | None = None         # None: the engine's dipole
     done: bool = False
     value: float = 0.0
     error: float = 0.0
@@ -153,12 +154,21 @@ class _Engine:
     jobs: list[_Job] = field(default_factory=list)
 
     def add(self, job: _Job) -> _Job:
+        if job.dipole is None:
+            job.dipole = self.dipole
         self.jobs.append(job)
         return job
 
+    @staticmethod
+    def _natives(group: list[_Job]):
+        """One native dipole for a group on one dipole, else one per job."""
+        first = group[0].dipole
+        if all(j.dipole is first for j in group):
+            return first.native(), None
+        return None, [j.dipole.native() for j in group]
+
     def run(self) -> None:
         precision = _precision(self.config)
-        native = self.dipole.native()
         pending = []
         todo = [j for j in self.jobs if not j.done]
         for job in todo:
@@ -166,7 +176,7 @@ class _Engine:
                 from nlo_bk_optimized_b200.dis.fixed_sobol import FIXED_SOBOL_EVALUATIONS, fixed_sobol_device
 
                 pol, quark = job.fixed
-                _, est = fixed_sobol_device(job.kin.Q2, job.kin.xbj, pol, quark, self.dipole, self.config,
+                _, est = fixed_sobol_device(job.kin.Q2, job.kin.xbj, pol, quark, job.dipole, self.config,
                                             seed=job.seed, device=self.device, precision=precision)
                 pending.append(("fixed", [job], est))
         todo = [j for j in todo if j.fixed is None]
@@ -184,19 +194,22 @@ class _Engine:
         for key in order:
             lo_Y, term, points = key
             group = gl_groups[key]
-            if lo_Y is not None and isinstance(self.dipole, BKDipole):
-                self.dipole.initialize_interpolation(lo_Y)
-                native = self.dipole.native()
+            if lo_Y is not None:
+                tables = {id(j.dipole): j.dipole for j in group if isinstance(j.dipole, BKDipole)}
+                for table in tables.values():
+                    table.initialize_interpolation(lo_Y)
+            native, natives = self._natives(group)
             out = gauss_legendre_terms(term, [j.kin for j in group], native, points, precision=precision,
-                                       device=self.device)
+                                       device=self.device, dipoles=natives)
             pending.append(("gl", group, out))
         vegas_groups: dict[tuple, list[_Job]] = {}
         for job in todo:
             if job.options is not None:
                 vegas_groups.setdefault((job.term, job.options), []).append(job)
         for (term, options), group in vegas_groups.items():
+            native, natives = self._natives(group)
             state = vegas_terms(term, [j.kin for j in group], native, options, [j.seed for j in group],
-                                precision=precision, device=self.device)
+                                precision=precision, device=self.device, dipoles=natives)
             pending.append(("vegas", group, state_results(state, term, options.bins)))
         for kind, group, out in pending:
             for job in group:
@@ -246,6 +259,7 @@ class _SigmaPlan:
     qg: list[list[_Job]]
     seed: int
     qg_fixed: list[_Job] = field(default_factory=list)
+    dipole: Dipole | None = None
     Q2: float = 0.0
     xbj: float = 0.0
     pol: Polarization = Polarization.T
@@ -271,7 +285,7 @@ def _plan_qg_vegas(engine: "_Engine", plan: _SigmaPlan) -> None:
         opts = _vegas_options(config, config.maxeval, plan.overrides)
         jobs = []
         for term in ("I1", "I2N" if nested else "I2", "I3N" if nested else "I3"):
-            jobs.append(engine.add(_Job(TERMS[term], kin, seed=qg_seed + offset, options=opts)))
+            jobs.append(engine.add(_Job(TERMS[term], kin, seed=qg_seed + offset, options=opts, dipole=plan.dipole)))
             offset += 1
         qg.append(jobs)
     plan.qg = qg
@@ -297,17 +311,20 @@ def _vegas_options(config: DISConfig, maxeval: int, overrides: dict) -> VegasOpt
                         inner_points=config.cuda_nested_points)
 
 
-def _plan_lo(engine: _Engine, Q2: float, xbj: float, pol: Polarization, points: int) -> _Job:
+def _plan_lo(engine: _Engine, Q2: float, xbj: float, pol: Polarization, points: int,
+             dipole: Dipole | None = None) -> _Job:
+    dipole = dipole if dipole is not None else engine.dipole
     kin = kinematics(Q2, xbj, pol, engine.config)
-    return engine.add(_Job(TERMS["LO"], kin, points=points, lo_Y=_lo_Y(engine.dipole, xbj)))
+    return engine.add(_Job(TERMS["LO"], kin, points=points, lo_Y=_lo_Y(dipole, xbj), dipole=dipole))
 
 
 def _plan_sigma(engine: _Engine, Q2: float, xbj: float, pol: Polarization, *, seed: int, points: int,
-                overrides: dict, fixed: bool = False) -> _SigmaPlan:
-    config, dipole = engine.config, engine.dipole
+                overrides: dict, fixed: bool = False, dipole: Dipole | None = None) -> _SigmaPlan:
+    config = engine.config
+    dipole = dipole if dipole is not None else engine.dipole
     if config.order is DISOrder.LO:
-        return _SigmaPlan(_plan_lo(engine, Q2, xbj, pol, points), [], [], seed)
-    lo = _plan_lo(engine, Q2, dipole.X0(), pol, points)
+        return _SigmaPlan(_plan_lo(engine, Q2, xbj, pol, points, dipole), [], [], seed, dipole=dipole)
+    lo = _plan_lo(engine, Q2, dipole.X0(), pol, points, dipole)
     if isinstance(dipole, BKDipole):
         Ymax = max(dipole_rapidity(Q2, xbj, q.mass, config.heavy_quark_x_scheme) for q in config.quarks)
         dipole.check_rapidity(max(Ymax, math.log(Q2 / xbj / Q0sqr)))
@@ -315,16 +332,17 @@ def _plan_sigma(engine: _Engine, Q2: float, xbj: float, pol: Polarization, *, se
     for quark in config.quarks:
         kin = kinematics(Q2, xbj, pol, config, quark)
         opts = _vegas_options(config, config.maxeval * (10 if quark.mass < 0.4 else 1), overrides)
-        jobs = [engine.add(_Job(TERMS["DIP0"], kin, points=points))]
+        jobs = [engine.add(_Job(TERMS["DIP0"], kin, points=points, dipole=dipole))]
         for term in ("DIP1", "DIP2"):
-            jobs.append(engine.add(_Job(TERMS[term], kin, seed=seed + offset, options=opts)))
+            jobs.append(engine.add(_Job(TERMS[term], kin, seed=seed + offset, options=opts, dipole=dipole)))
             offset += 1
         dip.append(jobs)
-    plan = _SigmaPlan(lo, dip, [], seed, Q2=Q2, xbj=xbj, pol=pol, overrides=overrides)
+    plan = _SigmaPlan(lo, dip, [], seed, dipole=dipole, Q2=Q2, xbj=xbj, pol=pol, overrides=overrides)
     if fixed and fixed_sobol_supported(dipole, config, True):
         for index, quark in enumerate(config.quarks):
             kin = kinematics(Q2, xbj, pol, config, quark)
-            plan.qg_fixed.append(engine.add(_Job(-1, kin, seed=seed + 100 + index, fixed=(pol, quark))))
+            plan.qg_fixed.append(engine.add(_Job(-1, kin, seed=seed + 100 + index, fixed=(pol, quark),
+                                                 dipole=dipole)))
     else:
         _plan_qg_vegas(engine, plan)
     return plan
@@ -508,6 +526,59 @@ def structure_functions(Q2: torch.Tensor, xbj: torch.Tensor, dipole: Dipole, con
         out["F2_error"][i] = math.hypot(float(rt.error), float(rl.error))
     if sqrt_s is not None:
         y = Q2h / (sqrt_s**2 * xh)
+        f = y * y / (1 + (1 - y) ** 2)
+        out["sigma_r"] = out["FT"] + (1 - f) * out["FL"]
+        out["sigma_r_error"] = torch.sqrt(out["FT_error"] ** 2 + ((1 - f) * out["FL_error"]) ** 2)
+    return {k: v.to(device) for k, v in out.items()}
+
+
+def structure_functions_many(Q2, xbj, dipoles, config: DISConfig, *, sqrt_s: float | None = None, seed: int = 0,
+                             seeds=None, options=None, quadrature_points: int = 24,
+                             fixed_sobol: bool | None = None, **common_options) -> dict[str, torch.Tensor]:
+    """``structure_functions`` for points of different dipoles (``dipoles[i]`` is point i's:
+    e.g. the tables of many parameter sets or requests) in one batched device run: every term
+    of every point goes into the same few launches whatever its dipole.  ``seeds[i]`` and
+    ``options[i]`` (dicts of the integration keywords) override ``seed`` and the common
+    keywords per point; points whose integration settings agree share the launches.  Entry
+    i equals ``structure_functions(Q2[i], xbj[i], dipoles[i], ..., seed=seeds[i],
+    **options[i])`` run alone."""
+    Q2h = [float(v) for v in torch.as_tensor(Q2, dtype=torch.float64).reshape(-1).tolist()]
+    xh = [float(v) for v in torch.as_tensor(xbj, dtype=torch.float64).reshape(-1).tolist()]
+    if not (len(Q2h) == len(xh) == len(dipoles)):
+        raise ValueError("Q2, xbj and dipoles must have one entry per point")
+    if not Q2h:
+        raise ValueError("at least one point is required")
+    if any(q <= 0 for q in Q2h) or any(not 0 < x <= 1 for x in xh):
+        raise ValueError("Q2 must be positive and xbj must lie in (0, 1]")
+    first = dipoles[0]
+    device = first.device if isinstance(first, BKDipole) else _device(Q2 if isinstance(Q2, torch.Tensor) else None)
+    engine = _Engine(first, config, device)
+    n = len(Q2h)
+    seeds = [seed] * n if seeds is None else [int(v) for v in seeds]
+    per_point = [common_options] * n if options is None else [dict(common_options, **o) for o in options]
+    if len(seeds) != n or len(per_point) != n:
+        raise ValueError("seeds and options need one entry per point")
+    fixed = (config.precision == "mixed") if fixed_sobol is None else fixed_sobol
+    plans = []
+    for q2, x, d, sd, opts in zip(Q2h, xh, dipoles, seeds, per_point):
+        overrides = _integration_overrides(opts)
+        plans.append((_plan_sigma(engine, q2, x, Polarization.T, seed=sd, points=quadrature_points,
+                                  overrides=overrides, fixed=fixed, dipole=d),
+                      _plan_sigma(engine, q2, x, Polarization.L, seed=sd + 1000, points=quadrature_points,
+                                  overrides=overrides, fixed=fixed, dipole=d)))
+    _run_with_fallback(engine, [p for pair in plans for p in pair])
+    out = {k: torch.empty(n, dtype=torch.float64) for k in ("FT", "FL", "F2", "FT_error", "FL_error", "F2_error")}
+    for i, (pt, pl) in enumerate(plans):
+        factor = _sf_factor(Q2h[i], config)
+        rt = _scale_result(_sigma_result(pt, config, torch.device("cpu")), factor)
+        rl = _scale_result(_sigma_result(pl, config, torch.device("cpu")), factor)
+        out["FT"][i], out["FL"][i] = rt.value, rl.value
+        out["FT_error"][i], out["FL_error"][i] = rt.error, rl.error
+        out["F2"][i] = rt.value + rl.value
+        out["F2_error"][i] = math.hypot(float(rt.error), float(rl.error))
+    if sqrt_s is not None:
+        q2t, xt = torch.tensor(Q2h, dtype=torch.float64), torch.tensor(xh, dtype=torch.float64)
+        y = q2t / (sqrt_s**2 * xt)
         f = y * y / (1 + (1 - y) ** 2)
         out["sigma_r"] = out["FT"] + (1 - f) * out["FL"]
         out["sigma_r_error"] = torch.sqrt(out["FT_error"] ** 2 + ((1 - f) * out["FL_error"]) ** 2)

@@ -225,11 +225,19 @@ def kinematics_array(kins: list[_native.DisKinematics]) -> ctypes.Array:
     return arr
 
 
-def vegas_terms(term: int, kins: list[_native.DisKinematics], dipole: _native.Dipole, options: VegasOptions,
+def _dipole_array(dipoles: list[_native.Dipole]) -> ctypes.Array:
+    arr = (_native.Dipole * len(dipoles))()
+    for i, d in enumerate(dipoles):
+        arr[i] = d
+    return arr
+
+
+def vegas_terms(term: int, kins: list[_native.DisKinematics], dipole: _native.Dipole | None, options: VegasOptions,
                 seeds: list[int], *, precision: int, device: torch.device,
-                edges: torch.Tensor | None = None) -> torch.Tensor:
+                edges: torch.Tensor | None = None, dipoles: list[_native.Dipole] | None = None) -> torch.Tensor:
     """Run Vegas for len(kins) integrals of one term; returns the device state
-    [jobs, state_doubles] (edges followed by value, error, n_eval, iterations, converged)."""
+    [jobs, state_doubles] (edges followed by value, error, n_eval, iterations, converged).
+    ``dipoles`` (one per job) replaces the common ``dipole``."""
     lib = _native.load()
     jobs = len(kins)
     dims = _native.DIS_DIMS[term]
@@ -245,9 +253,16 @@ def vegas_terms(term: int, kins: list[_native.DisKinematics], dipole: _native.Di
     karr = kinematics_array(kins)
     darr = sobol_dirs_array(max(dims, 1), seeds)
     with torch.cuda.device(device):
-        _native.check(lib.nlo_dis_vegas(karr, jobs, term, ctypes.byref(dipole), ctypes.byref(opts), darr,
-                                        state.data_ptr(), workspace.data_ptr(), ws_bytes,
-                                        _native.stream_handle(device)))
+        if dipoles is not None:
+            if len(dipoles) != jobs:
+                raise ValueError("one dipole per job is required")
+            _native.check(lib.nlo_dis_vegas_dipoles(karr, jobs, term, _dipole_array(dipoles), ctypes.byref(opts),
+                                                    darr, state.data_ptr(), workspace.data_ptr(), ws_bytes,
+                                                    _native.stream_handle(device)))
+        else:
+            _native.check(lib.nlo_dis_vegas(karr, jobs, term, ctypes.byref(dipole), ctypes.byref(opts), darr,
+                                            state.data_ptr(), workspace.data_ptr(), ws_bytes,
+                                            _native.stream_handle(device)))
     return state
 
 
@@ -265,9 +280,11 @@ def state_results(state: torch.Tensor, term: int, bins: int) -> dict[str, torch.
     }
 
 
-def gauss_legendre_terms(term: int, kins: list[_native.DisKinematics], dipole: _native.Dipole, points: int, *,
-                         precision: int, device: torch.device) -> torch.Tensor:
-    """Tensor Gauss-Legendre of a 2D term for len(kins) points: [jobs, 2] = (value, error)."""
+def gauss_legendre_terms(term: int, kins: list[_native.DisKinematics], dipole: _native.Dipole | None, points: int,
+                         *, precision: int, device: torch.device,
+                         dipoles: list[_native.Dipole] | None = None) -> torch.Tensor:
+    """Tensor Gauss-Legendre of a 2D term for len(kins) points: [jobs, 2] = (value, error).
+    ``dipoles`` (one per job) replaces the common ``dipole``."""
     lib = _native.load()
     jobs = len(kins)
     out = torch.empty((jobs, 2), dtype=torch.float64, device=device)
@@ -275,9 +292,16 @@ def gauss_legendre_terms(term: int, kins: list[_native.DisKinematics], dipole: _
     workspace = torch.empty(ws_bytes, dtype=torch.uint8, device=device)
     karr = kinematics_array(kins)
     with torch.cuda.device(device):
-        _native.check(lib.nlo_dis_gauss_legendre(karr, jobs, term, ctypes.byref(dipole), points, precision,
-                                                 out.data_ptr(), workspace.data_ptr(), ws_bytes,
-                                                 _native.stream_handle(device)))
+        if dipoles is not None:
+            if len(dipoles) != jobs:
+                raise ValueError("one dipole per job is required")
+            _native.check(lib.nlo_dis_gauss_legendre_dipoles(karr, jobs, term, _dipole_array(dipoles), points,
+                                                             precision, out.data_ptr(), workspace.data_ptr(),
+                                                             ws_bytes, _native.stream_handle(device)))
+        else:
+            _native.check(lib.nlo_dis_gauss_legendre(karr, jobs, term, ctypes.byref(dipole), points, precision,
+                                                     out.data_ptr(), workspace.data_ptr(), ws_bytes,
+                                                     _native.stream_handle(device)))
     return out
 
 

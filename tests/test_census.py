@@ -36,3 +36,10 @@ def test_bench_census_constants_are_the_workload_census():
     assert bench.CENSUS_EVAL_TRANSCENDENTALS == c["eval_special"]
     assert bench.CENSUS_SAMPLE_FLOPS == c["sample_arithmetic"]
     assert bench.CENSUS_SAMPLE_TRANSCENDENTALS == c["sample_special"]
+
+
+def test_bench_dis_census_constants_are_the_workload_census():
+    from oracle import census_dis
+
+    c = census_dis.workload_census()
+    assert bench.DIS_CENSUS == {"I2N": c["I2n"], "I3N": c["I3n"]}

@@ -50,23 +50,75 @@ def _requests():
 
 
 def test_served_results_equal_results_alone():
+    """Every served request's table equals its evolution alone bit for bit, and its structure
+    functions equal the plain single-solve path's to 1e-6: the merged DIS launches split
+    the samples of each integral over other CTAs, so the FP64 partial sums are added in
+    another order, and the adaptive grids carry that (~1e-15) to ~1e-9."""
     from nlo_bk_optimized_b200 import BKConfig
     from nlo_bk_optimized_b200.dis import DISConfig, DISOrder, Quark, QuarkType
     from nlo_bk_optimized_b200.serving import Server, run_alone
 
     bk = BKConfig(MCINTPOINTS=1 << 10, **BK)
     dis = DISConfig(order=DISOrder.NLO, quarks=(Quark(QuarkType.LIGHT, 0.14),))
-    server = Server(bk, dis, slots=3)
-    futures = [server.submit(req) for req in _requests()]
+    server = Server(bk, dis, slots=8, lanes=4)
+    requests = _requests()
+    futures = [server.submit(req) for req in requests[:3]]
     responses = [f.result(timeout=600) for f in futures]
+    responses.append(server.submit(requests[3]).result(timeout=600))  # after the first: its table is resident
     server.close()
     stats = server.stats.summary()
     assert stats["requests"] == 4 and stats["points"] == 8
     assert stats["p50_s"] is not None and stats["p99_s"] >= stats["p50_s"]
-    assert any(r.cached_table for r in responses[1:])
-    for req, resp in zip(_requests()[:2], responses[:2]):
+    assert responses[3].cached_table
+    assert sum(server.batches) == 4
+    for req, resp in zip(requests, responses):
         alone = run_alone(req, bk, dis)
         assert torch.equal(alone.table.N, resp.table.N)
         for key in ("F2", "FL", "FT", "sigma_r"):
             a, b = getattr(alone, key).cpu(), getattr(resp, key).cpu()
-            assert torch.allclose(a, b, rtol=1e-12, atol=0)
+            assert torch.allclose(a, b, rtol=1e-6, atol=0), key
+
+
+def test_merged_dis_batch_over_different_tables_equals_each_alone():
+    """structure_functions_many: the points of two tables (each its own seed) in one batch
+    equal each table's points run alone."""
+    from nlo_bk_optimized_b200 import MV, BKConfig, solve_bk
+    from nlo_bk_optimized_b200.dipole import BKDipole
+    from nlo_bk_optimized_b200.dis import DISConfig, DISOrder, Quark, QuarkType, structure_functions
+    from nlo_bk_optimized_b200.dis import structure_functions_many
+
+    bk = BKConfig(MCINTPOINTS=1 << 10, **BK)
+    dis = DISConfig(order=DISOrder.NLO, quarks=(Quark(QuarkType.LIGHT, 0.14),))
+    tables = [BKDipole(solve_bk(MV(qs0sqr=q), 8.0, bk, device="cuda", dtype=torch.float64, seed=0))
+              for q in (0.15, 0.4)]
+    pts = [[(5.0, 1e-2), (12.0, 3e-2)], [(2.0, 5e-2), (8.0, 2e-2), (20.0, 4e-2)]]
+    opts = {"vegas_samples": 4096, "vegas_iterations": 4, "vegas_min_iterations": 4}
+    Q2 = [q for group in pts for q, _ in group]
+    xs = [x for group in pts for _, x in group]
+    dipoles = [tables[k] for k, group in enumerate(pts) for _ in group]
+    seeds = [7 + k for k, group in enumerate(pts) for _ in group]
+    merged = structure_functions_many(Q2, xs, dipoles, dis, sqrt_s=318.0, seeds=seeds, **opts)
+    offset = 0
+    for k, group in enumerate(pts):
+        alone = structure_functions(torch.tensor([q for q, _ in group], dtype=torch.float64),
+                                    torch.tensor([x for _, x in group], dtype=torch.float64), tables[k], dis,
+                                    sqrt_s=318.0, seed=7 + k, **opts)
+        for key in ("F2", "FL", "sigma_r"):
+            got = merged[key][offset:offset + len(group)].cpu()
+            assert torch.allclose(got, alone[key].cpu(), rtol=1e-6, atol=0), key
+        offset += len(group)
+
+
+def test_admission_never_bypasses_the_memory_check():
+    from nlo_bk_optimized_b200 import BKConfig
+    from nlo_bk_optimized_b200.dis import DISConfig, DISOrder, Quark, QuarkType
+    from nlo_bk_optimized_b200.serving import Server
+
+    total = torch.cuda.get_device_properties(0).total_memory
+    bk = BKConfig(MCINTPOINTS=1 << 10, **BK)
+    dis = DISConfig(order=DISOrder.NLO, quarks=(Quark(QuarkType.LIGHT, 0.14),))
+    server = Server(bk, dis, slots=2, reserve_bytes=total)  # nothing can ever fit
+    future = server.submit(_requests()[0])
+    with pytest.raises(MemoryError):
+        future.result(timeout=60)
+    server.close()

@@ -26,7 +26,7 @@ def _line(*args: str) -> dict:
 
 
 def test_bench_line_contract():
-    d = _line("--steps", "2", "--warmup", "3", "--e2e-steps", "1", "--no-cpu-baseline", "--no-dis")
+    d = _line("--steps", "2", "--warmup", "3", "--e2e-steps", "1", "--no-cpu-baseline", "--no-dis", "--no-batch")
     for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
                 "vs_baseline", "dtype", "data", "config", "e2e", "gpu_launches", "roofline", "clocks",
                 "max_rel_err_vs_fp64", "accuracy"):
@@ -64,3 +64,14 @@ def test_fixed_sobol_workload_line():
     for name, (ref, ref_err) in cpp.items():
         value, err = d["terms"][name]
         assert abs(value - ref) <= 5 * (err * err + ref_err * ref_err) ** 0.5, name
+
+
+def test_batch_and_serve_lines():
+    d = _line("--workload", "batch", "--batch-sets", "6")
+    assert d["config"]["sets"] == 6 and d["config"]["points"] == 48
+    assert d["value"] > 0 and d["batched_s"] > 0
+    assert d["speedup_vs_plain_single_point"] > 0 and d["speedup_vs_plain_per_set"] > 0
+    assert d["single_vs_batched_max_rel"] <= 1e-6
+    s = _line("--workload", "serve", "--serve-seconds", "0.05", "--serve-rate", "100")
+    assert s["value"] > 0 and s["p99_s"] >= s["p50_s"] > 0
+    assert s["dis_batches"] >= 1 and s["speedup_vs_sequential"] > 0

@@ -69,7 +69,7 @@ MUFU_PER_SM_PER_CLOCK = 16
 # ncu capture of the kernel case (bench.py --kernel-case: 400 parents x 2^18 points): the
 # spline is staged into shared memory once per CTA and each CTA writes 3 doubles per
 # parent, so the bytes do not grow with the number of samples.
-K2KF_DRAM_BYTES_PER_LAUNCH = 52992
+K2KF_DRAM_BYTES_PER_LAUNCH = 52480
 # Launches of our kernels per RK4 step: 4 right-hand sides x (spline refit, active
 # list, K1, K2+Kf, K2+Kf finalize, assemble) + 4 stage combinations.
 LAUNCHES_PER_RK4_STEP = 4 * 6 + 4
@@ -361,7 +361,7 @@ def run_ours(args) -> None:
         line["fixed_sobol"] = measure_fixed()
     if not args.no_batch and world == 1:
         line["batch"] = measure_batch(args.line_batch_sets)
-        line["serve"] = measure_serve(args.line_serve_seconds, args.serve_rate, args.serve_slots, args.serve_lanes)
+        line["serve"] = measure_serve(args.line_serve_seconds, args.serve_rate, args.serve_slots, args.serve_waves)
     print(json.dumps(line))
 
 
@@ -882,14 +882,15 @@ def measure_batch(n_sets: int) -> dict:
     e_c ~ logU[1, 100], budgets 2^U{16..20} Sobol points per r per stage) evolved on 200 r in
     [1e-6, 1e2] (RK4 h = 0.2 to Y = 4, alpha_s capped at 0.7), then each set's 8 (Q^2, x_Bj)
     points (NLO F_T, F_L, F_2, sigma_r at sqrt(s) = 318 GeV, light quarks, Vegas of 4
-    iterations x budget/16 samples) -- all evolutions concurrently on CUDA streams and all
-    points of all sets in one merged DIS run -- against the plain single-solve path
+    iterations x budget/16 samples) -- all evolutions in one multi-set evolution (one launch per
+    kernel and stage for every set) and all points of all sets in one merged DIS run -- against
+    the plain single-solve path
     (solve_bk of one set, then sigma_r of one point at a time), timed on one set of each
     budget class and summed over the classes' set counts."""
     import torch
 
     from nlo_bk_optimized_b200 import MV, solve_bk
-    from nlo_bk_optimized_b200.bk.batch import evolve_batch, tune_streams
+    from nlo_bk_optimized_b200.bk.batch import evolve_batch, tune_waves
     from nlo_bk_optimized_b200.bk.evolution import _r_grid, _steps_to
     from nlo_bk_optimized_b200.dipole import BKDipole, DipoleTable
     from nlo_bk_optimized_b200.dis import DISConfig, DISOrder, Quark, QuarkType, sigma_r, structure_functions
@@ -910,7 +911,7 @@ def measure_batch(n_sets: int) -> dict:
     points = [_set_points(k) for k in range(n_sets)]
 
     def batched():
-        tables = evolve_batch(N0, r, len(ys), config, budgets, streams=streams)
+        tables = evolve_batch(N0, r, len(ys), config, budgets, waves=waves)
         dipoles = [BKDipole(DipoleTable(r=r, y=y, N=tables[k], x0=0.01)) for k in range(n_sets)]
         Q2 = [q for pts in points for q, _ in pts]
         xs = [x for pts in points for _, x in pts]
@@ -920,9 +921,9 @@ def measure_batch(n_sets: int) -> dict:
         out = structure_functions_many(Q2, xs, dips, dis, sqrt_s=DIS_SQRT_S, seeds=seeds, options=opts)
         return out["sigma_r"].cpu()
 
-    streams = tune_streams(N0, r, config, budgets)
+    waves = tune_waves(N0, r, config, budgets)
     # warm-up of every kernel on the path: a short evolution of two sets and two of their points
-    warm = evolve_batch(N0[:2], r, len(ys), config, [1 << 10] * 2, streams=2)
+    warm = evolve_batch(N0[:2], r, len(ys), config, [1 << 10] * 2, waves=waves)
     warm_dipoles = [BKDipole(DipoleTable(r=r, y=y, N=warm[k], x0=0.01)) for k in range(2)]
     structure_functions_many([points[0][0][0], points[1][0][0]], [points[0][0][1], points[1][0][1]], warm_dipoles,
                              dis, sqrt_s=DIS_SQRT_S, seeds=[0, 1], options=[dis_options_for(1 << 16)] * 2)
@@ -939,6 +940,15 @@ def measure_batch(n_sets: int) -> dict:
     per_class_point, per_class_set = {}, {}
     ic_of = lambda k: MV(qs0sqr=sets[k][0], gamma=sets[k][1], ec=sets[k][2])  # noqa: E731
     single_vs_batched = 0.0
+    # the plain path's own warm-up (its first solve_bk and sigma_r load what they need)
+    warm_table = BKDipole(solve_bk(ic_of(0), BATCH_MAXY, _small_bk_config(1 << 10), device=device,
+                                   dtype=torch.float64, seed=0))
+    sigma_r(torch.tensor(points[0][0][0], dtype=torch.float64, device=device),
+            torch.tensor(points[0][0][1], dtype=torch.float64, device=device), warm_table, dis, sqrt_s=DIS_SQRT_S,
+            seed=0, **dis_options_for(1 << 16))
+    structure_functions(torch.tensor([points[0][0][0]], dtype=torch.float64),
+                        torch.tensor([points[0][0][1]], dtype=torch.float64), warm_table, dis, sqrt_s=DIS_SQRT_S,
+                        seed=0, **dis_options_for(1 << 16))["sigma_r"].cpu()
     for b, members in sorted(classes.items()):
         k = members[0]
         cfg = _small_bk_config(b)
@@ -977,7 +987,7 @@ def measure_batch(n_sets: int) -> dict:
         "data": "synthetic: MV parameter sets from torch.Generator().manual_seed(0), seeded DIS points",
         "config": {"workload": f"{n_sets} MV sets, 200 r in [1e-6,1e2], RK4 h=0.2 to Y={BATCH_MAXY}, alpha_s cap 0.7, "
                                "budgets 2^U{16..20} per r per stage; 8 (Q^2,x) points per set, NLO sigma_r, "
-                               "Vegas 4 it x budget/16", "sets": n_sets, "points": n_points, "streams": streams},
+                               "Vegas 4 it x budget/16", "sets": n_sets, "points": n_points, "waves": waves},
         "batched_s": round(batched_s, 3),
         "dis_points_per_s": round(n_points / batched_s, 2),
         "plain_single_point_s": round(plain_points, 2),
@@ -1014,7 +1024,7 @@ def _requests_for(seconds: float, rate: float, seed: int = 0):
     return requests
 
 
-def measure_serve(seconds: float, rate: float, slots: int, lanes: int, sample: int = 8) -> dict:
+def measure_serve(seconds: float, rate: float, slots: int, waves: int, sample: int = 8) -> dict:
     """Poisson arrivals at `rate`/s for `seconds`: each request is one parameter set (drawn as
     in the batched workload), 1-64 points of the 32 x 16 DIS grid restricted to x >= 1e-3 and
     an MC budget log-uniform in [2^16, 2^20].  p50/p99 latency and points/s of the server
@@ -1031,7 +1041,7 @@ def measure_serve(seconds: float, rate: float, slots: int, lanes: int, sample: i
     bk = _small_bk_config()
     dis = DISConfig(order=DISOrder.NLO, quarks=(Quark(QuarkType.LIGHT, 0.14),))
     run_alone(requests[0][1], bk, dis)  # warm-up
-    server = Server(bk, dis, slots=slots, lanes=lanes)
+    server = Server(bk, dis, slots=slots, waves=waves)
     t0 = time.perf_counter()
     futures = []
     for at, req in requests:
@@ -1059,7 +1069,7 @@ def measure_serve(seconds: float, rate: float, slots: int, lanes: int, sample: i
         "dtype": "f32+f64",
         "data": "synthetic Poisson arrivals, seeded",
         "config": {"workload": f"Poisson {rate}/s for {seconds} s, 1-64 points per request, budgets logU[2^16, 2^20]",
-                   "slots": slots, "lanes": lanes, "requests": len(requests)},
+                   "slots": slots, "waves": waves, "requests": len(requests)},
         "p50_s": served["p50_s"],
         "p99_s": served["p99_s"],
         "requests_per_s": served["requests_per_s"],
@@ -1073,7 +1083,7 @@ def measure_serve(seconds: float, rate: float, slots: int, lanes: int, sample: i
 
 
 def run_serve(args) -> None:
-    print(json.dumps(measure_serve(args.serve_seconds, args.serve_rate, args.serve_slots, args.serve_lanes)))
+    print(json.dumps(measure_serve(args.serve_seconds, args.serve_rate, args.serve_slots, args.serve_waves)))
 
 
 def main() -> None:
@@ -1095,7 +1105,7 @@ def main() -> None:
     parser.add_argument("--serve-rate", type=float, default=200.0)
     parser.add_argument("--serve-seconds", type=float, default=1.0)
     parser.add_argument("--serve-slots", type=int, default=64)
-    parser.add_argument("--serve-lanes", type=int, default=8)
+    parser.add_argument("--serve-waves", type=int, default=4)
     parser.add_argument("--no-batch", action="store_true", help="skip the batched and served objects of the line")
     parser.add_argument("--line-batch-sets", type=int, default=32, help="parameter sets of the line's batch object")
     parser.add_argument("--line-serve-seconds", type=float, default=0.5, help="arrival window of the line's serve object")

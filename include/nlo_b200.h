@@ -241,6 +241,27 @@ int nlo_bk_evolve_history(const nlo_bk_params* params, const double* r, int32_t 
                           int64_t samples, const nlo_bk_box* box, double* table, uint32_t* status, void* workspace,
                           size_t workspace_bytes, void* stream);
 
+/* ------------------------------------------------------- many parameter sets at once
+ * nlo_bk_evolve for `sets` initial rows (1..256) on one r grid with one parameter block and
+ * per-set budgets and Sobol seeds: every stage runs one launch per kernel for all sets, and
+ * one K2+Kf launch takes lanes over (set, parent) pairs -- each CTA stages one tile of sample
+ * records per set it holds and its lanes sweep their own set's tile (sets of equal budget
+ * share CTAs, so the launch has no idle tail per set).  Set i's result equals nlo_bk_evolve's
+ * for that row, budget and seed up to the order of the FP64 sums of the CTA partials (no
+ * counterpart in the reference, which evolves one condition per call; the batched solve of
+ * many initial conditions with uneven budgets, and the request loop's step-level batching).
+ * tables: host array of `sets` device pointers, each a double[(steps+1)*points] table whose
+ * row 0 holds the set's initial row.  dirs: host array of `sets` Sobol direction sets (at
+ * least 4 dimensions each).  samples: host int64[sets], each 0..2^30.  waves (1..64): K2+Kf
+ * CTAs per launch ~ waves x 2 x SM count, spread over the sets' groups.  status: device
+ * uint32[sets], reset and then flagged per set as in nlo_bk_evolve.  The kinematical
+ * constraint is not accepted. */
+size_t nlo_bk_sets_workspace_bytes(int32_t points, int32_t sets, int32_t waves);
+int nlo_bk_evolve_sets(const nlo_bk_params* params, const double* r, int32_t points, int32_t sets,
+                       double* const* tables, int32_t steps, double step, int32_t stepper,
+                       const nlo_sobol_dirs* dirs, const int64_t* samples, const nlo_bk_box* box, int32_t waves,
+                       uint32_t* status, void* workspace, size_t workspace_bytes, void* stream);
+
 /* ------------------------------------------------------------------ K2+Kf by Vegas
  * The reference's default integrator of the NLO part (BKConfig.INTMETHOD_NLO = VEGAS;
  * rapidity_derivative_nlo, bk/derivatives.py:389-421, driving vegas(),

@@ -159,6 +159,8 @@ EXPORTED = (
     "nlo_bk_rhs",
     "nlo_bk_evolve",
     "nlo_bk_evolve_history",
+    "nlo_bk_sets_workspace_bytes",
+    "nlo_bk_evolve_sets",
     "nlo_bk_rhs_history",
     "nlo_ic_spline_doubles",
     "nlo_ic_spline",
@@ -229,6 +231,11 @@ def _declare(lib: ctypes.CDLL) -> None:
     lib.nlo_bk_evolve_history.restype = ctypes.c_int
     lib.nlo_bk_evolve_history.argtypes = [P(BKParams), vp, i32, vp, i32, i32, d, i32, P(SobolDirs), i64, P(Box), vp,
                                           vp, vp, sz, vp]
+    lib.nlo_bk_sets_workspace_bytes.restype = sz
+    lib.nlo_bk_sets_workspace_bytes.argtypes = [i32, i32, i32]
+    lib.nlo_bk_evolve_sets.restype = ctypes.c_int
+    lib.nlo_bk_evolve_sets.argtypes = [P(BKParams), vp, i32, i32, P(vp), i32, d, i32, P(SobolDirs), P(i64), P(Box),
+                                       i32, vp, vp, sz, vp]
     lib.nlo_ic_spline_doubles.restype = sz
     lib.nlo_ic_spline_doubles.argtypes = [i32]
     lib.nlo_ic_spline.restype = ctypes.c_int

@@ -6,11 +6,14 @@
 
 #include <cmath>
 #include <cstdio>
+#include <algorithm>
+#include <cstddef>
 #include <cstring>
 #include <map>
 #include <mutex>
 #include <string>
 #include <utility>
+#include <vector>
 
 #include "common.cuh"
 #include "internal.h"
@@ -144,19 +147,22 @@ int run_rhs(const nlo_bk_params& p, const double* r, const double* N, int points
         history.rows = rows;
         history.on = true;
     }
-    if ((e = launch_splines(r, N, points, p.force_positive, b.factor, factor_ready ? 0 : 1, b.spline, stream)) !=
+    if ((e = launch_splines(r, single_row(N), points, 1, p.force_positive, b.factor, factor_ready ? 0 : 1, b.spline,
+                            stream)) !=
         cudaSuccess)
         return cuda_fail(e, "splines");
     // Sobol QMC: K2+Kf takes every active parent (a shard owns a range of Sobol indices), K1
     // the active parents i with i % shards == shard.  Vegas: both take the shard's parents.
     const bool split_samples = vegas == nullptr;
-    if ((e = launch_active(N, points, split_samples ? 0 : shard, split_samples ? 1 : shards, b.active, b.count,
+    if ((e = launch_active(single_row(N), points, 1, split_samples ? 0 : shard, split_samples ? 1 : shards, b.active,
+                           b.count,
                            stream)) != cudaSuccess)
         return cuda_fail(e, "active");
     const int32_t* k1_active = b.active;
     const int32_t* k1_count = b.count;
     if (shards > 1 && split_samples) {
-        if ((e = launch_active(N, points, shard, shards, b.k1_active, b.k1_count, stream)) != cudaSuccess)
+        if ((e = launch_active(single_row(N), points, 1, shard, shards, b.k1_active, b.k1_count, stream)) !=
+            cudaSuccess)
             return cuda_fail(e, "active");
         k1_active = b.k1_active;
         k1_count = b.k1_count;
@@ -203,6 +209,48 @@ int run_rhs(const nlo_bk_params& p, const double* r, const double* N, int points
             return cuda_fail(e, "k1 copy");
     }
     return NLO_OK;
+}
+
+// The stage sequence of one rapidity step (_bk_steps with its Euler, Kutta RK3 and RK4 steppers,
+// bk/evolution.py:85-236): rhs(src, k) evaluates the right-hand side of the stage input src
+// (-1: the step's row, 0: the stage row) into derivative k; comb(nk, ks, coef, dst) forms
+// row + sum_j coef[j] k[ks[j]] into the stage row (dst 0) or the next row (dst 1).
+template <class Rhs, class Comb>
+int step_sequence(int stepper, double step, Rhs rhs, Comb comb)
+{
+    int rc;
+    if (stepper == NLO_STEPPER_EULER) {
+        if ((rc = rhs(-1, 0)) != NLO_OK) return rc;
+        const int k0[1] = {0};
+        const double c[1] = {step};
+        return comb(1, k0, c, 1);
+    }
+    if (stepper == NLO_STEPPER_RK3) {
+        // Kutta RK3 (bk/evolution.py:204-236)
+        if ((rc = rhs(-1, 0)) != NLO_OK) return rc;
+        const int k0[1] = {0}, k01[2] = {0, 1}, k012[3] = {0, 1, 2};
+        const double c1[1] = {0.5 * step};
+        if ((rc = comb(1, k0, c1, 0)) != NLO_OK) return rc;
+        if ((rc = rhs(0, 1)) != NLO_OK) return rc;
+        const double c2[2] = {-step, 2.0 * step};
+        if ((rc = comb(2, k01, c2, 0)) != NLO_OK) return rc;
+        if ((rc = rhs(0, 2)) != NLO_OK) return rc;
+        const double c3[3] = {step / 6.0, 4.0 * step / 6.0, step / 6.0};
+        return comb(3, k012, c3, 1);
+    }
+    // classical RK4
+    if ((rc = rhs(-1, 0)) != NLO_OK) return rc;
+    const int k0[1] = {0}, k1[1] = {1}, k2[1] = {2}, k0123[4] = {0, 1, 2, 3};
+    const double c1[1] = {0.5 * step};
+    if ((rc = comb(1, k0, c1, 0)) != NLO_OK) return rc;
+    if ((rc = rhs(0, 1)) != NLO_OK) return rc;
+    if ((rc = comb(1, k1, c1, 0)) != NLO_OK) return rc;
+    if ((rc = rhs(0, 2)) != NLO_OK) return rc;
+    const double c3[1] = {step};
+    if ((rc = comb(1, k2, c3, 0)) != NLO_OK) return rc;
+    if ((rc = rhs(0, 3)) != NLO_OK) return rc;
+    const double c4[4] = {step / 6.0, 2.0 * step / 6.0, 2.0 * step / 6.0, step / 6.0};
+    return comb(4, k0123, c4, 1);
 }
 
 }  // namespace
@@ -277,8 +325,6 @@ cudaError_t raise_dynamic_smem(const void* func, size_t bytes)
     return e;
 }
 
-size_t spline_doubles(int points) { return (size_t)points + 8 * (size_t)(points - 1); }
-
 // buffer size a caller provides to nlo_bk_splines: coefficients plus factorisation scratch
 size_t spline_buffer_doubles(int points) { return spline_doubles(points) + 2 * (size_t)points; }
 
@@ -322,7 +368,7 @@ int nlo_bk_splines(const double* r, const double* N, int32_t points, int32_t for
     if (!r || !N || !spline) return fail(NLO_ERR_INVALID, "NULL buffer");
     // the factorisation scratch is the tail of the caller's spline buffer (nlo_bk_spline_doubles)
     double* factor = spline + spline_doubles(points);
-    cudaError_t e = launch_splines(r, N, points, force_positive, factor, 1, spline, (cudaStream_t)stream);
+    cudaError_t e = launch_splines(r, single_row(N), points, 1, force_positive, factor, 1, spline, (cudaStream_t)stream);
     return e == cudaSuccess ? NLO_OK : cuda_fail(e, "splines");
 }
 
@@ -330,7 +376,7 @@ int nlo_bk_active(const double* N, int32_t points, int32_t* active, int32_t* cou
 {
     if (points < 1) return fail(NLO_ERR_INVALID, "points must be positive");
     if (!N || !active || !count) return fail(NLO_ERR_INVALID, "NULL buffer");
-    cudaError_t e = launch_active(N, points, 0, 1, active, count, (cudaStream_t)stream);
+    cudaError_t e = launch_active(single_row(N), points, 1, 0, 1, active, count, (cudaStream_t)stream);
     return e == cudaSuccess ? NLO_OK : cuda_fail(e, "active");
 }
 
@@ -490,54 +536,48 @@ static int evolve_rows(const nlo_bk_params* params, const double* r, int32_t poi
     if (e != cudaSuccess) return cuda_fail(e, "status reset");
     const int clamp = params->force_positive ? 1 : 0;
     const SideStream side;
+    // the spline factorisation depends on the grid only: form it on the first stage
+    bool factor_ready = false;
     for (int it = first; it < first + steps; ++it) {
         const double* N = table + (size_t)it * points;
         double* next = table + (size_t)(it + 1) * points;
-        int rc;
-        // the spline factorisation depends on the grid only: form it on the first stage
-        bool factor_ready = it > first;
-        auto f = [&](const double* in, double* out) {
-            const int code = run_rhs(*params, r, in, points, dirs_arg, (uint64_t)samples, *box, out, nullptr,
-                                     nullptr, b, factor_ready, s, 0, 1, y, table, it + 1, &side, vegas);
+        auto rhs = [&](int src, int k) {
+            const int code = run_rhs(*params, r, src < 0 ? N : tmp, points, dirs_arg, (uint64_t)samples, *box, kk[k],
+                                     nullptr, nullptr, b, factor_ready, s, 0, 1, y, table, it + 1, &side, vegas);
             factor_ready = true;
             return code;
         };
-        if (stepper == NLO_STEPPER_EULER) {
-            if ((rc = f(N, kk[0])) != NLO_OK) return rc;
-            const double c[1] = {step};
-            if ((e = launch_axpy_stage(N, kk, c, 1, points, next, clamp, status, s)) != cudaSuccess)
-                return cuda_fail(e, "stage");
-        } else if (stepper == NLO_STEPPER_RK3) {
-            // Kutta RK3 (bk/evolution.py:204-236)
-            if ((rc = f(N, kk[0])) != NLO_OK) return rc;
-            const double c1[1] = {0.5 * step};
-            if ((e = launch_axpy_stage(N, kk, c1, 1, points, tmp, 0, nullptr, s)) != cudaSuccess) return cuda_fail(e, "stage");
-            if ((rc = f(tmp, kk[1])) != NLO_OK) return rc;
-            const double c2[2] = {-step, 2.0 * step};
-            if ((e = launch_axpy_stage(N, kk, c2, 2, points, tmp, 0, nullptr, s)) != cudaSuccess) return cuda_fail(e, "stage");
-            if ((rc = f(tmp, kk[2])) != NLO_OK) return rc;
-            const double c3[3] = {step / 6.0, 4.0 * step / 6.0, step / 6.0};
-            if ((e = launch_axpy_stage(N, kk, c3, 3, points, next, clamp, status, s)) != cudaSuccess)
-                return cuda_fail(e, "stage");
-        } else {
-            // classical RK4
-            if ((rc = f(N, kk[0])) != NLO_OK) return rc;
-            const double c1[1] = {0.5 * step};
-            if ((e = launch_axpy_stage(N, kk, c1, 1, points, tmp, 0, nullptr, s)) != cudaSuccess) return cuda_fail(e, "stage");
-            if ((rc = f(tmp, kk[1])) != NLO_OK) return rc;
-            const double* k2p[1] = {kk[1]};
-            if ((e = launch_axpy_stage(N, k2p, c1, 1, points, tmp, 0, nullptr, s)) != cudaSuccess) return cuda_fail(e, "stage");
-            if ((rc = f(tmp, kk[2])) != NLO_OK) return rc;
-            const double* k3p[1] = {kk[2]};
-            const double c3[1] = {step};
-            if ((e = launch_axpy_stage(N, k3p, c3, 1, points, tmp, 0, nullptr, s)) != cudaSuccess) return cuda_fail(e, "stage");
-            if ((rc = f(tmp, kk[3])) != NLO_OK) return rc;
-            const double c4[4] = {step / 6.0, 2.0 * step / 6.0, 2.0 * step / 6.0, step / 6.0};
-            if ((e = launch_axpy_stage(N, kk, c4, 4, points, next, clamp, status, s)) != cudaSuccess)
-                return cuda_fail(e, "stage");
-        }
+        auto comb = [&](int nk, const int* ks, const double* coef, int dst) {
+            const double* kp[4];
+            for (int j = 0; j < nk; ++j) kp[j] = kk[ks[j]];
+            const cudaError_t err = launch_axpy_stage(N, kp, coef, nk, points, dst ? next : tmp, dst ? clamp : 0,
+                                                      dst ? status : nullptr, s);
+            return err == cudaSuccess ? NLO_OK : cuda_fail(err, "stage");
+        };
+        const int rc = step_sequence(stepper, step, rhs, comb);
+        if (rc != NLO_OK) return rc;
     }
     return NLO_OK;
+}
+
+// Workspace of a multi-set evolution: per set the spline tables, their factorisation, the
+// active list and count, K1, the K2+Kf sums and five stage rows; the K2+Kf partial sums of the
+// layout; the set table.
+static size_t sets_bytes(int points, int sets, const SetsLayout& L, size_t* offsets /*[9] or NULL*/)
+{
+    const size_t S = (size_t)sets, n = (size_t)points;
+    size_t o = 0, off[9];
+    off[0] = o; o = align_up(o + sizeof(double) * S * spline_doubles(points));
+    off[1] = o; o = align_up(o + sizeof(double) * S * 2 * n);
+    off[2] = o; o = align_up(o + sizeof(int32_t) * S * n);
+    off[3] = o; o = align_up(o + sizeof(int32_t) * S);
+    off[4] = o; o = align_up(o + sizeof(double) * S * n);
+    off[5] = o; o = align_up(o + sizeof(double) * S * 3 * n);
+    off[6] = o; o = align_up(o + sizeof(double) * sets_partial_doubles(L));
+    off[7] = o; o = align_up(o + sizeof(double) * 5 * S * n);
+    off[8] = o; o = align_up(o + sizeof(SetTable));
+    if (offsets) std::memcpy(offsets, off, sizeof(off));
+    return o;
 }
 
 int nlo_bk_evolve(const nlo_bk_params* params, const double* r, int32_t points, int32_t steps, double step,
@@ -634,6 +674,129 @@ int nlo_bk_evolve_vegas(const nlo_bk_params* params, const double* r, int32_t po
     const BkVegasCall call = vegas_call(workspace, points, options, state);
     return evolve_rows(params, r, points, y, first, steps, step, stepper, dirs, options->samples_per_iteration, box,
                        table, status, workspace, workspace_bytes, stream, &call);
+}
+
+size_t nlo_bk_sets_workspace_bytes(int32_t points, int32_t sets, int32_t waves)
+{
+    if (points < 3 || points > 4096 || sets < 1 || sets > kMaxSets || waves < 1 || waves > 64) return 0;
+    return sets_bytes(points, sets, sets_layout(points, sets, waves), nullptr);
+}
+
+int nlo_bk_evolve_sets(const nlo_bk_params* params, const double* r, int32_t points, int32_t sets,
+                       double* const* tables, int32_t steps, double step, int32_t stepper,
+                       const nlo_sobol_dirs* dirs, const int64_t* samples, const nlo_bk_box* box, int32_t waves,
+                       uint32_t* status, void* workspace, size_t workspace_bytes, void* stream)
+{
+    std::string why;
+    if (!check_params(params, why)) return fail(NLO_ERR_INVALID, why);
+    if (params->kinematical_constraint)
+        return fail(NLO_ERR_INVALID, "the kinematical constraint is not available for parameter sets");
+    if (points < 3 || points > 4096) return fail(NLO_ERR_INVALID, "points must be 3..4096");
+    if (sets < 1 || sets > kMaxSets) return fail(NLO_ERR_INVALID, "sets must be 1..256");
+    if (!dirs) return fail(NLO_ERR_INVALID, "dirs is NULL");
+    for (int i = 0; i < sets; ++i)
+        if (!check_dirs(dirs + i, 4, why)) return fail(NLO_ERR_INVALID, "set " + std::to_string(i) + ": " + why);
+    if (waves < 1 || waves > 64) return fail(NLO_ERR_INVALID, "waves must be 1..64");
+    if (steps < 0) return fail(NLO_ERR_INVALID, "steps must be non-negative");
+    if (!(step > 0) || !std::isfinite(step)) return fail(NLO_ERR_INVALID, "step must be positive");
+    if (stepper != NLO_STEPPER_EULER && stepper != NLO_STEPPER_RK3 && stepper != NLO_STEPPER_RK4)
+        return fail(NLO_ERR_INVALID, "unknown stepper");
+    if (!r || !tables || !samples || !status || !box) return fail(NLO_ERR_INVALID, "NULL buffer");
+    for (int i = 0; i < sets; ++i) {
+        if (!tables[i]) return fail(NLO_ERR_INVALID, "NULL table");
+        if (samples[i] < 0 || samples[i] > (int64_t(1) << 30)) return fail(NLO_ERR_INVALID, "samples out of range");
+    }
+    const SetsLayout L = sets_layout(points, sets, waves);
+    if (!workspace || workspace_bytes < sets_bytes(points, sets, L, nullptr))
+        return fail(NLO_ERR_WORKSPACE, "workspace too small for nlo_bk_evolve_sets");
+    cudaStream_t s = (cudaStream_t)stream;
+    size_t off[9];
+    sets_bytes(points, sets, L, off);
+    char* base = static_cast<char*>(workspace);
+    double* spline = reinterpret_cast<double*>(base + off[0]);
+    double* factor = reinterpret_cast<double*>(base + off[1]);
+    int32_t* active = reinterpret_cast<int32_t*>(base + off[2]);
+    int32_t* counts = reinterpret_cast<int32_t*>(base + off[3]);
+    double* k1 = reinterpret_cast<double*>(base + off[4]);
+    double* k2kf = reinterpret_cast<double*>(base + off[5]);
+    double* partial = reinterpret_cast<double*>(base + off[6]);
+    double* stage = reinterpret_cast<double*>(base + off[7]);
+    SetTable* table = reinterpret_cast<SetTable*>(base + off[8]);
+    const size_t S = (size_t)sets, n = (size_t)points;
+    double* kk[4] = {stage, stage + S * n, stage + 2 * S * n, stage + 3 * S * n};
+    double* tmp = stage + 4 * S * n;
+
+    // slots in order of decreasing budget (ties by set index), so that slot 0 of every group
+    // holds the group's largest budget and sets of one budget share CTAs
+    int32_t order[kMaxSets];
+    for (int i = 0; i < sets; ++i) order[i] = i;
+    std::stable_sort(order, order + sets, [&](int32_t a, int32_t b) { return samples[a] > samples[b]; });
+    const int slots = L.groups * L.per_cta;
+    int32_t slot_set[kMaxSlots];
+    for (int q = 0; q < slots; ++q) slot_set[q] = q < sets ? order[q] : -1;
+    const bool nlo = order_has_nlo(params->order);
+    std::vector<SobolDirsArg> set_dirs(sets);
+    const SobolDirsArg* dir_ptrs[kMaxSets];
+    for (int i = 0; i < sets; ++i) {
+        set_dirs[i] = to_arg(dirs + i);
+        dir_ptrs[i] = &set_dirs[i];
+    }
+    cudaError_t e = launch_sets_setup(tables, samples, slot_set, dir_ptrs, sets, slots, nlo, table, s);
+    if (e != cudaSuccess) return cuda_fail(e, "sets setup");
+    if ((e = cudaMemsetAsync(status, 0, sizeof(uint32_t) * S, s)) != cudaSuccess) return cuda_fail(e, "status reset");
+    double* const* rows = reinterpret_cast<double* const*>(base + off[8] + offsetof(SetTable, rows));
+    RowsArg work;
+    work.base = tmp;
+    work.stride = n;
+    const int clamp = params->force_positive ? 1 : 0;
+    const SideStream side;
+    bool factor_ready = false;
+    for (int it = 0; it < steps; ++it) {
+        RowsArg now, next;
+        now.ptrs = rows;
+        now.offset = (size_t)it * n;
+        next.ptrs = rows;
+        next.offset = (size_t)(it + 1) * n;
+        auto rhs = [&](int src, int k) {
+            const RowsArg& in = src < 0 ? now : work;
+            if ((e = launch_splines(r, in, points, sets, params->force_positive, factor, factor_ready ? 0 : 1, spline,
+                                    s)) != cudaSuccess)
+                return cuda_fail(e, "splines");
+            factor_ready = true;
+            if ((e = launch_active(in, points, sets, 0, 1, active, counts, s)) != cudaSuccess)
+                return cuda_fail(e, "active");
+            const bool beside = side.ok;
+            cudaStream_t k1_stream = beside ? side.aux : s;
+            if (beside && ((e = cudaEventRecord(side.fork, s)) != cudaSuccess ||
+                           (e = cudaStreamWaitEvent(side.aux, side.fork, 0)) != cudaSuccess))
+                return cuda_fail(e, "fork");
+            if ((e = launch_k1(*params, r, points, spline, active, counts, k1, k1_stream, K1History(), sets)) !=
+                cudaSuccess)
+                return cuda_fail(e, "k1");
+            if (beside && (e = cudaEventRecord(side.join, side.aux)) != cudaSuccess) return cuda_fail(e, "join");
+            if (nlo) {
+                if ((e = launch_k2kf_sets(*params, r, points, sets, spline, spline_doubles(points), active, counts,
+                                          *box, L, table, k2kf, partial, s)) != cudaSuccess)
+                    return cuda_fail(e, "k2kf sets");
+            } else if ((e = cudaMemsetAsync(k2kf, 0, sizeof(double) * 3 * S * n, s)) != cudaSuccess) {
+                return cuda_fail(e, "k2kf clear");
+            }
+            if (beside && (e = cudaStreamWaitEvent(s, side.join, 0)) != cudaSuccess) return cuda_fail(e, "join");
+            if ((e = launch_assemble_sets(k1, k2kf, points, sets, table, kk[k], s)) != cudaSuccess)
+                return cuda_fail(e, "assemble");
+            return (int)NLO_OK;
+        };
+        auto comb = [&](int nk, const int* ks, const double* coef, int dst) {
+            const double* kp[4];
+            for (int j = 0; j < nk; ++j) kp[j] = kk[ks[j]];
+            const cudaError_t err = launch_axpy_sets(now, kp, coef, nk, points, sets, dst ? next : work,
+                                                     dst ? clamp : 0, dst ? status : nullptr, s);
+            return err == cudaSuccess ? (int)NLO_OK : cuda_fail(err, "stage");
+        };
+        const int rc = step_sequence(stepper, step, rhs, comb);
+        if (rc != NLO_OK) return rc;
+    }
+    return NLO_OK;
 }
 
 int nlo_bk_evolve_history(const nlo_bk_params* params, const double* r, int32_t points, const double* y,

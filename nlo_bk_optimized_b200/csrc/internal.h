@@ -47,8 +47,57 @@ struct RhsBuffers {
     int k2kf_blocks;
 };
 
-size_t spline_doubles(int points);
+__host__ __device__ inline size_t spline_doubles(int points) { return (size_t)points + 8 * (size_t)(points - 1); }
 int k2kf_max_blocks();
+
+// Rows of several parameter sets: set s's row is ptrs[s] + offset (rows inside the caller's
+// tables) or base + s * stride + offset (rows inside the workspace).
+struct RowsArg {
+    double* const* ptrs = nullptr;
+    double* base = nullptr;
+    size_t stride = 0;
+    size_t offset = 0;
+    __host__ __device__ double* at(int s) const { return (ptrs ? ptrs[s] : base + (size_t)s * stride) + offset; }
+};
+inline RowsArg single_row(const double* row)
+{
+    RowsArg a;
+    a.base = const_cast<double*>(row);
+    return a;
+}
+
+// Multi-set K2+Kf (several parameter sets in one launch): a CTA holds `per_cta` set slots of
+// `lanes` lanes each; slot q of group g is set slot_set[g * per_cta + q] (-1: empty), and the
+// sets are ordered by budget so that slot 0 of a group holds its largest.  CTA row
+// blockIdx.y = g * parent_tiles + (parent tile of the set's active list).
+constexpr int kMaxSets = 256;
+constexpr int kMaxSlots = kMaxSets + 8;  // groups * per_cta (per_cta <= 7)
+struct SetsLayout {
+    int per_cta = 1, lanes = 64, parent_tiles = 1, groups = 1, threads = 64, blocks = 1;
+};
+SetsLayout sets_layout(int points, int sets, int waves);
+inline size_t sets_partial_doubles(const SetsLayout& L)
+{
+    return (size_t)L.groups * L.parent_tiles * L.blocks * L.threads * 3;
+}
+// Per-call set table in the workspace, written by launch_sets_setup.
+constexpr int kSetDirsWords = 4 * 30 + 4;  // state[4][30], shift[4]: the K2+Kf box's four dimensions
+struct SetTable {
+    double* rows[kMaxSets];      // each set's table (row 0 = the initial row)
+    uint32_t samples[kMaxSets];  // Sobol budget per set
+    int32_t slot_set[kMaxSlots]; // set of each slot, -1 empty
+    int32_t set_slot[kMaxSets];  // slot of each set
+    double inv[kMaxSets];        // 1 / samples (0 without NLO kernels)
+    uint32_t dirs[kMaxSets][kSetDirsWords];  // Sobol directions of dimensions 0..3 and their shifts
+};
+cudaError_t launch_sets_setup(double* const* rows, const int64_t* samples, const int32_t* slot_set,
+                              const SobolDirsArg* const* dirs, int sets, int slots, bool nlo, SetTable* table,
+                              cudaStream_t stream);
+// Sets with their own Sobol points (the set table's directions).
+cudaError_t launch_k2kf_sets(const nlo_bk_params& p, const double* r, int points, int sets, const double* spline,
+                             size_t spline_stride, const int32_t* active, const int32_t* counts,
+                             const nlo_bk_box& box, const SetsLayout& L, const SetTable* table, double* out,
+                             double* partial, cudaStream_t stream);
 
 // Records a message for nlo_last_error() and returns code.
 int set_last_error(int code, const char* message);
@@ -57,10 +106,13 @@ int set_last_error(int code, const char* message);
 // least `bytes`; safe when several host threads launch the same kernel with different sizes.
 cudaError_t raise_dynamic_smem(const void* func, size_t bytes);
 
-cudaError_t launch_splines(const double* r, const double* N, int n, int force_positive, double* factor,
+// Spline tables of `sets` rows: set s reads N.at(s) and writes out + s * spline_doubles(n)
+// and its factorisation at factor + s * 2n.
+cudaError_t launch_splines(const double* r, const RowsArg& N, int n, int sets, int force_positive, double* factor,
                            int compute_factor, double* out, cudaStream_t stream);
-// active parents (index > 0, N <= 0.99999) with index % shards == shard
-cudaError_t launch_active(const double* N, int n, int shard, int shards, int32_t* active, int32_t* count,
+// active parents (index > 0, N <= 0.99999) with index % shards == shard; set s reads N.at(s)
+// and writes active + s * n and count + s
+cudaError_t launch_active(const RowsArg& N, int n, int sets, int shard, int shards, int32_t* active, int32_t* count,
                           cudaStream_t stream);
 cudaError_t launch_sobol(const SobolDirsArg& dirs, uint64_t offset, uint64_t n, int precision, void* out,
                          cudaStream_t stream);
@@ -78,9 +130,11 @@ constexpr int kKcStride = 14;  // per r interval: start, local interval, 2 x 6 w
 inline size_t kc_weights_doubles(int points) { return (size_t)(points - 1) * kKcStride; }
 cudaError_t launch_kc_weights(const double* r, int points, double* weights, cudaStream_t stream);
 
+// K1 of `sets` sets: set s reads spline + s * spline_doubles(points), active + s * points and
+// count + s, and writes out + s * points (the constraint history: one set only).
 cudaError_t launch_k1(const nlo_bk_params& p, const double* r, int points, const double* spline,
                       const int32_t* active, const int32_t* count, double* out, cudaStream_t stream,
-                      const K1History& history = K1History());
+                      const K1History& history = K1History(), int sets = 1);
 cudaError_t launch_k2kf(const nlo_bk_params& p, const double* r, int points, const double* spline,
                         const int32_t* active, const int32_t* count, const SobolDirsArg& dirs, uint64_t offset,
                         uint64_t samples, const nlo_bk_box& box, double* out, double* partial, int max_blocks,
@@ -112,5 +166,11 @@ cudaError_t launch_assemble(const double* k1, const double* k2kf, int points, do
                             double* k2kf_total, cudaStream_t stream);
 cudaError_t launch_axpy_stage(const double* N, const double* const* k, const double* coef, int nk, int points,
                               double* out, int clamp, uint32_t* status, cudaStream_t stream);
+// Several sets: dndy + s * points = k1 + s * points + (k2kf + s * 3 points) * table->inv[s].
+cudaError_t launch_assemble_sets(const double* k1, const double* k2kf, int points, int sets, const SetTable* table,
+                                 double* dndy, cudaStream_t stream);
+// Several sets: out.at(s) = N.at(s) + sum_j coef[j] (k[j] + s * points); status + s when given.
+cudaError_t launch_axpy_sets(const RowsArg& N, const double* const* k, const double* coef, int nk, int points,
+                             int sets, const RowsArg& out, int clamp, uint32_t* status, cudaStream_t stream);
 
 }  // namespace nlo

@@ -414,6 +414,11 @@ __global__ void __cluster_dims__(1, kK1Split, 1) __launch_bounds__(kK1Threads, K
                                                         const int32_t* __restrict__ active,
                                                         const int32_t* __restrict__ count, double* __restrict__ out)
 {
+    // set blockIdx.z: its spline table, active list, count and output row
+    spline += (size_t)blockIdx.z * spline_doubles(n);
+    active += (size_t)blockIdx.z * n;
+    count += blockIdx.z;
+    out += (size_t)blockIdx.z * n;
     const int slot = blockIdx.x;
     if (slot >= *count) return;
     const int knot = active[slot];
@@ -598,8 +603,9 @@ cudaError_t launch_kc_weights(const double* r, int points, double* weights, cuda
 
 cudaError_t launch_k1(const nlo_bk_params& p, const double* r, int points, const double* spline,
                       const int32_t* active, const int32_t* count, double* out, cudaStream_t stream,
-                      const K1History& history)
+                      const K1History& history, int sets)
 {
+    if (history.on && sets != 1) return cudaErrorInvalidValue;
     K1Consts consts;
     consts.rule = k1_rule();
     for (int j = 0; j < 24; ++j) {
@@ -609,7 +615,7 @@ cudaError_t launch_k1(const nlo_bk_params& p, const double* r, int points, const
         consts.sh2[j] = sh * sh;
         consts.aw[j] = consts.rule.w24[j] * kPi * v;
     }
-    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(double) * (size_t)points, stream);
+    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(double) * (size_t)points * sets, stream);
     if (e != cudaSuccess) return e;
     const Phys<double> phd = make_phys<double>(p);
     const size_t per_split = (size_t)((points - 1 + kK1Split - 1) / kK1Split) * 8;
@@ -626,7 +632,7 @@ cudaError_t launch_k1(const nlo_bk_params& p, const double* r, int points, const
         const void* fn = (const void*)k1_kernel<TF, KC>;
         cudaError_t err = raise_dynamic_smem(fn, smem);
         if (err != cudaSuccess) return err;
-        k1_kernel<TF, KC><<<dim3(points, kK1Split), kK1Threads, smem, stream>>>(make_phys<TF>(p), phd, consts, history,
+        k1_kernel<TF, KC><<<dim3(points, kK1Split, sets), kK1Threads, smem, stream>>>(make_phys<TF>(p), phd, consts, history,
                                                                                r, points, spline, active, count, out);
         return cudaGetLastError();
     };

@@ -17,6 +17,9 @@
 
 #include <cuda_runtime.h>
 
+#include <cstring>
+#include <type_traits>
+
 #include "common.cuh"
 #include "internal.h"
 #include "k2kf_integrand.cuh"
@@ -242,61 +245,128 @@ __device__ __forceinline__ void k2_pair_fast(const FastSpline& s, const Phys<flo
 constexpr int kFoldPairs = 16;
 
 
-template <typename T, bool SYM, int COUPLING>
+// Set slots of a multi-set launch (MULTI): see SetsLayout.
+struct SetsArg {
+    int per_cta, lanes, parent_tiles;
+    size_t spline_stride;
+    const SetTable* table;
+};
+
+// Shared-memory bytes of one set slot's spline tables: the T-typed log S coefficients, the
+// pre-scaled FP32 rows with their edge rows (FP32 build) and the knots.
+template <typename T>
+__host__ __device__ inline size_t k2_slot_bytes(int n)
+{
+    const size_t b = sizeof(T) * 4 * (size_t)(n - 1) + (sizeof(T) == sizeof(float) ? sizeof(float4) * (size_t)(n + 1) : 0) +
+                     sizeof(T) * (size_t)n;
+    return (b + 15) & ~(size_t)15;
+}
+
+// MULTI = false: one parameter set, lanes = the CTA's threads.  MULTI = true: thread t holds
+// set slot t / lanes of its group (its own spline tables in shared memory) and parent slot
+// tile * lanes + t % lanes of that set's active list; a tile stages `lanes` samples per slot,
+// each slot's records from its own set's amplitudes, while the Sobol points (one seed for all
+// sets) and the geometry are the same for every slot.
+template <typename T, bool SYM, int COUPLING, bool MULTI>
 __global__ void __launch_bounds__(448, (sizeof(T) == 4 ? 2 : 1)) k2kf_kernel(Phys<T> ph, K2Box<T> box, SobolDirsArg dirs,
                                                     const double* __restrict__ r_grid, int n,
                                                     const double* __restrict__ spline,
                                                     const int32_t* __restrict__ active,
                                                     const int32_t* __restrict__ count, uint64_t offset,
-                                                    uint64_t samples, double* __restrict__ partial)
+                                                    uint64_t samples, double* __restrict__ partial, SetsArg sa)
 {
+    const int slots = MULTI ? sa.per_cta : 1;
+    const int lanes = MULTI ? sa.lanes : (int)blockDim.x;
+    const int my_slot = MULTI ? (int)threadIdx.x / lanes : 0;
+    const int lt = (int)threadIdx.x - my_slot * lanes;
+    const int group = MULTI ? (int)blockIdx.y / sa.parent_tiles : 0;
+    const int ptile = MULTI ? (int)blockIdx.y - group * sa.parent_tiles : (int)blockIdx.y;
+    int my_set = 0;
+    uint64_t my_samples = samples, max_samples = samples;
+    if (MULTI) {
+        my_set = sa.table->slot_set[group * slots + my_slot];
+        my_samples = my_set >= 0 ? sa.table->samples[my_set] : 0;
+        // slot 0 of a group holds its largest budget
+        max_samples = sa.table->samples[sa.table->slot_set[group * slots]];
+    }
+    const uint64_t tile = lanes;
+    const uint64_t tiles = (max_samples + tile - 1) / tile;
+    // MULTI: a CTA past its group's tiles has nothing to add (the finalize reads only the CTAs
+    // below the tile count)
+    if (MULTI && blockIdx.x >= tiles) return;
+
     extern __shared__ __align__(16) unsigned char k2_smem[];
     K2Rec<T>* recs = reinterpret_cast<K2Rec<T>*>(k2_smem);  // [blockDim.x], 16-byte aligned rows
-    T* cs = reinterpret_cast<T*>(recs + blockDim.x);          // [n-1][4] natural units, 16-byte aligned
-    float4* cs2 = reinterpret_cast<float4*>(cs + 4 * (n - 1)); // [n+1] pre-scaled with edge rows (FP32 path)
-    T* xs = reinterpret_cast<T*>(cs2 + (sizeof(T) == sizeof(float) ? n + 1 : 0));
-    uint32_t* st = reinterpret_cast<uint32_t*>(xs + n);         // [4][30] + shift[4]
-    const double* src_coef = spline + n + 4 * (size_t)(n - 1);     // log S block
+    unsigned char* slot_base = reinterpret_cast<unsigned char*>(recs + blockDim.x);
+    const size_t slot_bytes = k2_slot_bytes<T>(n);
+    uint32_t* st = reinterpret_cast<uint32_t*>(slot_base + slots * slot_bytes);  // per slot [4][30] + shift[4]
+    // slot q: cs [n-1][4] natural units, cs2 [n+1] pre-scaled with edge rows (FP32 path), xs [n]
+    auto cs_of = [&](int q) { return reinterpret_cast<T*>(slot_base + q * slot_bytes); };
+    auto cs2_of = [&](int q) { return reinterpret_cast<float4*>(cs_of(q) + 4 * (n - 1)); };
+    auto xs_of = [&](int q) {
+        return reinterpret_cast<T*>(cs2_of(q) + (sizeof(T) == sizeof(float) ? n + 1 : 0));
+    };
     const double h64 = (spline[n - 1] - spline[0]) / (double)(n - 1);
-    for (int i = threadIdx.x; i < n; i += blockDim.x) xs[i] = (T)spline[i];
-    for (int i = threadIdx.x; i < 4 * (n - 1); i += blockDim.x) cs[i] = (T)src_coef[i];
-    if (sizeof(T) == sizeof(float)) {
-        const double l2e = 1.4426950408889634;
-        for (int i = threadIdx.x; i < n - 1; i += blockDim.x) {
-            const double* c = src_coef + 4 * (size_t)i;
-            cs2[i + 1] = make_float4((float)(c[0] * l2e), (float)(c[1] * h64 * l2e),
-                                     (float)(c[2] * h64 * h64 * l2e), (float)(c[3] * h64 * h64 * h64 * l2e));
-        }
-        if (threadIdx.x == 0) {
-            cs2[0] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            cs2[n] = make_float4(-150.0f, 0.0f, 0.0f, 0.0f);
+    for (int q = 0; q < slots; ++q) {
+        const int set_q = MULTI ? sa.table->slot_set[group * slots + q] : 0;
+        if (set_q < 0) continue;
+        const double* sp = spline + (MULTI ? (size_t)set_q * sa.spline_stride : 0);
+        const double* src_coef = sp + n + 4 * (size_t)(n - 1);  // log S block
+        T* cs = cs_of(q);
+        float4* cs2 = cs2_of(q);
+        T* xs = xs_of(q);
+        for (int i = threadIdx.x; i < n; i += blockDim.x) xs[i] = (T)sp[i];
+        for (int i = threadIdx.x; i < 4 * (n - 1); i += blockDim.x) cs[i] = (T)src_coef[i];
+        if (sizeof(T) == sizeof(float)) {
+            const double l2e = 1.4426950408889634;
+            for (int i = threadIdx.x; i < n - 1; i += blockDim.x) {
+                const double* c = src_coef + 4 * (size_t)i;
+                cs2[i + 1] = make_float4((float)(c[0] * l2e), (float)(c[1] * h64 * l2e),
+                                         (float)(c[2] * h64 * h64 * l2e), (float)(c[3] * h64 * h64 * h64 * l2e));
+            }
+            if (threadIdx.x == 0) {
+                cs2[0] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                cs2[n] = make_float4(-150.0f, 0.0f, 0.0f, 0.0f);
+            }
         }
     }
-    for (int i = threadIdx.x; i < 120; i += blockDim.x) st[i] = dirs.state[i / 30][i % 30];
-    if (threadIdx.x < 4) st[120 + threadIdx.x] = dirs.shift[threadIdx.x];
+    if (MULTI) {  // each slot's own Sobol directions
+        for (int i = threadIdx.x; i < slots * kSetDirsWords; i += blockDim.x) {
+            const int q = i / kSetDirsWords;
+            const int set_q = sa.table->slot_set[group * slots + q];
+            st[i] = set_q >= 0 ? sa.table->dirs[set_q][i - q * kSetDirsWords] : 0u;
+        }
+    } else {
+        for (int i = threadIdx.x; i < 120; i += blockDim.x) st[i] = dirs.state[i / 30][i % 30];
+        if (threadIdx.x < 4) st[120 + threadIdx.x] = dirs.shift[threadIdx.x];
+    }
     __syncthreads();
+    // this thread's slot (an empty slot reads slot 0's tables and prepares zero-weight records)
+    const int view = MULTI && my_set < 0 ? 0 : my_slot;
+    const uint32_t* my_st = st + (MULTI ? view * kSetDirsWords : 0);
     SplineView<T> s;
-    s.x = xs;
-    s.coef = cs;
+    s.x = xs_of(view);
+    s.coef = cs_of(view);
     s.n = n;
-    s.x0 = xs[0];
+    s.x0 = s.x[0];
     s.inv_h = (T)((double)(n - 1) / (spline[n - 1] - spline[0]));
 
     // per-evaluation spline: uniform-grid FP32 form in the mixed build, the exact
     // knot search in the FP64 build
     FastSpline fs;
-    fs.coef = cs2;
+    fs.coef = cs2_of(view);
     fs.u_scale = (float)(0.5 * 0.69314718055994531 / h64);
     fs.u_off = (float)(-spline[0] / h64);
     fs.u_top = (float)(n - 1);
 
-    const int n_active = *count;
-    const int slot = blockIdx.y * blockDim.x + threadIdx.x;
+    const int32_t* act = active + (MULTI && my_set > 0 ? (size_t)my_set * n : 0);
+    const int n_active = MULTI ? (my_set >= 0 ? count[my_set] : 0) : *count;
+    const int slot = ptile * lanes + lt;
     const bool has_parent = slot < n_active;
     K2Parent<T> P;
     K2ParentF PF;
     {
-        const double r = has_parent ? r_grid[active[slot]] : 1.0;
+        const double r = has_parent ? r_grid[act[slot]] : 1.0;
         P.r = (T)r;
         P.r2 = P.r * P.r;
         P.lr = (T)log(r);
@@ -310,27 +380,29 @@ __global__ void __launch_bounds__(448, (sizeof(T) == 4 ? 2 : 1)) k2kf_kernel(Phy
         PF.alpha_r = (float)P.alpha_r;
     }
     double acc_k2 = 0.0, acc_kf = 0.0, acc_sq = 0.0;
-    const uint64_t tile = blockDim.x;
-    const uint64_t tiles = (samples + tile - 1) / tile;
     // CTAs whose parent tile is empty still stage samples for nobody: skip them.
-    const bool any_parent = blockIdx.y * blockDim.x < (unsigned)n_active;
+    const bool any_parent =
+        MULTI ? __syncthreads_or(has_parent) != 0 : blockIdx.y * blockDim.x < (unsigned)n_active;
     if (any_parent) {
+        // this slot's records start at record my_slot * lanes (pair my_slot * lanes / 2)
+        const size_t rec0 = (size_t)my_slot * lanes;
         for (uint64_t tix = blockIdx.x; tix < tiles; tix += gridDim.x) {
-            const uint64_t local = tix * tile + threadIdx.x;
-            const uint64_t remaining = samples - tix * tile;
+            const uint64_t local = tix * tile + lt;
+            const uint64_t done = tix * tile;
+            const uint64_t remaining = my_samples > done ? my_samples - done : 0;
             const int count_here = (int)(remaining < tile ? remaining : tile);
             if constexpr (sizeof(T) == sizeof(float)) {
-                // pair layout: the fields of samples 2p and 2p+1 side by side (blockDim.x is even;
-                // a padding sample past `samples` carries zero weight)
+                // pair layout: the fields of samples 2p and 2p+1 side by side (lanes is even;
+                // a padding sample past the budget carries zero weight)
                 float rec[kRecLen];
-                k2_prepare<float>(s, box, st, st + 120, offset + local, local < samples, rec);
+                k2_prepare<float>(s, box, my_st, my_st + 120, offset + local, local < my_samples, rec);
                 float* dst = reinterpret_cast<float*>(recs) + (size_t)(threadIdx.x >> 1) * (2 * kRecLen) +
                              (threadIdx.x & 1);
 #pragma unroll
                 for (int f = 0; f < kRecLen; ++f) dst[2 * f] = rec[f];
                 __syncthreads();
                 if (has_parent) {
-                    const float4* pr = reinterpret_cast<const float4*>(recs);
+                    const float4* pr = reinterpret_cast<const float4*>(recs) + (rec0 / 2) * (kRecLen / 2);
                     f2 sq = bc2(0.0f);  // variance estimate only: plain sum per tile
                     const int pairs = (count_here + 1) >> 1;
                     // FP32x2 partial sums of 16 pairs (32 samples), folded into FP64: the
@@ -351,7 +423,7 @@ __global__ void __launch_bounds__(448, (sizeof(T) == 4 ? 2 : 1)) k2kf_kernel(Phy
                     acc_sq += (double)sq.x + (double)sq.y;
                 }
             } else {
-                k2_prepare<T>(s, box, st, st + 120, offset + local, local < samples, recs[threadIdx.x].v);
+                k2_prepare<T>(s, box, my_st, my_st + 120, offset + local, local < my_samples, recs[threadIdx.x].v);
                 __syncthreads();
                 if (has_parent) {
                     Kahan<T> sk2, skf;
@@ -360,7 +432,7 @@ __global__ void __launch_bounds__(448, (sizeof(T) == 4 ? 2 : 1)) k2kf_kernel(Phy
                     T sq = (T)0;  // variance estimate only: plain sum per tile
                     for (int j = 0; j < count_here; ++j) {
                         T k2w, kfw;
-                        k2_point<T, SYM>(s, ph, P, recs[j].v, k2w, kfw);
+                        k2_point<T, SYM>(s, ph, P, recs[rec0 + j].v, k2w, kfw);
                         sk2.add(k2w);
                         skf.add(kfw);
                         const T tot = k2w + kfw;
@@ -374,8 +446,12 @@ __global__ void __launch_bounds__(448, (sizeof(T) == 4 ? 2 : 1)) k2kf_kernel(Phy
             __syncthreads();
         }
     }
-    if (slot < n) {
-        double* o = partial + ((size_t)blockIdx.x * n + slot) * 3;
+    double* o = nullptr;
+    if (MULTI)
+        o = partial + (((size_t)blockIdx.y * gridDim.x + blockIdx.x) * blockDim.x + threadIdx.x) * 3;
+    else if (slot < n)
+        o = partial + ((size_t)blockIdx.x * n + slot) * 3;
+    if (o) {
         o[0] = acc_k2;
         o[1] = acc_kf;
         o[2] = acc_sq;
@@ -412,30 +488,48 @@ __global__ void __launch_bounds__(256) k2kf_finalize_kernel(const double* __rest
     }
 }
 
-template <typename T, bool SYM, int COUPLING>
-cudaError_t launch_typed(const nlo_bk_params& p, const double* r, int points, const double* spline,
-                         const int32_t* active, const int32_t* count, const SobolDirsArg& dirs, uint64_t offset,
-                         uint64_t samples, const nlo_bk_box& box, double* partial, int max_blocks, int threads,
-                         int parent_tiles, int* used_blocks, cudaStream_t stream)
+// Multi-set finalize: one warp per (set blockIdx.y, active parent); the set's slot gives its
+// CTA row and lane, and the CTAs below its group's tile count hold its partial sums.
+__global__ void __launch_bounds__(256) k2kf_finalize_sets_kernel(const double* __restrict__ partial, int blocks,
+                                                                 int threads, int n, SetsArg sa,
+                                                                 const int32_t* __restrict__ active,
+                                                                 const int32_t* __restrict__ count,
+                                                                 double* __restrict__ out)
 {
-    const size_t smem = sizeof(K2Rec<T>) * threads + sizeof(T) * (size_t)(points + 4 * (points - 1)) +
-                        (sizeof(T) == sizeof(float) ? sizeof(float4) * (size_t)(points + 1) : 0) +
-                        sizeof(uint32_t) * 124;
-    cudaError_t e = raise_dynamic_smem((const void*)k2kf_kernel<T, SYM, COUPLING>, smem);
-    if (e != cudaSuccess) return e;
-    int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k2kf_kernel<T, SYM, COUPLING>, threads, smem);
-    if (e != cudaSuccess) return e;
-    int device = 0, sms = 0;
-    cudaGetDevice(&device);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    if (per_sm < 1) per_sm = 1;
-    const uint64_t tiles = (samples + threads - 1) / threads;
-    uint64_t blocks = (uint64_t)per_sm * sms / (uint64_t)parent_tiles;
-    if (blocks < 1) blocks = 1;
-    if (blocks > (uint64_t)max_blocks) blocks = (uint64_t)max_blocks;
-    if (blocks > tiles) blocks = tiles;
-    *used_blocks = (int)blocks;
+    const int slot = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const int set = blockIdx.y;
+    if (slot >= n || slot >= count[set]) return;
+    const int set_slot = sa.table->set_slot[set];
+    const int group = set_slot / sa.per_cta, q = set_slot - group * sa.per_cta;
+    const int row = group * sa.parent_tiles + slot / sa.lanes;
+    const int thread = q * sa.lanes + slot % sa.lanes;
+    const uint64_t max_samples = sa.table->samples[sa.table->slot_set[group * sa.per_cta]];
+    const uint64_t tiles = (max_samples + sa.lanes - 1) / sa.lanes;
+    const int used = (uint64_t)blocks < tiles ? blocks : (int)tiles;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    for (int c = lane; c < used; c += 32) {
+        const double* p = partial + (((size_t)row * blocks + c) * threads + thread) * 3;
+        s0 += p[0];
+        s1 += p[1];
+        s2 += p[2];
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        s0 += __shfl_down_sync(0xffffffffu, s0, o);
+        s1 += __shfl_down_sync(0xffffffffu, s1, o);
+        s2 += __shfl_down_sync(0xffffffffu, s2, o);
+    }
+    if (lane == 0) {
+        double* o = out + 3 * ((size_t)set * n + active[(size_t)set * n + slot]);
+        o[0] = s0;
+        o[1] = s1;
+        o[2] = s2;
+    }
+}
+
+template <typename T>
+K2Box<T> make_box(const nlo_bk_params& p, const nlo_bk_box& box, bool sym)
+{
     K2Box<T> kb;
     double volume = 1.0;
     for (int d = 0; d < 4; ++d) {
@@ -450,13 +544,93 @@ cudaError_t launch_typed(const nlo_bk_params& p, const double* r, int points, co
         volume = box.width[0] * box.width[1] * box.width[2] * box.width[3];
     }
     // the FP32 path folds the symmetrisation's 1/2 into the per-sample weight
-    const double half = (sizeof(T) == sizeof(float) && SYM) ? 0.5 : 1.0;
+    const double half = (sizeof(T) == sizeof(float) && sym) ? 0.5 : 1.0;
     kb.cpt_scale = (T)(half * volume * p.nc * p.nc / (8.0 * kPi * kPi * kPi * kPi));
-    dim3 grid((unsigned)blocks, (unsigned)parent_tiles);
-    k2kf_kernel<T, SYM, COUPLING><<<grid, threads, smem, stream>>>(make_phys<T>(p), kb, dirs, r, points, spline,
-                                                                  active, count, offset, samples, partial);
+    return kb;
+}
+
+template <typename T>
+size_t k2_smem_bytes(int threads, int slots, int points)
+{
+    return sizeof(K2Rec<T>) * threads + slots * k2_slot_bytes<T>(points) + sizeof(uint32_t) * kSetDirsWords * slots;
+}
+
+template <typename T, bool SYM, int COUPLING>
+cudaError_t launch_sets_typed(const nlo_bk_params& p, const double* r, int points, const double* spline,
+                              size_t spline_stride, const int32_t* active, const int32_t* counts,
+                              const nlo_bk_box& box, const SetsLayout& L, const SetTable* table, double* partial,
+                              cudaStream_t stream)
+{
+    const size_t smem = k2_smem_bytes<T>(L.threads, L.per_cta, points);
+    cudaError_t e = raise_dynamic_smem((const void*)k2kf_kernel<T, SYM, COUPLING, true>, smem);
+    if (e != cudaSuccess) return e;
+    SetsArg sa{L.per_cta, L.lanes, L.parent_tiles, spline_stride, table};
+    dim3 grid((unsigned)L.blocks, (unsigned)(L.groups * L.parent_tiles));
+    SobolDirsArg unused;
+    std::memset(&unused, 0, sizeof(unused));
+    k2kf_kernel<T, SYM, COUPLING, true><<<grid, L.threads, smem, stream>>>(
+        make_phys<T>(p), make_box<T>(p, box, SYM), unused, r, points, spline, active, counts, 0, 0, partial, sa);
     return cudaGetLastError();
 }
+
+template <typename T, bool SYM, int COUPLING>
+cudaError_t launch_typed(const nlo_bk_params& p, const double* r, int points, const double* spline,
+                         const int32_t* active, const int32_t* count, const SobolDirsArg& dirs, uint64_t offset,
+                         uint64_t samples, const nlo_bk_box& box, double* partial, int max_blocks, int threads,
+                         int parent_tiles, int* used_blocks, cudaStream_t stream)
+{
+    const size_t smem = k2_smem_bytes<T>(threads, 1, points);
+    cudaError_t e = raise_dynamic_smem((const void*)k2kf_kernel<T, SYM, COUPLING, false>, smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k2kf_kernel<T, SYM, COUPLING, false>, threads, smem);
+    if (e != cudaSuccess) return e;
+    int device = 0, sms = 0;
+    cudaGetDevice(&device);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (per_sm < 1) per_sm = 1;
+    const uint64_t tiles = (samples + threads - 1) / threads;
+    uint64_t blocks = (uint64_t)per_sm * sms / (uint64_t)parent_tiles;
+    if (blocks < 1) blocks = 1;
+    if (blocks > (uint64_t)max_blocks) blocks = (uint64_t)max_blocks;
+    if (blocks > tiles) blocks = tiles;
+    *used_blocks = (int)blocks;
+    dim3 grid((unsigned)blocks, (unsigned)parent_tiles);
+    k2kf_kernel<T, SYM, COUPLING, false><<<grid, threads, smem, stream>>>(
+        make_phys<T>(p), make_box<T>(p, box, SYM), dirs, r, points, spline, active, count, offset, samples, partial,
+        SetsArg{});
+    return cudaGetLastError();
+}
+
+// The kernel instantiation of a parameter set: FP64 (one form for every coupling) or the
+// FP32 coupling variant; f(T(), SYM, COUPLING) with std::integral_constant tags.
+template <class F>
+cudaError_t dispatch_variant(const nlo_bk_params& p, F f)
+{
+    using std::integral_constant;
+    const bool sym = p.symmetrize != 0;
+    const int coupling = p.fixed_coupling                 ? 2
+                         : p.rc_nlo == NLO_RC_NLO_PARENT ? 4
+                         : p.nf > 3.0                    ? 3
+                         : p.alpha_cap > 0.0             ? 1
+                                                         : 0;
+#define NLO_K2_VARIANT(T, C)                                                                  \
+    (sym ? f(T(), integral_constant<bool, true>(), integral_constant<int, C>())                \
+         : f(T(), integral_constant<bool, false>(), integral_constant<int, C>()))
+    if (p.precision == NLO_PRECISION_FP64) return NLO_K2_VARIANT(double, 0);
+    switch (coupling) {
+        case 0: return NLO_K2_VARIANT(float, 0);
+        case 1: return NLO_K2_VARIANT(float, 1);
+        case 2: return NLO_K2_VARIANT(float, 2);
+        case 3: return NLO_K2_VARIANT(float, 3);
+        default: return NLO_K2_VARIANT(float, 4);
+    }
+#undef NLO_K2_VARIANT
+}
+
+// at most 448 lanes (parents) per CTA: the FP32 kernel's bounds (448 threads, two CTAs per
+// SM) give it 72 registers without spills; larger grids take several parent tiles
+constexpr int kLaneCap = 448;
 
 }  // namespace
 
@@ -467,38 +641,58 @@ cudaError_t launch_k2kf(const nlo_bk_params& p, const double* r, int points, con
 {
     cudaError_t e = cudaMemsetAsync(out, 0, sizeof(double) * 3 * (size_t)points, stream);
     if (e != cudaSuccess || samples == 0) return e;
-    // at most 448 lanes (parents) per CTA: the FP32 kernel's bounds (448 threads, two CTAs per
-    // SM) give it 72 registers without spills; larger grids take several parent tiles
-    const int cap = 448;
-    int threads = ((points < cap ? points : cap) + 31) / 32 * 32;
+    int threads = ((points < kLaneCap ? points : kLaneCap) + 31) / 32 * 32;
     if (threads < 64) threads = 64;
     const int parent_tiles = (points + threads - 1) / threads;
     int used = 0;
-    const bool fp64 = p.precision == NLO_PRECISION_FP64;
-    const bool sym = p.symmetrize != 0;
-    const int coupling = p.fixed_coupling                 ? 2
-                         : p.rc_nlo == NLO_RC_NLO_PARENT ? 4
-                         : p.nf > 3.0                    ? 3
-                         : p.alpha_cap > 0.0             ? 1
-                                                         : 0;
-#define NLO_K2_LAUNCH(T, S, C)                                                                                  \
-    launch_typed<T, S, C>(p, r, points, spline, active, count, dirs, offset, samples, box, partial, max_blocks, \
-                          threads, parent_tiles, &used, stream)
-    if (fp64)
-        e = sym ? NLO_K2_LAUNCH(double, true, 0) : NLO_K2_LAUNCH(double, false, 0);
-    else if (coupling == 0)
-        e = sym ? NLO_K2_LAUNCH(float, true, 0) : NLO_K2_LAUNCH(float, false, 0);
-    else if (coupling == 1)
-        e = sym ? NLO_K2_LAUNCH(float, true, 1) : NLO_K2_LAUNCH(float, false, 1);
-    else if (coupling == 2)
-        e = sym ? NLO_K2_LAUNCH(float, true, 2) : NLO_K2_LAUNCH(float, false, 2);
-    else if (coupling == 3)
-        e = sym ? NLO_K2_LAUNCH(float, true, 3) : NLO_K2_LAUNCH(float, false, 3);
-    else
-        e = sym ? NLO_K2_LAUNCH(float, true, 4) : NLO_K2_LAUNCH(float, false, 4);
-#undef NLO_K2_LAUNCH
+    e = dispatch_variant(p, [&](auto t, auto sym, auto c) {
+        return launch_typed<decltype(t), decltype(sym)::value, decltype(c)::value>(
+            p, r, points, spline, active, count, dirs, offset, samples, box, partial, max_blocks, threads, parent_tiles,
+            &used, stream);
+    });
     if (e != cudaSuccess) return e;
     k2kf_finalize_kernel<<<(points * 32 + 255) / 256, 256, 0, stream>>>(partial, used, points, active, count, out);
+    return cudaGetLastError();
+}
+
+SetsLayout sets_layout(int points, int sets, int waves)
+{
+    SetsLayout L;
+    L.lanes = ((points < kLaneCap ? points : kLaneCap) + 31) / 32 * 32;
+    if (L.lanes < 64) L.lanes = 64;
+    L.per_cta = kLaneCap / L.lanes;
+    if (L.per_cta > sets) L.per_cta = sets;
+    if (L.per_cta < 1) L.per_cta = 1;
+    L.parent_tiles = (points + L.lanes - 1) / L.lanes;
+    L.groups = (sets + L.per_cta - 1) / L.per_cta;
+    L.threads = L.per_cta * L.lanes;
+    int device = 0, sms = 148;
+    if (cudaGetDevice(&device) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (sms < 1) sms = 148;
+    // about `waves` waves of the FP32 kernel's two CTAs per SM over all groups and parent
+    // tiles; a group with fewer tiles than CTAs leaves the rest idle (they return at once)
+    const long rows = (long)L.groups * L.parent_tiles;
+    long blocks = ((long)(waves < 1 ? 1 : waves) * 2 * sms + rows - 1) / rows;
+    if (blocks > 4L * sms) blocks = 4L * sms;
+    L.blocks = (int)(blocks < 1 ? 1 : blocks);
+    return L;
+}
+
+cudaError_t launch_k2kf_sets(const nlo_bk_params& p, const double* r, int points, int sets, const double* spline,
+                             size_t spline_stride, const int32_t* active, const int32_t* counts,
+                             const nlo_bk_box& box, const SetsLayout& L, const SetTable* table, double* out,
+                             double* partial, cudaStream_t stream)
+{
+    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(double) * 3 * (size_t)points * sets, stream);
+    if (e != cudaSuccess) return e;
+    e = dispatch_variant(p, [&](auto t, auto sym, auto c) {
+        return launch_sets_typed<decltype(t), decltype(sym)::value, decltype(c)::value>(
+            p, r, points, spline, spline_stride, active, counts, box, L, table, partial, stream);
+    });
+    if (e != cudaSuccess) return e;
+    SetsArg sa{L.per_cta, L.lanes, L.parent_tiles, spline_stride, table};
+    k2kf_finalize_sets_kernel<<<dim3((points * 32 + 255) / 256, sets), 256, 0, stream>>>(
+        partial, L.blocks, L.threads, points, sa, active, counts, out);
     return cudaGetLastError();
 }
 

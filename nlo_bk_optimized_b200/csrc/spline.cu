@@ -19,10 +19,15 @@ namespace nlo {
 // factor: [2][n] = 1/denominator and upper coefficient of the Thomas sweep for
 // the natural-spline system on the knots log r (it depends on the grid only).
 // With compute_factor set, thread 0 forms it first (and stores it for later calls).
-__global__ void __launch_bounds__(256) splines_kernel(const double* __restrict__ r, const double* __restrict__ N,
+// One CTA per set (blockIdx.x): row N.at(set), tables at out + set * spline_doubles(n), its own
+// factorisation copy at factor + set * 2n.
+__global__ void __launch_bounds__(256) splines_kernel(const double* __restrict__ r, RowsArg rows,
                                                       int n, int force_positive, double* __restrict__ factor,
                                                       int compute_factor, double* __restrict__ out)
 {
+    const double* __restrict__ N = rows.at(blockIdx.x);
+    factor += (size_t)blockIdx.x * 2 * n;
+    out += (size_t)blockIdx.x * spline_doubles(n);
     extern __shared__ double smem[];
     double* x = smem;             // [n]
     double* y = x + n;            // [2][n]
@@ -113,10 +118,13 @@ __global__ void __launch_bounds__(256) splines_kernel(const double* __restrict__
 }
 
 // Active parents: index > 0 and N <= 0.99999 (bk/evolution.py:501), compacted in
-// index order by a single-CTA ballot scan.
-__global__ void __launch_bounds__(1024) active_kernel(const double* __restrict__ N, int n, int shard, int shards,
+// index order by a ballot scan, one CTA per set (blockIdx.x).
+__global__ void __launch_bounds__(1024) active_kernel(RowsArg rows, int n, int shard, int shards,
                                                       int32_t* __restrict__ active, int32_t* __restrict__ count)
 {
+    const double* __restrict__ N = rows.at(blockIdx.x);
+    active += (size_t)blockIdx.x * n;
+    count += blockIdx.x;
     __shared__ int warp_counts[32];
     __shared__ int base;
     if (threadIdx.x == 0) base = 0;
@@ -155,7 +163,7 @@ __global__ void sobol_draw_kernel(SobolDirsArg dirs, uint64_t offset, uint64_t n
     }
 }
 
-cudaError_t launch_splines(const double* r, const double* N, int n, int force_positive, double* factor,
+cudaError_t launch_splines(const double* r, const RowsArg& N, int n, int sets, int force_positive, double* factor,
                            int compute_factor, double* out, cudaStream_t stream)
 {
     const size_t smem = sizeof(double) * 9 * (size_t)n;
@@ -163,14 +171,14 @@ cudaError_t launch_splines(const double* r, const double* N, int n, int force_po
         cudaError_t e = raise_dynamic_smem((const void*)splines_kernel, smem);
         if (e != cudaSuccess) return e;
     }
-    splines_kernel<<<1, 256, smem, stream>>>(r, N, n, force_positive, factor, compute_factor, out);
+    splines_kernel<<<sets, 256, smem, stream>>>(r, N, n, force_positive, factor, compute_factor, out);
     return cudaGetLastError();
 }
 
-cudaError_t launch_active(const double* N, int n, int shard, int shards, int32_t* active, int32_t* count,
+cudaError_t launch_active(const RowsArg& N, int n, int sets, int shard, int shards, int32_t* active, int32_t* count,
                           cudaStream_t stream)
 {
-    active_kernel<<<1, 1024, 0, stream>>>(N, n, shard, shards, active, count);
+    active_kernel<<<sets, 1024, 0, stream>>>(N, n, shard, shards, active, count);
     return cudaGetLastError();
 }
 

@@ -7,23 +7,29 @@ Monte Carlo budget.  The server
   request needs (evicting least-recently-used resident tables first; a request is never
   admitted past the memory check, and one that cannot fit even on an idle device fails
   with MemoryError);
-* evolves each admitted request's table (``nlo_bk_evolve``) on one of several CUDA streams,
-  so evolutions of requests that arrived at different times run side by side, and keeps
-  evolved N(Y, r) tables resident in an LRU cache keyed by what determines them (parameter
-  set, budget, seed, rapidity range);
+* batches the BK evolutions at the level of rapidity steps: one engine thread advances every
+  in-flight evolution by one step per ``nlo_bk_evolve_sets`` call (one launch per kernel and
+  stage for all of them, each with its own initial row, budget and seed); a request admitted
+  while others are evolving joins at the next step, and one that reaches its rapidity leaves
+  -- the iteration-level batching of a decode loop, applied to the rapidity steps;
+* keeps evolved N(Y, r) tables resident in an LRU cache keyed by what determines them
+  (parameter set, budget, seed, rapidity range); a request whose table is resident or being
+  evolved for an earlier request takes that table;
 * runs the DIS integrals of every request whose table is ready in one batch
   (``structure_functions_many``: all points of all those requests, each with its own table
-  and seed, in the same few launches per term), on its own stream while the next
-  evolutions proceed; requests that become ready during a batch join the next one.
+  and seed, in the same few launches per term), on its own stream while the next rapidity
+  steps proceed; requests that become ready during a batch join the next one.
 
-Each request's integrals are the same computation as when it runs alone; only the CTA
-partition of the merged launches (and so the order of FP64 partial sums) differs, which the
-adaptive grids carry to ~1e-9 relative.  Latency is measured per request from ``submit`` to
-completion; ``stats`` reports p50/p99 and the point throughput.
+Each request's results are the same computation as when it runs alone: its table equals its
+own evolution up to the order of the FP64 sums of the multi-set launches' CTA partials
+(~1e-15), and its integrals differ only by the CTA partition of the merged launches, which
+the adaptive grids carry to ~1e-9 relative.  Latency is measured per request from ``submit``
+to completion; ``stats`` reports p50/p99 and the point throughput.
 """
 
 from __future__ import annotations
 
+import ctypes
 import math
 import queue
 import threading
@@ -35,6 +41,7 @@ from dataclasses import dataclass, field
 import torch
 
 from nlo_bk_optimized_b200 import _native
+from nlo_bk_optimized_b200.bk.batch import DEFAULT_WAVES, MAX_SETS
 from nlo_bk_optimized_b200.bk.config import BKConfig, require_sobol
 from nlo_bk_optimized_b200.bk.initial_conditions import MV
 from nlo_bk_optimized_b200.dipole.amplitude import BKDipole
@@ -147,27 +154,48 @@ def request_table(request: Request, config: BKConfig, device: torch.device, stre
 class _Ready:
     job: _Job
     table: DipoleTable
-    dipole: BKDipole
     cached: bool
+    done: torch.cuda.Event | None  # recorded after the table's last rapidity step
+
+
+@dataclass
+class _Flight:
+    """An evolution in progress: rows [steps+1, R], row `step` the current amplitude."""
+
+    key: tuple
+    jobs: list
+    rows: torch.Tensor
+    y: torch.Tensor
+    x0: float
+    steps: int
+    budget: int
+    dirs: object
+    step: int = 0
 
 
 class Server:
     def __init__(self, bk_config: BKConfig, dis_config: DISConfig, *, device: torch.device | str = "cuda",
-                 slots: int = 64, lanes: int = 8, cache_tables: int = 64, reserve_bytes: int = 1 << 30,
+                 slots: int = 64, waves: int = DEFAULT_WAVES, cache_tables: int = 64, reserve_bytes: int = 1 << 30,
                  sqrt_s: float | None = 318.0):
+        from nlo_bk_optimized_b200.bk.evolution import _r_grid, nlo_box, params_of, precision_of
+
         require_sobol(bk_config, "the request loop")
+        if bk_config.KINEMATICAL_CONSTRAINT:
+            raise NotImplementedError("the request loop evolves without the kinematical constraint")
         self.bk_config = bk_config
         self.dis_config = dis_config
         self.device = torch.device(device)
         if self.device.type != "cuda":
             raise ValueError("the server runs on a CUDA device")
         self.slots = slots
+        self.waves = waves
         self.reserve_bytes = reserve_bytes
         self.sqrt_s = sqrt_s
         self.cache: OrderedDict = OrderedDict()
         self.cache_tables = cache_tables
         self._cache_lock = threading.Lock()
-        self._queue: queue.Queue = queue.Queue()
+        self._queue: queue.Queue = queue.Queue()    # submitted jobs
+        self._joining: queue.Queue = queue.Queue()  # admitted jobs for the engine
         self._free = threading.Semaphore(slots)
         self._inflight = 0
         self._inflight_lock = threading.Lock()
@@ -176,18 +204,27 @@ class Server:
         self._stop = threading.Event()
         self.stats = ServerStats()
         self._stats_lock = threading.Lock()
-        self.batches: list[int] = []  # requests per DIS batch
+        self.batches: list[int] = []     # requests per DIS batch
+        self.step_sets: list[int] = []  # evolutions advanced per engine step
         lib = _native.load()
-        points = bk_config.RPOINTS + 1
-        self._lanes: queue.Queue = queue.Queue()
-        for _ in range(max(1, lanes)):
-            self._lanes.put((torch.cuda.Stream(device=self.device),
-                             torch.empty(int(lib.nlo_bk_rhs_workspace_bytes(points)), dtype=torch.uint8,
-                                         device=self.device)))
+        r_host = _r_grid(bk_config, device="cpu", dtype=torch.float64)
+        self._r_host = r_host
+        self._r = r_host.to(self.device)
+        self._points = r_host.numel()
+        lower, width = nlo_box(float(r_host[0]), float(r_host[-1]))
+        self._box = _native.box(lower, width)
+        self._params = params_of(bk_config, precision_of(bk_config, torch.float32))
+        self._per_call = max(1, min(slots, MAX_SETS))
+        ws = max(int(lib.nlo_bk_sets_workspace_bytes(self._points, n, waves)) for n in range(1, self._per_call + 1))
+        self._workspace = torch.empty(ws, dtype=torch.uint8, device=self.device)
+        self._status = torch.zeros(self._per_call, dtype=torch.int32, device=self.device)
+        self._bk_stream = torch.cuda.Stream(device=self.device)
         self._dis_stream = torch.cuda.Stream(device=self.device)
         self._scheduler = threading.Thread(target=self._schedule, daemon=True)
+        self._engine = threading.Thread(target=self._bk_loop, daemon=True)
         self._batcher = threading.Thread(target=self._dis_loop, daemon=True)
         self._scheduler.start()
+        self._engine.start()
         self._batcher.start()
 
     # ------------------------------------------------------------------ client side
@@ -202,6 +239,7 @@ class Server:
         for _ in range(self.slots):  # every admitted request has finished
             self._free.acquire()
         self._stop.set()
+        self._engine.join()
         with self._ready_cv:
             self._ready_cv.notify_all()
         self._batcher.join()
@@ -209,9 +247,8 @@ class Server:
 
     # ------------------------------------------------------------------ server side
     def _bytes_needed(self, request: Request) -> int:
-        points = self.bk_config.RPOINTS + 1
         steps = int(round(maxy_for(request.points, step=self.bk_config.DE_SOLVER_STEP) / self.bk_config.DE_SOLVER_STEP))
-        table = 8 * (steps + 1) * points
+        table = 8 * (steps + 1) * self._points
         dis = (4 << 20) * max(1, len(request.points))  # the request's share of a merged DIS batch
         return table + dis
 
@@ -250,36 +287,104 @@ class Server:
                         torch.cuda.empty_cache()
                         continue
                 time.sleep(0.005)
-            threading.Thread(target=self._evolve, args=(job,), daemon=True).start()
+            self._joining.put(job)
 
-    def _table(self, request: Request, stream: torch.cuda.Stream, workspace: torch.Tensor) -> tuple[DipoleTable, bool]:
+    def _key(self, request: Request) -> tuple:
         maxy = maxy_for(request.points, step=self.bk_config.DE_SOLVER_STEP)
-        key = (request.qs0sqr, request.gamma, request.ec, request.budget, request.seed, maxy)
+        return (request.qs0sqr, request.gamma, request.ec, request.budget, request.seed, maxy)
+
+    def _ready_add(self, item: _Ready) -> None:
+        with self._ready_cv:
+            self._ready.append(item)
+            self._ready_cv.notify()
+
+    def _join(self, job: _Job, flights: list[_Flight]) -> None:
+        """A newly admitted request: a resident table, a table already being evolved, or a new
+        evolution starting at the next step."""
+        from nlo_bk_optimized_b200.bk.evolution import _steps_to
+
+        request = job.request
+        key = self._key(request)
         with self._cache_lock:
             if key in self.cache:
                 self.cache.move_to_end(key)
-                return self.cache[key], True
-        table = request_table(request, self.bk_config, self.device, stream, workspace)
-        with self._cache_lock:
-            self.cache[key] = table
-            while len(self.cache) > self.cache_tables:
-                self.cache.popitem(last=False)
-        return table, False
+                table, done = self.cache[key]
+                self._ready_add(_Ready(job, table, True, done))
+                return
+        for flight in flights:
+            if flight.key == key:
+                flight.jobs.append(job)
+                return
+        ys = _steps_to(0.0, key[-1], self.bk_config.DE_SOLVER_STEP)
+        ic = MV(qs0sqr=request.qs0sqr, gamma=request.gamma, ec=request.ec)
+        rows = torch.empty((len(ys) + 1, self._points), dtype=torch.float64, device=self.device)
+        rows[0] = ic.dipole_amplitude(self._r_host).to(torch.float64).to(self.device)
+        y = torch.tensor([0.0, *ys], dtype=torch.float64, device=self.device)
+        flights.append(_Flight(key, [job], rows, y, ic.x0, len(ys), int(request.budget),
+                               _native.sobol_dirs(4, request.seed)))
 
-    def _evolve(self, job: _Job) -> None:
-        stream, workspace = self._lanes.get()
-        try:
-            with torch.cuda.device(self.device), torch.cuda.stream(stream):
-                table, cached = self._table(job.request, stream, workspace)
-                dipole = BKDipole(table)
-                stream.synchronize()
-            with self._ready_cv:
-                self._ready.append(_Ready(job, table, dipole, cached))
-                self._ready_cv.notify()
-        except BaseException as exc:  # the error goes to the caller's future
-            self._finish(job, exc)
-        finally:
-            self._lanes.put((stream, workspace))
+    def _step(self, flights: list[_Flight]) -> None:
+        """One rapidity step of every flight (at most MAX_SETS per call) on the engine stream."""
+        lib = _native.load()
+        R = self._points
+        for start in range(0, len(flights), self._per_call):
+            chunk = flights[start:start + self._per_call]
+            n = len(chunk)
+            ptrs = (ctypes.c_void_p * n)(*[f.rows.data_ptr() + 8 * R * f.step for f in chunk])
+            budgets = (ctypes.c_int64 * n)(*[f.budget for f in chunk])
+            dirs = (_native.SobolDirs * n)(*[f.dirs for f in chunk])
+            _native.check(lib.nlo_bk_evolve_sets(self._params, self._r.data_ptr(), R, n, ptrs, 1,
+                                                 float(self.bk_config.DE_SOLVER_STEP),
+                                                 _native.STEPPERS[self.bk_config.stepper], dirs, budgets, self._box,
+                                                 self.waves, self._status.data_ptr(), self._workspace.data_ptr(),
+                                                 self._workspace.numel(), self._bk_stream.cuda_stream))
+        for f in flights:
+            f.step += 1
+
+    def _bk_loop(self) -> None:
+        flights: list[_Flight] = []
+        previous: torch.cuda.Event | None = None
+        with torch.cuda.device(self.device):
+            while True:
+                # admitted requests join before the next step (wait only while nothing evolves)
+                while True:
+                    try:
+                        job = self._joining.get(block=not flights, timeout=0.02)
+                    except queue.Empty:
+                        break
+                    try:
+                        with torch.cuda.stream(self._bk_stream):
+                            self._join(job, flights)
+                    except BaseException as exc:  # the error goes to the caller's future
+                        self._finish(job, exc)
+                if not flights:
+                    if self._stop.is_set() and self._joining.empty():
+                        return
+                    continue
+                try:
+                    self._step(flights)
+                except BaseException as exc:
+                    for f in flights:
+                        for job in f.jobs:
+                            self._finish(job, exc)
+                    flights = []
+                    continue
+                self.step_sets.append(len(flights))
+                done = torch.cuda.Event()
+                done.record(self._bk_stream)
+                for f in [f for f in flights if f.step == f.steps]:
+                    table = DipoleTable(r=self._r, y=f.y, N=f.rows, x0=f.x0)
+                    with self._cache_lock:
+                        self.cache[f.key] = (table, done)
+                        while len(self.cache) > self.cache_tables:
+                            self.cache.popitem(last=False)
+                    for k, job in enumerate(f.jobs):
+                        self._ready_add(_Ready(job, table, k > 0, done))
+                flights = [f for f in flights if f.step < f.steps]
+                # keep at most two steps queued: new requests join within a step
+                if previous is not None:
+                    previous.synchronize()
+                previous = done
 
     def _dis_loop(self) -> None:
         from nlo_bk_optimized_b200.dis.observables import structure_functions_many
@@ -291,14 +396,30 @@ class Server:
                 if not self._ready and self._stop.is_set():
                     return
                 batch, self._ready = self._ready, []
+            good = []
+            with torch.cuda.device(self.device), torch.cuda.stream(self._dis_stream):
+                for item in batch:
+                    if item.done is not None:
+                        item.done.synchronize()
+                    if not bool(torch.isfinite(item.table.N).all()):
+                        self._finish(item.job, FloatingPointError("non-finite BK amplitude"))
+                    else:
+                        good.append(item)
+            batch = good
+            if not batch:
+                continue
             self.batches.append(len(batch))
             Q2, xs, dipoles, seeds, options, owner = [], [], [], [], [], []
             for k, item in enumerate(batch):
                 opts = dis_options_for(item.job.request.budget)
+                # the table was written on the engine stream: keep its memory until this stream is done
+                item.table.N.record_stream(self._dis_stream)
+                item.table.y.record_stream(self._dis_stream)
+                dipole = BKDipole(item.table)
                 for q2, x in item.job.request.points:
                     Q2.append(q2)
                     xs.append(x)
-                    dipoles.append(item.dipole)
+                    dipoles.append(dipole)
                     seeds.append(item.job.request.seed)
                     options.append(opts)
                     owner.append(k)

@@ -933,6 +933,16 @@ def measure_batch(n_sets: int) -> dict:
     torch.cuda.synchronize()
     batched_s = time.perf_counter() - t0
 
+    # the evolution alone (the same multi-set call) and its K2+Kf evaluations: budget x active
+    # parents of each step's row, four right-hand sides a step
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    tables = evolve_batch(N0, r, len(ys), config, budgets, waves=waves)
+    torch.cuda.synchronize()
+    evolve_s = time.perf_counter() - t0
+    active = (tables[:, :-1, 1:] <= 0.99999).sum(dim=2).to(torch.float64)  # [sets, steps]
+    k2kf_evals = float((active.sum(dim=1) * torch.tensor(budgets, dtype=torch.float64, device=device)).sum()) * 4
+
     # the plain path on one set of each budget class
     classes: dict[int, list[int]] = {}
     for k, b in enumerate(budgets):
@@ -989,6 +999,9 @@ def measure_batch(n_sets: int) -> dict:
                                "budgets 2^U{16..20} per r per stage; 8 (Q^2,x) points per set, NLO sigma_r, "
                                "Vegas 4 it x budget/16", "sets": n_sets, "points": n_points, "waves": waves},
         "batched_s": round(batched_s, 3),
+        "evolution_s": round(evolve_s, 3),
+        "evolution_k2kf_evals": k2kf_evals,
+        "evolution_k2kf_evals_per_s": round(k2kf_evals / evolve_s, 1),
         "dis_points_per_s": round(n_points / batched_s, 2),
         "plain_single_point_s": round(plain_points, 2),
         "plain_single_point_per_set_s": {str(b): round(t, 4) for b, t in sorted(per_class_point.items())},
@@ -1073,6 +1086,8 @@ def measure_serve(seconds: float, rate: float, slots: int, waves: int, sample: i
         "p50_s": served["p50_s"],
         "p99_s": served["p99_s"],
         "requests_per_s": served["requests_per_s"],
+        "engine_steps": len(server.step_sets),
+        "mean_evolutions_per_engine_step": round(sum(server.step_sets) / max(1, len(server.step_sets)), 2),
         "dis_batches": len(server.batches),
         "mean_requests_per_dis_batch": round(sum(server.batches) / max(1, len(server.batches)), 2),
         "sequential_points_per_s": round(sequential_pps, 3),

@@ -282,6 +282,12 @@ typedef struct nlo_bk_vegas_options {
                                       max(2, warmup_samples x fraction), none when either is 0 */
     double epsrel;                 /* [0.2] converged after min_iterations once error <= max(epsabs, epsrel |value|) */
     double epsabs;                 /* [0] */
+    int32_t replicas;              /* [6 in the reference's CUDA evolution with kept grids and a seed, else 0]
+                                      replica refinement (bk/evolution.py:411-456): a parent with
+                                      (|K1| + |K2| + |Kf|) / max(|K1 + K2 + Kf|, 0.05 (|K1| + |K2| + |Kf|)) >= 4
+                                      or N > 0.9 gets `replicas` more integrals on fresh grids, Sobol points
+                                      of dirs[1..replicas] (the reference's seeds seed + 1000 k), and takes
+                                      the mean; 0..16 */
 } nlo_bk_vegas_options;
 
 /* Per-parent Vegas state in doubles for a grid of `points` parents: per parent the grid
@@ -297,7 +303,9 @@ size_t nlo_bk_vegas_workspace_bytes(int32_t points, const nlo_bk_vegas_options* 
  * so the shards' rows add up to the whole right-hand side).  hist_y may be NULL without the
  * kinematical constraint; hist_N's last row is the amplitude.  state: device
  * double[nlo_bk_vegas_state_doubles(points, bins)], read and updated.  k2kf (optional)
- * receives the Vegas value of each parent (the combined estimate of its iterations). */
+ * receives the Vegas value of each parent (the combined estimate of its iterations, or the
+ * replica mean of a refined parent).  dirs: host array of 1 + options->replicas direction
+ * sets, dirs[0] the main integrals', dirs[k] replica k's. */
 int nlo_bk_rhs_vegas(const nlo_bk_params* params, const double* r, int32_t points, const double* hist_y,
                      const double* hist_N, int32_t rows, int32_t shard, int32_t shards,
                      const nlo_bk_vegas_options* options, const nlo_sobol_dirs* dirs, const nlo_bk_box* box,

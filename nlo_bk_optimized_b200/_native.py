@@ -127,6 +127,7 @@ class BKVegasOptions(ctypes.Structure):
         ("reuse_warmup_fraction", ctypes.c_double),
         ("epsrel", ctypes.c_double),
         ("epsabs", ctypes.c_double),
+        ("replicas", ctypes.c_int32),
     ]
 
 

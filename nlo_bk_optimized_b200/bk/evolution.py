@@ -110,6 +110,27 @@ def vegas_options_of(config: BKConfig) -> _native.BKVegasOptions | None:
     return o
 
 
+VEGAS_REPLICAS = 6  # bk/evolution.py:437: replicas 1..6 with seeds seed + 1000 k
+
+
+def vegas_evolution_setup(config: BKConfig, seed: int | None):
+    """Options and direction sets of an evolution with K2+Kf by Vegas: the replica refinement of
+    bk/evolution.py:411-456 runs where the reference's evolution keeps per-parent grids
+    (VEGAS_REUSE_GRID) and a seed is given -- 6 more integrals on fresh grids with the seeds
+    seed + 1000 k for a parent whose K1 and K2, Kf cancel strongly or whose N exceeds 0.9.  The
+    reference does this on its CUDA float32 path; both builds here do it, so that the all-FP64
+    build checks the mixed one.  Returns (options, dirs array of 1 + replicas), or (None, dirs)
+    for the QMC integrator."""
+    base = 0 if seed is None else int(seed)
+    opts = vegas_options_of(config)
+    replicas = VEGAS_REPLICAS if (opts is not None and seed is not None and opts.reuse_grid) else 0
+    if opts is not None:
+        opts.replicas = replicas
+    dirs = (_native.SobolDirs * (1 + replicas))(*[_native.sobol_dirs(4, base + 1000 * k)
+                                                   for k in range(1 + replicas)])
+    return opts, dirs
+
+
 def vegas_state(device: torch.device, points: int) -> torch.Tensor:
     """A zero-filled per-parent Vegas state (no grids yet) for one evolution."""
     lib = _native.load()
@@ -270,9 +291,9 @@ def _evolve_rows(
     status = torch.zeros(1, dtype=torch.int32, device=device)
     params = params_of(config, precision)
     lower, width = nlo_box(float(r64[0]), float(r64[-1]))
-    dirs = _native.sobol_dirs(4, 0 if seed is None else seed)
     box = _native.box(lower, width)
-    opts = vegas_options_of(config)
+    opts, dirs_all = vegas_evolution_setup(config, seed)
+    dirs = dirs_all[0]
     ws = workspace(device, points, opts)
     lib = _native.load()
     if opts is not None:
@@ -291,7 +312,7 @@ def _evolve_rows(
             _native.check(
                 lib.nlo_bk_evolve_vegas(
                     params, r64.data_ptr(), points, y.data_ptr() if kc else None, before, steps,
-                    float(config.DE_SOLVER_STEP), _native.STEPPERS[config.stepper], opts, dirs, box,
+                    float(config.DE_SOLVER_STEP), _native.STEPPERS[config.stepper], opts, dirs_all, box,
                     grids.data_ptr(), table.data_ptr(), status.data_ptr(), ws.data_ptr(), ws.numel(),
                     _native.stream_handle(device),
                 )
@@ -429,4 +450,4 @@ def compute_dndy(
 
 
 __all__ = ["DNDYResult", "bk_steps", "compute_dndy", "evolve_table", "nlo_box", "rhs", "solve_bk",
-           "vegas_options_of", "vegas_state"]
+           "vegas_evolution_setup", "vegas_options_of", "vegas_state"]

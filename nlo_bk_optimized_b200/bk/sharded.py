@@ -124,7 +124,7 @@ def solve_bk_sharded(initial_condition, maxy: float, config: BKConfig = BKConfig
         nlo_box,
         params_of,
         precision_of,
-        vegas_options_of,
+        vegas_evolution_setup,
         workspace,
     )
 
@@ -140,8 +140,8 @@ def solve_bk_sharded(initial_condition, maxy: float, config: BKConfig = BKConfig
     points = r.numel()
     lower, width = nlo_box(float(r_host[0]), float(r_host[-1]))
     box = _native.box(lower, width)
-    dirs = _native.sobol_dirs(4, seed)
-    ws = workspace(device, points, vegas_options_of(config))
+    vegas, dirs_all = vegas_evolution_setup(config, seed)
+    ws = workspace(device, points, vegas)
     status = torch.zeros(1, dtype=torch.int32, device=device)
     stream = _native.stream_handle(device)
     ys = _steps_to(0.0, maxy, config.DE_SOLVER_STEP)
@@ -150,8 +150,8 @@ def solve_bk_sharded(initial_condition, maxy: float, config: BKConfig = BKConfig
 
     if config.KINEMATICAL_CONSTRAINT:
         raise ValueError("the sharded evolution has no kinematical constraint (it reads no amplitude history)")
-    sharded = ShardedRhs(params, r, dirs, int(config.MCINTPOINTS), box, rank, world, ws, status, stream,
-                         vegas=vegas_options_of(config))
+    sharded = ShardedRhs(params, r, dirs_all if vegas is not None else dirs_all[0], int(config.MCINTPOINTS), box,
+                         rank, world, ws, status, stream, vegas=vegas)
 
     def all_reduce(k: torch.Tensor) -> None:
         if world > 1:

@@ -201,6 +201,10 @@ int run_rhs(const nlo_bk_params& p, const double* r, const double* N, int points
         k2kf_factor = nlo_samples ? 1.0 / (double)nlo_samples : 0.0;
     }
     if (beside && (e = cudaStreamWaitEvent(stream, side->join, 0)) != cudaSuccess) return cuda_fail(e, "join");
+    // the replica refinement reads this right-hand side's K1
+    if (vegas && order_has_nlo(p.order) && vegas->options.replicas > 0 &&
+        (e = launch_k2kf_vegas_refine(p, r, N, points, b.spline, box, *vegas, b.k1, b.k2kf, stream)) != cudaSuccess)
+        return cuda_fail(e, "k2kf vegas replicas");
     if ((e = launch_assemble(b.k1, b.k2kf, points, k2kf_factor, dndy, k2kf_out, stream)) != cudaSuccess)
         return cuda_fail(e, "assemble");
     if (k1_out) {
@@ -613,6 +617,7 @@ static bool check_vegas(const nlo_bk_vegas_options* o, std::string& why)
         return false;
     }
     if (!(o->epsrel >= 0.0) || !(o->epsabs >= 0.0)) { why = "epsrel and epsabs must be non-negative"; return false; }
+    if (o->replicas < 0 || o->replicas > 16) { why = "replicas must be 0..16"; return false; }
     if (o->warmup_samples + (int64_t)o->max_iterations * o->samples_per_iteration > (int64_t(1) << 30)) {
         why = "the Vegas rounds of one right-hand side exceed 2^30 Sobol points";
         return false;
@@ -627,11 +632,27 @@ size_t nlo_bk_vegas_workspace_bytes(int32_t points, const nlo_bk_vegas_options* 
     return nlo_bk_rhs_workspace_bytes(points) + align_up(bk_vegas_scratch_bytes(points, options->bins));
 }
 
-// The Vegas buffers at the end of the workspace (after the right-hand side and stage rows).
-static BkVegasCall vegas_call(void* workspace, int points, const nlo_bk_vegas_options* options, double* state)
+// The Vegas buffers at the end of the workspace (after the right-hand side and stage rows);
+// the replicas' direction sets stay in `replica_dirs` for the call.
+static BkVegasCall vegas_call(void* workspace, int points, const nlo_bk_vegas_options* options, double* state,
+                              const nlo_sobol_dirs* dirs, std::vector<SobolDirsArg>& replica_dirs)
 {
     char* scratch = static_cast<char*>(workspace) + nlo_bk_rhs_workspace_bytes(points);
-    return bk_vegas_carve(scratch, points, *options, state);
+    BkVegasCall call = bk_vegas_carve(scratch, points, *options, state);
+    replica_dirs.clear();
+    for (int k = 0; k < options->replicas; ++k) replica_dirs.push_back(to_arg(dirs + 1 + k));
+    call.replica_dirs = replica_dirs.data();
+    return call;
+}
+
+static bool check_vegas_dirs(const nlo_sobol_dirs* dirs, const nlo_bk_vegas_options* o, std::string& why)
+{
+    for (int k = 0; k <= o->replicas; ++k)
+        if (!check_dirs(dirs + k, 4, why)) {
+            why = "dirs[" + std::to_string(k) + "]: " + why;
+            return false;
+        }
+    return true;
 }
 
 int nlo_bk_rhs_vegas(const nlo_bk_params* params, const double* r, int32_t points, const double* hist_y,
@@ -652,8 +673,10 @@ int nlo_bk_rhs_vegas(const nlo_bk_params* params, const double* r, int32_t point
     if (!r || !hist_N || !dndy || !box || !state) return fail(NLO_ERR_INVALID, "NULL buffer");
     if (!workspace || workspace_bytes < nlo_bk_vegas_workspace_bytes(points, options))
         return fail(NLO_ERR_WORKSPACE, "workspace too small for nlo_bk_rhs_vegas");
+    if (!check_vegas_dirs(dirs, options, why)) return fail(NLO_ERR_INVALID, why);
     const RhsBuffers b = carve(workspace, points);
-    const BkVegasCall call = vegas_call(workspace, points, options, state);
+    std::vector<SobolDirsArg> replica_dirs;
+    const BkVegasCall call = vegas_call(workspace, points, options, state, dirs, replica_dirs);
     const double* N = hist_N + (size_t)(rows - 1) * points;
     const SideStream side;
     return run_rhs(*params, r, N, points, to_arg(dirs), (uint64_t)options->samples_per_iteration, *box, dndy, k1, k2kf,
@@ -671,7 +694,10 @@ int nlo_bk_evolve_vegas(const nlo_bk_params* params, const double* r, int32_t po
     if (points < 3 || points > 4096) return fail(NLO_ERR_INVALID, "points must be 3..4096");
     if (!workspace || workspace_bytes < nlo_bk_vegas_workspace_bytes(points, options))
         return fail(NLO_ERR_WORKSPACE, "workspace too small for nlo_bk_evolve_vegas");
-    const BkVegasCall call = vegas_call(workspace, points, options, state);
+    if (!dirs) return fail(NLO_ERR_INVALID, "dirs is NULL");
+    if (!check_vegas_dirs(dirs, options, why)) return fail(NLO_ERR_INVALID, why);
+    std::vector<SobolDirsArg> replica_dirs;
+    const BkVegasCall call = vegas_call(workspace, points, options, state, dirs, replica_dirs);
     return evolve_rows(params, r, points, y, first, steps, step, stepper, dirs, options->samples_per_iteration, box,
                        table, status, workspace, workspace_bytes, stream, &call);
 }

@@ -148,6 +148,9 @@ struct BkVegasCall {
     double* partial = nullptr;  // [points][blocks][4 + 4 bins]
     double* reduced = nullptr;  // [points][4 + 4 bins]
     int32_t* counts = nullptr;  // [points][4 bins]
+    double* replica_state = nullptr;  // [points][stride], the replicas' fresh grids
+    double* replica_acc = nullptr;    // [points][3], the replica refinement's sums
+    const SobolDirsArg* replica_dirs = nullptr;  // [options.replicas]
 };
 size_t bk_vegas_state_doubles(int bins);
 int bk_vegas_blocks_per_job(int points);
@@ -158,6 +161,12 @@ BkVegasCall bk_vegas_carve(void* scratch, int points, const nlo_bk_vegas_options
 cudaError_t launch_k2kf_vegas(const nlo_bk_params& p, const double* r, const double* N, int points,
                               const double* spline, int shard, int shards, const SobolDirsArg& dirs,
                               const nlo_bk_box& box, const BkVegasCall& call, double* out, cudaStream_t stream);
+// The replica refinement of the parents launch_k2kf_vegas integrated (options.replicas > 0):
+// reads their K1 (k1[points]) and the amplitude row N, rewrites out[points][3] of the
+// refined parents.
+cudaError_t launch_k2kf_vegas_refine(const nlo_bk_params& p, const double* r, const double* N, int points,
+                                     const double* spline, const nlo_bk_box& box, const BkVegasCall& call,
+                                     const double* k1, double* out, cudaStream_t stream);
 // Fixed-order sum of per-CTA partial rows [jobs][blocks][keys] over the CTAs (dis.cu).
 cudaError_t vegas_launch_reduce(const double* partial, int keys, int blocks_per_job, int jobs, double* reduced,
                                 cudaStream_t stream);

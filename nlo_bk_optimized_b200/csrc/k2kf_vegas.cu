@@ -48,6 +48,9 @@ enum BkSlot {
     kBkCompKf = 14,   // sum over iterations of weight x Kf estimate
 };
 
+// Per-parent accumulators of the replica refinement: [selected, sum of values, sum of error^2].
+constexpr int kRepStride = 3;
+
 __device__ __forceinline__ bool parent_active(const double* N, int i, int shard, int shards)
 {
     return i > 0 && N[i] <= 0.99999 && i % shards == shard;
@@ -55,14 +58,15 @@ __device__ __forceinline__ bool parent_active(const double* N, int i, int shard,
 
 // Per parent: mark whether it is integrated, reset the per-call sums, and either start a
 // uniform grid with the full warm-up or keep the stored grid with the reuse warm-up.
+// select (replica rounds): the parents to integrate are those with select[i * kRepStride] != 0.
 __global__ void begin_kernel(const double* __restrict__ N, int points, int shard, int shards, double* state,
                              int stride, int bins, int reuse, uint64_t warmup, uint64_t reuse_warmup,
-                             int32_t* __restrict__ counts)
+                             int32_t* __restrict__ counts, const double* __restrict__ select)
 {
     const int i = blockIdx.x;
     double* st = state + (size_t)i * stride;
     double* sc = st + kDims * (bins + 1);
-    const bool on = parent_active(N, i, shard, shards);
+    const bool on = select ? select[(size_t)i * kRepStride] != 0.0 : parent_active(N, i, shard, shards);
     __syncthreads();
     const bool fresh = !reuse || sc[kBkHasGrid] == 0.0;
     if (on) {
@@ -289,6 +293,57 @@ __global__ void end_kernel(const double* state, int stride, int bins, int points
     out[3 * i + 2] = on ? sc[kStError] * sc[kStError] : 0.0;
 }
 
+// Replica refinement of bk/evolution.py:411-456 (the reference's CUDA mixed evolution with
+// per-parent grids): a parent whose K1 and combined K2, Kf estimates cancel strongly,
+// (|K1| + |K2| + |Kf|) / max(|K1 + K2 + Kf|, 0.05 (|K1| + |K2| + |Kf|)) >= 4, or whose
+// amplitude exceeds 0.9, gets `replicas` more Vegas integrals on fresh grids with the seeds
+// seed + 1000 k, and its K2+Kf becomes the mean of all of them, with the error
+// sqrt(sum error^2) / (replicas + 1).  The parent's own grid is kept.
+__global__ void replica_select_kernel(const double* __restrict__ N, const double* __restrict__ k1, int points,
+                                      const double* __restrict__ state, int stride, int bins,
+                                      double* __restrict__ acc)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= points) return;
+    const double* sc = state + (size_t)i * stride + kDims * (bins + 1);
+    double* a = acc + (size_t)i * kRepStride;
+    a[0] = 0.0;
+    if (sc[kBkActive] == 0.0 || !(sc[kStSumWeights] > 0.0)) return;
+    const double c2 = sc[kBkCompK2] / sc[kStSumWeights];
+    const double cf = sc[kBkCompKf] / sc[kStSumWeights];
+    const double scale = ::fabs(k1[i]) + ::fabs(c2) + ::fabs(cf);
+    const double net = ::fabs(k1[i] + c2 + cf);
+    const double condition = scale / (net > 0.05 * scale ? net : 0.05 * scale);
+    if (condition >= 4.0 || N[i] > 0.9) {
+        a[0] = 1.0;
+        a[1] = sc[kStValue];
+        a[2] = sc[kStError] * sc[kStError];
+    }
+}
+
+__global__ void replica_add_kernel(const double* __restrict__ state, int stride, int bins, int points,
+                                   double* __restrict__ acc)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= points) return;
+    double* a = acc + (size_t)i * kRepStride;
+    if (a[0] == 0.0) return;
+    const double* sc = state + (size_t)i * stride + kDims * (bins + 1);
+    a[1] += sc[kStValue];
+    a[2] += sc[kStError] * sc[kStError];
+}
+
+__global__ void replica_end_kernel(const double* __restrict__ acc, int points, int replicas, double* __restrict__ out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= points) return;
+    const double* a = acc + (size_t)i * kRepStride;
+    if (a[0] == 0.0) return;
+    const double m = (double)(replicas + 1);
+    out[3 * i + 0] = a[1] / m;
+    out[3 * i + 2] = a[2] / (m * m);
+}
+
 template <typename T, bool SYM>
 cudaError_t launch_round(const nlo_bk_params& p, const double* r, int points, const double* spline,
                          const SobolDirsArg& dirs, const nlo_bk_box& box, const BkVegasCall& call, int warmup,
@@ -314,6 +369,40 @@ cudaError_t launch_round(const nlo_bk_params& p, const double* r, int points, co
     return cudaGetLastError();
 }
 
+// The warm-up round (when `with_warmup`) and the iterations of one Vegas call over the
+// parents that `call.state` marks active.
+cudaError_t run_rounds(const nlo_bk_params& p, const double* r, int points, const double* spline,
+                       const SobolDirsArg& dirs, const nlo_bk_box& box, const BkVegasCall& call, bool with_warmup,
+                       cudaStream_t stream)
+{
+    const nlo_bk_vegas_options& o = call.options;
+    const bool fp64 = p.precision == NLO_PRECISION_FP64;
+    const bool sym = p.symmetrize != 0;
+    const int keys = 4 + kDims * o.bins;
+    const size_t fsmem = sizeof(double) * (kDims * o.bins + 2 * kDims * (o.bins + 1));
+    cudaError_t e = raise_dynamic_smem((const void*)finalize_kernel, fsmem);
+    if (e != cudaSuccess) return e;
+    const int rounds = o.max_iterations + (with_warmup ? 1 : 0);
+    for (int k = 0; k < rounds; ++k) {
+        const int is_warmup = with_warmup && k == 0;
+        if (fp64)
+            e = sym ? launch_round<double, true>(p, r, points, spline, dirs, box, call, is_warmup, stream)
+                    : launch_round<double, false>(p, r, points, spline, dirs, box, call, is_warmup, stream);
+        else
+            e = sym ? launch_round<float, true>(p, r, points, spline, dirs, box, call, is_warmup, stream)
+                    : launch_round<float, false>(p, r, points, spline, dirs, box, call, is_warmup, stream);
+        if (e != cudaSuccess) return e;
+        if ((e = vegas_launch_reduce(call.partial, keys, call.blocks_per_job, points, call.reduced, stream)) !=
+            cudaSuccess)
+            return e;
+        finalize_kernel<<<points, 128, fsmem, stream>>>(call.state, call.stride, o.bins, is_warmup,
+                                                        (uint64_t)o.samples_per_iteration, call.reduced, call.counts,
+                                                        o.min_iterations, o.epsrel, o.epsabs);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 }  // namespace
 
 size_t bk_vegas_state_doubles(int bins) { return (size_t)kDims * (bins + 1) + kStSlots; }
@@ -332,8 +421,9 @@ size_t bk_vegas_scratch_bytes(int points, int bins)
 {
     const size_t keys = 4 + (size_t)kDims * bins;
     const size_t blocks = (size_t)bk_vegas_blocks_per_job(points);
+    // round partials and sums, bin counts, then the replica grids and accumulators
     return sizeof(double) * keys * (size_t)points * (blocks + 1) + sizeof(int32_t) * (size_t)kDims * bins * points +
-           256;
+           256 + sizeof(double) * (bk_vegas_state_doubles(bins) + kRepStride) * (size_t)points + 256;
 }
 
 BkVegasCall bk_vegas_carve(void* scratch, int points, const nlo_bk_vegas_options& options, double* state)
@@ -348,6 +438,9 @@ BkVegasCall bk_vegas_carve(void* scratch, int points, const nlo_bk_vegas_options
     c.partial = reinterpret_cast<double*>(base);
     c.reduced = c.partial + keys * (size_t)points * (size_t)c.blocks_per_job;
     c.counts = reinterpret_cast<int32_t*>(c.reduced + keys * (size_t)points);
+    const size_t after = reinterpret_cast<size_t>(c.counts + (size_t)kDims * options.bins * points);
+    c.replica_state = reinterpret_cast<double*>((after + 255) & ~(size_t)255);
+    c.replica_acc = c.replica_state + bk_vegas_state_doubles(options.bins) * (size_t)points;
     return c;
 }
 
@@ -365,34 +458,41 @@ cudaError_t launch_k2kf_vegas(const nlo_bk_params& p, const double* r, const dou
         if (reuse_warmup < 2) reuse_warmup = 2;
     }
     begin_kernel<<<points, 64, 0, stream>>>(N, points, shard, shards, call.state, call.stride, o.bins,
-                                             o.reuse_grid ? 1 : 0, warmup, reuse_warmup, call.counts);
+                                             o.reuse_grid ? 1 : 0, warmup, reuse_warmup, call.counts, nullptr);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    const bool fp64 = p.precision == NLO_PRECISION_FP64;
-    const bool sym = p.symmetrize != 0;
-    const int keys = 4 + kDims * o.bins;
-    const size_t fsmem = sizeof(double) * (kDims * o.bins + 2 * kDims * (o.bins + 1));
-    e = raise_dynamic_smem((const void*)finalize_kernel, fsmem);
-    if (e != cudaSuccess) return e;
-    const int rounds = o.max_iterations + ((warmup > 0 || reuse_warmup > 0) ? 1 : 0);
-    for (int k = 0; k < rounds; ++k) {
-        const int is_warmup = (warmup > 0 || reuse_warmup > 0) && k == 0;
-        if (fp64)
-            e = sym ? launch_round<double, true>(p, r, points, spline, dirs, box, call, is_warmup, stream)
-                    : launch_round<double, false>(p, r, points, spline, dirs, box, call, is_warmup, stream);
-        else
-            e = sym ? launch_round<float, true>(p, r, points, spline, dirs, box, call, is_warmup, stream)
-                    : launch_round<float, false>(p, r, points, spline, dirs, box, call, is_warmup, stream);
-        if (e != cudaSuccess) return e;
-        if ((e = vegas_launch_reduce(call.partial, keys, call.blocks_per_job, points, call.reduced, stream)) !=
-            cudaSuccess)
-            return e;
-        finalize_kernel<<<points, 128, fsmem, stream>>>(call.state, call.stride, o.bins, is_warmup,
-                                                        (uint64_t)o.samples_per_iteration, call.reduced, call.counts,
-                                                        o.min_iterations, o.epsrel, o.epsabs);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    }
+    if ((e = run_rounds(p, r, points, spline, dirs, box, call, warmup > 0 || reuse_warmup > 0, stream)) !=
+        cudaSuccess)
+        return e;
     end_kernel<<<(points + 255) / 256, 256, 0, stream>>>(call.state, call.stride, o.bins, points, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_k2kf_vegas_refine(const nlo_bk_params& p, const double* r, const double* N, int points,
+                                     const double* spline, const nlo_bk_box& box, const BkVegasCall& call,
+                                     const double* k1, double* out, cudaStream_t stream)
+{
+    const nlo_bk_vegas_options& o = call.options;
+    if (o.replicas <= 0) return cudaSuccess;
+    const int threads = 128, blocks = (points + threads - 1) / threads;
+    replica_select_kernel<<<blocks, threads, 0, stream>>>(N, k1, points, call.state, call.stride, o.bins,
+                                                          call.replica_acc);
+    cudaError_t e = cudaGetLastError();
+    // each replica: a fresh grid with the full warm-up (the reference's new VegasState)
+    BkVegasCall rep = call;
+    rep.state = call.replica_state;
+    const uint64_t warmup = (uint64_t)o.warmup_samples;
+    for (int k = 0; k < o.replicas && e == cudaSuccess; ++k) {
+        begin_kernel<<<points, 64, 0, stream>>>(N, points, 0, 1, rep.state, rep.stride, o.bins, 0, warmup, 0,
+                                                 rep.counts, call.replica_acc);
+        if ((e = cudaGetLastError()) != cudaSuccess) break;
+        if ((e = run_rounds(p, r, points, spline, call.replica_dirs[k], box, rep, warmup > 0, stream)) != cudaSuccess)
+            break;
+        replica_add_kernel<<<blocks, threads, 0, stream>>>(rep.state, rep.stride, o.bins, points, call.replica_acc);
+        e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) return e;
+    replica_end_kernel<<<blocks, threads, 0, stream>>>(call.replica_acc, points, o.replicas, out);
     return cudaGetLastError();
 }
 

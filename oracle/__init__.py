@@ -525,10 +525,18 @@ def vegas_k2kf(r: float, sspline: Spline, phys: Physics, box: tuple[np.ndarray, 
 
 def derivative_vegas(N: np.ndarray, r: np.ndarray, phys: Physics, seed: int, *, samples: int,
                      grids: dict[int, VegasGrid] | None = None, reuse_warmup_fraction: float = 0.25,
-                     f32_points: bool = False, force_positive: bool = True, **options) -> dict:
+                     f32_points: bool = False, force_positive: bool = True, replicas: int = 0,
+                     **options) -> dict:
     """dN/dY with K2+Kf by Vegas per active parent (_derivative_components with
     IntegrationMethod.VEGAS, bk/evolution.py:354-424): `grids` keyed by grid index are the
-    per-parent states carried between calls (None: fresh grids, as without vegas_states)."""
+    per-parent states carried between calls (None: fresh grids, as without vegas_states).
+
+    replicas > 0 (with `grids`): the replica refinement of bk/evolution.py:411-456 -- a parent
+    whose condition (|K1| + |K2| + |Kf|) / max(|K1 + K2 + Kf|, 0.05 (|K1| + |K2| + |Kf|)), with
+    the combined K2 and Kf estimates of its integral, is at least 4, or whose N exceeds 0.9,
+    gets `replicas` more integrals on fresh grids with the seeds seed + 1000 k; its K2+Kf is
+    the mean of all of them (added in the order main, replica 1, 2, ...), its components the
+    mean, its error sqrt(sum error^2) / (replicas + 1); its grid stays the main integral's."""
     nspl = loglog_spline(r, N, 0, force_positive)
     sspl = loglog_spline(r, N, 1, force_positive)
     active = np.nonzero((np.arange(r.size) > 0) & (N <= 0.99999))[0]
@@ -547,6 +555,29 @@ def derivative_vegas(N: np.ndarray, r: np.ndarray, phys: Physics, seed: int, *, 
                                  f32_points=f32_points, **options)
                 K2Kf[i] = res.value
                 results[int(i)] = res
+            if replicas > 0 and grids is not None:
+                warm = max(2, samples // 5)
+                for i in active:
+                    comp = grids[int(i)].last_components
+                    if comp is None:
+                        continue
+                    scale = abs(K1[i]) + abs(comp[0]) + abs(comp[1])
+                    net = K1[i] + comp[0] + comp[1]
+                    condition = scale / max(abs(net), 0.05 * scale)
+                    if not (condition >= 4.0 or N[i] > 0.9):
+                        continue
+                    total, err2 = K2Kf[i], grids[int(i)].last_error ** 2
+                    comps = [comp]
+                    for k in range(1, replicas + 1):
+                        rep = VegasGrid()
+                        res = vegas_k2kf(float(r[i]), sspl, phys, box, seed + 1000 * k, samples=samples, warmup=warm,
+                                         state=rep, f32_points=f32_points, **options)
+                        total += res.value
+                        err2 += res.error ** 2
+                        comps.append(rep.last_components)
+                    K2Kf[i] = total / (replicas + 1)
+                    grids[int(i)].last_components = np.mean(np.stack(comps), axis=0)
+                    grids[int(i)].last_error = math.sqrt(err2) / (replicas + 1)
     dNdy = K1 + K2Kf
     return {"dNdy": np.where(np.isfinite(dNdy), dNdy, 0.0), "K1": K1, "K2Kf": K2Kf, "vegas": results}
 

@@ -51,8 +51,11 @@ def main() -> None:
     original = evolution._evolve_derivative
 
     def counted(*args, **kwargs):
+        out = original(*args, **kwargs)
         calls["n"] += 1
-        return original(*args, **kwargs)
+        # progress on stderr: a run stopped early still gives the time per derivative
+        print(f"derivative {calls['n']} done at {time.perf_counter() - t0:.1f} s", file=sys.stderr, flush=True)
+        return out
 
     evolution._evolve_derivative = counted
     config = BKConfig()

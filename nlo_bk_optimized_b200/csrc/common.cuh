@@ -75,8 +75,6 @@ struct M<float> {
     }
     static __device__ __forceinline__ float sin(float x) { return sinf(x); }
     static __device__ __forceinline__ float cos(float x) { return cosf(x); }
-    static __device__ __forceinline__ float j1(float x) { return j1f(x); }
-    static __device__ __forceinline__ float i1(float x) { return cyl_bessel_i1f(x); }
     static __device__ __forceinline__ float fmin(float a, float b) { return fminf(a, b); }
     static __device__ __forceinline__ float fmax(float a, float b) { return fmaxf(a, b); }
     static __device__ __forceinline__ float fabs(float a) { return fabsf(a); }
@@ -100,8 +98,6 @@ struct M<double> {
     static __device__ __forceinline__ double sqrt(double x) { return ::sqrt(x); }
     static __device__ __forceinline__ double sin(double x) { return ::sin(x); }
     static __device__ __forceinline__ double cos(double x) { return ::cos(x); }
-    static __device__ __forceinline__ double j1(double x) { return ::j1(x); }
-    static __device__ __forceinline__ double i1(double x) { return ::cyl_bessel_i1(x); }
     static __device__ __forceinline__ double fmin(double a, double b) { return ::fmin(a, b); }
     static __device__ __forceinline__ double fmax(double a, double b) { return ::fmax(a, b); }
     static __device__ __forceinline__ double fabs(double a) { return ::fabs(a); }

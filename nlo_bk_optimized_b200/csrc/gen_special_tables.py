@@ -16,6 +16,15 @@ as the ground truth; nothing is taken from another library's tables.
   ('t Hooft & Veltman, Nucl. Phys. B153 (1979) 365), after the standard reflection and
   inversion identities have brought x into [-1, 1/2].
 
+* The double-log resummation factor of the BK kernel, J1(2 sqrt(-v))/sqrt(-v) for v < 0 and
+  I1(2 sqrt(v))/sqrt(v) for v > 0, is one entire function G(v) = sum_k v^k / (k! (k+1)!).
+  FP32 tables, t = 2 sqrt|v|, s = 4/t:
+  - |v| <= 4: G = 1 + v q(v), q a least-squares polynomial (absolute error where |G| < 1,
+    relative above);
+  - v < -4: the modulus-phase form J1(t) = M1(t) cos(theta1(t)) (A&S 9.2.17), with
+    M1 sqrt(pi t / 2) = m(s) and theta1 - (t - 3 pi/4) = d(s) least-squares polynomials in s;
+  - v > 4: I1(t) = e^t / sqrt(2 pi t) h(s), h a least-squares polynomial in s (relative).
+
 Run: python nlo_bk_optimized_b200/csrc/gen_special_tables.py  (writes special_tables.cuh
 next to this file).
 """
@@ -83,6 +92,58 @@ def poly_fit(nu: int, degree: int):
     return [coeffs[j] for j in range(degree + 1)]
 
 
+DLA_T0 = 4  # t = 2 sqrt|v| where the polynomial hands over to the asymptotic forms
+DLA_POLY_DEGREE = 8  # q(v)
+DLA_J_DEGREE = 6     # m(s), d(s)
+DLA_I_DEGREE = 8     # h(s)
+
+
+def dla_g(v):
+    v = mp.mpf(v)
+    if v == 0:
+        return mp.mpf(1)
+    t = 2 * mp.sqrt(abs(v))
+    return 2 * (mp.besselj(1, t) if v < 0 else mp.besseli(1, t)) / t
+
+
+def least_squares(xs, targets, basis, weights, degree: int):
+    A = mp.matrix(len(xs), degree + 1)
+    b = mp.matrix(len(xs), 1)
+    for i, (x, f, w) in enumerate(zip(xs, targets, weights)):
+        for j in range(degree + 1):
+            A[i, j] = basis(x, j) * w
+        b[i] = f * w
+    coeffs = mp.lu_solve(A.T * A, A.T * b)
+    return [coeffs[j] for j in range(degree + 1)]
+
+
+def cheb_nodes(a, b, m: int):
+    return [a + (b - a) * (mp.cos(mp.pi * (k + mp.mpf(1) / 2) / m) + 1) / 2 for k in range(m)]
+
+
+def dla_tables():
+    v0 = mp.mpf(DLA_T0) ** 2 / 4
+    vs = cheb_nodes(-v0, v0, 8 * (DLA_POLY_DEGREE + 1))
+    gs = [dla_g(v) for v in vs]
+    q = least_squares(vs, [g - 1 for g in gs], lambda v, j: v ** (j + 1), [1 / max(1, abs(g)) for g in gs],
+                      DLA_POLY_DEGREE)
+    ss = cheb_nodes(mp.mpf(0), mp.mpf(1), 8 * (DLA_I_DEGREE + 1))
+
+    def modulus_phase(s):
+        t = DLA_T0 / s
+        j, y = mp.besselj(1, t), mp.bessely(1, t)
+        d = mp.atan2(y, j) - (t - 3 * mp.pi / 4)
+        return mp.sqrt(j * j + y * y) * mp.sqrt(mp.pi * t / 2), d - 2 * mp.pi * mp.nint(d / (2 * mp.pi))
+
+    mdv = [modulus_phase(s) for s in ss]
+    power = lambda s, j: s**j  # noqa: E731
+    m = least_squares(ss, [x[0] for x in mdv], power, [1] * len(ss), DLA_J_DEGREE)
+    d = least_squares(ss, [x[1] for x in mdv], power, [1] * len(ss), DLA_J_DEGREE)
+    hv = [mp.besseli(1, DLA_T0 / s) * mp.sqrt(2 * mp.pi * DLA_T0 / s) * mp.exp(-DLA_T0 / s) for s in ss]
+    h = least_squares(ss, hv, power, [1 / x for x in hv], DLA_I_DEGREE)
+    return q, m, d, h
+
+
 def bernoulli_tables(terms: int):
     # Li2 = u - u^2/4 + sum_{n>=1} B_{2n} u^{2n+1} / (2n+1)!
     return [mp.bernoulli(2 * n) / mp.factorial(2 * n + 1) for n in range(1, terms + 1)]
@@ -127,6 +188,10 @@ def main() -> None:
             fmt(bernoulli_tables(BERNOULLI_TERMS_F64)), "};"]
     out += [f"__device__ constexpr float kLi2BernoulliF[{BERNOULLI_TERMS_F32}] = {{",
             fmt(bernoulli_tables(BERNOULLI_TERMS_F32), "f"), "};"]
+    q, m, d, h = dla_tables()
+    out += ["", f"constexpr float kDlaT0 = {DLA_T0}.0f;"]
+    for name, table in (("kDlaPolyF", q), ("kDlaModF", m), ("kDlaPhaseF", d), ("kDlaExpF", h)):
+        out += [f"__device__ constexpr float {name}[{len(table)}] = {{", fmt(table, "f"), "};"]
     out += ["", "}  // namespace nlo_special", ""]
     Path(__file__).with_name("special_tables.cuh").write_text("\n".join(out))
 

@@ -17,6 +17,7 @@
 
 #include "common.cuh"
 #include "internal.h"
+#include "special_tables.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -142,6 +143,71 @@ __device__ __forceinline__ T kc_history_amplitude(const SplineView<T>& s, const 
     return v < (T)0 ? (T)0 : (v > (T)1 ? (T)1 : v);
 }
 
+// The double-log resummation factor of Kernel_lo (k1.py:109-119): with
+// x = 4 log(X/r) log(Y/r) and abar = alpha Nc / pi it is J1(2 sqrt(abar x))/sqrt(abar x) for
+// x > 0 and I1(2 sqrt(abar |x|))/sqrt(abar |x|) for x < 0, i.e. G(v) at v = -abar x of the
+// entire function G(v) = sum_k v^k / (k! (k+1)!) -- one function of one signed argument, so
+// the two Bessel branches need no separate evaluation.  FP32: tables of
+// gen_special_tables.py (mpmath fits) -- a polynomial for |v| <= 4, the modulus-phase form
+// of J1 for v < -4 (one cosine after a Cody-Waite reduction of t = 2 sqrt|v| by a 2 pi split
+// into an exact 8-bit part and the rest), e^t h(4/t) / sqrt(2 pi t) for v > 4 with e^t formed
+// as two factors e^(t/2) so that only a value beyond the FP32 range overflows.  Error against
+// G at the same FP32 t: 6e-7 of the envelope of G.
+__device__ __forceinline__ float dla_factor(float v)
+{
+    using namespace nlo_special;
+    const float av = fabsf(v);
+    if (av <= 0.25f * kDlaT0 * kDlaT0) {
+        float q = kDlaPolyF[8];
+#pragma unroll
+        for (int j = 7; j >= 0; --j) q = fmaf(q, v, kDlaPolyF[j]);
+        return fmaf(v, q, 1.0f);
+    }
+    const float t = 2.0f * M<float>::sqrt(av);
+    const float s = __fdividef(kDlaT0, t);
+    const float srt = s * rsqrtf(t);  // 4 t^(-3/2)
+    if (v < 0.0f) {
+        float m = kDlaModF[6], d = kDlaPhaseF[6];
+#pragma unroll
+        for (int j = 5; j >= 0; --j) {
+            m = fmaf(m, s, kDlaModF[j]);
+            d = fmaf(d, s, kDlaPhaseF[j]);
+        }
+        // phase t - 3 pi/4 + d reduced to about [-pi, pi]: t - k (6.28125 + 2 pi - 6.28125)
+        const float k = rintf(fmaf(t, 0.15915494309189535f, -0.375f));
+        float rr = fmaf(-k, 6.28125f, t);  // exact: k 6.28125 has few bits and rr is representable
+        rr = fmaf(-k, 1.9353071795864769e-3f, rr);
+        rr = (rr - 2.3561944901923449f) + d;
+        // 2 sqrt(2 / (pi t)) / t = sqrt(2 / pi) / 2 x 4 t^(-3/2)
+        return (0.39894228040143268f * m) * srt * __cosf(rr);
+    }
+    float h = kDlaExpF[8];
+#pragma unroll
+    for (int j = 7; j >= 0; --j) h = fmaf(h, s, kDlaExpF[j]);
+    const float half = __expf(0.5f * t);
+    // 2 e^t / (t sqrt(2 pi t)) = 1 / (2 sqrt(2 pi)) x 4 t^(-3/2) x e^t
+    return ((0.19947114020071634f * h) * srt * half) * half;
+}
+
+template <typename T>
+__device__ __forceinline__ T dla_resum(T abar, T xarg);
+
+template <>
+__device__ __forceinline__ float dla_resum<float>(float abar, float xarg)
+{
+    return dla_factor(-abar * xarg);
+}
+
+// FP64: the Bessel functions themselves
+template <>
+__device__ __forceinline__ double dla_resum<double>(double abar, double xarg)
+{
+    const double as_x = ::sqrt(abar * ::fabs(xarg));
+    if (as_x == 0.0) return 1.0;
+    const double bes = xarg >= 0.0 ? ::j1(2.0 * as_x) : ::cyl_bessel_i1(2.0 * as_x);
+    return bes / as_x;
+}
+
 // Kernel_lo x dipole at one (z, theta) node; sh2 = sin^2(theta/2).  The form of
 // Kernel_lo follows RC_LO (k1.py:37-94); orders without resummation stop at the bare
 // kernel (k1.py:97-98); the resummation coupling follows RESUM_RC (k1.py:100-107).
@@ -243,12 +309,7 @@ __device__ __forceinline__ T k1_point(const SplineView<T>& s, const K1Parent<T>&
                             : (ph.resum_rc == NLO_RESUM_RC_FIXED ? ph.fixed_as : alpha_min);
     const T xarg = (T)4 * dX * Z.dY;
     const T abar = alpha_res * ph.nc * (T)(1.0 / kPi);
-    const T as_x = M<T>::sqrt(abar * M<T>::fabs(xarg));
-    T dlog = (T)1;
-    if (as_x != (T)0) {
-        const T bes = xarg >= (T)0 ? M<T>::j1((T)2 * as_x) : M<T>::i1((T)2 * as_x);
-        dlog = M<T>::div(bes, as_x);
-    }
+    T dlog = dla_resum<T>(abar, xarg);
     if (!(r > (T)1.01 * ph.minr)) dlog = (T)1;
     if (!M<T>::finite(dlog)) return (T)0;
     // single-log resummation (k1.py:121-132): exp(-abar A1 |log(ksub (r/minxy)^2)|) and its
@@ -345,13 +406,8 @@ __device__ __forceinline__ f2 k1_pair_point(const SplineView<float>& s, const K1
                                  : (ph.resum_rc == NLO_RESUM_RC_FIXED ? bc2(ph.fixed_as) : alpha_min);
         const f2 xarg = mul2(bc2(4.0f * Z.dY), dX);
         const f2 abar = mul2(alpha_res, bc2(ph.nc * (float)(1.0 / kPi)));
-        const f2 as2 = mul2(abar, make_float2(fabsf(xarg.x), fabsf(xarg.y)));
-        const f2 as_x = make_float2(M<float>::sqrt(as2.x), M<float>::sqrt(as2.y));
-        f2 dlog = bc2(1.0f);
-        if (as_x.x != 0.0f)
-            dlog.x = __fdividef(xarg.x >= 0.0f ? j1f(2.0f * as_x.x) : cyl_bessel_i1f(2.0f * as_x.x), as_x.x);
-        if (as_x.y != 0.0f)
-            dlog.y = __fdividef(xarg.y >= 0.0f ? j1f(2.0f * as_x.y) : cyl_bessel_i1f(2.0f * as_x.y), as_x.y);
+        const f2 v = mul2(abar, make_float2(-xarg.x, -xarg.y));
+        f2 dlog = make_float2(dla_factor(v.x), dla_factor(v.y));
         if (!(r > 1.01f * ph.minr)) dlog = bc2(1.0f);
         // single-log resummation (k1.py:121-132)
         f2 slog = bc2(1.0f), slog_exp = bc2(0.0f);

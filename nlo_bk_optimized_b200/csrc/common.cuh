@@ -203,9 +203,11 @@ __device__ __forceinline__ T alpha_of_log(T log_d, const Phys<T>& ph)
 // ---------------------------------------------------------------------------
 // Log-log spline in shared memory: knots x[n] (log r), coefficients (a,b,c,d) per interval.
 // The r grid is logarithmically uniform, so the interval is found in O(1) from
-// (lx - x0)/h with a one-step fix-up against the stored knots; the result is the
-// interval that searchsorted(x, lx, right=True) - 1 (clamped) would return
-// (numerics/interpolation.py:70-76).
+// (lx - x0)/h.  FP64: a one-step fix-up against the stored knots gives the interval that
+// searchsorted(x, lx, right=True) - 1 (clamped) would return (numerics/interpolation.py:70-76).
+// FP32: the guess alone; it differs only within the FP32 rounding of lx from a knot, where
+// the neighbouring piece is evaluated that far outside its interval -- the pieces join with
+// continuous second derivatives, so the values agree to far below FP32 resolution.
 template <typename T>
 struct SplineView {
     const T* x;     // [n]
@@ -222,8 +224,10 @@ __device__ __forceinline__ int spline_interval(const SplineView<T>& s, T lx)
 {
     int i = floor_to_int((lx - s.x0) * s.inv_h);
     i = i < 0 ? 0 : (i > s.n - 2 ? s.n - 2 : i);
-    if (i > 0 && lx < s.x[i]) --i;
-    if (i < s.n - 2 && lx >= s.x[i + 1]) ++i;
+    if constexpr (sizeof(T) == sizeof(double)) {
+        if (i > 0 && lx < s.x[i]) --i;
+        if (i < s.n - 2 && lx >= s.x[i + 1]) ++i;
+    }
     return i;
 }
 

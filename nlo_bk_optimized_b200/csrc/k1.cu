@@ -339,23 +339,31 @@ __device__ __forceinline__ f2 k1_pair_point(const SplineView<float>& s, const K1
     if (!ok_x && !ok_y) return bc2(0.0f);
     const f2 xr2 = fma2(bc2(4.0f * Z.rho), sh2, bc2((1.0f - Z.rho) * (1.0f - Z.rho)));
     const f2 dX = mul2(bc2(0.5f), make_float2(__logf(xr2.x), __logf(xr2.y)));
-    const f2 alpha_X = make_float2(alpha_of_log(P.lr_abs + dX.x, ph), alpha_of_log(P.lr_abs + dX.y, ph));
     // X^2 - Y^2 = r (r - 2 z cos theta), cos theta = 1 - 2 sin^2(theta/2)
     const f2 XmY = mul2(bc2(r), fma2(bc2(-2.0f * z), fma2(bc2(-2.0f), sh2, bc2(1.0f)), bc2(r)));
     const f2 aY = bc2(Z.alpha_Y);
-    f2 dalpha;
+    // alpha_X, dalpha = alpha_Y - alpha_X and ratio = dalpha / (alpha_X alpha_Y)
+    f2 alpha_X, dalpha, ratio;
     if (ph.fixed) {
-        dalpha = bc2(0.0f);
+        alpha_X = bc2(ph.fixed_as);
+        dalpha = ratio = bc2(0.0f);
     } else if (ph.alpha_cap > 0.0f || ph.thresholds) {
+        alpha_X = make_float2(alpha_of_log(P.lr_abs + dX.x, ph), alpha_of_log(P.lr_abs + dX.y, ph));
         dalpha = sub2(aY, alpha_X);
+        ratio = make_float2(__fdividef(dalpha.x, alpha_X.x * Z.alpha_Y), __fdividef(dalpha.y, alpha_X.y * Z.alpha_Y));
     } else {
-        // alpha_Y - alpha_X = alpha_X alpha_Y b0 c (lae_X - lae_Y)
+        // smooth coupling, 1/alpha = b0 c lae: 1/alpha_X - 1/alpha_Y = b0 c (lae_X - lae_Y) = ratio,
+        // with lae_X - lae_Y from log1p/expm1 of the exact X^2 - Y^2 (no cancellation); so
+        // alpha_X = 1/(1/alpha_Y + ratio) and dalpha = alpha_X alpha_Y ratio
         const f2 delta = mul2(bc2(-5.0f), log1p_2(mul2(XmY, bc2(Z.inv_Ysq))));
         const f2 v = mul2(bc2(Z.sigma), expm1_2(delta));
         f2 shift = log1p_2(v);
         if (v.x <= -0.5f) shift.x = logf(Z.sigma_c + Z.sigma * __expf(delta.x));
         if (v.y <= -0.5f) shift.y = logf(Z.sigma_c + Z.sigma * __expf(delta.y));
-        dalpha = mul2(mul2(alpha_X, aY), mul2(bc2(ph.b0c), shift));
+        ratio = mul2(bc2(ph.b0c), shift);
+        const f2 inv_aX = add2(bc2(__fdividef(1.0f, Z.alpha_Y)), ratio);
+        alpha_X = make_float2(__fdividef(1.0f, inv_aX.x), __fdividef(1.0f, inv_aX.y));
+        dalpha = mul2(mul2(alpha_X, aY), ratio);
     }
     const f2 inv_XY = make_float2(__fdividef(1.0f, Xsq.x * Z.Ysq), __fdividef(1.0f, Xsq.y * Z.Ysq));
     const float pref = ph.nc * (float)(1.0 / (2.0 * kPi * kPi));
@@ -372,8 +380,7 @@ __device__ __forceinline__ f2 k1_pair_point(const SplineView<float>& s, const K1
         lo = mul2(mul2(bc2(pref), alpha_min), r2iXY);
     } else if (ph.rc_lo == NLO_RC_LO_FAC) {
         alpha_sc = bc2(P.alpha_r);
-        const f2 q = make_float2(__fdividef(dalpha.x, alpha_X.x * Z.alpha_Y), __fdividef(dalpha.y, alpha_X.y * Z.alpha_Y));
-        const f2 den = sub2(bc2(__fdividef(1.0f, P.alpha_r)), mul2(mul2(XmY, bc2(__fdividef(1.0f, P.r2))), q));
+        const f2 den = sub2(bc2(__fdividef(1.0f, P.alpha_r)), mul2(mul2(XmY, bc2(__fdividef(1.0f, P.r2))), ratio));
         lo = mul2(mul2(bc2(pref), r2iXY), make_float2(__fdividef(1.0f, den.x), __fdividef(1.0f, den.y)));
     } else if (ph.rc_lo == NLO_RC_LO_BEUF) {
         const f2 log_reff = fma2(mul2(bc2(-0.5f * __fdividef(1.0f, P.r2)), XmY), log1p_2(mul2(XmY, bc2(Z.inv_Ysq))),
@@ -383,9 +390,9 @@ __device__ __forceinline__ f2 k1_pair_point(const SplineView<float>& s, const K1
     } else {
         // Balitsky: r^2/(X^2Y^2) + (aY/aX - 1)/Y^2 + (aX/aY - 1)/X^2
         alpha_sc = bc2(P.alpha_r);
+        // = (r^2 + dalpha (alpha_Y (X^2 - Y^2) + Y^2 dalpha) / (alpha_X alpha_Y)) / (X^2 Y^2)
         const f2 num = fma2(aY, XmY, mul2(bc2(Z.Ysq), dalpha));
-        const f2 frac = make_float2(__fdividef(num.x, alpha_X.x * Z.alpha_Y), __fdividef(num.y, alpha_X.y * Z.alpha_Y));
-        const f2 bracket = mul2(fma2(dalpha, frac, bc2(P.r2)), inv_XY);
+        const f2 bracket = mul2(fma2(ratio, num, bc2(P.r2)), inv_XY);
         lo = mul2(bc2(pref * P.alpha_r), bracket);
     }
     lo = make_float2(isfinite(lo.x) ? lo.x : 0.0f, isfinite(lo.y) ? lo.y : 0.0f);

@@ -163,10 +163,15 @@ __device__ __forceinline__ void k2_pair_fast(const FastSpline& s, const Phys<flo
     fast_amplitude_pair(s, uX, vXx, vXy);
     fast_amplitude_pair(s, uX2, vX2x, vX2y);
     // kernels
+    // log(a/b)/(a - b) = 2 (1 + hm1)/(a + b), hm1 = atanh(t)/t - 1, t = (a - b)/(a + b): the series
+    // in t^2 where |a - b| < (a + b)/2, else log(a/b) directly; each case needs one reciprocal,
+    // of a + b or of a - b, and the test needs none
     const f2 a = mul2(Xsq, z2sq), b = mul2(X2sq, zsq);
-    const f2 rs = rcp2(add2(a, b));
-    const f2 d = mul2(r, fma2(r, P1, make_float2(-P2.x, -P2.y)));
-    const f2 t = mul2(d, rs);
+    const f2 sab = add2(a, b);
+    const f2 d = mul2(r, fma2(r, P1, make_float2(-P2.x, -P2.y)));  // a - b
+    const bool ser_x = fabsf(d.x) < 0.5f * sab.x, ser_y = fabsf(d.y) < 0.5f * sab.y;
+    const f2 rden = rcp2(sel2(ser_x, ser_y, sab, d));
+    const f2 t = mul2(d, rden);
     const f2 t2 = mul2(t, t);
     f2 g = fma2(bc2(0.15609439065092748f), t2, bc2(0.04106302733766397f));
     g = fma2(g, t2, bc2(0.09747851219255123f));
@@ -176,10 +181,11 @@ __device__ __forceinline__ void k2_pair_fast(const FastSpline& s, const Phys<flo
     g = fma2(g, t2, bc2(0.33333333435159396f));
     const f2 hm1_series = mul2(g, t2);
     const f2 Ld = fma2(bc2(LN2), sub2(L2X, L2X2), Dl);  // log(a/b)
-    const f2 hm1_log = fma2(Ld, mul2(bc2(0.5f), rcp2(t)), bc2(-1.0f));
-    const f2 hm1 = sel2(t2.x < 0.25f, t2.y < 0.25f, hm1_series, hm1_log);
-    const f2 rs2 = add2(rs, rs);
-    const f2 L = fma2(hm1, rs2, rs2);
+    // log case: 1 + hm1 = log(a/b) (a + b) / (2 (a - b)) and L = log(a/b) / (a - b)
+    const f2 Lr = mul2(Ld, rden);
+    const f2 hm1 = sel2(ser_x, ser_y, hm1_series, fma2(mul2(bc2(0.5f), Lr), sab, bc2(-1.0f)));
+    const f2 rs2 = add2(rden, rden);
+    const f2 L = sel2(ser_x, ser_y, fma2(hm1, rs2, rs2), Lr);
     const f2 r2Lq = mul2(mul2(bc2(P.r2), L), q);
     const f2 fq2 = mul2(add2(hm1, hm1), mul2(q, q));
     const f2 C0 = fma2(bc2(-4.0f), r2Lq, fq2);

@@ -21,7 +21,7 @@ from collections.abc import Sequence
 import torch
 
 from nlo_bk_optimized_b200 import _native
-from nlo_bk_optimized_b200.bk.config import BKConfig, require_sobol
+from nlo_bk_optimized_b200.bk.config import BKConfig, require_fixed_step, require_sobol
 from nlo_bk_optimized_b200.dipole.table import DipoleTable
 
 WAVE_CHOICES = (1, 2, 4, 8, 16)
@@ -37,6 +37,7 @@ def evolve_batch(N0: torch.Tensor, r: torch.Tensor, steps: int, config: BKConfig
     from nlo_bk_optimized_b200.bk.evolution import nlo_box, params_of, precision_of
 
     require_sobol(config, "the batched evolution")
+    require_fixed_step(config, "the batched evolution")
     if config.KINEMATICAL_CONSTRAINT:
         raise NotImplementedError("the kinematical constraint is not available for the batched evolution")
     device = r.device

@@ -13,8 +13,11 @@ so that user code constructs it unchanged.  Additions for the B200 path:
   headline benchmark uses.  MISER and MULTIPLE are accepted by the dataclass and rejected
   by the device path.
 * ``STEPPER`` -- "rk3" (the default: the reference's Kutta RK3 of its CUDA production
-  path, bk/evolution.py:190-236), "rk4" (classical) or "euler"; ``EULER_METHOD=True``
-  selects "euler".
+  path, bk/evolution.py:190-236), "rk4" (classical), "euler", or "rk2_adaptive" (the
+  reference's adaptive midpoint stepper with step doubling, its stepper off the CUDA float32
+  path, bk/evolution.py:239-326, with DE_SOLVER_ABSERR / DE_SOLVER_RELERR; driven from the
+  host, one error read per attempt; not for the batched, sharded or served evolutions);
+  ``EULER_METHOD=True`` selects "euler".
 * ``PRECISION`` -- "mixed" (FP32 integrands, FP64 sums/splines/RK update) or
   "fp64"; ``None`` picks "mixed" for float32 tables and "fp64" otherwise.
 * ``ALPHA_S_CAP`` -- if positive, alpha_s = min(alpha_s, ALPHA_S_CAP)
@@ -81,7 +84,7 @@ class BKOrder(Enum):
         return self in {BKOrder.LO_RESUM_DLOG_SLOG, BKOrder.NLO_RESUM_DLOG_SLOG}
 
 
-STEPPERS = ("rk3", "rk4", "euler")
+STEPPERS = ("rk3", "rk4", "euler", "rk2_adaptive")
 PRECISIONS = ("mixed", "fp64")
 
 
@@ -178,6 +181,13 @@ def require_sobol(config: BKConfig, what: str) -> None:
     if config.Order.has_nlo_kernels and config.INTMETHOD_NLO is not IntegrationMethod.SOBOL:
         raise ValueError(f"{what} integrates K2+Kf with IntegrationMethod.SOBOL (its budgets are Sobol point "
                          f"counts); got {config.INTMETHOD_NLO.name}")
+
+
+def require_fixed_step(config: BKConfig, what: str) -> None:
+    """The batched, sharded and served evolutions advance every row by fixed steps on the
+    device; the adaptive stepper's accept/retry decisions are per evolution on the host."""
+    if config.stepper == "rk2_adaptive":
+        raise ValueError(f"{what} takes the fixed-step steppers (rk3, rk4, euler), not rk2_adaptive")
 
 
 ORDER_CODES = {

@@ -13,6 +13,7 @@ one _bk_steps run (bk/evolution.py:85-100).
 
 from __future__ import annotations
 
+import ctypes
 import math
 from collections.abc import Iterator
 from dataclasses import dataclass
@@ -270,6 +271,78 @@ def rhs(
     return dndy, k1, k2kf
 
 
+class AdaptiveRK2:
+    """The adaptive RK2 stepper of the reference (_adaptive_rk2_to, bk/evolution.py:239-326;
+    its stepper off the CUDA float32 path) over the device right-hand side: a midpoint step
+    of size h against two of size h/2, the error |two halves - one step|/3 against
+    DE_SOLVER_ABSERR + DE_SOLVER_RELERR |two halves|, accepted when the largest ratio is at
+    most 1 -- h then grows by min(5, 0.9 ratio^(-1/3)), by 5 for a zero error -- else retried
+    with h shrunk by max(0.1, 0.9 ratio^(-1/3)).  ``h`` carries over from one output step to
+    the next.  Each attempt reads its error ratio back to the host; the stage combinations
+    run in nlo_bk_stage.  A retried attempt reuses the right-hand side at its starting row,
+    which does not change with h (same row, same points)."""
+
+    def __init__(self, config: BKConfig, r64: torch.Tensor, seed: int | None, precision: int):
+        self.config, self.r64, self.seed, self.precision = config, r64, seed, precision
+        self.h = float(config.DE_SOLVER_STEP)
+        self.eps = float(torch.finfo(torch.float32 if precision == _native.PRECISION_MIXED else torch.float64).eps)
+        self.lib = _native.load()
+        self.stream = _native.stream_handle(r64.device)
+
+    def _f(self, N: torch.Tensor) -> torch.Tensor:
+        return rhs(N, self.r64, self.config, seed=self.seed, precision=self.precision)[0]
+
+    def _stage(self, N: torch.Tensor, k: torch.Tensor, c: float) -> torch.Tensor:
+        out = torch.empty_like(N)
+        kp = (ctypes.c_void_p * 1)(k.data_ptr())
+        cf = (ctypes.c_double * 1)(c)
+        _native.check(self.lib.nlo_bk_stage(N.data_ptr(), kp, cf, 1, N.numel(), 0, out.data_ptr(), None,
+                                            self.stream))
+        return out
+
+    def advance(self, N: torch.Tensor, y: float, nexty: float) -> tuple[torch.Tensor, float]:
+        """(N, y) at the end of the accepted steps from y to nexty."""
+        cfg = self.config
+        k1 = None
+        with torch.cuda.device(self.r64.device):
+            while y < nexty:
+                step = min(self.h, nexty - y)
+                if k1 is None:
+                    k1 = self._f(N)
+                full = self._stage(N, self._f(self._stage(N, k1, 0.5 * step)), step)
+                half_step = step / 2
+                half = self._stage(N, self._f(self._stage(N, k1, 0.5 * half_step)), half_step)
+                k1h = self._f(half)
+                two = self._stage(half, self._f(self._stage(half, k1h, 0.5 * half_step)), half_step)
+                error = torch.abs(two - full) / 3
+                tolerance = cfg.DE_SOLVER_ABSERR + cfg.DE_SOLVER_RELERR * torch.abs(two)
+                ratio = float(torch.max(error / tolerance).item())
+                if ratio <= 1:
+                    N = two
+                    y += step
+                    k1 = None
+                    self.h = step * (5.0 if ratio == 0 else min(5.0, 0.9 * ratio ** (-1 / 3)))
+                else:
+                    self.h = step * max(0.1, 0.9 * ratio ** (-1 / 3))
+                    if self.h <= self.eps * max(1.0, abs(y)):
+                        raise RuntimeError(f"BK RK2 step underflow at y={y}")
+        return N, y
+
+    def rows(self, N0: torch.Tensor, steps: int) -> torch.Tensor:
+        """Rows [steps+1, R] of output steps of DE_SOLVER_STEP from N0 (clamped to [0, 1] after
+        each when FORCE_POSITIVE_N; a non-finite row raises FloatingPointError)."""
+        rows = [N0]
+        N, y = N0, 0.0
+        for _ in range(steps):
+            N, y = self.advance(N, y, y + float(self.config.DE_SOLVER_STEP))
+            if self.config.FORCE_POSITIVE_N:
+                N = N.clamp(0.0, 1.0)
+            if not bool(torch.isfinite(N).all()):
+                raise FloatingPointError(f"non-finite BK amplitude after rapidity step y={y}")
+            rows.append(N)
+        return torch.stack(rows)
+
+
 def _evolve_rows(
     N0: torch.Tensor,
     r64: torch.Tensor,
@@ -287,6 +360,8 @@ def _evolve_rows(
     rapidities of history, N0 and every new row.  ``vegas_grids`` (IntegrationMethod.VEGAS)
     holds the parents' grids; a fresh buffer is used when it is None."""
     device = r64.device
+    if config.stepper == "rk2_adaptive":
+        return AdaptiveRK2(config, r64, seed, precision).rows(N0.to(torch.float64), steps)
     points = r64.numel()
     status = torch.zeros(1, dtype=torch.int32, device=device)
     params = params_of(config, precision)
@@ -415,6 +490,22 @@ def bk_steps(table: DipoleTable, maxy: float, config: BKConfig = BKConfig(), *,
     the Vegas grids of the parents carry over from step to step as in the reference."""
 
     current = table
+    if config.stepper == "rk2_adaptive":  # one stepper for the whole generator: h carries over
+        device = _cuda_device(table.r.device)
+        stepper = AdaptiveRK2(config, table.r.to(torch.float64), seed, precision_of(config, table.r.dtype))
+        N, y0 = current.N[-1].to(torch.float64), float(current.y[-1].item())
+        for y in _steps_to(y0, maxy, config.DE_SOLVER_STEP):
+            N, _ = stepper.advance(N, y0, y)
+            y0 = y
+            if config.FORCE_POSITIVE_N:
+                N = N.clamp(0.0, 1.0)
+            if not bool(torch.isfinite(N).all()):
+                raise FloatingPointError(f"non-finite BK amplitude after rapidity step y={y}")
+            current = DipoleTable(r=current.r, y=torch.cat((current.y, torch.tensor([y], dtype=current.y.dtype,
+                                                                                    device=device))),
+                                  N=torch.cat((current.N, N.to(current.N.dtype).unsqueeze(0)), dim=0), x0=current.x0)
+            yield current
+        return
     grids = vegas_state(_cuda_device(table.r.device), table.r.numel()) \
         if config.INTMETHOD_NLO is IntegrationMethod.VEGAS else None
     for y in _steps_to(float(table.y[-1].item()), maxy, config.DE_SOLVER_STEP):
@@ -449,5 +540,5 @@ def compute_dndy(
                       N=N[keep].to(dtype))
 
 
-__all__ = ["DNDYResult", "bk_steps", "compute_dndy", "evolve_table", "nlo_box", "rhs", "solve_bk",
+__all__ = ["AdaptiveRK2", "DNDYResult", "bk_steps", "compute_dndy", "evolve_table", "nlo_box", "rhs", "solve_bk",
            "vegas_evolution_setup", "vegas_options_of", "vegas_state"]

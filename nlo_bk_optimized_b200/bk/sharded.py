@@ -25,7 +25,7 @@ from collections.abc import Callable
 import torch
 
 from nlo_bk_optimized_b200 import _native
-from nlo_bk_optimized_b200.bk.config import BKConfig
+from nlo_bk_optimized_b200.bk.config import BKConfig, require_fixed_step
 from nlo_bk_optimized_b200.dipole.table import DipoleTable
 
 Rhs = Callable[[torch.Tensor], torch.Tensor]
@@ -150,6 +150,7 @@ def solve_bk_sharded(initial_condition, maxy: float, config: BKConfig = BKConfig
 
     if config.KINEMATICAL_CONSTRAINT:
         raise ValueError("the sharded evolution has no kinematical constraint (it reads no amplitude history)")
+    require_fixed_step(config, "the sharded evolution")
     sharded = ShardedRhs(params, r, dirs_all if vegas is not None else dirs_all[0], int(config.MCINTPOINTS), box,
                          rank, world, ws, status, stream, vegas=vegas)
 

@@ -42,7 +42,7 @@ import torch
 
 from nlo_bk_optimized_b200 import _native
 from nlo_bk_optimized_b200.bk.batch import DEFAULT_WAVES, MAX_SETS
-from nlo_bk_optimized_b200.bk.config import BKConfig, require_sobol
+from nlo_bk_optimized_b200.bk.config import BKConfig, require_fixed_step, require_sobol
 from nlo_bk_optimized_b200.bk.initial_conditions import MV
 from nlo_bk_optimized_b200.dipole.amplitude import BKDipole
 from nlo_bk_optimized_b200.dipole.table import DipoleTable
@@ -180,6 +180,7 @@ class Server:
         from nlo_bk_optimized_b200.bk.evolution import _r_grid, nlo_box, params_of, precision_of
 
         require_sobol(bk_config, "the request loop")
+        require_fixed_step(bk_config, "the request loop")
         if bk_config.KINEMATICAL_CONSTRAINT:
             raise NotImplementedError("the request loop evolves without the kinematical constraint")
         self.bk_config = bk_config
@@ -455,6 +456,7 @@ def run_alone(request: Request, bk_config: BKConfig, dis_config: DISConfig, *, d
     from nlo_bk_optimized_b200.dis.observables import structure_functions
 
     require_sobol(bk_config, "the request loop")
+    require_fixed_step(bk_config, "the request loop")
     device = torch.device(device)
     submitted = time.perf_counter()
     lib = _native.load()

@@ -583,14 +583,23 @@ def derivative_vegas(N: np.ndarray, r: np.ndarray, phys: Physics, seed: int, *, 
 
 
 def evolve(N0: np.ndarray, r: np.ndarray, phys: Physics, points: np.ndarray, map_f32: bool, step: float,
-           maxy: float, stepper: str = "rk4", force_positive: bool = True, kinematical_constraint: bool = False):
+           maxy: float, stepper: str = "rk4", force_positive: bool = True, kinematical_constraint: bool = False,
+           abserr: float = 1e-6, relerr: float = 1e-4, eps: float = float(np.finfo(np.float64).eps)):
     """Rapidity stepping (bk/evolution.py:85-159); returns (y[steps+1], N[steps+1, R]).
-    With the kinematical constraint (Euler only) each step's K1 reads the rows so far."""
+    With the kinematical constraint (Euler only) each step's K1 reads the rows so far.
+
+    stepper "rk2_adaptive": _adaptive_rk2_to (bk/evolution.py:239-326) inside every output
+    step -- a midpoint step of size h against two of size h/2, error |two halves - one|/3
+    against abserr + relerr |two halves|; accepted when the largest ratio is at most 1 (h then
+    grows by min(5, 0.9 ratio^(-1/3)), by 5 for a zero error), else retried with h shrunk by
+    max(0.1, 0.9 ratio^(-1/3)); h carries over from one output step to the next, and the
+    row's rapidity is the sum of the accepted steps."""
 
     ys = [0.0]
     Ns = [np.array(N0, dtype=np.float64)]
     N = Ns[0].copy()
     y = 0.0
+    h_adaptive = step
     if kinematical_constraint and stepper != "euler":
         raise ValueError("the kinematical constraint requires the Euler stepper")
 
@@ -613,9 +622,30 @@ def evolve(N0: np.ndarray, r: np.ndarray, phys: Physics, points: np.ndarray, map
             k3 = f(N + 0.5 * h * k2)
             k4 = f(N + h * k3)
             N = N + h * (k1 + 2.0 * k2 + 2.0 * k3 + k4) / 6.0
+        elif stepper == "rk2_adaptive":
+            nexty = y + step
+            while y < nexty:
+                st = min(h_adaptive, nexty - y)
+                k1 = f(N)
+                full = N + st * f(N + 0.5 * st * k1)
+                hs = st / 2
+                half = N + hs * f(N + 0.5 * hs * k1)
+                k1h = f(half)
+                two = half + hs * f(half + 0.5 * hs * k1h)
+                error = np.abs(two - full) / 3
+                ratio = float(np.max(error / (abserr + relerr * np.abs(two))))
+                if ratio <= 1:
+                    N = two
+                    y += st
+                    h_adaptive = st * (5.0 if ratio == 0 else min(5.0, 0.9 * ratio ** (-1 / 3)))
+                else:
+                    h_adaptive = st * max(0.1, 0.9 * ratio ** (-1 / 3))
+                    if h_adaptive <= eps * max(1.0, abs(y)):
+                        raise RuntimeError(f"BK RK2 step underflow at y={y}")
         else:
             raise ValueError(stepper)
-        y = y + step
+        if stepper != "rk2_adaptive":
+            y = y + step
         if force_positive:
             N = np.clip(N, 0.0, 1.0)
         if not np.all(np.isfinite(N)):

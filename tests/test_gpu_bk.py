@@ -188,6 +188,30 @@ def test_one_step_each_stepper(stepper):
     np.testing.assert_allclose(got[-1], ref[-1], rtol=1e-10, atol=1e-300)
 
 
+@pytest.mark.parametrize("tolerances", [(1e-6, 1e-4), (1e-10, 1e-7)])
+def test_adaptive_rk2_matches_oracle(tolerances):
+    """The reference's adaptive RK2 (step doubling) over two output steps, FP64 build against
+    the oracle's restatement: the default DE_SOLVER_ABSERR / RELERR, and tolerances tight
+    enough that attempts are rejected and h shrinks."""
+    abserr, relerr = tolerances
+    config, r, N = _setup(rpoints=49, MCINTPOINTS=1024, DE_SOLVER_STEP=0.2, STEPPER="rk2_adaptive",
+                          PRECISION="fp64", DE_SOLVER_ABSERR=abserr, DE_SOLVER_RELERR=relerr)
+    table = solve_bk(MV(qs0sqr=0.2), 0.4, config, device=DEVICE, dtype=torch.float64, seed=0)
+    rn, Nn = r.cpu().numpy(), N.cpu().numpy()
+    _, ref = oracle.evolve(Nn, rn, oracle.physics(config), _sobol_points(1024, 0, False), False, 0.2, 0.4,
+                           stepper="rk2_adaptive", abserr=abserr, relerr=relerr)
+    got = table.N.cpu().numpy()
+    assert got.shape == ref.shape == (3, rn.size)
+    np.testing.assert_allclose(got, ref, rtol=1e-10, atol=1e-300)
+    # bk_steps keeps h from one output step to the next, as the reference's generator does
+    from nlo_bk_optimized_b200.bk.evolution import bk_steps
+    from nlo_bk_optimized_b200.dipole.table import DipoleTable
+
+    start = DipoleTable(r=r, y=torch.zeros(1, dtype=torch.float64, device=DEVICE), N=N.unsqueeze(0), x0=0.01)
+    last = list(bk_steps(start, 0.4, config, seed=0))[-1]
+    np.testing.assert_allclose(last.N.cpu().numpy(), ref, rtol=1e-10, atol=1e-300)
+
+
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])
 def test_short_evolution_matches_oracle(precision):
     config, r, N = _setup(rpoints=79, MCINTPOINTS=2048, DE_SOLVER_STEP=0.2, PRECISION=precision)

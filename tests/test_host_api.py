@@ -261,3 +261,19 @@ def test_kinematical_constraint_entry_points_validate_on_the_host():
     rc = lib.nlo_bk_evolve_history(params, fake, 32, fake, 0, 1, 0.2, _native.STEPPERS["rk4"], dirs, 16, box, fake,
                                    fake, fake, 1 << 30, None)
     assert rc == 1 and b"Euler" in lib.nlo_last_error()
+
+
+def test_fixed_step_evolutions_reject_the_adaptive_stepper():
+    """The batched, sharded and served evolutions advance rows by fixed device steps."""
+    import torch
+
+    from nlo_bk_optimized_b200 import BKConfig
+    from nlo_bk_optimized_b200.bk.batch import evolve_batch
+    from nlo_bk_optimized_b200.bk.config import IntegrationMethod, require_fixed_step
+
+    config = BKConfig(STEPPER="rk2_adaptive", INTMETHOD_NLO=IntegrationMethod.SOBOL)
+    with pytest.raises(ValueError, match="rk2_adaptive"):
+        evolve_batch(torch.zeros((1, 8), dtype=torch.float64), torch.ones(8, dtype=torch.float64), 1, config, [16])
+    with pytest.raises(ValueError, match="fixed-step"):
+        require_fixed_step(config, "the sharded evolution")
+    require_fixed_step(BKConfig(STEPPER="rk4"), "the sharded evolution")

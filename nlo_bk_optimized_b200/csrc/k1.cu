@@ -89,6 +89,72 @@ __device__ __forceinline__ K1Z<T> k1_prepare_z(const SplineView<T>& s, const K1P
     return Z;
 }
 
+// FP32 amplitude table of the production instantiation (mixed build, no kinematical
+// constraint).  Rows in natural-log units over the uniform log r grid: row j + 1 =
+// (a, b h, c h^2, d h^3) of interval j, so log N = a + t (b h + t (c h^2 + t d h^3)) with
+// t = (log X - x_j)/h; row 0 = (-200, 0, 0, 0) below the grid (N = 0) and row n = (0, 0, 0, 0)
+// above it (N = 1).  The position u = knot + log(X/r)/h picks the row with no search (the
+// grid is uniform).  For the two intervals beside the parent knot, where X -> r and
+// D = N_X - N_r must keep its relative precision, the per-parent rows rk (interval knot) and
+// rkm1 (interval knot - 1 re-expanded about the knot) give log N - log N_r directly as a cubic
+// without constant term in tau = log(X/r)/h, formed from log(X/r) itself.
+struct K1Table {
+    const float4* rows;  // [n + 1]
+    float inv_h, knot;   // 1/h and the knot index (u of the parent)
+    float top;           // n - 1
+    float4 rk, rkm1;
+};
+
+// N and D = N - N_r at distance exp(lx) r (lx = log(X/r)): the row by selects, one exponential
+// for N; D = N_r expm1(dp) near the knot (|dp| < 1/2, the polynomial of M<float>::expm1), else
+// N - N_r; N >= 1 clamps to (1, S_r) as in k1_amplitude.
+__device__ __forceinline__ void k1_amp_fast(const K1Table& t, const K1Parent<float>& P, float lx, float& N,
+                                            float& D)
+{
+    const float u = fminf(fmaxf(fmaf(lx, t.inv_h, t.knot), -1.0f), t.top);
+    // u + 2^23 + 1 rounded down is 2^23 + 1 + floor(u) (u >= -1): the row index sits in the low
+    // mantissa bits, and subtracting the constant again gives floor(u) exactly
+    const float shifted = __fadd_rd(u, 8388609.0f);
+    const float jf = shifted - 8388609.0f;
+    const float4 g = t.rows[__float_as_int(shifted) - 0x4B000000];
+    const bool at_k = jf == t.knot, at_km1 = jf == t.knot - 1.0f;
+    const bool near = at_k || at_km1;
+    const float tau = near ? lx * t.inv_h : u - jf;
+    const float4 c = at_k ? t.rk : (at_km1 ? t.rkm1 : make_float4(g.x - P.pr, g.y, g.z, g.w));
+    const float dp = fmaf(tau, fmaf(tau, fmaf(tau, c.w, c.z), c.y), c.x);
+    const float nv = __expf(P.pr + dp);
+    float q = 0.00019823966831129978f;
+    q = fmaf(q, dp, 0.0013997217938334417f);
+    q = fmaf(q, dp, 0.008333698847676367f);
+    q = fmaf(q, dp, 0.04166532151841506f);
+    q = fmaf(q, dp, 0.16666662318239217f);
+    q = fmaf(q, dp, 0.5000000415133041f);
+    q = fmaf(q, dp, 1.0000000006631342f);
+    const float d = fabsf(dp) < 0.5f ? P.Nr * (dp * q) : nv - P.Nr;
+    const bool sat = nv >= 1.0f;
+    N = sat ? 1.0f : nv;
+    D = sat ? P.Sr : d;
+}
+
+// k1_prepare_z with the table's amplitude (the node is never beside the knot: those
+// intervals are the FP64 panel's).
+__device__ __forceinline__ K1Z<float> k1_prepare_z_fast(const K1Table& t, const K1Parent<float>& P,
+                                                        const Phys<float>& ph, double dlz, double lz_abs)
+{
+    K1Z<float> Z;
+    Z.dY = (float)dlz;
+    Z.z = (float)::exp(lz_abs);
+    Z.rho = (float)::exp(dlz);
+    Z.Ysq = Z.z * Z.z;
+    Z.inv_Ysq = M<float>::rcp(Z.Ysq);
+    k1_amp_fast(t, P, Z.dY, Z.NY, Z.DY);
+    Z.alpha_Y = alpha_of_log((float)lz_abs, ph);
+    const float right_Y = (ph.log_sc - 2.0f * (float)lz_abs) * 5.0f;
+    Z.sigma = M<float>::rcp(1.0f + M<float>::exp_fast(ph.left - right_Y));
+    Z.sigma_c = M<float>::rcp(1.0f + M<float>::exp_fast(right_Y - ph.left));
+    return Z;
+}
+
 // logaddexp(c, t + delta) - logaddexp(c, t) with the sigmoids of t precomputed.
 template <typename T>
 __device__ __forceinline__ T lae_shift(const K1Z<T>& Z, T delta)
@@ -330,7 +396,7 @@ __device__ __forceinline__ T k1_point(const SplineView<T>& s, const K1Parent<T>&
 // k1_point for two angles of one radial node (x: angle j, y: angle j + 1) in the mixed
 // build without the kinematical constraint: the same arithmetic on the packed FP32x2
 // instructions, with the per-angle transcendental and table operations per component.
-__device__ __forceinline__ f2 k1_pair_point(const SplineView<float>& s, const K1Parent<float>& P,
+__device__ __forceinline__ f2 k1_pair_point(const K1Table& s, const K1Parent<float>& P,
                                             const K1Z<float>& Z, const Phys<float>& ph, f2 sh2)
 {
     const float r = P.r, z = Z.z;
@@ -398,8 +464,8 @@ __device__ __forceinline__ f2 k1_pair_point(const SplineView<float>& s, const K1
     lo = make_float2(isfinite(lo.x) ? lo.x : 0.0f, isfinite(lo.y) ? lo.y : 0.0f);
     // dipole N_X + N_Y - N_r - N_X N_Y = S_r (N_Y + D_X) - D_X D_Y  (or with X and Y exchanged)
     float NXx, DXx, NXy, DXy;
-    k1_amplitude(s, P, dX.x, NXx, DXx);
-    k1_amplitude(s, P, dX.y, NXy, DXy);
+    k1_amp_fast(s, P, dX.x, NXx, DXx);
+    k1_amp_fast(s, P, dX.y, NXy, DXy);
     const f2 DX = make_float2(DXx, DXy);
     const f2 base = make_float2(Z.NY <= NXx ? Z.NY + DXx : NXx + Z.DY, Z.NY <= NXy ? Z.NY + DXy : NXy + Z.DY);
     const f2 dipole = fma2(bc2(P.Sr), base, mul2(bc2(-Z.DY), DX));
@@ -500,9 +566,13 @@ __global__ void __cluster_dims__(1, kK1Split, 1) __launch_bounds__(kK1Threads, K
         cursor += (bytes + 15) & ~(size_t)15;
         return p;
     };
+    // FAST: the FP32 production instantiation reads the amplitude from the K1Table rows; the
+    // others from the knots and natural-unit coefficients of a SplineView
+    constexpr bool FAST = sizeof(TF) == sizeof(float) && !KC;
     double* x64 = reinterpret_cast<double*>(carve(sizeof(double) * n));
-    TF* xf = reinterpret_cast<TF*>(carve(sizeof(TF) * n));
-    TF* cf = reinterpret_cast<TF*>(carve(sizeof(TF) * 4 * (n - 1)));
+    TF* xf = FAST ? nullptr : reinterpret_cast<TF*>(carve(sizeof(TF) * n));
+    TF* cf = FAST ? nullptr : reinterpret_cast<TF*>(carve(sizeof(TF) * 4 * (n - 1)));
+    float4* tab = FAST ? reinterpret_cast<float4*>(carve(sizeof(float4) * (n + 1))) : nullptr;
     K1Z<TF>* zt = reinterpret_cast<K1Z<TF>*>(carve(sizeof(K1Z<TF>) * per_split));
     double* zw = reinterpret_cast<double*>(carve(sizeof(double) * per_split));
     K1Z<double>* zd = reinterpret_cast<K1Z<double>*>(carve(sizeof(K1Z<double>) * 16));
@@ -511,11 +581,24 @@ __global__ void __cluster_dims__(1, kK1Split, 1) __launch_bounds__(kK1Threads, K
     __shared__ TF sh2f[24], awf[24];
     const double* src_coef = spline + n;  // log N block
     const double x_knot = spline[knot];
+    const double h64 = (spline[n - 1] - spline[0]) / (double)(n - 1);
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         x64[i] = spline[i] - x_knot;
-        xf[i] = (TF)(spline[i] - x_knot);
+        if constexpr (!FAST) xf[i] = (TF)(spline[i] - x_knot);
     }
-    for (int i = threadIdx.x; i < 4 * (n - 1); i += blockDim.x) cf[i] = (TF)src_coef[i];
+    if constexpr (FAST) {
+        for (int i = threadIdx.x; i < n - 1; i += blockDim.x) {
+            const double* c = src_coef + 4 * (size_t)i;
+            tab[i + 1] = make_float4((float)c[0], (float)(c[1] * h64), (float)(c[2] * h64 * h64),
+                                     (float)(c[3] * h64 * h64 * h64));
+        }
+        if (threadIdx.x == 0) {
+            tab[0] = make_float4(-200.0f, 0.0f, 0.0f, 0.0f);
+            tab[n] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+    } else {
+        for (int i = threadIdx.x; i < 4 * (n - 1); i += blockDim.x) cf[i] = (TF)src_coef[i];
+    }
     if (threadIdx.x < 24) {
         sh2f[threadIdx.x] = (TF)consts.sh2[threadIdx.x];
         awf[threadIdx.x] = (TF)consts.aw[threadIdx.x];
@@ -528,11 +611,42 @@ __global__ void __cluster_dims__(1, kK1Split, 1) __launch_bounds__(kK1Threads, K
     sd.x = x64; sd.coef = src_coef; sd.n = n; sd.x0 = x64[0];
     sd.inv_h = (double)(n - 1) / (x64[n - 1] - x64[0]);
     SplineView<TF> sf;
-    sf.x = xf; sf.coef = cf; sf.n = n; sf.x0 = xf[0];
-    sf.inv_h = (TF)((double)(n - 1) / (x64[n - 1] - x64[0]));
+    if constexpr (!FAST) {
+        sf.x = xf; sf.coef = cf; sf.n = n; sf.x0 = xf[0];
+        sf.inv_h = (TF)((double)(n - 1) / (x64[n - 1] - x64[0]));
+    }
     const double r = r_grid[knot];
-    const K1Parent<TF> Pf = k1_parent<TF>(sf, phf, r, knot);
     const K1Parent<double> Pd = k1_parent<double>(sd, phd, r, knot);
+    K1Parent<TF> Pf;
+    K1Table tf;
+    if constexpr (FAST) {
+        // the parent in FP32 from its FP64 values
+        Pf.r = (float)r;
+        Pf.lr_abs = (float)::log(r);
+        Pf.r2 = Pf.r * Pf.r;
+        Pf.alpha_r = alpha_of_log(Pf.lr_abs, phf);
+        Pf.knot = knot;
+        Pf.pr = (float)Pd.pr;
+        Pf.Nr = (float)Pd.Nr;
+        Pf.Sr = (float)Pd.Sr;
+        tf.rows = tab;
+        tf.inv_h = (float)(1.0 / h64);
+        tf.knot = (float)knot;
+        tf.top = (float)(n - 1);
+        if (knot <= n - 2) {
+            const double* c = src_coef + 4 * (size_t)knot;
+            tf.rk = make_float4(0.0f, (float)(c[1] * h64), (float)(c[2] * h64 * h64), (float)(c[3] * h64 * h64 * h64));
+        } else {
+            tf.rk = make_float4(-Pf.pr, 0.0f, 0.0f, 0.0f);  // the last knot: above it N = 1
+        }
+        // interval knot - 1 about its right end (the knot): p(x) - p(x_knot) as a cubic in x - x_knot
+        const double* c = src_coef + 4 * (size_t)(knot - 1);
+        const double b1 = c[1] + h64 * (2.0 * c[2] + 3.0 * h64 * c[3]);
+        const double c1 = c[2] + 3.0 * h64 * c[3];
+        tf.rkm1 = make_float4(0.0f, (float)(b1 * h64), (float)(c1 * h64 * h64), (float)(c[3] * h64 * h64 * h64));
+    } else {
+        Pf = k1_parent<TF>(sf, phf, r, knot);
+    }
 
     // phase 1: per-node data of this CTA's range; the two intervals adjacent to the
     // parent knot (z -> x) are left to the FP64 table, which every CTA of the cluster
@@ -549,7 +663,10 @@ __global__ void __cluster_dims__(1, kK1Split, 1) __launch_bounds__(kK1Threads, K
         const double hw = 0.5 * (xb - xa);
         const double lz = 0.5 * (xa + xb) + hw * consts.rule.x8[m];
         const double rw = hw * consts.rule.w8[m];
-        zt[L] = k1_prepare_z<TF>(sf, Pf, phf, lz - x_knot, lz);
+        if constexpr (FAST)
+            zt[L] = k1_prepare_z_fast(tf, Pf, phf, lz - x_knot, lz);
+        else
+            zt[L] = k1_prepare_z<TF>(sf, Pf, phf, lz - x_knot, lz);
         const double z = (double)zt[L].z;
         zw[L] = 2.0 * z * z * rw;
     }
@@ -574,7 +691,7 @@ __global__ void __cluster_dims__(1, kK1Split, 1) __launch_bounds__(kK1Threads, K
             const int L = e / 12, j = 2 * (e - 12 * L);
             const double w = zw[L];
             if (w != 0.0) {
-                const f2 v = k1_pair_point(sf, Pf, zt[L], phf, make_float2(sh2f[j], sh2f[j + 1]));
+                const f2 v = k1_pair_point(tf, Pf, zt[L], phf, make_float2(sh2f[j], sh2f[j + 1]));
                 total += ((double)(v.x * awf[j]) + (double)(v.y * awf[j + 1])) * w;
             }
         }
@@ -682,16 +799,20 @@ cudaError_t launch_k1(const nlo_bk_params& p, const double* r, int points, const
     if (e != cudaSuccess) return e;
     const Phys<double> phd = make_phys<double>(p);
     const size_t per_split = (size_t)((points - 1 + kK1Split - 1) / kK1Split) * 8;
-    auto smem_for = [&](size_t tf) {
+    // the carve order of k1_kernel: x64, then the knots and coefficients (or, in the FP32
+    // production instantiation, the K1Table rows), the node tables
+    auto smem_for = [&](size_t tf, bool fast) {
         auto a16 = [](size_t v) { return (v + 15) & ~(size_t)15; };
-        return a16(8 * (size_t)points) + a16(tf * (size_t)points) +
-               a16(tf * 4 * (size_t)(points - 1)) + a16((tf == 4 ? sizeof(K1Z<float>) : sizeof(K1Z<double>)) * per_split) +
-               a16(8 * per_split) + a16(sizeof(K1Z<double>) * 16) + a16(8 * 16);
+        const size_t amplitude = fast ? a16(sizeof(float4) * (size_t)(points + 1))
+                                      : a16(tf * (size_t)points) + a16(tf * 4 * (size_t)(points - 1));
+        return a16(8 * (size_t)points) + amplitude +
+               a16((tf == 4 ? sizeof(K1Z<float>) : sizeof(K1Z<double>)) * per_split) + a16(8 * per_split) +
+               a16(sizeof(K1Z<double>) * 16) + a16(8 * 16);
     };
     auto launch = [&](auto tag, auto kc) -> cudaError_t {
         using TF = decltype(tag);
         constexpr bool KC = decltype(kc)::value;
-        const size_t smem = smem_for(sizeof(TF));
+        const size_t smem = smem_for(sizeof(TF), sizeof(TF) == sizeof(float) && !KC);
         const void* fn = (const void*)k1_kernel<TF, KC>;
         cudaError_t err = raise_dynamic_smem(fn, smem);
         if (err != cudaSuccess) return err;

@@ -277,7 +277,10 @@ __device__ __forceinline__ double dla_resum<double>(double abar, double xarg)
 // Kernel_lo x dipole at one (z, theta) node; sh2 = sin^2(theta/2).  The form of
 // Kernel_lo follows RC_LO (k1.py:37-94); orders without resummation stop at the bare
 // kernel (k1.py:97-98); the resummation coupling follows RESUM_RC (k1.py:100-107).
-template <typename T, bool KC>
+// F32_DLOG (the mixed build's FP64 panel nodes): the double-log factor from the FP32 G(v); the
+// panel runs in FP64 for the cancellation of N_Y - N_r as z -> x, which that factor has no
+// part in.
+template <typename T, bool KC, bool F32_DLOG = false>
 __device__ __forceinline__ T k1_point(const SplineView<T>& s, const K1Parent<T>& P, const K1Z<T>& Z,
                                       const Phys<T>& ph, T sh2, const K1History& H, const double* r_grid)
 {
@@ -375,7 +378,7 @@ __device__ __forceinline__ T k1_point(const SplineView<T>& s, const K1Parent<T>&
                             : (ph.resum_rc == NLO_RESUM_RC_FIXED ? ph.fixed_as : alpha_min);
     const T xarg = (T)4 * dX * Z.dY;
     const T abar = alpha_res * ph.nc * (T)(1.0 / kPi);
-    T dlog = dla_resum<T>(abar, xarg);
+    T dlog = F32_DLOG ? (T)dla_factor((float)(-abar * xarg)) : dla_resum<T>(abar, xarg);
     if (!(r > (T)1.01 * ph.minr)) dlog = (T)1;
     if (!M<T>::finite(dlog)) return (T)0;
     // single-log resummation (k1.py:121-132): exp(-abar A1 |log(ksub (r/minxy)^2)|) and its
@@ -708,7 +711,9 @@ __global__ void __cluster_dims__(1, kK1Split, 1) __launch_bounds__(kK1Threads, K
         const int idx = e / 24, j = e - 24 * (e / 24);
         const double w = zdw[idx];
         if (w != 0.0)
-            total += k1_point<double, KC>(sd, Pd, zd[idx], phd, consts.sh2[j], history, r_grid) * consts.aw[j] * w;
+            total += k1_point<double, KC, sizeof(TF) == sizeof(float)>(sd, Pd, zd[idx], phd, consts.sh2[j], history,
+                                                                         r_grid) *
+                     consts.aw[j] * w;
     }
     // deterministic block reduction, then the cluster's partials in rank order
     __shared__ double cta_total;

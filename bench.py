@@ -910,8 +910,12 @@ def measure_batch(n_sets: int) -> dict:
     y = torch.tensor([0.0, *ys], dtype=torch.float64, device=device)
     points = [_set_points(k) for k in range(n_sets)]
 
+    marks = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+
     def batched():
+        marks[0].record()
         tables = evolve_batch(N0, r, len(ys), config, budgets, waves=waves)
+        marks[1].record()
         dipoles = [BKDipole(DipoleTable(r=r, y=y, N=tables[k], x0=0.01)) for k in range(n_sets)]
         Q2 = [q for pts in points for q, _ in pts]
         xs = [x for pts in points for _, x in pts]
@@ -919,6 +923,7 @@ def measure_batch(n_sets: int) -> dict:
         seeds = [k for k, pts in enumerate(points) for _ in pts]
         opts = [dis_options_for(budgets[k]) for k, pts in enumerate(points) for _ in pts]
         out = structure_functions_many(Q2, xs, dips, dis, sqrt_s=DIS_SQRT_S, seeds=seeds, options=opts)
+        marks[2].record()
         return out["sigma_r"].cpu()
 
     waves = tune_waves(N0, r, config, budgets)
@@ -932,6 +937,7 @@ def measure_batch(n_sets: int) -> dict:
     sig_batched = batched()
     torch.cuda.synchronize()
     batched_s = time.perf_counter() - t0
+    split = (marks[0].elapsed_time(marks[1]) / 1e3, marks[1].elapsed_time(marks[2]) / 1e3)
 
     # the evolution alone (the same multi-set call) and its K2+Kf evaluations: budget x active
     # parents of each step's row, four right-hand sides a step
@@ -999,6 +1005,7 @@ def measure_batch(n_sets: int) -> dict:
                                "budgets 2^U{16..20} per r per stage; 8 (Q^2,x) points per set, NLO sigma_r, "
                                "Vegas 4 it x budget/16", "sets": n_sets, "points": n_points, "waves": waves},
         "batched_s": round(batched_s, 3),
+        "batched_split_s": {"evolution": round(split[0], 3), "dis": round(split[1], 3)},
         "evolution_s": round(evolve_s, 3),
         "evolution_k2kf_evals": k2kf_evals,
         "evolution_k2kf_evals_per_s": round(k2kf_evals / evolve_s, 1),

@@ -81,13 +81,14 @@ def evolve_batch(N0: torch.Tensor, r: torch.Tensor, steps: int, config: BKConfig
 def tune_waves(N0: torch.Tensor, r: torch.Tensor, config: BKConfig, samples: Sequence[int], *,
                sample_sets: int = 32, choices: Sequence[int] = WAVE_CHOICES, precision: int | None = None) -> int:
     """Pick the K2+Kf CTA count (``waves``) that evolves a sample of the sets one rapidity step
-    fastest."""
+    fastest.  Each candidate runs once untimed first, so that its workspace (whose size grows
+    with ``waves``) is allocated outside the timed call."""
     pick = list(range(0, N0.shape[0], max(1, N0.shape[0] // sample_sets)))[:sample_sets]
     N = N0[pick]
     S = [samples[i] for i in pick]
-    evolve_batch(N[:1], r, 1, config, S[:1], waves=choices[0], precision=precision)  # load kernels before timing
     best, best_t = choices[0], float("inf")
     for c in choices:
+        evolve_batch(N, r, 1, config, S, waves=c, precision=precision)
         torch.cuda.synchronize(r.device)
         t0 = time.perf_counter()
         evolve_batch(N, r, 1, config, S, waves=c, precision=precision)

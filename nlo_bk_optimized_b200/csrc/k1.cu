@@ -685,10 +685,21 @@ __global__ void __cluster_dims__(1, kK1Split, 1) __launch_bounds__(kK1Threads, K
     }
     __syncthreads();
 
+    double total = 0.0;
+    // phase 3 first: the FP64 evaluations of the panel nodes, every kK1Split-th one per CTA, on
+    // the last threads (the FP32 sweep below gives them no more items than the others), so that
+    // the FP32 warps overlap their FP64 latency instead of idling behind it at the reduction
+    for (int e = split + kK1Split * (int)(blockDim.x - 1 - threadIdx.x); e < 16 * 24; e += kK1Split * blockDim.x) {
+        const int idx = e / 24, j = e - 24 * (e / 24);
+        const double w = zdw[idx];
+        if (w != 0.0)
+            total += k1_point<double, KC, sizeof(TF) == sizeof(float)>(sd, Pd, zd[idx], phd, consts.sh2[j], history,
+                                                                         r_grid) *
+                     consts.aw[j] * w;
+    }
     // phase 2: the flattened (node, angle) evaluations, an equal share per thread; the
     // mixed build without the constraint takes two angles of a node per step on the
     // packed FP32x2 instructions
-    double total = 0.0;
     if constexpr (sizeof(TF) == sizeof(float) && !KC) {
         for (int e = threadIdx.x; e < k_count * 12; e += blockDim.x) {
             const int L = e / 12, j = 2 * (e - 12 * L);
@@ -705,15 +716,6 @@ __global__ void __cluster_dims__(1, kK1Split, 1) __launch_bounds__(kK1Threads, K
             if (w != 0.0)
                 total += (double)(k1_point<TF, KC>(sf, Pf, zt[L], phf, sh2f[j], history, r_grid) * awf[j]) * w;
         }
-    }
-    // phase 3: the FP64 evaluations of the panel nodes, every kK1Split-th one per CTA
-    for (int e = split + kK1Split * threadIdx.x; e < 16 * 24; e += kK1Split * blockDim.x) {
-        const int idx = e / 24, j = e - 24 * (e / 24);
-        const double w = zdw[idx];
-        if (w != 0.0)
-            total += k1_point<double, KC, sizeof(TF) == sizeof(float)>(sd, Pd, zd[idx], phd, consts.sh2[j], history,
-                                                                         r_grid) *
-                     consts.aw[j] * w;
     }
     // deterministic block reduction, then the cluster's partials in rank order
     __shared__ double cta_total;

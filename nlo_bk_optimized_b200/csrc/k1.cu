@@ -424,11 +424,25 @@ __device__ __forceinline__ f2 k1_pair_point(const K1Table& s, const K1Parent<flo
         // smooth coupling, 1/alpha = b0 c lae: 1/alpha_X - 1/alpha_Y = b0 c (lae_X - lae_Y) = ratio,
         // with lae_X - lae_Y from log1p/expm1 of the exact X^2 - Y^2 (no cancellation); so
         // alpha_X = 1/(1/alpha_Y + ratio) and dalpha = alpha_X alpha_Y ratio
-        const f2 delta = mul2(bc2(-5.0f), log1p_2(mul2(XmY, bc2(Z.inv_Ysq))));
-        const f2 v = mul2(bc2(Z.sigma), expm1_2(delta));
+        // the shift's exponent delta = -5 log(X^2/Y^2) enters only through e^delta - 1 =
+        // (1 + eps)^-5 - 1, eps = (X^2 - Y^2)/Y^2; since (1 + eps)^5 - 1 = eps P(eps),
+        // P = 5 + 10 eps + 10 eps^2 + 5 eps^3 + eps^4, it is -eps P(eps)/(1 + eps)^5 without
+        // cancellation near X = Y, and 1/(1 + eps)^5 - 1 farther away
+        const f2 eps = mul2(XmY, bc2(Z.inv_Ysq));
+        const f2 op = add2(bc2(1.0f), eps);
+        const f2 op2 = mul2(op, op);
+        const f2 op5 = mul2(mul2(op2, op2), op);
+        const f2 r5 = make_float2(__fdividef(1.0f, op5.x), __fdividef(1.0f, op5.y));
+        f2 P = fma2(eps, bc2(1.0f), bc2(5.0f));
+        P = fma2(P, eps, bc2(10.0f));
+        P = fma2(P, eps, bc2(10.0f));
+        P = fma2(P, eps, bc2(5.0f));
+        const f2 near = mul2(mul2(eps, P), make_float2(-r5.x, -r5.y));
+        const f2 em1 = make_float2(fabsf(eps.x) < 0.5f ? near.x : r5.x - 1.0f, fabsf(eps.y) < 0.5f ? near.y : r5.y - 1.0f);
+        const f2 v = mul2(bc2(Z.sigma), em1);
         f2 shift = log1p_2(v);
-        if (v.x <= -0.5f) shift.x = logf(Z.sigma_c + Z.sigma * __expf(delta.x));
-        if (v.y <= -0.5f) shift.y = logf(Z.sigma_c + Z.sigma * __expf(delta.y));
+        if (v.x <= -0.5f) shift.x = logf(Z.sigma_c + Z.sigma * r5.x);
+        if (v.y <= -0.5f) shift.y = logf(Z.sigma_c + Z.sigma * r5.y);
         ratio = mul2(bc2(ph.b0c), shift);
         const f2 inv_aX = add2(bc2(__fdividef(1.0f, Z.alpha_Y)), ratio);
         alpha_X = make_float2(__fdividef(1.0f, inv_aX.x), __fdividef(1.0f, inv_aX.y));

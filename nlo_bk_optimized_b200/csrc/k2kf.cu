@@ -155,8 +155,8 @@ __device__ __forceinline__ void k2_pair_fast(const FastSpline& s, const Phys<flo
     const f2 zsq = make_float2(w9.x, w9.y), z2sq = make_float2(w9.z, w9.w);
     const f2 r = bc2(P.r);
     const f2 rz = sub2(r, z), rz2 = sub2(r, z2);
-    const f2 Xsq = fma2(mul2(bc2(P.four_r), z), s1, mul2(rz, rz));
-    const f2 X2sq = fma2(mul2(bc2(P.four_r), z2), s2, mul2(rz2, rz2));
+    const f2 Xsq = fma2(bc2(P.four_r), s1, mul2(rz, rz));  // s1 = z sin^2(theta/2)
+    const f2 X2sq = fma2(bc2(P.four_r), s2, mul2(rz2, rz2));
     const f2 L2X = lg22(Xsq), L2X2 = lg22(X2sq);
     const f2 uX = fma2(L2X, bc2(s.u_scale), bc2(s.u_off)), uX2 = fma2(L2X2, bc2(s.u_scale), bc2(s.u_off));
     P2S vXx, vXy, vX2x, vX2y;

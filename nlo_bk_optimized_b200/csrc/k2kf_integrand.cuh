@@ -79,8 +79,8 @@ __device__ __forceinline__ void k2_prepare_x(const SplineView<T>& s, const K2Box
     const T dN = ndiff_s(Y2, Y);  // N_Y2 - N_Y
     rec[kZ] = z;
     rec[kZ2] = z2;
-    rec[kS1] = sh1 * sh1;
-    rec[kS2] = sh2 * sh2;
+    rec[kS1] = z * (sh1 * sh1);  // z sin^2(theta/2): X^2 = (r - z)^2 + 4 r rec[kS1]
+    rec[kS2] = z2 * (sh2 * sh2);
     rec[kP1] = (z2 - z) * (z2 + z);
     rec[kP2] = (T)2 * z * z2 * (z2 * c1 - z * c2);
     rec[kU1] = z2 - z * c12;
@@ -113,8 +113,8 @@ __device__ __forceinline__ void k2_point(const EvalSpline& s, const Phys<T>& ph,
 {
     const T r = P.r;
     const T z = rec[kZ], z2 = rec[kZ2];
-    const T Xsq = (r - z) * (r - z) + (T)4 * r * z * rec[kS1];
-    const T X2sq = (r - z2) * (r - z2) + (T)4 * r * z2 * rec[kS2];
+    const T Xsq = (r - z) * (r - z) + (T)4 * r * rec[kS1];
+    const T X2sq = (r - z2) * (r - z2) + (T)4 * r * rec[kS2];
     const bool valid = Xsq >= M<T>::tiny_square() && X2sq >= M<T>::tiny_square();
     const T lXs = M<T>::log_fast(Xsq), lX2s = M<T>::log_fast(X2sq);
     const PS<T> vX = eval_s_ps(s, (T)0.5 * lXs), vX2 = eval_s_ps(s, (T)0.5 * lX2s);

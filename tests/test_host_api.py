@@ -158,6 +158,29 @@ def test_library_rejects_bad_arguments_without_a_gpu():
     assert b"NF" in lib.nlo_last_error()
     assert lib.nlo_bk_k2kf_workspace_bytes(400) > 0
     assert lib.nlo_bk_spline_doubles(400) == 400 + 8 * 399 + 2 * 400
+    # the multi-set evolution checks its sets, budgets, directions and waves on the host
+    import ctypes
+
+    params.nf = 3.0
+    tables = (ctypes.c_void_p * 2)(16, 32)
+    budgets = (ctypes.c_int64 * 2)(1024, 1 << 31)
+    sets_dirs = (_native.SobolDirs * 2)(dirs, dirs)
+    box = _native.box([0.0] * 4, [1.0] * 4)
+
+    def sets_call(n, waves=4, tabs=tables, samples=budgets, d=sets_dirs):
+        return lib.nlo_bk_evolve_sets(params, 64, 64, n, tabs, 1, 0.2, 2, d, samples, box, waves, 128, 256,
+                                      1 << 30, None)
+
+    assert sets_call(0) == 1 and b"sets" in lib.nlo_last_error()
+    assert sets_call(300) == 1 and b"sets" in lib.nlo_last_error()
+    assert sets_call(2, waves=0) == 1 and b"waves" in lib.nlo_last_error()
+    assert sets_call(2) == 1 and b"samples" in lib.nlo_last_error()  # 2^31 > 2^30
+    assert sets_call(1, tabs=(ctypes.c_void_p * 1)(None)) == 1 and b"table" in lib.nlo_last_error()
+    bad = _native.sobol_dirs(4, 0)
+    bad.dims = 2
+    assert sets_call(1, d=(_native.SobolDirs * 1)(bad)) == 1 and b"set 0" in lib.nlo_last_error()
+    assert lib.nlo_bk_sets_workspace_bytes(64, 257, 4) == 0
+    assert lib.nlo_bk_sets_workspace_bytes(64, 2, 4) > 0
 
 
 def test_c_struct_layouts_match_ctypes(tmp_path):

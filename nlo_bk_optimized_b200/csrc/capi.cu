@@ -11,6 +11,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <set>
 #include <string>
 #include <utility>
 #include <vector>
@@ -130,6 +131,61 @@ struct SideStream {
     SideStream(const SideStream&) = delete;
     SideStream& operator=(const SideStream&) = delete;
 };
+
+// One rapidity step recorded as a CUDA graph and replayed for every later step: the step's
+// launches (4 x (spline refit, active list, K1 on the side stream, K2+Kf, its finalize,
+// assembly) + the stage combinations for RK4) then cost one graph launch, and the device runs
+// them without the per-launch gaps.  The recorded step reads and writes one fixed row (the
+// last stage combination runs in place, element by element), so the same graph serves every
+// step; the caller copies the row out to the table after each replay.  Capture runs on a
+// private stream in thread-local mode, so that the caller's stream (which may be the legacy
+// default stream) and other threads are untouched; if recording fails for any reason the
+// caller launches the step's kernels one by one instead.
+struct StepGraph {
+    cudaStream_t cap = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    StepGraph() = default;
+    StepGraph(const StepGraph&) = delete;
+    StepGraph& operator=(const StepGraph&) = delete;
+    ~StepGraph()
+    {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (cap) cudaStreamDestroy(cap);
+    }
+    // record(stream) enqueues the step on `stream`; true when a replayable graph came out
+    template <class F>
+    bool capture(F record)
+    {
+        if (cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) != cudaSuccess) {
+            cap = nullptr;
+            cudaGetLastError();
+            return false;
+        }
+        if (cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        const int rc = record(cap);
+        const cudaError_t end = cudaStreamEndCapture(cap, &graph);
+        if (rc != NLO_OK || end != cudaSuccess || !graph ||
+            cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
+            cudaGetLastError();
+            if (exec) cudaGraphExecDestroy(exec);
+            exec = nullptr;
+            return false;
+        }
+        return true;
+    }
+};
+
+// Measured on the B200 (RK4, 2^14..2^20 samples per parent): with 200 and 400 points a
+// replayed step took 0.74-0.98 of the launched one (0.95 at the 400-point, 2^20-sample
+// evolution); with 100 to 160 points, where the K2+Kf launch has CTAs of 128 or 160 lanes,
+// five to seven per SM, up to 1.6 times as long.  So grids of up to 192 points (the largest
+// with 192-lane CTAs, not measured) launch every step.
+inline bool replay_pays(int points) { return points > 192; }
 
 int run_rhs(const nlo_bk_params& p, const double* r, const double* N, int points, const SobolDirsArg& dirs,
             uint64_t samples, const nlo_bk_box& box, double* dndy, double* k1_out, double* k2kf_out,
@@ -330,6 +386,20 @@ cudaError_t raise_dynamic_smem(const void* func, size_t bytes)
 }
 
 // buffer size a caller provides to nlo_bk_splines: coefficients plus factorisation scratch
+cudaError_t prefer_shared_carveout(const void* func)
+{
+    static std::mutex lock;
+    static std::set<std::pair<int, const void*>> done;
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> guard(lock);
+    if (done.count({device, func})) return cudaSuccess;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (e == cudaSuccess) done.insert({device, func});
+    return e;
+}
+
 size_t spline_buffer_doubles(int points) { return spline_doubles(points) + 2 * (size_t)points; }
 
 int k2kf_max_blocks()
@@ -427,8 +497,9 @@ int nlo_bk_k2kf(const nlo_bk_params* params, const double* r, int32_t points, co
 size_t nlo_bk_rhs_workspace_bytes(int32_t points)
 {
     if (points < 3) return 0;
-    // one right-hand side plus five stage rows for the steppers
-    return rhs_bytes(points, nullptr) + align_up(sizeof(double) * 5 * (size_t)points);
+    // one right-hand side plus five stage rows for the steppers and the row a recorded step
+    // advances
+    return rhs_bytes(points, nullptr) + align_up(sizeof(double) * 6 * (size_t)points);
 }
 
 int nlo_bk_rhs(const nlo_bk_params* params, const double* r, const double* N, int32_t points,
@@ -535,6 +606,7 @@ static int evolve_rows(const nlo_bk_params* params, const double* r, int32_t poi
     double* stage = reinterpret_cast<double*>(static_cast<char*>(workspace) + rhs_bytes(points, nullptr));
     double* kk[4] = {stage, stage + points, stage + 2 * points, stage + 3 * points};
     double* tmp = stage + 4 * points;
+    double* cur = stage + 5 * points;  // the row a recorded step advances in place
     const SobolDirsArg dirs_arg = to_arg(dirs);
     cudaError_t e = cudaMemsetAsync(status, 0, sizeof(uint32_t), s);
     if (e != cudaSuccess) return cuda_fail(e, "status reset");
@@ -542,12 +614,17 @@ static int evolve_rows(const nlo_bk_params* params, const double* r, int32_t poi
     const SideStream side;
     // the spline factorisation depends on the grid only: form it on the first stage
     bool factor_ready = false;
-    for (int it = first; it < first + steps; ++it) {
-        const double* N = table + (size_t)it * points;
-        double* next = table + (size_t)(it + 1) * points;
+    // the steps of a fixed-step Sobol evolution are all alike: after the first (launched one
+    // by one, which also forms the factorisation and sets every kernel attribute) one step is
+    // recorded and replayed; the kinematical constraint (its history grows) and Vegas (its
+    // rounds depend on convergence checks) launch every step
+    const bool replay = !params->kinematical_constraint && !vegas && steps > 1 && replay_pays(points);
+    StepGraph graph;
+    bool recorded = false;
+    auto step_from = [&](const double* N, double* next, int it, cudaStream_t st) {
         auto rhs = [&](int src, int k) {
             const int code = run_rhs(*params, r, src < 0 ? N : tmp, points, dirs_arg, (uint64_t)samples, *box, kk[k],
-                                     nullptr, nullptr, b, factor_ready, s, 0, 1, y, table, it + 1, &side, vegas);
+                                     nullptr, nullptr, b, factor_ready, st, 0, 1, y, table, it + 1, &side, vegas);
             factor_ready = true;
             return code;
         };
@@ -555,18 +632,35 @@ static int evolve_rows(const nlo_bk_params* params, const double* r, int32_t poi
             const double* kp[4];
             for (int j = 0; j < nk; ++j) kp[j] = kk[ks[j]];
             const cudaError_t err = launch_axpy_stage(N, kp, coef, nk, points, dst ? next : tmp, dst ? clamp : 0,
-                                                      dst ? status : nullptr, s);
+                                                      dst ? status : nullptr, st);
             return err == cudaSuccess ? NLO_OK : cuda_fail(err, "stage");
         };
-        const int rc = step_sequence(stepper, step, rhs, comb);
+        return step_sequence(stepper, step, rhs, comb);
+    };
+    const size_t row_bytes = sizeof(double) * (size_t)points;
+    for (int it = first; it < first + steps; ++it) {
+        const double* N = table + (size_t)it * points;
+        double* next = table + (size_t)(it + 1) * points;
+        if (replay && it == first + 1) {
+            recorded = graph.capture([&](cudaStream_t st) { return step_from(cur, cur, it, st); });
+            if (recorded && (e = cudaMemcpyAsync(cur, N, row_bytes, cudaMemcpyDeviceToDevice, s)) != cudaSuccess)
+                return cuda_fail(e, "step row");
+        }
+        if (recorded) {
+            if ((e = cudaGraphLaunch(graph.exec, s)) != cudaSuccess) return cuda_fail(e, "step graph");
+            if ((e = cudaMemcpyAsync(next, cur, row_bytes, cudaMemcpyDeviceToDevice, s)) != cudaSuccess)
+                return cuda_fail(e, "step row");
+            continue;
+        }
+        const int rc = step_from(N, next, it, s);
         if (rc != NLO_OK) return rc;
     }
     return NLO_OK;
 }
 
 // Workspace of a multi-set evolution: per set the spline tables, their factorisation, the
-// active list and count, K1, the K2+Kf sums and five stage rows; the K2+Kf partial sums of the
-// layout; the set table.
+// active list and count, K1, the K2+Kf sums, five stage rows and the row a recorded step
+// advances; the K2+Kf partial sums of the layout; the set table.
 static size_t sets_bytes(int points, int sets, const SetsLayout& L, size_t* offsets /*[9] or NULL*/)
 {
     const size_t S = (size_t)sets, n = (size_t)points;
@@ -578,7 +672,7 @@ static size_t sets_bytes(int points, int sets, const SetsLayout& L, size_t* offs
     off[4] = o; o = align_up(o + sizeof(double) * S * n);
     off[5] = o; o = align_up(o + sizeof(double) * S * 3 * n);
     off[6] = o; o = align_up(o + sizeof(double) * sets_partial_doubles(L));
-    off[7] = o; o = align_up(o + sizeof(double) * 5 * S * n);
+    off[7] = o; o = align_up(o + sizeof(double) * 6 * S * n);
     off[8] = o; o = align_up(o + sizeof(SetTable));
     if (offsets) std::memcpy(offsets, off, sizeof(off));
     return o;
@@ -751,6 +845,7 @@ int nlo_bk_evolve_sets(const nlo_bk_params* params, const double* r, int32_t poi
     const size_t S = (size_t)sets, n = (size_t)points;
     double* kk[4] = {stage, stage + S * n, stage + 2 * S * n, stage + 3 * S * n};
     double* tmp = stage + 4 * S * n;
+    double* cur = stage + 5 * S * n;
 
     // slots in order of decreasing budget (ties by set index), so that slot 0 of every group
     // holds the group's largest budget and sets of one budget share CTAs
@@ -771,18 +866,19 @@ int nlo_bk_evolve_sets(const nlo_bk_params* params, const double* r, int32_t poi
     if (e != cudaSuccess) return cuda_fail(e, "sets setup");
     if ((e = cudaMemsetAsync(status, 0, sizeof(uint32_t) * S, s)) != cudaSuccess) return cuda_fail(e, "status reset");
     double* const* rows = reinterpret_cast<double* const*>(base + off[8] + offsetof(SetTable, rows));
-    RowsArg work;
+    RowsArg work, fixed;
     work.base = tmp;
     work.stride = n;
+    fixed.base = cur;
+    fixed.stride = n;
     const int clamp = params->force_positive ? 1 : 0;
     const SideStream side;
     bool factor_ready = false;
-    for (int it = 0; it < steps; ++it) {
-        RowsArg now, next;
-        now.ptrs = rows;
-        now.offset = (size_t)it * n;
-        next.ptrs = rows;
-        next.offset = (size_t)(it + 1) * n;
+    // as in evolve_rows: the first step launches its kernels one by one, the later ones
+    // replay a recording of one step that advances the fixed rows in place
+    StepGraph graph;
+    bool recorded = false;
+    auto step_from = [&](const RowsArg& now, const RowsArg& next, cudaStream_t s) {
         auto rhs = [&](int src, int k) {
             const RowsArg& in = src < 0 ? now : work;
             if ((e = launch_splines(r, in, points, sets, params->force_positive, factor, factor_ready ? 0 : 1, spline,
@@ -819,7 +915,28 @@ int nlo_bk_evolve_sets(const nlo_bk_params* params, const double* r, int32_t poi
                                                      dst ? clamp : 0, dst ? status : nullptr, s);
             return err == cudaSuccess ? (int)NLO_OK : cuda_fail(err, "stage");
         };
-        const int rc = step_sequence(stepper, step, rhs, comb);
+        return step_sequence(stepper, step, rhs, comb);
+    };
+    for (int it = 0; it < steps; ++it) {
+        RowsArg now, next;
+        now.ptrs = rows;
+        now.offset = (size_t)it * n;
+        next.ptrs = rows;
+        next.offset = (size_t)(it + 1) * n;
+        if (it == 1 && replay_pays(points)) {
+            recorded = graph.capture([&](cudaStream_t st) { return step_from(fixed, fixed, st); });
+            // a combination without terms copies the rows
+            if (recorded &&
+                (e = launch_axpy_sets(now, nullptr, nullptr, 0, points, sets, fixed, 0, nullptr, s)) != cudaSuccess)
+                return cuda_fail(e, "step rows");
+        }
+        if (recorded) {
+            if ((e = cudaGraphLaunch(graph.exec, s)) != cudaSuccess) return cuda_fail(e, "step graph");
+            if ((e = launch_axpy_sets(fixed, nullptr, nullptr, 0, points, sets, next, 0, nullptr, s)) != cudaSuccess)
+                return cuda_fail(e, "step rows");
+            continue;
+        }
+        const int rc = step_from(now, next, s);
         if (rc != NLO_OK) return rc;
     }
     return NLO_OK;

@@ -105,6 +105,9 @@ int set_last_error(int code, const char* message);
 // Raise (never lower) a kernel's dynamic shared-memory limit on the current device to at
 // least `bytes`; safe when several host threads launch the same kernel with different sizes.
 cudaError_t raise_dynamic_smem(const void* func, size_t bytes);
+// The BK kernels stage their tables and sample tiles in shared memory and read little through
+// L1: ask for the largest shared-memory carveout, once per kernel and device.
+cudaError_t prefer_shared_carveout(const void* func);
 
 // Spline tables of `sets` rows: set s reads N.at(s) and writes out + s * spline_doubles(n)
 // and its factorisation at factor + s * 2n.

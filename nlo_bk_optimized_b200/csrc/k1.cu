@@ -836,6 +836,7 @@ cudaError_t launch_k1(const nlo_bk_params& p, const double* r, int points, const
         const size_t smem = smem_for(sizeof(TF), sizeof(TF) == sizeof(float) && !KC);
         const void* fn = (const void*)k1_kernel<TF, KC>;
         cudaError_t err = raise_dynamic_smem(fn, smem);
+        if (err == cudaSuccess) err = prefer_shared_carveout(fn);
         if (err != cudaSuccess) return err;
         k1_kernel<TF, KC><<<dim3(points, kK1Split, sets), kK1Threads, smem, stream>>>(make_phys<TF>(p), phd, consts, history,
                                                                                r, points, spline, active, count, out);

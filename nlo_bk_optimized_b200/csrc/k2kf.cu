@@ -569,6 +569,7 @@ cudaError_t launch_sets_typed(const nlo_bk_params& p, const double* r, int point
 {
     const size_t smem = k2_smem_bytes<T>(L.threads, L.per_cta, points);
     cudaError_t e = raise_dynamic_smem((const void*)k2kf_kernel<T, SYM, COUPLING, true>, smem);
+    if (e == cudaSuccess) e = prefer_shared_carveout((const void*)k2kf_kernel<T, SYM, COUPLING, true>);
     if (e != cudaSuccess) return e;
     SetsArg sa{L.per_cta, L.lanes, L.parent_tiles, spline_stride, table};
     dim3 grid((unsigned)L.blocks, (unsigned)(L.groups * L.parent_tiles));
@@ -587,6 +588,7 @@ cudaError_t launch_typed(const nlo_bk_params& p, const double* r, int points, co
 {
     const size_t smem = k2_smem_bytes<T>(threads, 1, points);
     cudaError_t e = raise_dynamic_smem((const void*)k2kf_kernel<T, SYM, COUPLING, false>, smem);
+    if (e == cudaSuccess) e = prefer_shared_carveout((const void*)k2kf_kernel<T, SYM, COUPLING, false>);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k2kf_kernel<T, SYM, COUPLING, false>, threads, smem);

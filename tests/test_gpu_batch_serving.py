@@ -61,6 +61,25 @@ def test_batch_layouts(rpoints, n_sets):
         torch.testing.assert_close(tables[k].N, alone.N, rtol=1e-12, atol=0)
 
 
+def test_replayed_set_steps_equal_launched_steps():
+    """The multi-set evolution on more than 192 points replays a CUDA graph of one step after
+    its first; one-step calls from each previous row give the same rows bit for bit."""
+    from nlo_bk_optimized_b200 import BKConfig
+    from nlo_bk_optimized_b200.bk.batch import evolve_batch
+    from nlo_bk_optimized_b200.bk.evolution import _r_grid
+
+    config = BKConfig(MCINTPOINTS=1 << 10, **dict(BK, RPOINTS=199))
+    r = _r_grid(config, device="cuda", dtype=torch.float64)
+    N0 = torch.stack([ic.dipole_amplitude(r.cpu()).to(torch.float64) for ic in _ics()]).cuda()
+    budgets = [1 << 10, 1 << 12, 1 << 11, 1 << 12, 1000]
+    whole = evolve_batch(N0, r, 4, config, budgets, waves=2)
+    rows = [N0]
+    for _ in range(4):
+        rows.append(evolve_batch(rows[-1], r, 1, config, budgets, waves=2)[:, 1])
+    assert torch.equal(whole, torch.stack(rows, dim=1))
+    assert not torch.equal(whole[:, -1], whole[:, 1])
+
+
 def test_wave_autotuner_returns_a_choice():
     from nlo_bk_optimized_b200 import MV, BKConfig
     from nlo_bk_optimized_b200.bk.batch import WAVE_CHOICES, tune_waves

@@ -225,6 +225,21 @@ def test_short_evolution_matches_oracle(precision):
     assert err <= tol, f"N(Y=1) max relative error {err:.3e}"
 
 
+@pytest.mark.parametrize("stepper, precision", [("euler", "fp64"), ("rk3", "mixed"), ("rk4", "mixed"), ("rk4", "fp64")])
+def test_replayed_steps_equal_launched_steps(stepper, precision):
+    """An evolution on more than 192 points launches its first step kernel by kernel and
+    replays a CUDA graph of one step for the later ones; one-step calls (launched kernel by
+    kernel every time) give the same rows bit for bit."""
+    config, _, _ = _setup(rpoints=199, MCINTPOINTS=2048, DE_SOLVER_STEP=0.2, STEPPER=stepper, PRECISION=precision)
+    whole = solve_bk(MV(qs0sqr=0.2), 1.0, config, device=DEVICE, dtype=torch.float64, seed=0)
+    part = solve_bk(MV(qs0sqr=0.2), 0.2, config, device=DEVICE, dtype=torch.float64, seed=0)
+    for y in (0.4, 0.6, 0.8, 1.0):
+        part = evolve_table(part, y, config, seed=0)
+    assert whole.N.shape == part.N.shape == (6, 200)
+    assert torch.equal(whole.N, part.N)
+    assert not torch.equal(whole.N[-1], whole.N[1])
+
+
 def test_deterministic_and_seeded():
     config, r, N = _setup(rpoints=99)
     a = kernels.k2kf(r, N, config, samples=5000)

@@ -212,7 +212,9 @@ int nlo_bk_stage(const double* N, const double* const* k, const double* coef, in
  * (_bk_steps, bk/evolution.py:85-159): each step applies the stepper, clamps N to
  * [0,1] when force_positive, and stores the row.  table: device double[(steps+1)*points]
  * with row 0 = the initial condition (input).  status: device uint32[1], bit 0 set if
- * a non-finite amplitude appeared (the host raises FloatingPointError). */
+ * a non-finite amplitude appeared (the host raises FloatingPointError).  On grids of more
+ * than 192 points the steps after the first replay a CUDA graph of one step, recorded on a
+ * private stream during the call (the rows are the same as launching every step). */
 int nlo_bk_evolve(const nlo_bk_params* params, const double* r, int32_t points, int32_t steps, double step,
                   int32_t stepper, const nlo_sobol_dirs* dirs, int64_t samples, const nlo_bk_box* box,
                   double* table, uint32_t* status, void* workspace, size_t workspace_bytes, void* stream);

@@ -69,7 +69,7 @@ MUFU_PER_SM_PER_CLOCK = 16
 # ncu capture of the kernel case (bench.py --kernel-case: 400 parents x 2^18 points): the
 # spline is staged into shared memory once per CTA and each CTA writes 3 doubles per
 # parent, so the bytes do not grow with the number of samples.
-K2KF_DRAM_BYTES_PER_LAUNCH = 52480
+K2KF_DRAM_BYTES_PER_LAUNCH = 52224
 # Launches of our kernels per RK4 step: 4 right-hand sides x (spline refit, active
 # list, K1, K2+Kf, K2+Kf finalize, assemble) + 4 stage combinations.
 LAUNCHES_PER_RK4_STEP = 4 * 6 + 4

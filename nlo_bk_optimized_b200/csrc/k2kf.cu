@@ -136,7 +136,7 @@ __device__ __forceinline__ f2 fast_ndiff2(const P2S& Ax, const P2S& Ay, const P2
 
 template <bool SYM, int COUPLING>
 __device__ __forceinline__ void k2_pair_fast(const FastSpline& s, const Phys<float>& ph, const K2ParentF& P,
-                                             const float4* __restrict__ rec4, f2& k2w, f2& kfw, f2& total)
+                                             const float4* __restrict__ rec4, f2& kfw, f2& total)
 {
     constexpr float LN2 = 0.69314718055994531f;
     constexpr float L2E = 1.4426950408889634f;
@@ -236,14 +236,13 @@ __device__ __forceinline__ void k2_pair_fast(const FastSpline& s, const Phys<flo
         }
     }
     const f2 scale = mul2(mul2(alpha, alpha), cpt);
-    k2w = mul2(k2part, scale);
+    const f2 k2w = mul2(k2part, scale);
     kfw = mul2(make_float2(-fermion.x, -fermion.y), scale);
     const f2 tot = add2(k2w, kfw);
     // X^2 or X'^2 below the normal range (the oracle's validity cut) gives infinite kernels
     // (the approximate reciprocal flushes denormals), so the finite test covers it
     const bool ok_x = fabsf(tot.x) < INFINITY;
     const bool ok_y = fabsf(tot.y) < INFINITY;
-    k2w = sel2(ok_x, ok_y, k2w, bc2(0.0f));
     kfw = sel2(ok_x, ok_y, kfw, bc2(0.0f));
     total = sel2(ok_x, ok_y, tot, bc2(0.0f));
 }
@@ -412,18 +411,21 @@ __global__ void __launch_bounds__(448, (sizeof(T) == 4 ? 2 : 1)) k2kf_kernel(Phy
                     f2 sq = bc2(0.0f);  // variance estimate only: plain sum per tile
                     const int pairs = (count_here + 1) >> 1;
                     // FP32x2 partial sums of 16 pairs (32 samples), folded into FP64: the
-                    // rounding of a 32-term FP32 sum instead of compensated summation
+                    // rounding of a 32-term FP32 sum instead of compensated summation.  The
+                    // sums are of K2 + Kf and of Kf (K2 is their difference, formed once at
+                    // the end): the total is needed anyway for the variance, and this saves
+                    // the finite-test select of K2 per sample
                     for (int j0 = 0; j0 < pairs; j0 += kFoldPairs) {
                         const int jn = j0 + kFoldPairs < pairs ? j0 + kFoldPairs : pairs;
-                        f2 pk2 = bc2(0.0f), pkf = bc2(0.0f);
+                        f2 ptot = bc2(0.0f), pkf = bc2(0.0f);
                         for (int j = j0; j < jn; ++j) {
-                            f2 k2w, kfw, tot;
-                            k2_pair_fast<SYM, COUPLING>(fs, ph, PF, pr + (kRecLen / 2) * j, k2w, kfw, tot);
-                            pk2 = add2(pk2, k2w);
+                            f2 kfw, tot;
+                            k2_pair_fast<SYM, COUPLING>(fs, ph, PF, pr + (kRecLen / 2) * j, kfw, tot);
+                            ptot = add2(ptot, tot);
                             pkf = add2(pkf, kfw);
                             sq = fma2(tot, tot, sq);
                         }
-                        acc_k2 += (double)pk2.x + (double)pk2.y;
+                        acc_k2 += (double)ptot.x + (double)ptot.y;  // K2 + Kf until the end
                         acc_kf += (double)pkf.x + (double)pkf.y;
                     }
                     acc_sq += (double)sq.x + (double)sq.y;
@@ -458,7 +460,7 @@ __global__ void __launch_bounds__(448, (sizeof(T) == 4 ? 2 : 1)) k2kf_kernel(Phy
     else if (slot < n)
         o = partial + ((size_t)blockIdx.x * n + slot) * 3;
     if (o) {
-        o[0] = acc_k2;
+        o[0] = sizeof(T) == sizeof(float) ? acc_k2 - acc_kf : acc_k2;
         o[1] = acc_kf;
         o[2] = acc_sq;
     }

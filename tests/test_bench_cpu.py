@@ -9,6 +9,8 @@ import subprocess
 import sys
 from pathlib import Path
 
+import pytest
+
 ROOT = Path(__file__).resolve().parents[1]
 
 
@@ -42,3 +44,20 @@ def test_reference_arm_other_ranks_exit_silently():
     result = _run({"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"})
     assert result.returncode == 0, result.stderr[-2000:]
     assert result.stdout.strip() == ""
+
+
+def test_reference_cpu_timing_partial_record():
+    """A reference CPU run stopped before Y = 0.4 is recorded from its progress lines,
+    marked incomplete, with the time per derivative of the lines it printed."""
+    from oracle.reference_cpu_timing import partial_record
+
+    log = "\n".join(["starting", "derivative 1 done at 500.0 s", "derivative 2 done at 1010.0 s",
+                     "derivative 3 done at 1530.0 s"])
+    rec = partial_record(log, 1800.0, 8, "x")
+    assert rec["completed"] is False and rec["seconds_to_y_0_4"] is None
+    assert rec["derivatives"] == 3 and rec["seconds_per_derivative"] == 510.0
+    assert rec["stopped_after_s"] == 1800.0 and rec["threads"] == 8
+    with pytest.raises(ValueError):
+        partial_record("nothing here", 10.0, 8, "x")
+    with pytest.raises(ValueError):
+        partial_record(log, 1000.0, 8, "x")
